@@ -1,0 +1,138 @@
+/* raishin_gpu.h -- C ABI of the B200-native RAISHIN GRMHD update.
+ *
+ * The reference (gustavo689/raishinsource) is Fortran 90: main.f90 drives one
+ * RK3 step per pass of its time loop (main.f90:586-1151) by calling the
+ * routines of rec.f90, calcha.f90, hll.f90, ct.f90, calsf.f90, rkt.f90,
+ * recov.f90, bnd.f90, correction.f90 and cdtcfl.f90 on whole local blocks
+ * uri(nv,is1:ie1,js1:je1,ks1:ke1).  This library replaces those calls with
+ * sm_100a kernels on one GPU.  Every entry point is extern "C" with plain
+ * pointers and sizes so that the Fortran driver can bind it with
+ * ISO_C_BINDING.
+ *
+ * Conventions
+ *  - Host arrays of primitives/conserved variables use the reference layout
+ *    a(nv,i,j,k), nv = 9, variable fastest, then i, j, k, ghosts included
+ *    (imax*jmax*kmax cells).  Flux arrays use ww(3,nv,i,j,k).
+ *  - Every function returns an rg_status (0 = RG_OK).  Nothing aborts the
+ *    process and no kernel traps; CUDA errors are returned as RG_ECUDA.
+ *  - The library owns device memory.  Host buffers are only read or written
+ *    during the call.  One host thread per rg_ctx.
+ */
+#ifndef RAISHIN_GPU_H
+#define RAISHIN_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  RG_OK = 0,
+  RG_EINVAL_CONFIG = 1, /* parameters outside what the kernels support */
+  RG_ENOMEM_ADMIT = 2,  /* the run's device footprint does not fit */
+  RG_ECUDA = 3,         /* a CUDA call failed (message in rg_last_error) */
+  RG_ENR_CAP = 4,       /* an unbounded reference loop hit its cap (see stats) */
+  RG_ENAN = 5,          /* non-finite primitives found */
+  RG_ENOTFOUND = 6,     /* unknown run id */
+  RG_EOVERFLOW = 7      /* a bounded device list overflowed (see stats) */
+} rg_status;
+
+typedef enum { RG_FP64 = 0, RG_MIXED = 1 } rg_precision;
+
+/* One run's parameters: the runtime form of module pram (pram.f90:1-80). */
+typedef struct rg_run_params {
+  int imax, jmax, kmax; /* cells incl. ghosts; i = r, j = phi, k = theta (pram.f90:11) */
+  int metric;           /* 1 Minkowski, 303 Kerr-Schild, 403 modified KS (pram.f90:67) */
+  int ix1, ix2, ix3;    /* grid kinds: ix1 1 uniform / 2 log; ix3 1 uniform / 2 MKS theta */
+  int irec;             /* 5 PPM, 6 MP5, 7 WENO5 (pram.f90:73) */
+  int model;            /* 2 shock tube, 7 Fishbone-Moncrief torus (pram.f90:66) */
+  int iter;             /* Newton-Raphson iteration cap, 5000 in the reference */
+  double xmin, xmax, ymin, ymax, zmin, zmax; /* first/last cell centres (grid.f90) */
+  double R0, hslope, akm, gam;
+  double cfl, dmin, pmin, pmax, tmax, dtmin;
+  int ibc[6][9]; /* iboux1in, iboux1ot, iboux2in, iboux2ot, iboux3in, iboux3ot */
+  int guard;     /* 0 reference semantics.  Bit 1: first-order fallback for reconstructed face
+                    states with rho<=0 or p<=0 (MP5/WENO5 undershoot at a torus surface);
+                    bit 2: zero flux of the normal B component before flux-CT (Toth 2000),
+                    which the reference's LLF term breaks (hll.f90:109).  Not in the reference. */
+  int precision; /* rg_precision */
+} rg_run_params;
+
+typedef struct rg_step_stats {
+  long long steps;        /* full RK3 steps taken */
+  long long recov_calls;  /* interior cells inverted */
+  long long recov_nr2;    /* cells that needed the entropy Newton-Raphson (recov.f90:1022) */
+  long long recov_fail;   /* cells that kept their previous primitives (recov.f90:1196) */
+  long long recov_carry;  /* cells whose W guess came from the previous cell (recov.f90:810) */
+  long long recov_cap;    /* capped W rescale loops (unbounded "go to 95", recov.f90:823) */
+  long long floor_cap;    /* capped pminmax2b loops (unbounded "go to 95", correction.f90:870) */
+  long long carry_overflow; /* carry cells beyond the device list capacity */
+  double time;            /* simulation time at the loop top of the next step */
+  double dt;              /* dt of the last step */
+} rg_step_stats;
+
+typedef struct rg_ctx rg_ctx;
+
+/* Library / context ------------------------------------------------------ */
+const char* rg_last_error(void);
+int rg_ctx_create(int device, rg_ctx** out);
+int rg_ctx_destroy(rg_ctx* ctx);
+int rg_sync(rg_ctx* ctx);
+/* Run all later work of ctx on a caller-owned cudaStream_t (passed as void*) of
+ * the same device, e.g. the stream of an enclosing framework; the context
+ * then no longer owns or destroys a stream. */
+int rg_ctx_set_stream(rg_ctx* ctx, void* stream);
+
+/* Runs ------------------------------------------------------------------- */
+/* Admit a run: checks the parameters, computes grid (grid.f90:2-266), metric
+ * (coord.f90:5-146) and Christoffel symbols (coord.f90:1089-1321) and
+ * allocates the device state.  RG_ENOMEM_ADMIT if it does not fit. */
+int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id);
+int rg_run_release(rg_ctx* ctx, int run);
+/* Device bytes a run with these parameters needs (admission by footprint). */
+int rg_run_footprint(const rg_run_params* p, size_t* bytes);
+
+/* Initial data: Fishbone-Moncrief torus of mdtorus1 (mdgrmhd.f90:879-1654);
+ * the pressure perturbation is p *= 1 + amp*(U-0.5) with U a counter-based
+ * uniform keyed by (seed, cell).  Also sets time = 0 (main.f90:530-548). */
+int rg_run_ic_torus(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin, double rmax,
+                    double beta, double kappa);
+/* Host <-> device primitives, layout a(nv,i,j,k).  Upload also sets time = t0. */
+int rg_run_upload_prims(rg_ctx* ctx, int run, const double* uri, double t0);
+int rg_run_download_prims(rg_ctx* ctx, int run, double* uri);
+
+/* Advance nsteps full RK3 steps of main.f90:586-1147 on the device (CFL
+ * reduction, three stages, ghost fill, floors).  Stops early once the loop-top
+ * time exceeds tmax.  Asynchronous on the context stream unless stats != NULL. */
+int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats);
+int rg_run_stats(rg_ctx* ctx, int run, rg_step_stats* stats);
+
+/* Kernel timing: rg_profile(ctx, 1) clears the counters and brackets every
+ * following launch of rg_step with CUDA events on the context stream;
+ * rg_profile_read returns accumulated milliseconds and launch counts per kind:
+ * 0 cfl, 1 flux r, 2 flux phi, 3 flux theta, 4 flux-CT, 5 update (+ W carry),
+ * 6 ghost fill, 7 floors, 8 scalar bookkeeping.  Launch counts are kept with
+ * profiling off too.  No counterpart in the reference (cpu_time only). */
+int rg_profile(rg_ctx* ctx, int enable);
+int rg_profile_read(rg_ctx* ctx, double* ms, long long* launches, int nkinds);
+
+/* Reference-interface entry points (host arrays in the reference layout);
+ * each runs the named routine(s) on the GPU for per-routine parity. */
+/* caluu1 (caluu.f90:2-126) */
+int rg_caluu1(rg_ctx* ctx, int run, const double* uri, double* uu);
+/* rec2 + calcha + hll + ct (rec.f90:2-142, calflx.f90:391-795, calcha.f90:2-126,
+ * hll.f90:47-192, ct.f90:30-118): ww(3,nv,i,j,k) on the hll range */
+int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww);
+/* recov1a (recov.f90:578-1228) on the interior: uu in (conserved), uri in/out */
+int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri);
+/* cdtcfl4 (cdtcfl.f90:2-129): dtcfl before the cfl factor */
+int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl);
+/* bnd4 + infchk + atmosphere1a + pminmax2b (bnd.f90, correction.f90) on uri in/out */
+int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RAISHIN_GPU_H */

@@ -1,0 +1,186 @@
+// oracle_api.cpp -- C entry points of the CPU oracle (test infrastructure only;
+// see oracle.hpp).  Arrays crossing this boundary use the reference layout
+// a(nv,i,j,k): variable fastest, then i, j, k.
+#include <cstring>
+#include <string>
+
+#include "oracle.hpp"
+
+using orc::State;
+
+extern "C" {
+
+void* orc_create(const orc_params* p) {
+  State* s = new State();
+  s->p = *p;
+  s->imax = p->imax; s->jmax = p->jmax; s->kmax = p->kmax;
+  s->ncell = (size_t)p->imax * p->jmax * p->kmax;
+  // ghost widths (main.f90:176-196): MP5/WENO5 nm0 = 3, PPM nm0 = 4; flux-CT nm1 = nm0+1
+  s->nm0 = (p->irec == 5) ? 4 : 3;
+  s->nm1 = s->nm0 + 1;
+  orc::grid(*s);
+  orc::coord1(*s);
+  orc::calchrist(*s);
+  const size_t n9 = s->ncell * orc::NV;
+  for (auto* v : {&s->uu, &s->uo, &s->uh, &s->us, &s->un, &s->uri, &s->urio, &s->uriir, &s->uriil,
+                  &s->urijr, &s->urijl, &s->urikr, &s->urikl, &s->uuir, &s->uuil, &s->uujr, &s->uujl,
+                  &s->uukr, &s->uukl, &s->wwir, &s->wwil, &s->wwjr, &s->wwjl, &s->wwkr, &s->wwkl})
+    v->assign(n9, 0.0);
+  s->ww.assign(3 * n9, 0.0);
+  s->sf.assign(4 * s->ncell, 0.0);
+  for (auto* v : {&s->cmaxi, &s->cmini, &s->cmaxj, &s->cminj, &s->cmaxk, &s->cmink}) v->assign(s->ncell, 0.0);
+  return s;
+}
+
+void orc_destroy(void* h) { delete static_cast<State*>(h); }
+
+int orc_nm1(void* h) { return static_cast<State*>(h)->nm1; }
+
+// mdtorus1 followed by the copies of main.f90:530-548
+void orc_ic_torus(void* h, unsigned long long seed, double amp, double rin, double rmax, double beta,
+                  double kappa) {
+  State* s = static_cast<State*>(h);
+  orc::mdtorus1(*s, seed, amp, rin, rmax, beta, kappa);
+}
+
+void orc_set_prims(void* h, const double* uri) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+}
+
+void orc_get_prims(void* h, double* uri) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(uri, s->uri.data(), s->uri.size() * sizeof(double));
+}
+
+void orc_get_cons(void* h, double* uu) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(uu, s->uu.data(), s->uu.size() * sizeof(double));
+}
+
+// main.f90:530-548: conserved from primitives, time = 0
+void orc_init_cons(void* h) {
+  State* s = static_cast<State*>(h);
+  orc::caluu1(*s, s->uri, s->uu);
+  s->uo = s->uu;
+  s->urio = s->uri;
+  s->time = 0.0; s->timeh = 0.0; s->it = 0;
+}
+
+// Runs up to nsteps passes of the time loop; stops early (returns the count
+// done) when the loop-top time exceeds tmax (main.f90:617-632).
+int orc_step(void* h, int nsteps) {
+  State* s = static_cast<State*>(h);
+  for (int n = 0; n < nsteps; ++n) {
+    if (s->timeh > s->p.tmax) return n;
+    orc::step(*s);
+  }
+  return nsteps;
+}
+
+double orc_time(void* h) { return static_cast<State*>(h)->timeh; }
+double orc_dt(void* h) { return static_cast<State*>(h)->dt; }
+void orc_get_stats(void* h, orc_stats* out) { *out = static_cast<State*>(h)->st; }
+
+// Per-routine hooks used by the parity tests ------------------------------
+
+// caluu1 on the given primitives
+void orc_caluu1(void* h, const double* uri, double* uu) {
+  State* s = static_cast<State*>(h);
+  std::vector<double> p(uri, uri + s->uri.size()), u(s->uu.size());
+  orc::caluu1(*s, p, u);
+  std::memcpy(uu, u.data(), u.size() * sizeof(double));
+}
+
+// rec2 + calcha + hll + ct on the given primitives; ww(3,nv,i,j,k) out
+void orc_fluxes(void* h, const double* uri, double* ww) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  orc::rec2(*s);
+  orc::calcha(*s);
+  orc::hlle(*s);
+  orc::fluxct(*s);
+  std::memcpy(ww, s->ww.data(), s->ww.size() * sizeof(double));
+}
+
+// recov1a over the interior: uu (in/out, uu(6) rewritten), uri (in: guess, out)
+void orc_recov(void* h, double* uu, double* uri) {
+  State* s = static_cast<State*>(h);
+  std::vector<double> u(uu, uu + s->uu.size());
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  orc::recov1a(*s, u);
+  std::memcpy(uu, u.data(), u.size() * sizeof(double));
+  std::memcpy(uri, s->uri.data(), s->uri.size() * sizeof(double));
+}
+
+// cdtcfl4 on the given primitives
+double orc_cdtcfl(void* h, const double* uri) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  return orc::cdtcfl4(*s);
+}
+
+// bnd4 + infchk + atmosphere1a + pminmax2b on uri (in/out) with urio
+void orc_bnd_floor(void* h, double* uri, const double* urio) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  std::memcpy(s->urio.data(), urio, s->urio.size() * sizeof(double));
+  orc::bnd4(*s);
+  if (s->p.model >= 7 && s->p.model <= 20) orc::infchk(*s);
+  if (s->p.model >= 7 && s->p.model <= 15) orc::atmosphere1a(*s);
+  orc::pminmax2b(*s);
+  std::memcpy(uri, s->uri.data(), s->uri.size() * sizeof(double));
+}
+
+// Grid and metric arrays by name.  1D grid arrays: n = extent (1-based values
+// copied to out[0..n-1]).  Metric per (i,k): 16 (gcov*/gcon*) or 1 (detg*)
+// or 64 (christ) values per point, point index i-1 + imax*(k-1).
+long long orc_get_array(void* h, const char* name, double* out, long long cap) {
+  State* s = static_cast<State*>(h);
+  const std::string n(name);
+  auto vec1 = [&](const std::vector<double>& v, int len) -> long long {
+    if (cap < len) return -1;
+    for (int i = 1; i <= len; ++i) out[i - 1] = v[i];
+    return len;
+  };
+  if (n == "x1") return vec1(s->x1, s->imax);
+  if (n == "x1a") return vec1(s->x1a, s->imax);
+  if (n == "x1b") return vec1(s->x1b, s->imax);
+  if (n == "dx1b") return vec1(s->dx1b, s->imax);
+  if (n == "x2") return vec1(s->x2, s->jmax);
+  if (n == "dx2b") return vec1(s->dx2b, s->jmax);
+  if (n == "x3") return vec1(s->x3, s->kmax);
+  if (n == "x3a") return vec1(s->x3a, s->kmax);
+  if (n == "x3b") return vec1(s->x3b, s->kmax);
+  if (n == "dx3b") return vec1(s->dx3b, s->kmax);
+  const size_t nik = (size_t)s->imax * s->kmax;
+  auto m4 = [&](const std::vector<orc::M4>& v) -> long long {
+    if ((size_t)cap < 16 * nik) return -1;
+    for (size_t q = 0; q < nik; ++q)
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) out[16 * q + 4 * a + b] = v[q].a[a][b];
+    return (long long)(16 * nik);
+  };
+  auto sc = [&](const std::vector<double>& v) -> long long {
+    if ((size_t)cap < nik) return -1;
+    std::memcpy(out, v.data(), nik * sizeof(double));
+    return (long long)nik;
+  };
+  if (n == "gcov") return m4(s->gcov);
+  if (n == "gcon") return m4(s->gcon);
+  if (n == "gcovi") return m4(s->gcovi);
+  if (n == "gconi") return m4(s->gconi);
+  if (n == "gcovk") return m4(s->gcovk);
+  if (n == "gconk") return m4(s->gconk);
+  if (n == "detg") return sc(s->detg);
+  if (n == "detgi") return sc(s->detgi);
+  if (n == "detgk") return sc(s->detgk);
+  if (n == "christ") {
+    if ((size_t)cap < 64 * nik) return -1;
+    std::memcpy(out, s->christ.data(), 64 * nik * sizeof(double));
+    return (long long)(64 * nik);
+  }
+  return -2;
+}
+
+}  // extern "C"

@@ -1,0 +1,192 @@
+"""ctypes binding of oracle/_build/liboracle.so (test infrastructure only).
+
+Arrays use the reference layout a(nv,i,j,k), which as a C-ordered numpy array
+has shape (kmax, jmax, imax, 9).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build_oracle as _build_mod
+
+_LIB = None
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("imax", C.c_int), ("jmax", C.c_int), ("kmax", C.c_int),
+        ("metric", C.c_int), ("ix1", C.c_int), ("ix2", C.c_int), ("ix3", C.c_int),
+        ("irec", C.c_int), ("model", C.c_int), ("iter", C.c_int),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
+        ("zmin", C.c_double), ("zmax", C.c_double),
+        ("R0", C.c_double), ("hslope", C.c_double), ("akm", C.c_double), ("gam", C.c_double),
+        ("cfl", C.c_double), ("dmin", C.c_double), ("pmin", C.c_double), ("pmax", C.c_double),
+        ("tmax", C.c_double), ("dtmin", C.c_double),
+        ("ibc", (C.c_int * 9) * 6),
+        ("guard", C.c_int),
+    ]
+
+
+class OrcStats(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in
+                ("recov_calls", "recov_nr2", "recov_fail", "recov_carry", "recov_cap", "floor_cap")]
+
+
+def build(force: bool = False) -> str:
+    return _build_mod.build(force=force)
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        path = build()
+        lib = C.CDLL(path)
+        P = C.c_void_p
+        D = C.POINTER(C.c_double)
+        lib.orc_create.restype = P
+        lib.orc_create.argtypes = [C.POINTER(OrcParams)]
+        lib.orc_destroy.argtypes = [P]
+        lib.orc_nm1.argtypes = [P]
+        lib.orc_nm1.restype = C.c_int
+        lib.orc_ic_torus.argtypes = [P, C.c_ulonglong, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     C.c_double]
+        for f in ("orc_set_prims", "orc_get_prims", "orc_get_cons"):
+            getattr(lib, f).argtypes = [P, D]
+        lib.orc_init_cons.argtypes = [P]
+        lib.orc_step.argtypes = [P, C.c_int]
+        lib.orc_step.restype = C.c_int
+        lib.orc_time.argtypes = [P]
+        lib.orc_time.restype = C.c_double
+        lib.orc_dt.argtypes = [P]
+        lib.orc_dt.restype = C.c_double
+        lib.orc_get_stats.argtypes = [P, C.POINTER(OrcStats)]
+        lib.orc_caluu1.argtypes = [P, D, D]
+        lib.orc_fluxes.argtypes = [P, D, D]
+        lib.orc_recov.argtypes = [P, D, D]
+        lib.orc_cdtcfl.argtypes = [P, D]
+        lib.orc_cdtcfl.restype = C.c_double
+        lib.orc_bnd_floor.argtypes = [P, D, D]
+        lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
+        lib.orc_get_array.restype = C.c_longlong
+        _LIB = lib
+    return _LIB
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_params(p: dict) -> OrcParams:
+    o = OrcParams()
+    for name, _ in OrcParams._fields_:
+        if name == "ibc":
+            for s in range(6):
+                for m in range(9):
+                    o.ibc[s][m] = int(p["ibc"][s][m])
+        else:
+            setattr(o, name, p.get(name, 0) if name == "guard" else p[name])
+    return o
+
+
+class Oracle:
+    """One reference-semantics run on the CPU (single MPI rank)."""
+
+    def __init__(self, params: dict):
+        self.params = dict(params)
+        self._p = make_params(params)
+        self.lib = _lib()
+        self.h = self.lib.orc_create(C.byref(self._p))
+        self.shape = (params["kmax"], params["jmax"], params["imax"], 9)
+        self.nm1 = self.lib.orc_nm1(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def zeros(self):
+        return np.zeros(self.shape, dtype=np.float64)
+
+    def ic_torus(self, seed=2012, amp=0.04, rin=6.0, rmax=12.0, beta=100.0, kappa=1e-3):
+        self.lib.orc_ic_torus(self.h, seed, amp, rin, rmax, beta, kappa)
+
+    def set_prims(self, uri: np.ndarray):
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        self.lib.orc_set_prims(self.h, _ptr(uri))
+
+    def prims(self) -> np.ndarray:
+        out = self.zeros()
+        self.lib.orc_get_prims(self.h, _ptr(out))
+        return out
+
+    def cons(self) -> np.ndarray:
+        out = self.zeros()
+        self.lib.orc_get_cons(self.h, _ptr(out))
+        return out
+
+    def init_cons(self):
+        self.lib.orc_init_cons(self.h)
+
+    def step(self, n: int = 1) -> int:
+        return self.lib.orc_step(self.h, int(n))
+
+    @property
+    def time(self) -> float:
+        return self.lib.orc_time(self.h)
+
+    @property
+    def dt(self) -> float:
+        return self.lib.orc_dt(self.h)
+
+    def stats(self) -> dict:
+        st = OrcStats()
+        self.lib.orc_get_stats(self.h, C.byref(st))
+        return {n: getattr(st, n) for n, _ in OrcStats._fields_}
+
+    def caluu1(self, uri):
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = self.zeros()
+        self.lib.orc_caluu1(self.h, _ptr(uri), _ptr(out))
+        return out
+
+    def fluxes(self, uri):
+        """ww(3,nv,i,j,k) as shape (kmax, jmax, imax, 9, 3)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = np.zeros(self.shape + (3,), dtype=np.float64)
+        self.lib.orc_fluxes(self.h, _ptr(uri), _ptr(out))
+        return out
+
+    def recov(self, uu, uri):
+        uu = np.array(uu, dtype=np.float64, order="C").reshape(self.shape)
+        uri = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
+        self.lib.orc_recov(self.h, _ptr(uu), _ptr(uri))
+        return uu, uri
+
+    def cdtcfl(self, uri) -> float:
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        return self.lib.orc_cdtcfl(self.h, _ptr(uri))
+
+    def bnd_floor(self, uri, urio):
+        uri = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
+        urio = np.ascontiguousarray(urio, dtype=np.float64).reshape(self.shape)
+        self.lib.orc_bnd_floor(self.h, _ptr(uri), _ptr(urio))
+        return uri
+
+    def array(self, name: str) -> np.ndarray:
+        p = self.params
+        cap = 64 * p["imax"] * p["kmax"] + max(p["imax"], p["jmax"], p["kmax"])
+        buf = np.zeros(cap, dtype=np.float64)
+        n = self.lib.orc_get_array(self.h, name.encode(), _ptr(buf), cap)
+        if n < 0:
+            raise KeyError(name)
+        return buf[:n].copy()

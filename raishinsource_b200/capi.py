@@ -1,0 +1,260 @@
+"""ctypes binding of the in-tree libraishin_gpu.so (include/raishin_gpu.h).
+
+This is the host-side mirror of the reference's driver interface: a run is
+admitted with its ``pram``-style parameter block, given initial data
+(``mdtorus1`` or uploaded primitives), stepped on the GPU, and read back in the
+reference layout a(nv,i,j,k).  The per-routine entry points keep the names of
+the Fortran subroutines they replace (caluu1, calflx, recov, cdtcfl, bnd4).
+
+There is no CPU fallback: every call goes through the CUDA library, and
+loading fails loudly if the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .config import ghost_widths
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libraishin_gpu.so")
+
+STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA", 4: "RG_ENR_CAP",
+          5: "RG_ENAN", 6: "RG_ENOTFOUND", 7: "RG_EOVERFLOW"}
+
+#: every entry point include/raishin_gpu.h declares
+EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
+           "rg_run_footprint", "rg_run_ic_torus", "rg_run_upload_prims", "rg_run_download_prims", "rg_step",
+           "rg_run_stats", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor")
+
+
+class RgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class RunParams(C.Structure):
+    _fields_ = [
+        ("imax", C.c_int), ("jmax", C.c_int), ("kmax", C.c_int),
+        ("metric", C.c_int), ("ix1", C.c_int), ("ix2", C.c_int), ("ix3", C.c_int),
+        ("irec", C.c_int), ("model", C.c_int), ("iter", C.c_int),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
+        ("zmin", C.c_double), ("zmax", C.c_double),
+        ("R0", C.c_double), ("hslope", C.c_double), ("akm", C.c_double), ("gam", C.c_double),
+        ("cfl", C.c_double), ("dmin", C.c_double), ("pmin", C.c_double), ("pmax", C.c_double),
+        ("tmax", C.c_double), ("dtmin", C.c_double),
+        ("ibc", (C.c_int * 9) * 6),
+        ("guard", C.c_int),
+        ("precision", C.c_int),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in
+                ("steps", "recov_calls", "recov_nr2", "recov_fail", "recov_carry", "recov_cap", "floor_cap",
+                 "carry_overflow")] + [("time", C.c_double), ("dt", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library (building it first if the .so is absent or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    from . import build as _build
+    path = _build.build() if path == LIB_PATH else path
+    lib = C.CDLL(path)
+    P, D, I = C.c_void_p, C.POINTER(C.c_double), C.c_int
+    lib.rg_last_error.restype = C.c_char_p
+    lib.rg_ctx_create.argtypes = [I, C.POINTER(C.c_void_p)]
+    lib.rg_ctx_destroy.argtypes = [P]
+    lib.rg_sync.argtypes = [P]
+    lib.rg_ctx_set_stream.argtypes = [P, P]
+    lib.rg_run_admit.argtypes = [P, C.POINTER(RunParams), C.POINTER(C.c_int)]
+    lib.rg_run_release.argtypes = [P, I]
+    lib.rg_run_footprint.argtypes = [C.POINTER(RunParams), C.POINTER(C.c_size_t)]
+    lib.rg_run_ic_torus.argtypes = [P, I, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double,
+                                    C.c_double]
+    lib.rg_run_upload_prims.argtypes = [P, I, C.c_void_p, C.c_double]
+    lib.rg_run_download_prims.argtypes = [P, I, C.c_void_p]
+    lib.rg_step.argtypes = [P, I, I, C.POINTER(StepStats)]
+    lib.rg_run_stats.argtypes = [P, I, C.POINTER(StepStats)]
+    lib.rg_profile.argtypes = [P, I]
+    lib.rg_profile_read.argtypes = [P, D, C.POINTER(C.c_longlong), I]
+    lib.rg_caluu1.argtypes = [P, I, D, D]
+    lib.rg_calflx.argtypes = [P, I, D, D]
+    lib.rg_recov.argtypes = [P, I, D, D]
+    lib.rg_cdtcfl.argtypes = [P, I, D, D]
+    lib.rg_bnd_floor.argtypes = [P, I, D, D]
+    _lib = lib
+    return lib
+
+
+def _check(lib, rc: int):
+    if rc != 0:
+        raise RgError(rc, lib.rg_last_error().decode(errors="replace"))
+
+
+def make_params(p: dict) -> RunParams:
+    o = RunParams()
+    for name, _ in RunParams._fields_:
+        if name == "ibc":
+            for s in range(6):
+                for m in range(9):
+                    o.ibc[s][m] = int(p["ibc"][s][m])
+        elif name == "guard":
+            o.guard = int(p.get("guard", 0))
+        elif name == "precision":
+            o.precision = {"fp64": 0, "mixed": 1}[p.get("precision", "fp64")]
+        else:
+            setattr(o, name, p[name])
+    return o
+
+
+def footprint(p: dict) -> int:
+    lib = load()
+    n = C.c_size_t(0)
+    _check(lib, lib.rg_run_footprint(C.byref(make_params(p)), C.byref(n)))
+    return n.value
+
+
+def _dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Context:
+    """One CUDA stream on one device (rg_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        _check(self.lib, self.lib.rg_ctx_create(int(device), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.rg_ctx_destroy(self.h)
+            self.h = None
+
+    def sync(self):
+        _check(self.lib, self.lib.rg_sync(self.h))
+
+    def set_stream(self, stream_handle: int):
+        """Issue all later work on a caller-owned cudaStream_t (e.g. torch's current stream)."""
+        _check(self.lib, self.lib.rg_ctx_set_stream(self.h, C.c_void_p(stream_handle)))
+
+    KINDS = ("cfl", "flux_r", "flux_phi", "flux_theta", "flux_ct", "update", "ghost_fill", "floors", "scalar")
+
+    def profile(self, enable: bool = True):
+        """Clear kernel timers/launch counters; with enable, time every launch with CUDA events."""
+        _check(self.lib, self.lib.rg_profile(self.h, int(bool(enable))))
+
+    def profile_read(self) -> dict:
+        n = len(self.KINDS)
+        ms = (C.c_double * n)()
+        cnt = (C.c_longlong * n)()
+        _check(self.lib, self.lib.rg_profile_read(self.h, ms, cnt, n))
+        return {k: {"ms": ms[i], "launches": cnt[i]} for i, k in enumerate(self.KINDS)}
+
+    def admit(self, params: dict) -> "Run":
+        return Run(self, params)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Run:
+    """One admitted run: device-resident state of one grid."""
+
+    def __init__(self, ctx: Context, params: dict):
+        self.ctx, self.lib = ctx, ctx.lib
+        self.params = dict(params)
+        self._p = make_params(params)
+        rid = C.c_int(0)
+        _check(self.lib, self.lib.rg_run_admit(ctx.h, C.byref(self._p), C.byref(rid)))
+        self.id = rid.value
+        self.shape = (params["kmax"], params["jmax"], params["imax"], 9)
+        self.nm0, self.nm1 = ghost_widths(params["irec"])
+
+    def release(self):
+        if self.id:
+            self.lib.rg_run_release(self.ctx.h, self.id)
+            self.id = 0
+
+    def zeros(self):
+        return np.zeros(self.shape, dtype=np.float64)
+
+    # initial data / state transfer
+    def ic_torus(self, seed=2012, amp=0.04, rin=6.0, rmax=12.0, beta=100.0, kappa=1e-3):
+        _check(self.lib, self.lib.rg_run_ic_torus(self.ctx.h, self.id, seed, amp, rin, rmax, beta, kappa))
+
+    def upload_prims(self, uri, t0: float = 0.0):
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        _check(self.lib, self.lib.rg_run_upload_prims(self.ctx.h, self.id, uri.ctypes.data, float(t0)))
+
+    def upload_prims_ptr(self, host_ptr: int, t0: float = 0.0):
+        """Upload from a raw host pointer (e.g. pinned memory), layout a(nv,i,j,k)."""
+        _check(self.lib, self.lib.rg_run_upload_prims(self.ctx.h, self.id, C.c_void_p(host_ptr), float(t0)))
+
+    def prims(self) -> np.ndarray:
+        out = self.zeros()
+        _check(self.lib, self.lib.rg_run_download_prims(self.ctx.h, self.id, out.ctypes.data))
+        return out
+
+    def download_prims_ptr(self, host_ptr: int):
+        _check(self.lib, self.lib.rg_run_download_prims(self.ctx.h, self.id, C.c_void_p(host_ptr)))
+
+    # time stepping
+    def step(self, n: int = 1, stats: bool = False):
+        st = StepStats()
+        _check(self.lib, self.lib.rg_step(self.ctx.h, self.id, int(n), C.byref(st) if stats else None))
+        return st.as_dict() if stats else None
+
+    def stats(self) -> dict:
+        st = StepStats()
+        _check(self.lib, self.lib.rg_run_stats(self.ctx.h, self.id, C.byref(st)))
+        return st.as_dict()
+
+    # reference-interface entry points (host arrays, layout a(nv,i,j,k))
+    def caluu1(self, uri) -> np.ndarray:
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = self.zeros()
+        _check(self.lib, self.lib.rg_caluu1(self.ctx.h, self.id, _dptr(uri), _dptr(out)))
+        return out
+
+    def calflx(self, uri) -> np.ndarray:
+        """ww(3,nv,i,j,k) as shape (kmax, jmax, imax, 9, 3)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = np.zeros(self.shape + (3,), dtype=np.float64)
+        _check(self.lib, self.lib.rg_calflx(self.ctx.h, self.id, _dptr(uri), _dptr(out)))
+        return out
+
+    def recov(self, uu, uri) -> np.ndarray:
+        uu = np.ascontiguousarray(uu, dtype=np.float64).reshape(self.shape)
+        out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
+        _check(self.lib, self.lib.rg_recov(self.ctx.h, self.id, _dptr(uu), _dptr(out)))
+        return out
+
+    def cdtcfl(self, uri) -> float:
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = C.c_double(0.0)
+        _check(self.lib, self.lib.rg_cdtcfl(self.ctx.h, self.id, _dptr(uri), C.byref(out)))
+        return out.value
+
+    def bnd_floor(self, uri, urio) -> np.ndarray:
+        out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
+        urio = np.ascontiguousarray(urio, dtype=np.float64).reshape(self.shape)
+        _check(self.lib, self.lib.rg_bnd_floor(self.ctx.h, self.id, _dptr(out), _dptr(urio)))
+        return out

@@ -1,0 +1,984 @@
+// rg_kernels.cu -- sm_100a kernels of one RK3 stage of the RAISHIN GRMHD
+// update (main.f90:807-911) on one GPU.
+//
+// Per stage:  k_flux<1..3>  reconstruction + face state + LLF flux per face
+//             k_ct          flux-CT averaging of the induction fluxes
+//             k_update      RK combine + geometric source + primitive recovery
+//             k_carry_fix   loop-order W carry of recov1a (only when queued)
+//             k_bc_*        ghost fill in the reference's pass order
+//             k_floor       infchk + atmosphere1a + pminmax2b (pointwise)
+// Per step:   k_step_begin, k_cfl (block min + atomicMin), k_dt, k_step_end.
+// All state is FP64 structure-of-arrays; a step never synchronises the host.
+#include <cuda_runtime.h>
+
+#include "rg_device.cuh"
+#include "rg_kernels.cuh"
+
+namespace rg {
+
+namespace {
+
+__device__ __forceinline__ void count_event(const DevRun& r, int which, bool flag) {
+  const unsigned mask = __activemask();
+  const unsigned b = __ballot_sync(mask, flag);
+  if (b && (threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(r.cnt + which, (unsigned long long)__popc(b));
+}
+
+__device__ __forceinline__ void load9(const double* __restrict__ P, size_t N, size_t c, double q[9]) {
+#pragma unroll
+  for (int v = 0; v < 9; ++v) q[v] = P[(size_t)v * N + c];
+}
+
+// ----------------------------------------------------------------- recov1a
+struct RecovOut {
+  double wg;
+  bool nr2, fail, cap;
+};
+
+constexpr int kRescaleCap = 1000;  // the reference's "go to 95" loop (recov.f90:823-850) is unbounded
+
+// recov.f90:578-1228 for one interior cell.  u: conserved (sqrt(-g) scaled),
+// q: previous primitives (initial guess and failure fallback), out: new
+// primitives.  Returns false, touching nothing, when the W quadratic has no
+// non-negative root and no carried-in W is given: the reference then keeps W
+// from the previous cell of its loop (recov.f90:810-815), which the caller
+// resolves in loop order.
+__device__ bool recov_cell(const double u[9], const double q[9], double out[9], const Met& m, double gam,
+                           int iter, double dmin, double pmin, double x1i, const double* wg_carry, RecovOut& res) {
+  const double safty = 1.0e-4, saftybig = 1.0e5, dv = 1.0e-2;
+  const double gam1 = gam / (gam - 1.0), gam2 = 1.0 / gam1;
+  const double detg1 = m.detg;
+  double delta = 1.0, deltaend = 1.e-7;
+  int irecov = 0;
+  const double alpha1 = 1. / sqrt(-m.gc[0][0]);
+  const double dro = alpha1 * u[0] * (1. / detg1);
+  double qcov[4], qcon[4], bcon[4], bcov[4], oncov[4], oncon[4];
+  qcov[0] = alpha1 * (u[4] - u[0]) * (1. / detg1);
+  qcov[1] = alpha1 * u[1] * (1. / detg1);
+  qcov[2] = alpha1 * u[2] * (1. / detg1);
+  qcov[3] = alpha1 * u[3] * (1. / detg1);
+  const double gss = alpha1 * u[5] * (1. / detg1);
+  bcon[0] = 0.0;
+  bcon[1] = alpha1 * u[6] * (1. / detg1);
+  bcon[2] = alpha1 * u[7] * (1. / detg1);
+  bcon[3] = alpha1 * u[8] * (1. / detg1);
+  double ro = q[0], pp = q[4];
+  double util[4] = {0.0, q[1], q[2], q[3]};
+  lower4(bcon, bcov, m.g);
+  lower4(qcov, qcon, m.gc);
+  const double bsq = bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
+  const double qdotb = qcov[0] * bcon[0] + qcov[1] * bcon[1] + qcov[2] * bcon[2] + qcov[3] * bcon[3];
+  const double qdotbsq = qdotb * qdotb;
+  oncov[0] = -1.0 * alpha1; oncov[1] = 0.0; oncov[2] = 0.0; oncov[3] = 0.0;
+  lower4(oncov, oncon, m.gc);
+  const double qdotn = qcon[0] * oncov[0];
+  const double qsq = qcov[0] * qcon[0] + qcov[1] * qcon[1] + qcov[2] * qcon[2] + qcov[3] * qcon[3];
+  const double qtsq = qsq + (qdotn * qdotn);
+  double utsq = 0.0;
+#pragma unroll
+  for (int a = 1; a <= 3; ++a)
+#pragma unroll
+    for (int b = 1; b <= 3; ++b) utsq = utsq + m.g[a][b] * util[a] * util[b];
+  if (utsq < 0.0 && fabs(utsq) <= safty) utsq = fabs(utsq);
+  if (fabs(utsq) > 1.e4) utsq = 1.e4;
+  double gfsq = 1. + utsq;
+  double gf = sqrt(gfsq);
+  double vsq = (gfsq - 1.) * (1. / gfsq);
+  const double t1a = 4. - vsq;
+  const double t1b = 4. * (bsq + qdotn);
+  const double t1c = qtsq + bsq * bsq + 2. * bsq * qdotn;
+  double t1d = (t1b * t1b) - 4. * t1a * t1c;
+  if (t1d <= 0.0) t1d = fabs(t1d);
+  const double wgp = (-t1b + sqrt(t1d)) * (1. / (2. * t1a));
+  const double wgm = (-t1b - sqrt(t1d)) * (1. / (2. * t1a));
+  double wg;
+  if (wgp > 0.0) wg = wgp;
+  else if (wgm >= 0.0) wg = wgm;
+  else {
+    if (!wg_carry) return false;
+    wg = *wg_carry;
+  }
+  bool cap = false;
+  for (int cnt = 0;; ++cnt) {
+    if (cnt >= kRescaleCap) { cap = true; break; }
+    pp = gam2 * (wg * gf - dro * sqrt(gf));
+    const double t3a = (wg * wg * wg) * (wg + 2. * bsq) - qdotbsq * (2. * wg + bsq);
+    const double t3b = (wg * wg) * (qtsq - bsq * bsq);
+    const double t3c = (wg * wg * wg) + (wg * wg) * (0.5 * bsq + qdotn - pp) - 0.5 * qdotbsq;
+    if (t3a <= t3b) { wg = fabs(1.5 * wg); continue; }
+    if (t3c > 0.0) { wg = fabs((double)0.9f * wg); continue; }
+    break;
+  }
+  res.nr2 = false;
+  if (!cap) {
+    double wsq = wg * wg;
+    const double xsq = (bsq + wg) * (bsq + wg);
+    vsq = fabs((wsq * qtsq + qdotbsq * (bsq + 2. * wg)) * (1. / (wsq * xsq)));
+    if (vsq > 1.0) vsq = 1.0 - dv;
+    const double vsqo = vsq;
+    double xxn = wg, yyn = vsq;
+    // 2D Newton-Raphson on (W, v^2) (recov.f90:877-960)
+    for (int nnn = 1; nnn <= iter; ++nnn) {
+      if (!(fabs(delta) >= deltaend && irecov == 0)) break;
+      if (nnn == iter) { irecov = 1; break; }
+      wg = xxn;
+      vsq = yyn;
+      wsq = wg * wg;
+      const double w3 = wsq * wg;
+      double gtmp = 1. - vsq;
+      if (gtmp < 0.0 || gtmp < safty) { gtmp = safty; vsq = 1. - gtmp; }
+      const double ptmp = gam2 * (wg * gtmp - dro * sqrt(gtmp));
+      const double f1 = qtsq - vsq * (wg + bsq) * (wg + bsq) + (qdotbsq * (bsq + 2. * wg)) * (1. / wsq);
+      const double g1 = -qdotn - 0.5 * bsq * (1. + vsq) + 0.5 * (qdotbsq * (1. / wsq)) - wg + ptmp;
+      const double dpdw = gam2 * gtmp;
+      const double dpdvsq = -(gam2 * wg) + 0.5 * gam2 * dro * (1. / (sqrt(gtmp)));
+      const double dfx = -(2. * (wg + bsq) * (vsq + qdotbsq * (1. / w3)));
+      const double dfy = -((wg + bsq) * (wg + bsq));
+      const double dgx = -1. - (qdotbsq * (1. / w3)) + dpdw;
+      const double dgy = -(0.5 * bsq) + dpdvsq;
+      double det = dfx * dgy - dfy * dgx;
+      if (det == 0.0) det = 1.0;
+      const double dx = (-(dgy * f1) + dfy * g1) * (1. / det);
+      const double dy = (dgx * f1 - dfx * g1) * (1. / det);
+      delta = 0.5 * (fabs(dx) + fabs(dy));
+      xxn = wg + dx;
+      yyn = vsq + dy;
+      if (xxn < 0.0) xxn = fabs(xxn);
+      if (xxn > saftybig) xxn = saftybig;
+      if (yyn < 0.0) yyn = fabs(yyn);
+      if (fabs(yyn) > 1.0) yyn = 1.0 - dv;
+    }
+    if (irecov == 0) {
+      wg = xxn;
+      vsq = yyn;
+      double gtmp = 1. - vsq;
+      if (gtmp < 0.0 || gtmp < safty) { gtmp = safty; vsq = 1. - gtmp; }
+      gf = 1. / sqrt(gtmp);
+      ro = dro * (1. / gf);
+      const double w2 = wg * (gtmp);
+      pp = gam2 * (w2 - ro);
+      if (ro < 0.0 || pp < 0.0) irecov = 1;
+      if (irecov == 0) {
+#pragma unroll
+        for (int a = 1; a <= 3; ++a) {
+          const double qt = qcon[a] + oncon[a] * qdotn;
+          util[a] = (gf * (1. / (wg + bsq))) * (qt + qdotb * bcon[a] * (1. / wg));
+        }
+      }
+      wg = xxn;
+      vsq = yyn;
+    }
+    // entropy Newton-Raphson on v^2 (recov.f90:1022-1147)
+    if (irecov == 1) {
+      res.nr2 = true;
+      delta = 1.0;
+      deltaend = 1.e-6;
+      irecov = 0;
+      xxn = vsqo;
+      for (int nnn = 1; nnn <= iter; ++nnn) {
+        if (!(fabs(delta) >= deltaend && irecov == 0)) break;
+        if (nnn == iter) { irecov = 1; break; }
+        vsq = xxn;
+        double gtmp = 1. - vsq;
+        if (gtmp < 0.0 || gtmp < safty) { gtmp = safty; vsq = 1. - gtmp; }
+        gf = 1. / sqrt(gtmp);
+        gfsq = gf * gf;
+        ro = dro * (1. / gf);
+        pp = (gss / dro) * pow(ro, gam);
+        const double roh = ro + gam1 * pp;
+        wg = fabs(gfsq * roh);
+        wsq = wg * wg;
+        const double w3 = wsq * wg;
+        const double dgfdvsq = 0.5 * pow(gtmp, -1.5);
+        const double dwdvsq =
+            dro * dgfdvsq + gam1 * gss * pow(dro, gam - 1.) * (2. - gam) * pow(gf, 1. - gam) * dgfdvsq;
+        const double f = qtsq - vsq * (wg + bsq) * (wg + bsq) + (qdotbsq * (bsq + 2. * wg)) / wsq;
+        const double ta = -((wg + bsq) * (wg + bsq));
+        const double tb = -(2. * vsq * (wg + bsq));
+        const double tc = -(2. * qdotbsq * (bsq + 2. * wg) * (1. / w3));
+        const double td = 2. * qdotbsq * (1. / wsq);
+        const double df = ta + (tb + tc + td) * dwdvsq;
+        delta = f / df;
+        xxn = vsq - delta;
+        if (xxn < 0.0) xxn = fabs(xxn);
+        if (fabs(xxn) >= 1.0) xxn = 1. - dv;
+      }
+      if (irecov == 0) {
+        vsq = xxn;
+        double gtmp = 1. - vsq;
+        if (gtmp < 0.0 || gtmp < safty) gtmp = safty;
+        gf = 1. / sqrt(gtmp);
+        gfsq = gf * gf;
+        ro = dro * (1. / gf);
+        pp = (gss * (1. / gf)) * pow(ro, gam - 1.);
+        if (ro < 0.0) ro = dmin * pow(x1i, -1.5);
+        if (pp < 0.0) pp = (gam - 1.) * pmin * pow(x1i, -2.5);
+        const double roh = ro + gam1 * pp;
+        wg = fabs(gfsq * roh);
+#pragma unroll
+        for (int a = 1; a <= 3; ++a) {
+          const double qt = qcon[a] + oncon[a] * qdotn;
+          util[a] = (gf / (wg + bsq)) * (qt + qdotb * bcon[a] * (1. / wg));
+        }
+      }
+    }
+  } else {
+    irecov = 1;
+  }
+  res.cap = cap;
+  res.fail = (irecov != 0);
+  res.wg = wg;
+  // recov.f90:1174-1216 (the uu(6) rewrite is overwritten by caluu1 and is not kept)
+  if (irecov == 0) {
+    out[0] = ro; out[1] = util[1]; out[2] = util[2]; out[3] = util[3]; out[4] = pp;
+    out[5] = ro * pp / pow(ro, gam - 1.);
+  } else {
+    out[0] = q[0]; out[1] = q[1]; out[2] = q[2]; out[3] = q[3]; out[4] = q[4];
+    out[5] = q[0] * q[4] / pow(q[0], gam);
+  }
+  out[6] = u[6] * (1. / detg1);
+  out[7] = u[7] * (1. / detg1);
+  out[8] = u[8] * (1. / detg1);
+  return true;
+}
+
+// ------------------------------------------------------------ stage update
+// Conserved state after the RK combine and source (rkt.f90:2-320) of one
+// interior cell.  U = P2C(P) always holds in the reference (caluu1 runs after
+// every stage, main.f90:899), so the stage inputs uu/uo/uh/us are recomputed
+// from the stored primitives here.
+template <int STAGE>
+__device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pn,
+                          const double* __restrict__ Pc, const double* __restrict__ F1, const double* __restrict__ F2,
+                          const double* __restrict__ F3, const double* __restrict__ CT, double dt, double u[9]) {
+  const size_t N = r.N, c = r.cell(i, j, k), q = r.ik(i, k);
+  const double gam = r.gam;
+  double qc[9];
+  load9(Pc, N, c, qc);
+  PS s;
+  pstate(qc, m, gam, s);
+  double ucur[9];
+  p2c(s, gam, m.detg, ucur);
+  // geometric source (calsf.f90:6-151): S_nu = sqrt(-g) T^m_n Gamma^n_{nu m}
+  double sf[4];
+  {
+    const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
+    double ta = 0.0, tb = 0.0, tc = 0.0, td = 0.0;
+    const size_t nik = r.nik;
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const double t = a * s.ucon[mm] * s.ucov[n] + b * (mm == n ? 1.0 : 0.0) - s.bbcon[mm] * s.bbcov[n];
+        ta = ta + t * __ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
+        tb = tb + t * __ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
+        tc = tc + t * __ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
+        td = td + t * __ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
+      }
+    sf[0] = m.detg * ta; sf[1] = m.detg * tb; sf[2] = m.detg * tc; sf[3] = m.detg * td;
+  }
+  double uo[9];
+  if (STAGE > 1) {
+    double qn[9];
+    load9(Pn, N, c, qn);
+    PS sn;
+    pstate(qn, m, gam, sn);
+    p2c(sn, gam, m.detg, uo);
+  }
+  const double a1 = dt / __ldg(r.dx1b + i - 1), a2 = dt / __ldg(r.dx2b + j - 1), a3 = dt / __ldg(r.dx3b + k - 1);
+  const size_t ci = c - 1, cj = c - (size_t)r.imax, ck = c - (size_t)r.imax * r.jmax;
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    // flux-CT replaces ww(2,7) ww(3,7) ww(1,8) ww(3,8) ww(1,9) ww(2,9) (ct.f90:98-109)
+    double d1, d2, d3;
+    if (v == 7) d1 = CT[2 * N + c] - CT[2 * N + ci];
+    else if (v == 8) d1 = CT[4 * N + c] - CT[4 * N + ci];
+    else d1 = F1[(size_t)v * N + c] - F1[(size_t)v * N + ci];
+    if (v == 6) d2 = CT[0 * N + c] - CT[0 * N + cj];
+    else if (v == 8) d2 = CT[5 * N + c] - CT[5 * N + cj];
+    else d2 = F2[(size_t)v * N + c] - F2[(size_t)v * N + cj];
+    if (v == 6) d3 = CT[1 * N + c] - CT[1 * N + ck];
+    else if (v == 7) d3 = CT[3 * N + c] - CT[3 * N + ck];
+    else d3 = F3[(size_t)v * N + c] - F3[(size_t)v * N + ck];
+    if (STAGE == 1) u[v] = ucur[v] - a1 * d1 - a2 * d2 - a3 * d3;
+    else if (STAGE == 2) u[v] = (3.0 * uo[v] + ucur[v]) * 0.25 + (-(a1 * d1) - a2 * d2 - a3 * d3) * 0.25;
+    else u[v] = (uo[v] + 2. * ucur[v]) * (double)(1.0f / 3.0f) + (-(a1 * d1) - a2 * d2 - a3 * d3) * (double)(2.0f / 3.0f);
+  }
+#pragma unroll
+  for (int v = 1; v <= 4; ++v) {
+    if (STAGE == 1) u[v] = u[v] + sf[v - 1] * dt;
+    else if (STAGE == 2) u[v] = u[v] + sf[v - 1] * dt * 0.25;
+    else u[v] = u[v] + sf[v - 1] * dt * (double)(2.0f / 3.0f);
+  }
+}
+
+__device__ __forceinline__ bool is_interior(const DevRun& r, int i, int j, int k) {
+  return i > r.nm1 && i <= r.imax - r.nm1 && j > r.nm1 && j <= r.jmax - r.nm1 && k > r.nm1 && k <= r.kmax - r.nm1;
+}
+
+__device__ __forceinline__ void queue_carry(const DevRun& r, int i, int j, int k) {
+  const int ni = r.imax - 2 * r.nm1, nj = r.jmax - 2 * r.nm1;
+  const int lin = (i - r.nm1 - 1) + ni * ((j - r.nm1 - 1) + nj * (k - r.nm1 - 1));
+  const int slot = atomicAdd(&r.scal->carry_count, 1);
+  if (slot < r.carry_cap) r.carry_list[slot] = lin;
+  else atomicAdd(r.cnt + C_CARRY_OVF, 1ull);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
+                                                double* __restrict__ Pw, const double* __restrict__ F1,
+                                                const double* __restrict__ F2, const double* __restrict__ F3,
+                                                const double* __restrict__ CT) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > r.imax || j > r.jmax || k > r.kmax) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  // A finished run (time > tmax) copies its state through the stage so that the
+  // host-side buffer rotation stays valid without a host synchronisation.
+  if (!r.scal->active || !is_interior(r, i, j, k)) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = Pc[(size_t)v * N + c];
+    return;
+  }
+  Met m;
+  load_met(r.mc, r.nik, r.ik(i, k), m);
+  double u[9];
+  stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
+  double qo[9], qn[9];
+  load9(Pc, N, c, qo);
+  RecovOut o{0.0, false, false, false};
+  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.iter, r.dmin, r.pmin, __ldg(r.x1 + i - 1), nullptr, o);
+  if (!ok) {
+    queue_carry(r, i, j, k);
+  } else {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = qn[v];
+  }
+  count_event(r, C_NR2, ok && o.nr2);
+  count_event(r, C_FAIL, ok && o.fail);
+  count_event(r, C_CAP, ok && o.cap);
+}
+
+// Resolve cells queued by k_update / k_recov in the reference's loop order
+// (k, j, i over the interior): each takes the final W of its predecessor cell.
+// One thread; runs only when cells were queued, which the reference data
+// rarely produces.  MODE 0: stage update; MODE 1: recov-only entry point.
+template <int MODE, int STAGE>
+__global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
+                            double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
+                            const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (MODE == 0 && !r.scal->active) return;
+  int n = r.scal->carry_count;
+  if (n <= 0) return;
+  if (n > r.carry_cap) n = r.carry_cap;
+  int* L = r.carry_list;
+  for (int a = 1; a < n; ++a) {  // insertion sort: the list is short
+    const int x = L[a];
+    int b = a - 1;
+    while (b >= 0 && L[b] > x) { L[b + 1] = L[b]; --b; }
+    L[b + 1] = x;
+  }
+  const int ni = r.imax - 2 * r.nm1, nj = r.jmax - 2 * r.nm1;
+  const double dt = (MODE == 0) ? r.scal->dt : 0.0;
+  auto coords = [&](int lin, int& i, int& j, int& k) {
+    i = lin % ni + r.nm1 + 1;
+    j = (lin / ni) % nj + r.nm1 + 1;
+    k = lin / (ni * nj) + r.nm1 + 1;
+  };
+  auto run_cell = [&](int lin, const double* carry, double& wg_out, bool write, RecovOut& o) -> bool {
+    int i, j, k;
+    coords(lin, i, j, k);
+    const size_t c = r.cell(i, j, k);
+    Met m;
+    load_met(r.mc, r.nik, r.ik(i, k), m);
+    double u[9], qo[9], qn[9];
+    if (MODE == 0) stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, dt, u);
+    else load9(U, r.N, c, u);
+    load9(Pc, r.N, c, qo);
+    const bool ok = recov_cell(u, qo, qn, m, r.gam, r.iter, r.dmin, r.pmin, r.x1[i - 1], carry, o);
+    if (ok) {
+      wg_out = o.wg;
+      if (write)
+        for (int v = 0; v < 9; ++v) Pw[(size_t)v * r.N + c] = qn[v];
+    }
+    return ok;
+  };
+  int prev_lin = -2;
+  double prev_wg = 0.0;
+  for (int a = 0; a < n; ++a) {
+    const int lin = L[a];
+    double wg_in = 0.0;  // the first cell of the sweep starts from W = 0 (recov.f90:642)
+    if (lin > 0) {
+      if (prev_lin == lin - 1) {
+        wg_in = prev_wg;
+      } else {
+        RecovOut po{0.0, false, false, false};
+        double w = 0.0;
+        run_cell(lin - 1, nullptr, w, false, po);  // the predecessor has a root of its own
+        wg_in = w;
+      }
+    }
+    RecovOut o{0.0, false, false, false};
+    double w = 0.0;
+    run_cell(lin, &wg_in, w, true, o);
+    prev_lin = lin;
+    prev_wg = w;
+    atomicAdd(r.cnt + C_CARRY, 1ull);
+    if (o.nr2) atomicAdd(r.cnt + C_NR2, 1ull);
+    if (o.fail) atomicAdd(r.cnt + C_FAIL, 1ull);
+    if (o.cap) atomicAdd(r.cnt + C_CAP, 1ull);
+  }
+  r.scal->carry_count = 0;
+}
+
+// ------------------------------------------------------------- face fluxes
+// One thread per face f+1/2 in direction D over the hll range nm0..n-nm0 in
+// every dimension (hll.f90:83-85).  The left state comes from cell f
+// (uriil(f)), the right state from cell f+1 (uriir(f), rec.f90:2138).
+template <int D, int IREC>
+__global__ void __launch_bounds__(128) k_flux(DevRun r, const double* __restrict__ P, double* __restrict__ F) {
+  if (!r.scal->active) return;
+  const int nm0 = r.nm0;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + nm0;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + nm0;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + nm0;
+  if (i > r.imax - nm0 || j > r.jmax - nm0 || k > r.kmax - nm0) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.imax : (long long)r.imax * r.jmax);
+  double qL[9], qR[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    if (v == 5) { qL[v] = 0.0; qR[v] = 0.0; continue; }  // var 6 faces are never read downstream
+    const double* p = P + (size_t)v * N + c;
+    const double um2 = p[-2 * st], um1 = p[-st], u0 = p[0], up1 = p[st], up2 = p[2 * st], up3 = p[3 * st];
+    if (IREC == 6) {
+      qL[v] = mp5_left(um2, um1, u0, up1, up2);
+      qR[v] = mp5_right(um1, u0, up1, up2, up3);
+    } else {
+      qL[v] = weno5_state(um2, um1, u0, up1, up2);
+      qR[v] = weno5_state(up3, up2, up1, u0, um1);
+    }
+  }
+  if (r.guard & 1) {
+    if (!(qL[0] > 0.0 && qL[4] > 0.0)) load9(P, N, c, qL);
+    if (!(qR[0] > 0.0 && qR[4] > 0.0)) load9(P, N, c + st, qR);
+  }
+  Met m;
+  if (D == 1) load_met(r.mi, r.nik, r.ik(i, k), m);
+  else if (D == 2) load_met(r.mc, r.nik, r.ik(i, k), m);
+  else load_met(r.mk, r.nik, r.ik(i, k), m);
+  const double gam = r.gam;
+  double uL[9], wL[9], uR[9], wR[9], vpL, vmL, vpR, vmR;
+  {
+    PS s;
+    pstate(qL, m, gam, s);
+    p2c(s, gam, m.detg, uL);
+    flux<D>(s, gam, m.detg, wL);
+    wavespeed<D>(qL, s, m, gam, vpL, vmL);
+  }
+  {
+    PS s;
+    pstate(qR, m, gam, s);
+    p2c(s, gam, m.detg, uR);
+    flux<D>(s, gam, m.detg, wR);
+    wavespeed<D>(qR, s, m, gam, vpR, vmR);
+  }
+  // calcha.f90:96-120 (cmink uses the R-state plus speed, calcha.f90:107)
+  const double cmax = fmax3(0.0, vpR, vpL);
+  const double cmin = (D == 3) ? fmin3(0.0, vpR, vmL) : fmin3(0.0, vmR, vmL);
+  // hll.f90:83-183
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    double w;
+    if (cmin > 0.0) w = wL[v];
+    else if (cmin <= 0.0 && cmax > 0.0) {
+      const double c1 = dmax2(fabs(cmax), fabs(cmin));
+      w = 0.5 * (wL[v] + wR[v] - c1 * (uR[v] - uL[v]));
+    } else if (cmax <= 0.0) w = wR[v];
+    else continue;  // NaN speeds: the reference keeps the previous ww
+    if (fabs(w) < 1.0e-40) w = 0.0;
+    if ((r.guard & 2) && v == 5 + D) w = 0.0;  // Toth: no flux of the normal field component
+    F[(size_t)v * N + c] = w;
+  }
+}
+
+// ---------------------------------------------------------------- flux-CT
+// ct.f90:30-118 on nm1..n-nm1 in every dimension.
+__global__ void __launch_bounds__(256) k_ct(DevRun r, const double* __restrict__ F1, const double* __restrict__ F2,
+                                            const double* __restrict__ F3, double* __restrict__ CT) {
+  if (!r.scal->active) return;
+  const int nm1 = r.nm1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + nm1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + nm1;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + nm1;
+  if (i > r.imax - nm1 || j > r.jmax - nm1 || k > r.kmax - nm1) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  const size_t di = 1, dj = (size_t)r.imax, dk = (size_t)r.imax * r.jmax;
+  const double* fyx = F2 + 6 * N;  // ww(2,7)
+  const double* fzx = F3 + 6 * N;  // ww(3,7)
+  const double* fxy = F1 + 7 * N;  // ww(1,8)
+  const double* fzy = F3 + 7 * N;  // ww(3,8)
+  const double* fxz = F1 + 8 * N;  // ww(1,9)
+  const double* fyz = F2 + 8 * N;  // ww(2,9)
+  const double e = 1.0 / 8.0;
+  CT[0 * N + c] = e * (2.0 * fyx[c] + fyx[c + di] + fyx[c - di] - fxy[c] - fxy[c + dj] - fxy[c - di] - fxy[c - di + dj]);
+  CT[1 * N + c] = e * (2.0 * fzx[c] + fzx[c + di] + fzx[c - di] - fxz[c] - fxz[c + dk] - fxz[c - di] - fxz[c - di + dk]);
+  CT[2 * N + c] = e * (2.0 * fxy[c] + fxy[c + dj] + fxy[c - dj] - fyx[c] - fyx[c + di] - fyx[c - dj] - fyx[c + di - dj]);
+  CT[3 * N + c] = e * (2.0 * fzy[c] + fzy[c + dj] + fzy[c - dj] - fyz[c] - fyz[c + dk] - fyz[c - dj] - fyz[c - dj + dk]);
+  CT[4 * N + c] = e * (2.0 * fxz[c] + fxz[c + dk] + fxz[c - dk] - fzx[c] - fzx[c + di] - fzx[c - dk] - fzx[c + di - dk]);
+  CT[5 * N + c] = e * (2.0 * fyz[c] + fyz[c + dk] + fyz[c - dk] - fzy[c] - fzy[c + dj] - fzy[c - dk] - fzy[c + dj - dk]);
+}
+
+// ------------------------------------------------------------ boundaries
+// Layer n (1-based) along direction D of column (t1, t2).
+template <int D>
+__device__ __forceinline__ size_t col_cell(const DevRun& r, int t1, int t2, int n) {
+  if (D == 1) return r.cell(n, t1, t2);
+  if (D == 2) return r.cell(t1, n, t2);
+  return r.cell(t1, t2, n);
+}
+
+// bnd.f90:45-70, 156-180, 266-292: single-rank periodic copy for columns whose
+// transverse indices are interior.
+template <int D>
+__global__ void k_bc_periodic(DevRun r, double* __restrict__ P) {
+  if (!r.scal->active) return;
+  const int nm1 = r.nm1;
+  const int n1 = (D == 1) ? r.jmax : r.imax;
+  const int n2 = (D == 3) ? r.jmax : r.kmax;
+  const int t1 = blockIdx.x * blockDim.x + threadIdx.x + nm1 + 1;
+  const int t2 = blockIdx.y * blockDim.y + threadIdx.y + nm1 + 1;
+  if (t1 > n1 - nm1 || t2 > n2 - nm1) return;
+  const int len = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
+  const int ib0 = 1 + nm1, ib1 = len - nm1;
+  const size_t N = r.N;
+  for (int n = 1; n <= nm1; ++n)
+    for (int v = 0; v < 9; ++v) {
+      if (r.ibc[2 * (D - 1)][v] == 1 || r.ibc[2 * (D - 1) + 1][v] == 1) {
+        double* p = P + (size_t)v * N;
+        p[col_cell<D>(r, t1, t2, ib0 - n)] = p[col_cell<D>(r, t1, t2, ib1 + 1 - n)];
+        p[col_cell<D>(r, t1, t2, ib1 + n)] = p[col_cell<D>(r, t1, t2, ib0 - 1 + n)];
+      }
+    }
+}
+
+// bnd.f90:384-1058: physical boundary codes for every column of direction D.
+template <int D>
+__global__ void k_bc_phys(DevRun r, double* __restrict__ P, const double* __restrict__ Po) {
+  if (!r.scal->active) return;
+  const int n1 = (D == 1) ? r.jmax : r.imax;
+  const int n2 = (D == 3) ? r.jmax : r.kmax;
+  const int t1 = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int t2 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (t1 > n1 || t2 > n2) return;
+  const int nm1 = r.nm1;
+  const int L = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
+  const size_t N = r.N;
+  for (int v = 0; v < 9; ++v) {
+    double* u = P + (size_t)v * N;
+    const double* uo = Po + (size_t)v * N;
+    auto at = [&](int n) { return col_cell<D>(r, t1, t2, n); };
+    switch (r.ibc[2 * (D - 1)][v]) {  // inner side
+      case 2: for (int n = 1; n <= nm1; ++n) u[at(n)] = uo[at(n)]; break;
+      case 3: for (int n = nm1; n >= 1; --n) u[at(n)] = (4.0 * u[at(n + 1)] - u[at(n + 2)]) / 3.0; break;
+      case 4: for (int n = nm1; n >= 1; --n) u[at(n)] = 2.0 * u[at(n + 1)] - u[at(n + 2)]; break;
+      case 5: for (int n = nm1; n >= 1; --n) u[at(n)] = u[at(1 + nm1)]; break;
+      case 12: for (int n = 1; n <= nm1; ++n) u[at(n)] = -u[at(2 * nm1 - n + 1)]; break;
+      case 13: for (int n = 1; n <= nm1; ++n) u[at(n)] = 0.0; break;
+      case 14: for (int n = 1; n <= nm1; ++n) u[at(n)] = u[at(2 * nm1 - n + 1)]; break;
+      case 7: for (int n = nm1; n >= 1; --n) u[at(n)] = uo[at(n)] + u[at(n + 1)] - uo[at(n + 1)]; break;
+      default: break;
+    }
+    switch (r.ibc[2 * (D - 1) + 1][v]) {  // outer side
+      case 2: for (int n = 0; n <= nm1 - 1; ++n) u[at(L - n)] = uo[at(L - n)]; break;
+      case 3: for (int n = nm1 - 1; n >= 0; --n) u[at(L - n)] = (4.0 * u[at(L - n - 1)] - u[at(L - n - 2)]) / 3.0; break;
+      case 4: for (int n = nm1 - 1; n >= 0; --n) u[at(L - n)] = 2.0 * u[at(L - n - 1)] - u[at(L - n - 2)]; break;
+      case 5: for (int n = nm1 - 1; n >= 0; --n) u[at(L - n)] = u[at(L - nm1)]; break;
+      case 12: for (int n = 0; n <= nm1 - 1; ++n) u[at(L - n)] = -u[at(L - 2 * nm1 + 1 + n)]; break;
+      case 13: for (int n = 0; n <= nm1 - 1; ++n) u[at(L - n)] = 0.0; break;
+      case 14: for (int n = 0; n <= nm1 - 1; ++n) u[at(L - n)] = u[at(L - 2 * nm1 + 1 + n)]; break;
+      case 7:
+        for (int n = nm1 - 1; n >= 0; --n) u[at(L - n)] = uo[at(L - n)] + u[at(L - n - 1)] - uo[at(L - n - 1)];
+        break;
+      case 18:  // x1 outer only (bnd.f90:598-610): zero when u^r of the last interior cell is negative
+        if (D == 1) {
+          const bool neg = P[(size_t)1 * N + at(L - nm1)] < 0.0;
+          for (int n = nm1 - 1; n >= 0; --n) u[at(L - n)] = neg ? 0.0 : u[at(L - nm1)];
+        }
+        break;
+      default: break;
+    }
+  }
+}
+
+// ----------------------------------------------------------------- floors
+// infchk (bnd.f90:1636-1824, outer radial ghosts), atmosphere1a
+// (correction.f90:226-447) and pminmax2b (correction.f90:744-999) over every
+// cell, in place.  pminmax2b stores rho alone when its rescale loop changed rho
+// (the "elseif" at correction.f90:887-893).
+__global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P) {
+  if (!r.scal->active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > r.imax || j > r.jmax || k > r.kmax) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  double q[9];
+  load9(P, N, c, q);
+  Met m;
+  load_met(r.mc, r.nik, r.ik(i, k), m);
+  const double gam = r.gam, rr = __ldg(r.x1 + i - 1);
+  if (r.model >= 7 && r.model <= 20 && i > r.imax - r.nm1) {
+    const double gflmax = 10.0;
+    double gfl = calgfl(q[1], q[2], q[3], m);
+    double vel[4] = {0.0, q[1] * (1. / gfl), q[2] * (1. / gfl), q[3] * (1. / gfl)};
+    if (vel[1] < 0.0) {
+      const double alpha1 = 1. / sqrt(-m.gc[0][0]);
+      const double b1 = alpha1 * alpha1 * m.gc[0][1];
+      vel[1] = b1 * (1. / alpha1);
+      double vsq = 0.0;
+#pragma unroll
+      for (int a = 1; a <= 3; ++a)
+#pragma unroll
+        for (int b = 1; b <= 3; ++b) vsq = vsq + m.g[a][b] * vel[a] * vel[b];
+      if (vsq >= 1.0) vsq = 1. - 1. / (gflmax * gflmax);
+      gfl = 1. / sqrt(1. - vsq);
+      q[1] = vel[1] * gfl; q[2] = vel[2] * gfl; q[3] = vel[3] * gfl;
+    }
+  }
+  if (r.model >= 7 && r.model <= 15) {
+    const double epsilon = 1.e-2, gflmax = 10.0;
+    const double demin = r.dmin * pow(rr, -1.5);
+    const double prmin = (gam - 1.) * r.pmin * pow(rr, -2.5);
+    const double dthe = 1.0 * (1. + epsilon) * demin;
+    const double dthe1 = 1.0 * (1. + epsilon) * prmin;
+    const double bsq = q[6] * q[6] + q[7] * q[7] + q[8] * q[8];
+    if (q[0] < dthe || (q[4] < dthe1 && bsq <= 1.e-20)) {
+      q[0] = demin;
+      q[4] = prmin;
+      const double vel[4] = {0.0, 0.0, 0.0, 0.0};
+      double vsq = 0.0;
+#pragma unroll
+      for (int a = 1; a <= 3; ++a)
+#pragma unroll
+        for (int b = 1; b <= 3; ++b) vsq = vsq + m.g[a][b] * vel[a] * vel[b];
+      if (vsq >= 1.0) vsq = 1. - 1. / (gflmax * gflmax);
+      const double gfl = 1. / sqrt(1. - vsq);
+      q[1] = vel[1] * gfl; q[2] = vel[2] * gfl; q[3] = vel[3] * gfl;
+    }
+    q[5] = 0.0;
+  }
+  {  // pminmax2b
+    const double gflmax = 20.0;
+    double de = q[0], pr = q[4];
+    double gfl = calgfl(q[1], q[2], q[3], m);
+    const double vel[4] = {0.0, q[1] * (1. / gfl), q[2] * (1. / gfl), q[3] * (1. / gfl)};
+    double vsq = 0.0;
+#pragma unroll
+    for (int a = 1; a <= 3; ++a)
+#pragma unroll
+      for (int b = 1; b <= 3; ++b) vsq = vsq + (m.g[a][b] + (0.0 * 0.0)) * vel[a] * vel[b];
+    if (vsq >= 1.0 || gfl > gflmax) vsq = 1. - 1. / (gflmax * gflmax);
+    gfl = 1. / sqrt(1. - vsq);
+    double lim[9];
+#pragma unroll
+    for (int v = 0; v < 9; ++v) lim[v] = q[v];
+    lim[1] = vel[1] * gfl; lim[2] = vel[2] * gfl; lim[3] = vel[3] * gfl;
+    PS s;
+    pstate(lim, m, gam, s);
+    const double bbsq = s.bbsq;
+    gfl = s.gfl;
+    const double bcon[4] = {0.0, q[6], q[7], q[8]};
+    double bcov[4];
+    lower4(bcon, bcov, m.g);
+    const double bsq = bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
+    const double f105 = (double)1.05f, f005 = (double)0.05f;
+    bool capped = false;
+    for (int cnt = 0;; ++cnt) {
+      if (cnt >= 100000) { capped = true; break; }
+      const double roh = de + (gam / (gam - 1.0)) * pr;
+      const double t1a = roh * gfl * gfl - pr;
+      const double t1b = fabs(f005 * bsq);
+      if (t1a <= t1b) { de = f105 * de; pr = f105 * pr; continue; }
+      break;
+    }
+    if (capped) atomicAdd(r.cnt + C_FLOORCAP, 1ull);
+    if (de != q[0]) q[0] = de;
+    else if (pr != q[4]) q[4] = pr;
+    const double demin = r.dmin * pow(rr, -1.5);
+    const double prmin = (gam - 1.) * r.pmin * pow(rr, -2.5);
+    const double bbromax = 50.0, bbprmax = 2.e3, prromax = 1.e6;
+    if (pr < prmin) q[4] = prmin;
+    if (pr > r.pmax) q[4] = r.pmax;
+    if (de < demin) q[0] = demin;
+    const double prro = q[4] * (1. / q[0]);
+    if (prro > prromax) q[0] = q[4] / prromax;
+    const double bbro = bbsq * (1. / q[0]);
+    const double bbpr = bbsq * (1. / q[4]);
+    if (bbro > bbromax) q[0] = bbsq / bbromax;
+    if (bbpr > bbprmax) q[4] = bbsq / bbprmax;
+  }
+#pragma unroll
+  for (int v = 0; v < 6; ++v) P[(size_t)v * N + c] = q[v];
+}
+
+// ------------------------------------------------------------------- CFL
+// cdtcfl4 (cdtcfl.f90:2-129) with calcha4 (calcha.f90:129-367) over
+// is1+1..ie1-1 (every dimension); min over cells, then over blocks with an
+// atomicMin on the bit pattern (positive doubles order like their bits).
+__global__ void __launch_bounds__(128) k_cfl(DevRun r, const double* __restrict__ P) {
+  if (!r.scal->active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+  double dtc = 1.0;
+  if (i <= r.imax - 1 && j <= r.jmax - 1 && k <= r.kmax - 1) {
+    const size_t c = r.cell(i, j, k);
+    double q[9];
+    load9(P, r.N, c, q);
+    Met m;
+    load_met(r.mc, r.nik, r.ik(i, k), m);
+    PS s;
+    pstate(q, m, r.gam, s);
+    double vp1, vm1, vp2, vm2, vp3, vm3;
+    wavespeed<1>(q, s, m, r.gam, vp1, vm1);
+    wavespeed<2>(q, s, m, r.gam, vp2, vm2);
+    wavespeed<3>(q, s, m, r.gam, vp3, vm3);
+    const double small = 1.e-12;
+    double vfi = fmax3(0.0, fabs(vp1), fabs(vm1));
+    double vfj = fmax3(0.0, fabs(vp2), fabs(vm2));
+    double vfk = fmax3(0.0, fabs(vp3), fabs(vm3));
+    double d1 = 1.e10, d2 = 1.e10, d3 = 1.e10;
+    if (r.imax > r.nmax_cfl && vfi > 0.0) { if (vfi > 1.0) vfi = 1.0; d1 = fabs(__ldg(r.dx1b + i - 1) / (vfi + small)); }
+    if (r.jmax > r.nmax_cfl && vfj > 0.0) { if (vfj > 1.0) vfj = 1.0; d2 = fabs(__ldg(r.dx2b + j - 1) / (vfj + small)); }
+    if (r.kmax > r.nmax_cfl && vfk > 0.0) { if (vfk > 1.0) vfk = 1.0; d3 = fabs(__ldg(r.dx3b + k - 1) / (vfk + small)); }
+    dtc = dmin2(dtc, d1);
+    dtc = dmin2(dtc, d2);
+    dtc = dmin2(dtc, d3);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dtc = dmin2(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+  __shared__ double red[32];
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  if ((t & 31) == 0) red[t >> 5] = dtc;
+  __syncthreads();
+  if (t < 32) {
+    double x = (t < (nt + 31) / 32) ? red[t] : 1.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = dmin2(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if (t == 0 && x > 0.0) atomicMin(&r.scal->dtcfl_bits, (unsigned long long)__double_as_longlong(x));
+  }
+}
+
+__global__ void k_step_begin(DevRun r) {
+  Scal* s = r.scal;
+  if (!s->active) return;
+  s->time = s->timeh;  // main.f90:617-620
+  if (s->time > r.tmax) { s->active = 0; return; }
+  s->dtcfl_bits = (unsigned long long)__double_as_longlong(1.0);
+}
+
+__global__ void k_dt(DevRun r) {
+  Scal* s = r.scal;
+  if (!s->active) return;
+  const double dtcfl = __longlong_as_double((long long)s->dtcfl_bits);
+  s->dt = r.cfl * dtcfl;  // main.f90:763
+  s->timeh = s->time + s->dt;
+}
+
+__global__ void k_step_end(DevRun r) {
+  if (!r.scal->active) return;
+  atomicAdd(r.cnt + C_STEPS, 1ull);
+}
+
+// ------------------------------------------------- per-routine entry points
+__global__ void __launch_bounds__(128) k_recov(DevRun r, const double* __restrict__ U, const double* __restrict__ Pc,
+                                               double* __restrict__ Pw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > r.imax || j > r.jmax || k > r.kmax) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  if (!is_interior(r, i, j, k)) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = Pc[(size_t)v * N + c];
+    return;
+  }
+  Met m;
+  load_met(r.mc, r.nik, r.ik(i, k), m);
+  double u[9], qo[9], qn[9];
+  load9(U, N, c, u);
+  load9(Pc, N, c, qo);
+  RecovOut o{0.0, false, false, false};
+  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.iter, r.dmin, r.pmin, __ldg(r.x1 + i - 1), nullptr, o);
+  if (!ok) queue_carry(r, i, j, k);
+  else
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = qn[v];
+  count_event(r, C_NR2, ok && o.nr2);
+  count_event(r, C_FAIL, ok && o.fail);
+  count_event(r, C_CAP, ok && o.cap);
+}
+
+// caluu1 (caluu.f90:2-126) on every cell
+__global__ void __launch_bounds__(128) k_p2c(DevRun r, const double* __restrict__ P, double* __restrict__ U) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > r.imax || j > r.jmax || k > r.kmax) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  double q[9], u[9];
+  load9(P, N, c, q);
+  Met m;
+  load_met(r.mc, r.nik, r.ik(i, k), m);
+  PS s;
+  pstate(q, m, r.gam, s);
+  p2c(s, r.gam, m.detg, u);
+#pragma unroll
+  for (int v = 0; v < 9; ++v) U[(size_t)v * N + c] = u[v];
+}
+
+// a(nv, cell) <-> SoA
+__global__ void k_aos_to_soa(const double* __restrict__ a, double* __restrict__ s, size_t N) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+#pragma unroll
+  for (int v = 0; v < 9; ++v) s[(size_t)v * N + c] = a[9 * c + v];
+}
+__global__ void k_soa_to_aos(const double* __restrict__ s, double* __restrict__ a, size_t N) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+#pragma unroll
+  for (int v = 0; v < 9; ++v) a[9 * c + v] = s[(size_t)v * N + c];
+}
+__global__ void k_fill(double* p, double v, size_t n) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) p[c] = v;
+}
+
+inline dim3 grid3(int nx, int ny, int nz, dim3 b) {
+  return dim3((unsigned)((nx + (int)b.x - 1) / (int)b.x), (unsigned)((ny + (int)b.y - 1) / (int)b.y),
+              (unsigned)((nz + (int)b.z - 1) / (int)b.z));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers
+cudaError_t launch_step_begin(const DevRun& r, cudaStream_t s) {
+  k_step_begin<<<1, 1, 0, s>>>(r);
+  return cudaGetLastError();
+}
+cudaError_t launch_dt(const DevRun& r, cudaStream_t s) {
+  k_dt<<<1, 1, 0, s>>>(r);
+  return cudaGetLastError();
+}
+cudaError_t launch_step_end(const DevRun& r, cudaStream_t s) {
+  k_step_end<<<1, 1, 0, s>>>(r);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  k_cfl<<<grid3(r.imax - 2, r.jmax - 2, r.kmax - 2, b), b, 0, s>>>(r, P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s) {
+  const int n = r.imax - 2 * r.nm0 + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
+  const dim3 b(64, 2, 1);
+  const dim3 g = grid3(n, m, l, b);
+  if (r.irec == 6) {
+    if (dir == 1) k_flux<1, 6><<<g, b, 0, s>>>(r, P, F);
+    else if (dir == 2) k_flux<2, 6><<<g, b, 0, s>>>(r, P, F);
+    else k_flux<3, 6><<<g, b, 0, s>>>(r, P, F);
+  } else {
+    if (dir == 1) k_flux<1, 7><<<g, b, 0, s>>>(r, P, F);
+    else if (dir == 2) k_flux<2, 7><<<g, b, 0, s>>>(r, P, F);
+    else k_flux<3, 7><<<g, b, 0, s>>>(r, P, F);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
+                      cudaStream_t s) {
+  const int n = r.imax - 2 * r.nm1 + 1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
+  const dim3 b(64, 4, 1);
+  k_ct<<<grid3(n, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
+                          const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  const dim3 g = grid3(r.imax, r.jmax, r.kmax, b);
+  if (stage == 1) {
+    k_update<1><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    k_carry_fix<0, 1><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  } else if (stage == 2) {
+    k_update<2><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    k_carry_fix<0, 2><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  } else {
+    k_update<3><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    k_carry_fix<0, 3><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  }
+  return cudaGetLastError();
+}
+
+static bool any_code(const DevRun& r, int side0, bool periodic) {
+  for (int sd = side0; sd <= side0 + 1; ++sd)
+    for (int v = 0; v < 9; ++v) {
+      const int c = r.ibc[sd][v];
+      if (periodic ? (c == 1) : (c != 1 && c != 0)) return true;
+    }
+  return false;
+}
+
+cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t s) {
+  const dim3 b(32, 4, 1);
+  const int nm1 = r.nm1;
+  // periodic passes on interior columns (bndpefb4), then physical passes on all columns (bndryfb4)
+  if (any_code(r, 0, true)) k_bc_periodic<1><<<grid3(r.jmax - 2 * nm1, r.kmax - 2 * nm1, 1, b), b, 0, s>>>(r, P);
+  if (any_code(r, 2, true)) k_bc_periodic<2><<<grid3(r.imax - 2 * nm1, r.kmax - 2 * nm1, 1, b), b, 0, s>>>(r, P);
+  if (any_code(r, 4, true)) k_bc_periodic<3><<<grid3(r.imax - 2 * nm1, r.jmax - 2 * nm1, 1, b), b, 0, s>>>(r, P);
+  if (any_code(r, 0, false)) k_bc_phys<1><<<grid3(r.jmax, r.kmax, 1, b), b, 0, s>>>(r, P, Po);
+  if (any_code(r, 2, false)) k_bc_phys<2><<<grid3(r.imax, r.kmax, 1, b), b, 0, s>>>(r, P, Po);
+  if (any_code(r, 4, false)) k_bc_phys<3><<<grid3(r.imax, r.jmax, 1, b), b, 0, s>>>(r, P, Po);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  k_floor<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  k_recov<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
+  k_carry_fix<1, 1><<<1, 1, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  k_p2c<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P, U);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_aos_to_soa(const double* aos, double* soa, size_t N, cudaStream_t s) {
+  k_aos_to_soa<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(aos, soa, N);
+  return cudaGetLastError();
+}
+cudaError_t launch_soa_to_aos(const double* soa, double* aos, size_t N, cudaStream_t s) {
+  k_soa_to_aos<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(soa, aos, N);
+  return cudaGetLastError();
+}
+cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s) {
+  k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, v, n);
+  return cudaGetLastError();
+}
+
+}  // namespace rg

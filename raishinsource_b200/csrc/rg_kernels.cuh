@@ -1,0 +1,36 @@
+// rg_kernels.cuh -- kernel declarations and launch helpers shared by the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "rg_types.h"
+
+namespace rg {
+
+// Buffers of one run on the device.
+struct DevBufs {
+  double* P[3];   // rotating primitive buffers, 9*N each (SoA)
+  double* F[3];   // raw LLF face fluxes per direction, 9*N each
+  double* CT;     // 6*N flux-CT averaged induction fluxes
+  double* stage;  // 9*N staging buffer (layout conversion, per-routine entry points)
+  double* stage2; // 9*N second staging buffer
+};
+
+cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s);
+cudaError_t launch_step_begin(const DevRun& r, cudaStream_t s);
+cudaError_t launch_dt(const DevRun& r, cudaStream_t s);
+cudaError_t launch_step_end(const DevRun& r, cudaStream_t s);
+cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s);
+cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
+                      cudaStream_t s);
+cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
+                          const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s);
+cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t s);
+cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s);
+// per-routine entry points
+cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s);
+cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s);
+cudaError_t launch_aos_to_soa(const double* aos, double* soa, size_t N, cudaStream_t s);
+cudaError_t launch_soa_to_aos(const double* soa, double* aos, size_t N, cudaStream_t s);
+cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s);
+
+}  // namespace rg

@@ -1,0 +1,65 @@
+// rg_types.h -- device-side description of one run (passed to every kernel by
+// value) and the host-side run record.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/raishin_gpu.h"
+
+namespace rg {
+
+constexpr int NV = 9;
+
+// Device scalars of a run (one small block of device memory).
+struct Scal {
+  unsigned long long dtcfl_bits;  // min-reduced CFL time step (bits of a positive double)
+  double dt;                      // cfl * dtcfl of the current step
+  double time;                    // loop-top time of the current step
+  double timeh;                   // time + dt
+  int active;                     // 0 once time > tmax: every kernel of the step returns early
+  int carry_count;                // cells queued for the loop-order W carry fix-up
+};
+
+// Counters (device, atomically accumulated).
+enum Counter {
+  C_STEPS = 0, C_RECOV, C_NR2, C_FAIL, C_CARRY, C_CAP, C_FLOORCAP, C_CARRY_OVF, C_NCOUNTERS
+};
+
+// Everything a kernel needs, by value.  Arrays are structure-of-arrays with
+// the cell index c = (i-1) + imax*((j-1) + jmax*(k-1)) (1-based i, j, k) and
+// variable v at offset v*N.  Metric caches are per (i,k) point
+// q = (i-1) + imax*(k-1), 33 components each (gcov 16, gcon 16, detg).
+struct DevRun {
+  int imax, jmax, kmax;
+  int nm0, nm1;
+  int irec, model, guard, iter;
+  int nmax_cfl;          // nm1*2 + (nm1-1) (cdtcfl.f90:38)
+  size_t N;              // cells
+  size_t nik;            // (i,k) points
+  double gam, cfl, dmin, pmin, pmax, tmax;
+  const double* mc;      // metric at cell centres (also the phi faces)
+  const double* mi;      // metric at the r faces x1a(i)
+  const double* mk;      // metric at the theta faces x3a(k)
+  const double* chr;     // Christoffel symbols, 64 per point: christ(l,m,n) at l+4m+16n
+  const double* x1;      // cell-centre r, index i-1
+  const double* dx1b;    // dx1b(i) at index i-1 (grid.f90:134-141)
+  const double* dx2b;
+  const double* dx3b;
+  const double* x2;      // phi centres (PPM contact detection)
+  const double* x3;      // theta centres
+  const double* dx1s;    // rec2's shifted dx1b: dummy dx1b(i) = actual dx1b(i-1), index i-1
+  const double* dx2s;
+  const double* dx3s;
+  int ibc[6][9];
+  Scal* scal;
+  unsigned long long* cnt;
+  int* carry_list;       // interior cells queued for the W carry fix-up
+  int carry_cap;
+
+  __host__ __device__ size_t cell(int i, int j, int k) const {
+    return (size_t)(i - 1) + (size_t)imax * ((size_t)(j - 1) + (size_t)jmax * (size_t)(k - 1));
+  }
+  __host__ __device__ size_t ik(int i, int k) const { return (size_t)(i - 1) + (size_t)imax * (size_t)(k - 1); }
+};
+
+}  // namespace rg

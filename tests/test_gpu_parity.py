@@ -1,0 +1,178 @@
+"""GPU parity: the sm_100a path (through the C ABI) against the oracle.
+
+Tolerance: the FP64 build compiles with --fmad=false and keeps the
+reference's evaluation order, so the only differences left are last-bit
+differences between CUDA's and glibc's pow/exp/log/sin/cos.  Per-routine
+results must agree to 1e-12 of each field's maximum (relative L-infinity per
+variable); one full RK3 step likewise (the north-star bound of 1e-12 per step).
+"""
+import numpy as np
+import pytest
+
+from conftest import field_err
+from oracle import Oracle
+from raishinsource_b200 import config
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _pair(gpu_ctx, p, seed=2012):
+    o = Oracle(p)
+    o.ic_torus(seed=seed)
+    r = gpu_ctx.admit(p)
+    r.upload_prims(o.prims())
+    return o, r
+
+
+@pytest.fixture(scope="module")
+def torus2d(gpu_ctx):
+    p = config.torus(nr=64, nth=64)
+    p["guard"] = 1
+    o, r = _pair(gpu_ctx, p)
+    yield p, o, r
+    r.release()
+
+
+@pytest.fixture(scope="module")
+def torus3d(gpu_ctx):
+    p = config.torus(nr=40, nth=24, nph=16)
+    p["guard"] = 1
+    o, r = _pair(gpu_ctx, p, seed=99)
+    yield p, o, r
+    r.release()
+
+
+def test_ic_torus_matches_oracle(gpu_ctx):
+    p = config.torus(nr=64, nth=48, nph=12)
+    o = Oracle(p)
+    o.ic_torus(seed=123, amp=0.04)
+    r = gpu_ctx.admit(p)
+    r.ic_torus(seed=123, amp=0.04)
+    err = field_err(r.prims(), o.prims())
+    r.release()
+    assert err.max() < 1e-13, err
+
+
+def test_caluu1(torus2d):
+    _, o, r = torus2d
+    u = o.prims()
+    err = field_err(r.caluu1(u), o.caluu1(u))
+    assert err.max() < TOL, err
+
+
+@pytest.mark.parametrize("irec", [config.IREC_MP5, config.IREC_WENO5])
+def test_calflx_guarded(gpu_ctx, irec):
+    p = config.torus(nr=48, nth=40, nph=12, irec=irec)
+    p["guard"] = 1
+    o, r = _pair(gpu_ctx, p, seed=5)
+    u = o.prims()
+    wg, wo = r.calflx(u), o.fluxes(u)
+    r.release()
+    n = o.nm1 - 1  # hll range nm0 .. n-nm0 (1-based) == slice(nm0-1, -nm0)
+    reg = (slice(n, -n), slice(n, -n), slice(n, -n))
+    for d in range(3):
+        err = field_err(wg[..., d], wo[..., d], reg)
+        assert err.max() < TOL, (d, err)
+
+
+def test_calflx_reference_semantics_nan_pattern(gpu_ctx):
+    """guard = 0: both paths produce the same non-finite entropy fluxes and
+    agree everywhere else."""
+    p = config.torus(nr=48, nth=40, nph=10)
+    o, r = _pair(gpu_ctx, p, seed=5)
+    u = o.prims()
+    wg, wo = r.calflx(u), o.fluxes(u)
+    r.release()
+    n = o.nm1 - 1
+    reg = (slice(n, -n), slice(n, -n), slice(n, -n))
+    a, b = wg[reg], wo[reg]
+    assert np.array_equal(np.isfinite(a), np.isfinite(b))
+    fin = np.isfinite(b)
+    assert (~fin).any()
+    scale = np.abs(np.where(fin, b, 0)).max(axis=(0, 1, 2))
+    diff = np.abs(np.where(fin, a - b, 0)).max(axis=(0, 1, 2))
+    assert (diff <= TOL * np.maximum(scale, 1e-300)).all()
+
+
+def test_recov(torus3d):
+    p, o, r = torus3d
+    u = o.prims()
+    rng = np.random.default_rng(0)
+    uu = o.caluu1(u)
+    n = o.nm1
+    pert = uu.copy()
+    pert[n:-n, n:-n, n:-n, :5] *= 1 + 1e-3 * rng.standard_normal(pert[n:-n, n:-n, n:-n, :5].shape)
+    _, want = o.recov(pert, u)
+    got = r.recov(pert, u)
+    err = field_err(got, want, (slice(n, -n), slice(n, -n), slice(n, -n)))
+    assert err[[0, 1, 2, 3, 4, 6, 7, 8]].max() < TOL, err
+
+
+def test_cdtcfl(torus3d):
+    _, o, r = torus3d
+    u = o.prims()
+    assert r.cdtcfl(u) == pytest.approx(o.cdtcfl(u), rel=TOL)
+
+
+def test_bnd_floor(torus3d):
+    _, o, r = torus3d
+    u = o.prims()
+    rng = np.random.default_rng(1)
+    v = u * (1 + 1e-2 * rng.standard_normal(u.shape))
+    v[..., 0] = np.abs(v[..., 0])
+    err = field_err(r.bnd_floor(v, u), o.bnd_floor(v, u))
+    assert err.max() < TOL, err
+
+
+def _step_err(gpu_ctx, p, steps, seed):
+    o = Oracle(p)
+    o.ic_torus(seed=seed)
+    r = gpu_ctx.admit(p)
+    r.upload_prims(o.prims())
+    o.init_cons()
+    errs = []
+    for _ in range(steps):
+        o.step(1)
+        st = r.step(1, stats=True)
+        errs.append(field_err(r.prims(), o.prims()).max())
+        r.upload_prims(o.prims(), t0=o.time)  # per-step bound: restart both from the oracle state
+    r.release()
+    return np.array(errs), st
+
+
+def test_step_2d_mp5(gpu_ctx):
+    p = dict(config.torus(nr=64, nth=64), guard=1)
+    errs, _ = _step_err(gpu_ctx, p, 3, seed=2012)
+    assert errs.max() < TOL, errs
+
+
+def test_step_3d_mp5(gpu_ctx):
+    p = dict(config.torus(nr=40, nth=24, nph=16), guard=1)
+    errs, _ = _step_err(gpu_ctx, p, 2, seed=77)
+    assert errs.max() < TOL, errs
+
+
+def test_step_3d_weno5(gpu_ctx):
+    p = dict(config.torus(nr=40, nth=24, nph=16, irec=config.IREC_WENO5), guard=1)
+    errs, _ = _step_err(gpu_ctx, p, 2, seed=78)
+    assert errs.max() < TOL, errs
+
+
+def test_multistep_drift(gpu_ctx):
+    """20 steps without re-synchronisation stay within a loose bound (round-off growth)."""
+    p = dict(config.torus(nr=48, nth=48), guard=3)
+    o = Oracle(p)
+    o.ic_torus(seed=4)
+    r = gpu_ctx.admit(p)
+    r.upload_prims(o.prims())
+    o.init_cons()
+    o.step(20)
+    st = r.step(20, stats=True)
+    got = r.prims()
+    r.release()
+    assert st["steps"] == 20 and st["time"] == pytest.approx(o.time, rel=1e-12)
+    n = o.nm1
+    l1 = np.abs(got - o.prims())[n:-n, n:-n, n:-n].sum(axis=(0, 1, 2)) / np.abs(o.prims()[n:-n, n:-n, n:-n]).sum(axis=(0, 1, 2)).clip(1e-300)
+    assert l1[[0, 4, 6, 8]].max() < 1e-10, l1

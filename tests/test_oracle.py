@@ -1,0 +1,156 @@
+"""CPU checks of the oracle (the C++ restatement of the reference).
+
+The reference ships no golden vectors, so the oracle is checked against
+properties the reference's own formulas imply: the LU inverse of the metric,
+exact prim -> conserved -> prim round trips through recov1a, flux-CT keeping
+the corner-centred divergence of B at round-off, the positivity guard being a
+no-op where no face state is negative, and thread-count independence.
+"""
+import numpy as np
+import pytest
+
+from conftest import field_err
+from oracle import Oracle
+from raishinsource_b200 import config
+
+
+@pytest.fixture(scope="module")
+def torus_small():
+    p = config.torus(nr=48, nth=48, irec=config.IREC_MP5)
+    p["guard"] = 1
+    o = Oracle(p)
+    o.ic_torus(seed=7)
+    return p, o
+
+
+def test_metric_inverse_and_detg(torus_small):
+    _, o = torus_small
+    for loc in ("", "i", "k"):
+        g = o.array("gcov" + loc).reshape(-1, 4, 4)
+        gc = o.array("gcon" + loc).reshape(-1, 4, 4)
+        err = np.abs(np.einsum("qab,qbc->qac", g, gc) - np.eye(4)).max()
+        assert err < 1e-13, loc
+        detg = o.array("detg" + loc)
+        assert np.all(detg > 0)
+        assert np.allclose(detg, np.sqrt(-np.linalg.det(g)), rtol=1e-12)
+
+
+def test_grid_matches_reference_formulas(torus_small):
+    p, o = torus_small
+    x1 = o.array("x1")
+    assert x1[0] == pytest.approx(p["xmin"], rel=1e-14)
+    # grid.f90:37 scales by the single-precision 1./float(imax-1): r_out misses xmax at 1e-7
+    assert x1[-1] == pytest.approx(p["xmax"], rel=1e-6) and x1[-1] != p["xmax"]
+    x1b = o.array("x1b")
+    assert np.allclose(np.diff(x1b), np.diff(x1b)[0], rtol=1e-6)  # uniform in log r (MKS)
+    x3b = o.array("x3b")
+    assert x3b[0] == pytest.approx(0.02, rel=1e-14)
+    assert x3b[-1] == pytest.approx(np.pi - 0.02, rel=1e-12)
+
+
+def test_torus_ic_physical(torus_small):
+    p, o = torus_small
+    u = o.prims()
+    assert np.isfinite(u).all()
+    assert u[..., 0].max() == pytest.approx(1.0, rel=0.05)
+    assert (u[..., 0] > 0).all() and (u[..., 4] > 0).all()
+    assert np.abs(u[..., 6:]).max() > 0
+
+
+def test_recov_round_trip_is_exact(torus_small):
+    _, o = torus_small
+    u = o.prims()
+    uu = o.caluu1(u)
+    _, u2 = o.recov(uu, u)
+    n = o.nm1
+    err = field_err(u2, u, (slice(n, -n), slice(n, -n), slice(n, -n)))
+    assert err[[0, 1, 2, 4, 6, 7, 8]].max() < 1e-12, err
+    assert o.stats()["recov_nr2"] == 0
+
+
+def corner_divb(u, o):
+    """Toth's corner-centred div(sqrt(-g) B) in the (r, theta) plane (2D, j-invariant)."""
+    detg = o.array("detg").reshape(o.params["kmax"], o.params["imax"])
+    dx1 = o.array("dx1b")[1]
+    dx3 = o.array("dx3b")[1]
+    j = o.params["jmax"] // 2
+    b1 = detg * u[:, j, :, 6]
+    b3 = detg * u[:, j, :, 8]
+    d1 = (b1[1:, 1:] + b1[:-1, 1:] - b1[1:, :-1] - b1[:-1, :-1]) / (2 * dx1)
+    d3 = (b3[1:, 1:] + b3[1:, :-1] - b3[:-1, 1:] - b3[:-1, :-1]) / (2 * dx3)
+    return d1 + d3
+
+
+def _divb_drift(guard):
+    p = config.torus(nr=40, nth=40)
+    o = Oracle(dict(p, guard=guard))
+    o.ic_torus(seed=3, amp=0.0)  # phi-uniform data: the 2D corner divergence is the full one
+    o.init_cons()
+    n = o.nm1
+    d0 = corner_divb(o.prims(), o)[n:-n, n:-n]
+    o.step(3)
+    d1 = corner_divb(o.prims(), o)[n:-n, n:-n]
+    bscale = np.abs(o.prims()[..., 6:]).max() / o.array("dx1b")[1]
+    return np.abs(d1 - d0).max() / bscale
+
+
+def test_fluxct_preserves_divb_with_zero_normal_flux():
+    """Toth's flux-CT (ct.f90:30-118) keeps the corner divergence at round-off
+    once the normal-component flux is zero (guard bit 2)."""
+    assert _divb_drift(guard=3) < 1e-11
+
+
+def test_reference_llf_normal_flux_breaks_divb():
+    """Reference semantics: hll.f90 leaves the LLF diffusion of B^d in ww(d,6+d),
+    which ct does not replace, so the divergence drifts at O(1e-1)."""
+    assert _divb_drift(guard=1) > 1e-3
+
+
+def test_guard_is_noop_for_ppm():
+    p = config.torus(nr=32, nth=32, irec=config.IREC_PPM)
+    outs = []
+    for g in (0, 1):
+        q = dict(p, guard=g)
+        o = Oracle(q)
+        o.ic_torus(seed=11)
+        o.init_cons()
+        o.step(2)
+        outs.append(o.prims())
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_mp5_faithful_reference_goes_nonfinite_guarded_does_not():
+    """Reference semantics: MP5's absolute switch leaves floor-level density
+    unlimited, face rho < 0, and de**gam turns the entropy flux NaN."""
+    p = config.torus(nr=40, nth=40)
+    o = Oracle(dict(p, guard=0))
+    o.ic_torus(seed=5)
+    ww = o.fluxes(o.prims())
+    assert not np.isfinite(ww[..., 5, :]).all()
+    og = Oracle(dict(p, guard=1))
+    og.ic_torus(seed=5)
+    og.init_cons()
+    og.step(5)
+    assert np.isfinite(og.prims()).all()
+
+
+def test_thread_count_independence(monkeypatch):
+    """OpenMP over k does not change a single bit (recov's loop-order carry included)."""
+    import subprocess
+    import sys
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import numpy as np\n"
+        "from oracle import Oracle\n"
+        "from raishinsource_b200 import config\n"
+        "p = config.torus(nr=32, nth=32); p['guard'] = 1\n"
+        "o = Oracle(p); o.ic_torus(seed=9); o.init_cons(); o.step(2)\n"
+        "sys.stdout.buffer.write(o.prims().tobytes())\n"
+    )
+    from conftest import ROOT
+    outs = []
+    for nt in ("1", "4"):
+        env = dict(__import__("os").environ, OMP_NUM_THREADS=nt)
+        r = subprocess.run([sys.executable, "-c", code % ROOT], capture_output=True, env=env, check=True)
+        outs.append(r.stdout)
+    assert outs[0] == outs[1]
