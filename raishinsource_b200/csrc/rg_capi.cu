@@ -83,8 +83,8 @@ void free_run(Run* R) {
 
 int check_params(const rg_run_params* p) {
   if (!p) return fail(RG_EINVAL_CONFIG, "null parameters");
-  if (p->irec != 6 && p->irec != 7)
-    return fail(RG_EINVAL_CONFIG, "irec must be 6 (MP5) or 7 (WENO5) in this build");
+  if (p->irec != 5 && p->irec != 6 && p->irec != 7)
+    return fail(RG_EINVAL_CONFIG, "irec must be 5 (PPM), 6 (MP5) or 7 (WENO5)");
   if (p->metric != 1 && p->metric != 303 && p->metric != 403)
     return fail(RG_EINVAL_CONFIG, "metric must be 1, 303 or 403");
   if (p->ix1 != 1 && p->ix1 != 2) return fail(RG_EINVAL_CONFIG, "ix1 must be 1 or 2");

@@ -251,4 +251,124 @@ __device__ __forceinline__ double weno5_state(double a2, double a1, double u0, d
   return o0 * q0 + o1 * q1 + o2 * q2;
 }
 
+
+// ------------------------------------------------------------------- PPM
+// rPPM of Marti & Muller (1996) as restated by rec.f90:1261-2058.  The four
+// passes (interp, detect, flaten, monoto) touch only the two face states of
+// one cell each, so both states of cell c follow from the cells c-3..c+3:
+// L = state at c-1/2 (the reference's uriir(c-1)), R = state at c+1/2
+// (uriil(c)).  dx is rec2's shifted dx?b (dummy dx?b(m) = actual dx?b(m-1),
+// rec.f90:58), x the cell centres (contact detection).
+
+// interp Eq. (60)-(61) (rec.f90:1346-1418); the theta direction lacks the
+// factor 2 of r and phi (rec.f90:1414).
+__device__ __forceinline__ double ppm_dma(double um, double u0, double up, double dxm, double dx0, double dxp,
+                                          bool kdir) {
+  const double t1a = dx0 / (dxm + dx0 + dxp);
+  const double t1b = (2.0 * dxm + dx0) / (dxp + dx0);
+  const double t1c = (dx0 + 2.0 * dxp) / (dxm + dx0);
+  const double sp1 = up - u0, sm1 = u0 - um;
+  const double spm1 = sp1 * sm1;
+  const double da = t1a * (t1b * sp1 + t1c * sm1);
+  if (spm1 <= 0.0) return 0.0;
+  const double t1 = (da < 0.0) ? -1.0 : 1.0;
+  const double t1d = dmin2(fabs(sm1), fabs(sp1));
+  return kdir ? t1 * dmin2(fabs(da), t1d) : t1 * dmin2(fabs(da), 2.0 * t1d);
+}
+
+// interp Eq. (51) (rec.f90:1422-1468): interface value at c+1/2.
+__device__ __forceinline__ double ppm_face(double u0, double u1, double dma0, double dma1, double dxm, double dx0,
+                                           double dx1, double dx2) {
+  const double t2 = (dx0 / (dx0 + dx1)) * (u1 - u0);
+  const double t3a = 1.0 / (dxm + dx0 + dx1 + dx2);
+  const double t3b = (2.0 * dx1 * dx0) / (dx0 + dx1);
+  const double t3c = ((dxm + dx0) / (2.0 * dx0 + dx1)) - ((dx2 + dx1) / (2.0 * dx1 + dx0));
+  const double t3 = t3a * t3b * t3c * (u1 - u0);
+  const double t4 = t3a * dx0 * ((dxm + dx0) / (2.0 * dx0 + dx1));
+  const double t5 = t3a * dx1 * ((dx1 + dx2) / (dx0 + 2.0 * dx1));
+  return u0 + t2 + t3 - t4 * dma1 + t5 * dma0;
+}
+
+// Both face states of the cell at p (primitive v at p[v*N]), stride st along
+// the direction D; dx[o], x[o] are the shifted spacing and centre at offset o
+// from the cell (o in -4..4).  gam enters the contact test (rec.f90:1623).
+template <int D>
+__device__ void ppm_cell(const double* __restrict__ p, size_t N, long long st, const double dx[9], const double x[9],
+                         double gam, double L[9], double R[9]) {
+  auto U = [&](int v, int o) { return p[(size_t)v * N + o * st]; };
+  auto DX = [&](int o) { return dx[o + 4]; };
+  // detect (rec.f90:1479-1686): contact steepening factor eta on density
+  double eta;
+  {
+    const double eta1 = 5.0, eta2 = 0.05, eps1 = 0.1, ak0 = 1.0;
+    auto dda = [&](int o) {
+      const double t0a = 1.0 / (DX(o - 1) + DX(o) + DX(o + 1));
+      const double t0b = (U(0, o + 1) - U(0, o)) / (DX(o + 1) + DX(o));
+      const double t0c = (U(0, o) - U(0, o - 1)) / (DX(o) + DX(o - 1));
+      return t0a * (t0b - t0c);
+    };
+    const double ddp = dda(1), ddm = dda(-1);
+    const double rp = U(0, 1), rm = U(0, -1);
+    const double t1 = ddp * ddm;
+    const double t2 = fabs(rp - rm) - eps1 * dmin2(fabs(rp), fabs(rm));
+    double etatil;
+    if (t1 >= 0.0 && t2 <= 0.0) {
+      etatil = 0.0;
+    } else {
+      const double t2a = -(ddp - ddm) / (x[5] - x[3]);
+      const double a = x[4] - x[3], b = x[5] - x[4];
+      const double t2b = (a * a * a + b * b * b) / (rp - rm);
+      etatil = t2a * t2b;
+    }
+    eta = dmax2(0.0, dmin2(eta1 * (etatil - eta2), 1.0));
+    const double pp = U(4, 1), pm = U(4, -1);
+    const double t3 = fabs(rp - rm) / dmin2(rp, rm);
+    const double t4 = fabs(pp - pm) / dmin2(pp, pm);
+    if (gam * ak0 * t3 < t4) eta = 0.0;
+  }
+  // flaten (rec.f90:1689-1884): shock flattening f2a from p and u^D
+  double f2a;
+  {
+    const double eps2 = 1.0, omg2 = 0.52, omg3 = 10.0;
+    auto f1a = [&](int o) {
+      const double pp1 = U(4, o + 1), pm1 = U(4, o - 1);
+      const double t3a = fabs(pp1 - pm1);
+      const double t1 = eps2 * dmin2(pp1, pm1) - t3a;
+      const double t2 = U(D, o + 1) - U(D, o - 1);
+      const double omg1 = (t1 < 0.0 && t2 < 0.0) ? 1.0 : 0.0;
+      const double t3b = U(4, o + 2) - U(4, o - 2);
+      double t4;
+      if (t3b == 0.0) t4 = (t3a == 0.0) ? -omg2 : 1.0 - omg2;
+      else t4 = (t3a / t3b) - omg2;
+      return dmin2(1.0, omg1 * dmax2(0.0, t4 * omg3));
+    };
+    const double f1b = (U(4, 1) - U(4, -1) < 0.0) ? f1a(1) : f1a(-1);
+    f2a = dmax2(f1a(0), f1b);
+  }
+#pragma unroll 1
+  for (int v = 0; v < 9; ++v) {
+    if (v == 5) { L[v] = 0.0; R[v] = 0.0; continue; }  // var 6 faces are never read downstream
+    const double um2 = U(v, -2), um1 = U(v, -1), u0 = U(v, 0), up1 = U(v, 1), up2 = U(v, 2);
+    const double dm = ppm_dma(um2, um1, u0, DX(-2), DX(-1), DX(0), D == 3);
+    const double d0 = ppm_dma(um1, u0, up1, DX(-1), DX(0), DX(1), D == 3);
+    const double dp = ppm_dma(u0, up1, up2, DX(0), DX(1), DX(2), D == 3);
+    double l = ppm_face(um1, u0, dm, d0, DX(-2), DX(-1), DX(0), DX(1));
+    double r = ppm_face(u0, up1, d0, dp, DX(-1), DX(0), DX(1), DX(2));
+    if (v == 0) {
+      r = r * (1.0 - eta) + (up1 - 0.5 * dp) * eta;
+      l = l * (1.0 - eta) + (um1 + 0.5 * dm) * eta;
+    }
+    r = u0 * f2a + r * (1.0 - f2a);
+    l = u0 * f2a + l * (1.0 - f2a);
+    // monoto (rec.f90:1887-2056)
+    if ((r - u0) * (l - u0) >= 0.0) { r = u0; l = u0; }
+    const double t3 = 6.0 * (r - l) * (u0 - 0.5 * (r + l));
+    const double t4 = (r - l) * (r - l);
+    if (t3 > t4) l = 3.0 * u0 - 2.0 * r;
+    if (-t3 > t4) r = 3.0 * u0 - 2.0 * l;
+    L[v] = l;
+    R[v] = r;
+  }
+}
+
 }  // namespace rg

@@ -448,6 +448,22 @@ __global__ void __launch_bounds__(128) k_flux(DevRun r, const double* __restrict
   const size_t N = r.N, c = r.cell(i, j, k);
   const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.imax : (long long)r.imax * r.jmax);
   double qL[9], qR[9];
+  if (IREC == 5) {
+    const int f = (D == 1) ? i : (D == 2 ? j : k);
+    const double* dxs = (D == 1) ? r.dx1s : (D == 2 ? r.dx2s : r.dx3s);
+    const double* xs = (D == 1) ? r.x1 : (D == 2 ? r.x2 : r.x3);
+    double dx[9], xx[9], tmp[9];
+#pragma unroll
+    for (int o = -2; o <= 2; ++o) dx[o + 4] = __ldg(dxs + f - 1 + o);
+#pragma unroll
+    for (int o = -1; o <= 1; ++o) xx[o + 4] = __ldg(xs + f - 1 + o);
+    ppm_cell<D>(P + c, N, st, dx, xx, r.gam, tmp, qL);  // uriil(f): R state of cell f
+#pragma unroll
+    for (int o = -2; o <= 2; ++o) dx[o + 4] = __ldg(dxs + f + o);
+#pragma unroll
+    for (int o = -1; o <= 1; ++o) xx[o + 4] = __ldg(xs + f + o);
+    ppm_cell<D>(P + c + st, N, st, dx, xx, r.gam, qR, tmp);  // uriir(f): L state of cell f+1
+  } else
 #pragma unroll
   for (int v = 0; v < 9; ++v) {
     if (v == 5) { qL[v] = 0.0; qR[v] = 0.0; continue; }  // var 6 faces are never read downstream
@@ -890,7 +906,11 @@ cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cu
   const int n = r.imax - 2 * r.nm0 + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b(64, 2, 1);
   const dim3 g = grid3(n, m, l, b);
-  if (r.irec == 6) {
+  if (r.irec == 5) {
+    if (dir == 1) k_flux<1, 5><<<g, b, 0, s>>>(r, P, F);
+    else if (dir == 2) k_flux<2, 5><<<g, b, 0, s>>>(r, P, F);
+    else k_flux<3, 5><<<g, b, 0, s>>>(r, P, F);
+  } else if (r.irec == 6) {
     if (dir == 1) k_flux<1, 6><<<g, b, 0, s>>>(r, P, F);
     else if (dir == 2) k_flux<2, 6><<<g, b, 0, s>>>(r, P, F);
     else k_flux<3, 6><<<g, b, 0, s>>>(r, P, F);

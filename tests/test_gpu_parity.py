@@ -62,7 +62,7 @@ def test_caluu1(torus2d):
     assert err.max() < TOL, err
 
 
-@pytest.mark.parametrize("irec", [config.IREC_MP5, config.IREC_WENO5])
+@pytest.mark.parametrize("irec", [config.IREC_MP5, config.IREC_WENO5, config.IREC_PPM])
 def test_calflx_guarded(gpu_ctx, irec):
     p = config.torus(nr=48, nth=40, nph=12, irec=irec)
     p["guard"] = 1
@@ -70,7 +70,7 @@ def test_calflx_guarded(gpu_ctx, irec):
     u = o.prims()
     wg, wo = r.calflx(u), o.fluxes(u)
     r.release()
-    n = o.nm1 - 1  # hll range nm0 .. n-nm0 (1-based) == slice(nm0-1, -nm0)
+    n = o.nm1 - 1  # inside the hll range nm0 .. n-nm0 (1-based)
     reg = (slice(n, -n), slice(n, -n), slice(n, -n))
     for d in range(3):
         err = field_err(wg[..., d], wo[..., d], reg)
@@ -176,3 +176,10 @@ def test_multistep_drift(gpu_ctx):
     n = o.nm1
     l1 = np.abs(got - o.prims())[n:-n, n:-n, n:-n].sum(axis=(0, 1, 2)) / np.abs(o.prims()[n:-n, n:-n, n:-n]).sum(axis=(0, 1, 2)).clip(1e-300)
     assert l1[[0, 4, 6, 8]].max() < 1e-10, l1
+
+
+def test_step_3d_ppm_reference_semantics(gpu_ctx):
+    """PPM needs no guard: reference semantics (guard = 0) stay finite."""
+    p = config.torus(nr=40, nth=24, nph=16, irec=config.IREC_PPM)
+    errs, st = _step_err(gpu_ctx, p, 2, seed=79)
+    assert errs.max() < TOL, errs
