@@ -132,6 +132,24 @@ int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl);
 /* bnd4 + infchk + atmosphere1a + pminmax2b (bnd.f90, correction.f90) on uri in/out */
 int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio);
 
+/* Allocation-free variant of rg_calflx, for callers that cannot call
+ * cudaMalloc when they need the fluxes (code running inside a CUDA stream
+ * capture, or a host program whose device memory comes only from its own pool).
+ * No counterpart in the reference.  The caller passes device buffers:
+ * d_prims, the primitives in structure-of-arrays order (variable v of cell c
+ * at v*N + c, c = (i-1) + imax*((j-1) + jmax*(k-1))), and d_ww, 27*N doubles
+ * receiving ww(d,v) of cell c at ((d-1)*9 + v)*N + c on the hll range, with
+ * flux-CT applied on its range.  The flux-CT intermediate lives in a
+ * file-scope device array that holds grids of at most 262144 cells (larger
+ * grids return RG_EINVAL_CONFIG); every GPU that loads the library keeps that
+ * array (about 12.6 MB) until exit.  The run's geometry, allocated by
+ * rg_run_admit beforehand, is read; nothing is allocated or freed.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and should therefore come before any stream capture.  All calls share the
+ * array: calls whose work overlaps on the GPU (other contexts or streams) race.
+ * The call returns after its work has completed on the context stream. */
+int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, double* d_ww);
+
 #ifdef __cplusplus
 }
 #endif

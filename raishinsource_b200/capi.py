@@ -27,7 +27,7 @@ STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA"
 #: every entry point include/raishin_gpu.h declares
 EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_upload_prims", "rg_run_download_prims", "rg_step",
-           "rg_run_stats", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor")
+           "rg_run_stats", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -94,6 +94,7 @@ def load(path: str = LIB_PATH):
     lib.rg_recov.argtypes = [P, I, D, D]
     lib.rg_cdtcfl.argtypes = [P, I, D, D]
     lib.rg_bnd_floor.argtypes = [P, I, D, D]
+    lib.rg_calflx_static.argtypes = [P, I, P, P]
     _lib = lib
     return lib
 
@@ -252,6 +253,11 @@ class Run:
         out = C.c_double(0.0)
         _check(self.lib, self.lib.rg_cdtcfl(self.ctx.h, self.id, _dptr(uri), C.byref(out)))
         return out.value
+
+    def calflx_static(self, d_prims: int, d_ww: int):
+        """Allocation-free flux call on caller-owned device buffers (raw device
+        pointers): d_prims 9*N SoA primitives in, d_ww 27*N fluxes out."""
+        _check(self.lib, self.lib.rg_calflx_static(self.ctx.h, self.id, C.c_void_p(d_prims), C.c_void_p(d_ww)))
 
     def bnd_floor(self, uri, urio) -> np.ndarray:
         out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)

@@ -588,3 +588,85 @@ int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ allocation-free fluxes
+// rg_calflx_static serves callers that cannot call cudaMalloc when they need
+// the fluxes: a driver running inside a CUDA stream capture, or a host code
+// whose device memory comes only from its own pool or arena.  The caller owns
+// the input and output device buffers; the flux-CT intermediate (the six
+// averaged induction fluxes) and the kernels' scalar block live in the
+// file-scope device arrays below, sized for grids of at most
+// kStaticMaxCells cells.  Every GPU that loads this library holds these
+// arrays (about 12.6 MB) until the process exits.
+namespace {
+
+constexpr size_t kStaticMaxCells = (size_t)1 << 18;
+__device__ __align__(256) double g_static_ct[6 * kStaticMaxCells];
+__device__ __align__(256) Scal g_static_scal;
+
+constexpr int kMaxDevices = 64;
+double* g_static_ct_addr[kMaxDevices] = {};
+Scal* g_static_scal_addr[kMaxDevices] = {};
+
+// Copy the flux-CT values from the static array into the caller's fluxes over
+// the CT range nm1..n-nm1 (ct.f90:60-109); elsewhere the raw LLF fluxes stay.
+__global__ void k_ct_scatter(DevRun r, const double* __restrict__ ct, double* __restrict__ ww) {
+  const int nm1 = r.nm1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + nm1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + nm1;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + nm1;
+  if (i > r.imax - nm1 || j > r.jmax - nm1 || k > r.kmax - nm1) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  // (direction, variable) of the six replaced fluxes: ww(2,7) ww(3,7) ww(1,8) ww(3,8) ww(1,9) ww(2,9)
+  const int dir[6] = {1, 2, 0, 2, 0, 1}, var[6] = {6, 6, 7, 7, 8, 8};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) ww[((size_t)dir[q] * 9 + var[q]) * N + c] = ct[(size_t)q * N + c];
+}
+
+// Reset the static scalar block: zero, then mark the kernels' work as active.
+__global__ void k_static_scal_reset(Scal* s) {
+  Scal z{};
+  z.active = 1;
+  *s = z;
+}
+
+}  // namespace
+
+extern "C" int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, double* d_ww) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!d_prims || !d_ww) return fail(RG_EINVAL_CONFIG, "null device buffer");
+  const size_t N = R->d.N;
+  if (N > kStaticMaxCells)
+    return fail(RG_EINVAL_CONFIG, "rg_calflx_static: grid of " + std::to_string(N) +
+                                      " cells exceeds the static scratch maximum of " +
+                                      std::to_string(kStaticMaxCells) + " cells");
+  if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(RG_EINVAL_CONFIG, "device index out of range");
+  RG_CUDA(cudaSetDevice(ctx->device));
+  // Set-up once per device, with that device current: the host-side names of
+  // the arrays are not device addresses, so their addresses are looked up here.
+  if (!g_static_ct_addr[ctx->device]) {
+    void* a = nullptr;
+    void* b = nullptr;
+    RG_CUDA(cudaGetSymbolAddress(&a, g_static_ct));
+    RG_CUDA(cudaGetSymbolAddress(&b, g_static_scal));
+    g_static_ct_addr[ctx->device] = static_cast<double*>(a);
+    g_static_scal_addr[ctx->device] = static_cast<Scal*>(b);
+  }
+  double* ct = g_static_ct_addr[ctx->device];
+  DevRun d = R->d;
+  d.scal = g_static_scal_addr[ctx->device];  // the run's own time state is not touched
+  cudaStream_t s = ctx->stream;
+  // The arrays keep the previous call's contents: clear them first.
+  RG_CUDA(cudaMemsetAsync(ct, 0, 6 * N * sizeof(double), s));
+  k_static_scal_reset<<<1, 1, 0, s>>>(d.scal);
+  RG_CUDA(cudaGetLastError());
+  for (int dir = 1; dir <= 3; ++dir) RG_CUDA(launch_flux(d, dir, d_prims, d_ww + (size_t)(dir - 1) * 9 * N, s));
+  RG_CUDA(launch_ct(d, d_ww, d_ww + 9 * N, d_ww + 18 * N, ct, s));
+  const dim3 b(64, 4, 1);
+  const int n = d.imax - 2 * d.nm1 + 1, m = d.jmax - 2 * d.nm1 + 1, l = d.kmax - 2 * d.nm1 + 1;
+  k_ct_scatter<<<dim3((n + 63) / 64, (m + 3) / 4, l), b, 0, s>>>(d, ct, d_ww);
+  RG_CUDA(cudaGetLastError());
+  RG_CUDA(cudaStreamSynchronize(s));
+  return RG_OK;
+}
