@@ -208,21 +208,30 @@ def run_gpu(args) -> dict | None:
                "ms_per_step": e_ms / args.e2e_steps, "api": "rg_run_upload_prims + rg_step + rg_run_download_prims"}
 
     # per-kernel device times (separate pass: CUDA events around every launch on the library stream)
-    ctx.profile(True)
-    run.step(args.prof_steps)
-    prof = ctx.profile_read()
-    ctx.profile(False)
-    total = sum(v["ms"] for v in prof.values())
-    top = max((k for k in prof if k in BYTES_PER_UNIT), key=lambda k: prof[k]["ms"])
-    n_launch = prof[top]["launches"] / (2 if top == "update" else 1)
-    nm0, nm1 = run.nm0, run.nm1
-    faces = (p["imax"] - 2 * nm0 + 1) * (p["jmax"] - 2 * nm0 + 1) * (p["kmax"] - 2 * nm0 + 1)
-    units = {"update": zones, "flux_ct": (p["imax"] - 2 * nm1 + 1) * (p["jmax"] - 2 * nm1 + 1) * (p["kmax"] - 2 * nm1 + 1),
-             "floors": p["imax"] * p["jmax"] * p["kmax"], "cfl": (p["imax"] - 2) * (p["jmax"] - 2) * (p["kmax"] - 2)}
-    u = units.get(top, faces)
-    per_launch_ms = prof[top]["ms"] / max(n_launch, 1)
-    peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_UNIT[top] * u / (per_launch_ms * 1e-3) / 1e9
+    roofline, shares = None, {}
+    if args.prof_steps > 0:
+        ctx.profile(True)
+        run.step(args.prof_steps)
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        total = sum(v["ms"] for v in prof.values())
+        shares = {k: round(v["ms"] / total, 4) for k, v in prof.items()}
+        top = max((k for k in prof if k in BYTES_PER_UNIT), key=lambda k: prof[k]["ms"])
+        n_launch = prof[top]["launches"] / (2 if top == "update" else 1)
+        nm0, nm1 = run.nm0, run.nm1
+        faces = (p["imax"] - 2 * nm0 + 1) * (p["jmax"] - 2 * nm0 + 1) * (p["kmax"] - 2 * nm0 + 1)
+        units = {"update": zones,
+                 "flux_ct": (p["imax"] - 2 * nm1 + 1) * (p["jmax"] - 2 * nm1 + 1) * (p["kmax"] - 2 * nm1 + 1),
+                 "floors": p["imax"] * p["jmax"] * p["kmax"],
+                 "cfl": (p["imax"] - 2) * (p["jmax"] - 2) * (p["kmax"] - 2)}
+        u = units.get(top, faces)
+        per_launch_ms = prof[top]["ms"] / max(n_launch, 1)
+        peak, peak_kind = measured_peaks()
+        achieved = BYTES_PER_UNIT[top] * u / (per_launch_ms * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+                    "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                    "bytes_per_unit": BYTES_PER_UNIT[top], "units_per_launch": u, "ms_per_launch": per_launch_ms,
+                    "note": "FP64-pipe bound path: HBM fraction of algorithmic bytes, see profiles/"}
     run.release()
     ctx.close()
     if ws > 1:
@@ -237,11 +246,8 @@ def run_gpu(args) -> dict | None:
         "data": "synthetic (seeded Fishbone-Moncrief torus initial data)",
         "config": dict(config_block(args, p), parallelism=f"replicas x{ws}"),
         "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-        "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                     "bytes_per_unit": BYTES_PER_UNIT[top], "units_per_launch": u, "ms_per_launch": per_launch_ms,
-                     "note": "FP64-pipe bound path: HBM fraction of algorithmic bytes, see profiles/"},
-        "kernel_share": {k: round(v["ms"] / total, 4) for k, v in prof.items() if total > 0},
+        "roofline": roofline,
+        "kernel_share": shares,
         "recov": {k: st[k] for k in ("recov_nr2", "recov_fail", "recov_carry", "recov_cap")},
     }
     return line
