@@ -65,11 +65,15 @@ _lib = None
 
 
 def load(path: str = LIB_PATH):
-    """Load the CUDA library (building it first if the .so is absent or stale)."""
+    """Load the CUDA library (building it first if the .so is absent or stale).
+
+    RAISHIN_GPU_LIB names an already built variant of the library to load
+    instead (e.g. the uncontracted RG_FMAD=0 build)."""
     global _lib
     if _lib is not None:
         return _lib
     from . import build as _build
+    path = os.environ.get("RAISHIN_GPU_LIB", path)
     path = _build.build() if path == LIB_PATH else path
     lib = C.CDLL(path)
     P, D, I = C.c_void_p, C.POINTER(C.c_double), C.c_int

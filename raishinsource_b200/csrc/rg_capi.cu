@@ -111,7 +111,7 @@ size_t footprint_bytes(const rg_run_params* p) {
   const size_t N = (size_t)p->imax * p->jmax * p->kmax;
   const size_t nik = (size_t)p->imax * p->kmax;
   const size_t state = (3 * 9 + 3 * 9 + 6 + 2 * 9 + 9) * N * sizeof(double);
-  const size_t geom = (3 * 33 + 64) * nik * sizeof(double) + 16 * (size_t)(p->imax + p->jmax + p->kmax) * sizeof(double);
+  const size_t geom = (3 * kMetComps + 64) * nik * sizeof(double) + 16 * (size_t)(p->imax + p->jmax + p->kmax) * sizeof(double);
   return state + geom + sizeof(Scal) + C_NCOUNTERS * 8 + kCarryCap * sizeof(int);
 }
 
@@ -332,6 +332,10 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
   Run* R = new Run();
   R->p = *p;
   build_geometry(*p, R->geom);
+  if (!R->geom.compact_ok) {
+    delete R;
+    return fail(RG_EINVAL_CONFIG, "metric couples theta to (t,r,phi): not representable by the compact cache");
+  }
   DevRun& d = R->d;
   d.imax = p->imax; d.jmax = p->jmax; d.kmax = p->kmax;
   d.nm0 = (p->irec == 5) ? 4 : 3;

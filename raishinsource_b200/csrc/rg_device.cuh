@@ -10,24 +10,59 @@
 
 namespace rg {
 
-// Metric at one point: covariant and contravariant 4-metric and sqrt(-g).
+// Metric at one point.  Every metric of this build (Minkowski 1, Kerr-Schild
+// 303, modified Kerr-Schild 403, coord.f90:149-792) couples only (t, r, phi)
+// and keeps theta diagonal, so g^{mu 3} and g_{mu 3} vanish for mu != 3 (the
+// host checks this at admission).  gcov is symmetric; gcon, an LU inverse
+// (coord.f90:1504), is not symmetric to the last bit and keeps its full 3x3
+// block.  Sums below run over the nonzero terms in the reference's order.
 struct Met {
-  double g[4][4];
-  double gc[4][4];
-  double detg;
+  double g00, g01, g02, g11, g12, g22, g33;                 // gcov
+  double c00, c01, c02, c10, c11, c12, c20, c21, c22, c33;  // gcon
+  double detg;                                              // sqrt(-g)
 };
+constexpr int kMetComps = 18;
 
-// Metric cache layout (per (i,k) point, 33 components, structure of arrays):
-// component c in [0,16) gcov(c/4, c%4), [16,32) gcon, 32 detg.
+// Metric cache layout: per (i,k) point q, component c at c*nik + q, in the
+// order of the Met fields.
 __device__ __forceinline__ void load_met(const double* __restrict__ base, size_t nik, size_t q, Met& m) {
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      m.g[a][b] = __ldg(base + (size_t)(4 * a + b) * nik + q);
-      m.gc[a][b] = __ldg(base + (size_t)(16 + 4 * a + b) * nik + q);
-    }
-  m.detg = __ldg(base + (size_t)32 * nik + q);
+  const double* b = base + q;
+  m.g00 = __ldg(b + 0 * nik); m.g01 = __ldg(b + 1 * nik); m.g02 = __ldg(b + 2 * nik);
+  m.g11 = __ldg(b + 3 * nik); m.g12 = __ldg(b + 4 * nik); m.g22 = __ldg(b + 5 * nik);
+  m.g33 = __ldg(b + 6 * nik);
+  m.c00 = __ldg(b + 7 * nik); m.c01 = __ldg(b + 8 * nik); m.c02 = __ldg(b + 9 * nik);
+  m.c10 = __ldg(b + 10 * nik); m.c11 = __ldg(b + 11 * nik); m.c12 = __ldg(b + 12 * nik);
+  m.c20 = __ldg(b + 13 * nik); m.c21 = __ldg(b + 14 * nik); m.c22 = __ldg(b + 15 * nik);
+  m.c33 = __ldg(b + 16 * nik);
+  m.detg = __ldg(b + 17 * nik);
+}
+
+// sum_{a,b=1..3} g_ab x_a x_b over the nonzero terms in (a,b) order
+// (physfunc.f90:16-20, calcha.f90:251-256, correction.f90:806-811).
+__device__ __forceinline__ double qform3(const Met& m, double x1, double x2, double x3) {
+  double s = 0.0;
+  s = s + m.g11 * x1 * x1;
+  s = s + m.g12 * x1 * x2;
+  s = s + m.g12 * x2 * x1;  // g_21 = g_12
+  s = s + m.g22 * x2 * x2;
+  s = s + m.g33 * x3 * x3;
+  return s;
+}
+
+// g_ab v^b (physfunc.f90:161-195)
+__device__ __forceinline__ void lower_g(const double v[4], double o[4], const Met& m) {
+  o[0] = m.g00 * v[0] + m.g01 * v[1] + m.g02 * v[2];
+  o[1] = m.g01 * v[0] + m.g11 * v[1] + m.g12 * v[2];
+  o[2] = m.g02 * v[0] + m.g12 * v[1] + m.g22 * v[2];
+  o[3] = m.g33 * v[3];
+}
+
+// g^ab v_b (physfunc.f90:198-232)
+__device__ __forceinline__ void upper_gc(const double v[4], double o[4], const Met& m) {
+  o[0] = m.c00 * v[0] + m.c01 * v[1] + m.c02 * v[2];
+  o[1] = m.c10 * v[0] + m.c11 * v[1] + m.c12 * v[2];
+  o[2] = m.c20 * v[0] + m.c21 * v[1] + m.c22 * v[2];
+  o[3] = m.c33 * v[3];
 }
 
 __device__ __forceinline__ double sgn1(double x) { return copysign(1.0, x); }
@@ -48,12 +83,7 @@ __device__ __forceinline__ double dmax2(double a, double b) { return (b > a) ? b
 
 // physfunc.f90:2-42
 __device__ __forceinline__ double calgfl(const double u1, const double u2, const double u3, const Met& m) {
-  const double ut[4] = {0.0, u1, u2, u3};
-  double utsq = 0.0;
-#pragma unroll
-  for (int a = 1; a <= 3; ++a)
-#pragma unroll
-    for (int b = 1; b <= 3; ++b) utsq = utsq + m.g[a][b] * ut[a] * ut[b];
+  double utsq = qform3(m, u1, u2, u3);
   if (utsq < 0.0) {
     if (fabs(utsq) <= 1.0e-10) utsq = fabs(utsq);
     else utsq = 1.e-10;
@@ -64,20 +94,13 @@ __device__ __forceinline__ double calgfl(const double u1, const double u2, const
 
 // physfunc.f90:45-78
 __device__ __forceinline__ void calucon(double u1, double u2, double u3, double gfl, const Met& m, double ucon[4]) {
-  const double alpha1 = 1. / sqrt(-m.gc[0][0]);
-  const double b1 = alpha1 * alpha1 * m.gc[0][1];
-  const double b2 = alpha1 * alpha1 * m.gc[0][2];
-  const double b3 = alpha1 * alpha1 * m.gc[0][3];
+  const double alpha1 = 1. / sqrt(-m.c00);
+  const double b1 = alpha1 * alpha1 * m.c01;
+  const double b2 = alpha1 * alpha1 * m.c02;
   ucon[0] = gfl * (1. / alpha1);
   ucon[1] = u1 - gfl * b1 * (1. / alpha1);
   ucon[2] = u2 - gfl * b2 * (1. / alpha1);
-  ucon[3] = u3 - gfl * b3 * (1. / alpha1);
-}
-
-// physfunc.f90:161-195 / 198-232
-__device__ __forceinline__ void lower4(const double v[4], double o[4], const double g[4][4]) {
-#pragma unroll
-  for (int a = 0; a < 4; ++a) o[a] = g[a][0] * v[0] + g[a][1] * v[1] + g[a][2] * v[2] + g[a][3] * v[3];
+  ucon[3] = u3;  // beta^theta = 0
 }
 
 // Velocity and magnetic 4-vectors of one primitive state (the common head of
@@ -94,25 +117,40 @@ __device__ __forceinline__ void pstate(const double q[9], const Met& m, double g
   s.roh = s.de + (gam / (gam - 1.0)) * s.pr;
   s.gfl = calgfl(q[1], q[2], q[3], m);
   calucon(q[1], q[2], q[3], s.gfl, m, s.ucon);
-  lower4(s.ucon, s.ucov, m.g);
+  lower_g(s.ucon, s.ucov, m);
   // physfunc.f90:81-100
   s.bbcon[0] = s.b1 * s.ucov[1] + s.b2 * s.ucov[2] + s.b3 * s.ucov[3];
   s.bbcon[1] = (s.b1 + s.bbcon[0] * s.ucon[1]) * (1. / s.ucon[0]);
   s.bbcon[2] = (s.b2 + s.bbcon[0] * s.ucon[2]) * (1. / s.ucon[0]);
   s.bbcon[3] = (s.b3 + s.bbcon[0] * s.ucon[3]) * (1. / s.ucon[0]);
-  lower4(s.bbcon, s.bbcov, m.g);
+  lower_g(s.bbcon, s.bbcov, m);
   s.bbsq = s.bbcon[0] * s.bbcov[0] + s.bbcon[1] * s.bbcov[1] + s.bbcon[2] * s.bbcov[2] + s.bbcon[3] * s.bbcov[3];
 }
 
-// caluu.f90:92-118: sqrt(-g) (rho u^t, T^t_i, T^t_t + rho u^t, s u^t, B^i).
-// delta(0,n) is the literal identity of caldelta (physfunc.f90:122-158).
+// p / rho^Gamma of a state (caluu.f90:303, calflx.f90:474), computed once per state.
+__device__ __forceinline__ double ent_ratio(const PS& s, double gam) { return s.pr / pow(s.de, gam); }
+
 __device__ __forceinline__ void p2c(const PS& s, double gam, double detg, double u[9]) {
   const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
   u[0] = s.de * s.ucon[0];
 #pragma unroll
   for (int m = 1; m <= 3; ++m) u[m] = a * s.ucon[0] * s.ucov[m] + b * 0.0 - s.bbcon[0] * s.bbcov[m];
   u[4] = a * s.ucon[0] * s.ucov[0] + b * 1.0 - s.bbcon[0] * s.bbcov[0] + s.de * s.ucon[0];
-  u[5] = s.de * (s.pr / pow(s.de, gam)) * s.ucon[0];
+  u[5] = s.de * ent_ratio(s, gam) * s.ucon[0];
+  u[6] = s.b1; u[7] = s.b2; u[8] = s.b3;
+#pragma unroll
+  for (int n = 0; n < 9; ++n) u[n] = detg * u[n];
+}
+
+// caluu.f90:92-118: sqrt(-g) (rho u^t, T^t_i, T^t_t + rho u^t, s u^t, B^i).
+// delta(0,n) is the literal identity of caldelta (physfunc.f90:122-158).
+__device__ __forceinline__ void p2c(const PS& s, double gam, double detg, double u[9], double sr) {
+  const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
+  u[0] = s.de * s.ucon[0];
+#pragma unroll
+  for (int m = 1; m <= 3; ++m) u[m] = a * s.ucon[0] * s.ucov[m] + b * 0.0 - s.bbcon[0] * s.bbcov[m];
+  u[4] = a * s.ucon[0] * s.ucov[0] + b * 1.0 - s.bbcon[0] * s.bbcov[0] + s.de * s.ucon[0];
+  u[5] = s.de * sr * s.ucon[0];
   u[6] = s.b1; u[7] = s.b2; u[8] = s.b3;
 #pragma unroll
   for (int n = 0; n < 9; ++n) u[n] = detg * u[n];
@@ -121,7 +159,7 @@ __device__ __forceinline__ void p2c(const PS& s, double gam, double detg, double
 // calflx.f90:391-795, direction D (1 = r, 2 = phi, 3 = theta).  The induction
 // flux is (u^D/u^0) B^m - (u^m/u^0) B^D with the D component set to 0.
 template <int D>
-__device__ __forceinline__ void flux(const PS& s, double gam, double detg, double w[9]) {
+__device__ __forceinline__ void flux(const PS& s, double gam, double detg, double w[9], double sr) {
   const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
   const double ud = s.ucon[D];
   const double bc[4] = {0.0, s.b1, s.b2, s.b3};
@@ -129,7 +167,7 @@ __device__ __forceinline__ void flux(const PS& s, double gam, double detg, doubl
 #pragma unroll
   for (int m = 1; m <= 3; ++m) w[m] = a * ud * s.ucov[m] + b * (D == m ? 1.0 : 0.0) - s.bbcon[D] * s.bbcov[m];
   w[4] = a * ud * s.ucov[0] + b * 0.0 - s.bbcon[D] * s.bbcov[0] + s.de * ud;
-  w[5] = s.de * (s.pr / pow(s.de, gam)) * ud;
+  w[5] = s.de * sr * ud;
 #pragma unroll
   for (int m = 1; m <= 3; ++m) {
     if (m == D) w[5 + m] = 0.0;
@@ -145,17 +183,13 @@ __device__ __forceinline__ void flux(const PS& s, double gam, double detg, doubl
 template <int D>
 __device__ __forceinline__ void wavespeed(const double q[9], const PS& s, const Met& m, double gam, double& vfp,
                                           double& vfm) {
-  const double alpha1 = 1. / sqrt(-m.gc[0][0]);
-  const double beta[4] = {0.0, alpha1 * alpha1 * m.gc[0][1], alpha1 * alpha1 * m.gc[0][2],
-                          alpha1 * alpha1 * m.gc[0][3]};
-  const double oncon_d = beta[D] / alpha1;
-  const double gc3dd = m.gc[D][D] + (oncon_d * oncon_d);
+  const double alpha1 = 1. / sqrt(-m.c00);
+  const double betad = (D == 1) ? alpha1 * alpha1 * m.c01 : (D == 2 ? alpha1 * alpha1 * m.c02 : 0.0);
+  const double oncon_d = betad / alpha1;
+  const double gcdd = (D == 1) ? m.c11 : (D == 2 ? m.c22 : m.c33);
+  const double gc3dd = gcdd + (oncon_d * oncon_d);
   const double vcon[4] = {0.0, q[1] * (1. / s.gfl), q[2] * (1. / s.gfl), q[3] * (1. / s.gfl)};
-  double vsq = 0.0;
-#pragma unroll
-  for (int a = 1; a <= 3; ++a)
-#pragma unroll
-    for (int b = 1; b <= 3; ++b) vsq = vsq + (m.g[a][b] + (0.0 * 0.0)) * vcon[a] * vcon[b];
+  const double vsq = qform3(m, vcon[1], vcon[2], vcon[3]);
   const double cssq = gam * s.pr / s.roh;
   const double vasq = s.bbsq * (1. / (s.roh + s.bbsq));
   const double omsq = vasq + cssq * (1.0 - vasq);
@@ -164,8 +198,8 @@ __device__ __forceinline__ void wavespeed(const double q[9], const PS& s, const 
   const double f3 = omsq * (1.0 - vsq) * ((1.0 - vsq * omsq) * gc3dd - (1.0 - omsq) * vcon[D] * vcon[D]);
   vfp = (f1 + sqrt(f3)) * (1. / f2);
   vfm = (f1 - sqrt(f3)) * (1. / f2);
-  vfp = alpha1 * vfp - beta[D];
-  vfm = alpha1 * vfm - beta[D];
+  vfp = alpha1 * vfp - betad;
+  vfm = alpha1 * vfm - betad;
   if (fabs(vfp) > 1.0) vfp = 1.0;
   if (fabs(vfm) > 1.0) vfm = -1.0;
 }
@@ -182,49 +216,32 @@ __device__ __forceinline__ double dm4(double ww, double xx, double yy, double zz
   return 0.125 * (sgn1(ww) + sgn1(xx)) * fabs(sgn1(ww) + sgn1(yy)) * (sgn1(ww) + sgn1(zz)) * mn;
 }
 
-// rec.f90:2095-2130: MP5 state at the +1/2 face of cell 0 from u(-2..+2).
-__device__ __forceinline__ double mp5_left(double um2, double um1, double u0, double up1, double up2) {
+// rec.f90:2095-2178: MP5 face state of cell 0 from u(-2..+2) given in the
+// order (a2, a1, u0, b1, b2): the left state at +1/2 takes
+// (u-2, u-1, u0, u+1, u+2) and sg = +1; the right state at -1/2 takes the
+// mirrored stencil (u+2, u+1, u0, u-1, u-2) and sg = -1, because the
+// reference's right state flips the signs of the dm4 terms of md and lc
+// (rec.f90:2172-2176).  Negation is exact, so both equal the reference's
+// separate formulas bit for bit, and the two lanes of a face run one code path.
+__device__ __forceinline__ double mp5_state(double a2, double a1, double u0, double b1, double b2, double sg) {
   const double tmp1 = 1.0 / 60.0, tmp2 = 4.0 / 3.0, alpha = 4.0, eps1 = 1.0e-10;
-  const double ul1 = tmp1 * (2. * um2 - 13. * um1 + 47. * u0 + 27. * up1 - 3. * up2);
-  const double ulmp = u0 + dmm(up1 - u0, alpha * (u0 - um1));
+  const double ul1 = tmp1 * (2. * a2 - 13. * a1 + 47. * u0 + 27. * b1 - 3. * b2);
+  const double ulmp = u0 + dmm(b1 - u0, alpha * (u0 - a1));
   const double t = (ul1 - u0) * (ul1 - ulmp);
   if (t <= eps1) return ul1;
-  const double dim1 = um2 - 2. * um1 + u0;
-  const double di1 = um1 - 2. * u0 + up1;
-  const double dip1 = u0 - 2. * up1 + up2;
-  const double dm4iph = dm4(4. * di1 - dip1, 4. * dip1 - di1, di1, dip1);
-  const double dm4imh = dm4(4. * di1 - dim1, 4. * dim1 - di1, di1, dim1);
-  const double ul = u0 + alpha * (u0 - um1);
-  const double av = 0.5 * (u0 + up1);
-  const double md = av - 0.5 * dm4iph;
-  const double lc = u0 + 0.5 * (u0 - um1) + tmp2 * dm4imh;
-  const double m1 = fmin3(u0, up1, md), m2 = fmin3(u0, ul, lc);
-  const double m3 = fmax3(u0, up1, md), m4 = fmax3(u0, ul, lc);
+  const double dim1 = a2 - 2. * a1 + u0;
+  const double di1 = a1 - 2. * u0 + b1;
+  const double dip1 = u0 - 2. * b1 + b2;
+  const double dm4p = dm4(4. * di1 - dip1, 4. * dip1 - di1, di1, dip1);
+  const double dm4m = dm4(4. * di1 - dim1, 4. * dim1 - di1, di1, dim1);
+  const double ul = u0 + alpha * (u0 - a1);
+  const double av = 0.5 * (u0 + b1);
+  const double md = av - (sg * 0.5) * dm4p;
+  const double lc = u0 + 0.5 * (u0 - a1) + (sg * tmp2) * dm4m;
+  const double m1 = fmin3(u0, b1, md), m2 = fmin3(u0, ul, lc);
+  const double m3 = fmax3(u0, b1, md), m4 = fmax3(u0, ul, lc);
   const double umax = dmax2(m1, m2), umin = dmin2(m3, m4);
   return ul1 + dmm(umin - ul1, umax - ul1);
-}
-
-// rec.f90:2134-2178: MP5 state at the -1/2 face of cell 0 from u(-2..+2),
-// with the reference's sign convention for md/lc (rec.f90:2172-2176).
-__device__ __forceinline__ double mp5_right(double um2, double um1, double u0, double up1, double up2) {
-  const double tmp1 = 1.0 / 60.0, tmp2 = 4.0 / 3.0, alpha = 4.0, eps1 = 1.0e-10;
-  const double ur1 = tmp1 * (2. * up2 - 13. * up1 + 47. * u0 + 27. * um1 - 3. * um2);
-  const double urmp = u0 + dmm(um1 - u0, alpha * (u0 - up1));
-  const double t = (ur1 - u0) * (ur1 - urmp);
-  if (t <= eps1) return ur1;
-  const double dim1 = um2 - 2. * um1 + u0;
-  const double di1 = um1 - 2. * u0 + up1;
-  const double dip1 = u0 - 2. * up1 + up2;
-  const double dm4iph = dm4(4. * di1 - dip1, 4. * dip1 - di1, di1, dip1);
-  const double dm4imh = dm4(4. * di1 - dim1, 4. * dim1 - di1, di1, dim1);
-  const double ul = u0 + alpha * (u0 - up1);
-  const double av = 0.5 * (u0 + um1);
-  const double md = av + 0.5 * dm4imh;
-  const double lc = u0 + 0.5 * (u0 - up1) - tmp2 * dm4iph;
-  const double m1 = fmin3(u0, um1, md), m2 = fmin3(u0, ul, lc);
-  const double m3 = fmax3(u0, um1, md), m4 = fmax3(u0, ul, lc);
-  const double umax = dmax2(m1, m2), umin = dmin2(m3, m4);
-  return ur1 + dmm(umin - ur1, umax - ur1);
 }
 
 // rec.f90:2373-2643 (WENO5-JS); left state at +1/2 and right state at -1/2

@@ -182,13 +182,18 @@ void metric_at(const rg_run_params& p, double r, double th, double th_mks, Mat g
   }
 }
 
-void store_met(std::vector<double>& dst, size_t nik, size_t q, const Mat g, const Mat gc) {
-  for (int a = 0; a < 4; ++a)
-    for (int b = 0; b < 4; ++b) {
-      dst[(size_t)(4 * a + b) * nik + q] = g[a][b];
-      dst[(size_t)(16 + 4 * a + b) * nik + q] = gc[a][b];
-    }
-  dst[(size_t)32 * nik + q] = sqrt_minus_det(g);
+// Compact cache of one point: gcov (t,r,phi) block + g_thth, the full
+// (t,r,phi) block of gcon (not symmetric to the last bit) + g^thth, sqrt(-g).
+// Returns false if an entry coupling theta to (t,r,phi) is nonzero or gcov is
+// not symmetric, which the compact kernels do not represent.
+bool store_met(std::vector<double>& dst, size_t nik, size_t q, const Mat g, const Mat gc) {
+  const double v[kMetComps] = {g[0][0], g[0][1], g[0][2], g[1][1], g[1][2], g[2][2], g[3][3],
+                               gc[0][0], gc[0][1], gc[0][2], gc[1][0], gc[1][1], gc[1][2],
+                               gc[2][0], gc[2][1], gc[2][2], gc[3][3], sqrt_minus_det(g)};
+  for (int c = 0; c < kMetComps; ++c) dst[(size_t)c * nik + q] = v[c];
+  bool ok = g[1][0] == g[0][1] && g[2][0] == g[0][2] && g[2][1] == g[1][2];
+  for (int a = 0; a < 3; ++a) ok = ok && g[a][3] == 0.0 && g[3][a] == 0.0 && gc[a][3] == 0.0 && gc[3][a] == 0.0;
+  return ok;
 }
 
 }  // namespace
@@ -248,9 +253,10 @@ void build_geometry(const rg_run_params& p, HostGeom& G) {
   const int imax = p.imax, kmax = p.kmax;
   const size_t nik = (size_t)imax * kmax;
   G.nik = nik;
-  G.mc.assign(33 * nik, 0.0);
-  G.mi.assign(33 * nik, 0.0);
-  G.mk.assign(33 * nik, 0.0);
+  G.mc.assign(kMetComps * nik, 0.0);
+  G.mi.assign(kMetComps * nik, 0.0);
+  G.mk.assign(kMetComps * nik, 0.0);
+  G.compact_ok = true;
   G.chr.assign(64 * nik, 0.0);
   const Axis& X1 = G.ax[0];
   const Axis& X3 = G.ax[2];
@@ -259,11 +265,11 @@ void build_geometry(const rg_run_params& p, HostGeom& G) {
       const size_t q = (size_t)(i - 1) + (size_t)imax * (k - 1);
       Mat g, gc;
       metric_at(p, X1.x[i], X3.x[k], X3.xb[k], g, gc);
-      store_met(G.mc, nik, q, g, gc);
+      G.compact_ok &= store_met(G.mc, nik, q, g, gc);
       metric_at(p, X1.xa[i], X3.x[k], X3.xb[k], g, gc);
-      store_met(G.mi, nik, q, g, gc);
+      G.compact_ok &= store_met(G.mi, nik, q, g, gc);
       metric_at(p, X1.x[i], X3.xa[k], X3.xb[k], g, gc);  // hfac at the centre theta_MKS (coord.f90:96-98)
-      store_met(G.mk, nik, q, g, gc);
+      G.compact_ok &= store_met(G.mk, nik, q, g, gc);
       // Christoffel symbols by central differences, delta = 1e-5 (coord.f90:1134-1317)
       const double delta = 1.0e-5, small = 1.e-12;
       double r0 = X1.x[i], th0 = X3.x[k], thm = X3.xb[k];
@@ -567,7 +573,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
     for (int j = 1; j <= jmax; ++j)
       for (int i = 2; i <= imax - 1; ++i) {
         auto A = [&](int ii, int kk) { return apot[cidx(ii, j, kk)]; };
-        const double dg = G.mc[(size_t)32 * nik + (size_t)(i - 1) + (size_t)imax * (k - 1)];
+        const double dg = G.mc[(size_t)(kMetComps - 1) * nik + (size_t)(i - 1) + (size_t)imax * (k - 1)];
         const double c1 = 0.5 * (A(i + 1, k + 1) + A(i, k + 1) - A(i + 1, k) - A(i, k));
         const double h3 = mks ? 0.5 * (X3.xb[k + 1] + X3.xb[k]) - 0.5 * (X3.xb[k] + X3.xb[k - 1])
                               : 0.5 * (X3.x[k + 1] + X3.x[k]) - 0.5 * (X3.x[k] + X3.x[k - 1]);
@@ -594,11 +600,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
       for (int i = 1; i <= imax; ++i) {
         const size_t q = (size_t)(i - 1) + (size_t)imax * (k - 1);
         Mat g, gc;
-        for (int x = 0; x < 4; ++x)
-          for (int y = 0; y < 4; ++y) {
-            g[x][y] = G.mc[(size_t)(4 * x + y) * nik + q];
-            gc[x][y] = G.mc[(size_t)(16 + 4 * x + y) * nik + q];
-          }
+        metric_at(p, X1.x[i], X3.x[k], X3.xb[k], g, gc);
         const double u1 = at(1, i, j, k), u2 = at(2, i, j, k), u3 = at(3, i, j, k);
         const double ut[4] = {0.0, u1, u2, u3};
         double utsq = 0.0;

@@ -13,10 +13,13 @@ struct Axis {
   std::vector<double> x, xa, xb, xab, dx, dxb;
 };
 
+constexpr int kMetComps = 18;  // compact metric per point (rg_device.cuh, Met)
+
 struct HostGeom {
   Axis ax[3];                      // i = r, j = phi, k = theta
   size_t nik = 0;
-  std::vector<double> mc, mi, mk;  // 33 components per (i,k) point, SoA
+  bool compact_ok = false;         // every point has the (t,r,phi)+theta block structure
+  std::vector<double> mc, mi, mk;  // kMetComps components per (i,k) point, SoA
   std::vector<double> chr;         // 64 components per point, SoA
 };
 

@@ -50,7 +50,7 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
   const double detg1 = m.detg;
   double delta = 1.0, deltaend = 1.e-7;
   int irecov = 0;
-  const double alpha1 = 1. / sqrt(-m.gc[0][0]);
+  const double alpha1 = 1. / sqrt(-m.c00);
   const double dro = alpha1 * u[0] * (1. / detg1);
   double qcov[4], qcon[4], bcon[4], bcov[4], oncov[4], oncon[4];
   qcov[0] = alpha1 * (u[4] - u[0]) * (1. / detg1);
@@ -64,21 +64,17 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
   bcon[3] = alpha1 * u[8] * (1. / detg1);
   double ro = q[0], pp = q[4];
   double util[4] = {0.0, q[1], q[2], q[3]};
-  lower4(bcon, bcov, m.g);
-  lower4(qcov, qcon, m.gc);
+  lower_g(bcon, bcov, m);
+  upper_gc(qcov, qcon, m);
   const double bsq = bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
   const double qdotb = qcov[0] * bcon[0] + qcov[1] * bcon[1] + qcov[2] * bcon[2] + qcov[3] * bcon[3];
   const double qdotbsq = qdotb * qdotb;
   oncov[0] = -1.0 * alpha1; oncov[1] = 0.0; oncov[2] = 0.0; oncov[3] = 0.0;
-  lower4(oncov, oncon, m.gc);
+  upper_gc(oncov, oncon, m);
   const double qdotn = qcon[0] * oncov[0];
   const double qsq = qcov[0] * qcon[0] + qcov[1] * qcon[1] + qcov[2] * qcon[2] + qcov[3] * qcon[3];
   const double qtsq = qsq + (qdotn * qdotn);
-  double utsq = 0.0;
-#pragma unroll
-  for (int a = 1; a <= 3; ++a)
-#pragma unroll
-    for (int b = 1; b <= 3; ++b) utsq = utsq + m.g[a][b] * util[a] * util[b];
+  double utsq = qform3(m, util[1], util[2], util[3]);
   if (utsq < 0.0 && fabs(utsq) <= safty) utsq = fabs(utsq);
   if (fabs(utsq) > 1.e4) utsq = 1.e4;
   double gfsq = 1. + utsq;
@@ -434,89 +430,88 @@ __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const doubl
 }
 
 // ------------------------------------------------------------- face fluxes
-// One thread per face f+1/2 in direction D over the hll range nm0..n-nm0 in
-// every dimension (hll.f90:83-85).  The left state comes from cell f
-// (uriil(f)), the right state from cell f+1 (uriir(f), rec.f90:2138).
+// Face f+1/2 in direction D over the hll range nm0..n-nm0 in every dimension
+// (hll.f90:83-85).  Two neighbouring threads share a face: the even lane
+// builds the left state from cell f (uriil(f)), the odd lane the right state
+// from cell f+1 (uriir(f), rec.f90:2138); each evaluates its state's conserved
+// variables, flux and wave speeds, and the pair exchanges them by warp shuffle
+// for the LLF flux.  Lanes past the edge of the range work on the last face
+// and store nothing, so every lane takes part in the shuffles.
 template <int D, int IREC>
 __global__ void __launch_bounds__(128) k_flux(DevRun r, const double* __restrict__ P, double* __restrict__ F) {
   if (!r.scal->active) return;
   const int nm0 = r.nm0;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + nm0;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + nm0;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + nm0;
-  if (i > r.imax - nm0 || j > r.jmax - nm0 || k > r.kmax - nm0) return;
+  const int side = threadIdx.x & 1;
+  const int i0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 1) + nm0;
+  const int j0 = blockIdx.y * blockDim.y + threadIdx.y + nm0;
+  const int k0 = blockIdx.z * blockDim.z + threadIdx.z + nm0;
+  const bool valid = i0 <= r.imax - nm0 && j0 <= r.jmax - nm0 && k0 <= r.kmax - nm0;
+  const int i = min(i0, r.imax - nm0), j = min(j0, r.jmax - nm0), k = min(k0, r.kmax - nm0);
   const size_t N = r.N, c = r.cell(i, j, k);
   const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.imax : (long long)r.imax * r.jmax);
-  double qL[9], qR[9];
+  double q[9];
   if (IREC == 5) {
-    const int f = (D == 1) ? i : (D == 2 ? j : k);
+    const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;  // owner cell of this lane's state
     const double* dxs = (D == 1) ? r.dx1s : (D == 2 ? r.dx2s : r.dx3s);
     const double* xs = (D == 1) ? r.x1 : (D == 2 ? r.x2 : r.x3);
-    double dx[9], xx[9], tmp[9];
+    double dx[9], xx[9], other[9];
 #pragma unroll
     for (int o = -2; o <= 2; ++o) dx[o + 4] = __ldg(dxs + f - 1 + o);
 #pragma unroll
     for (int o = -1; o <= 1; ++o) xx[o + 4] = __ldg(xs + f - 1 + o);
-    ppm_cell<D>(P + c, N, st, dx, xx, r.gam, tmp, qL);  // uriil(f): R state of cell f
+    if (side == 0) ppm_cell<D>(P + c, N, st, dx, xx, r.gam, other, q);  // uriil(f)
+    else ppm_cell<D>(P + c + st, N, st, dx, xx, r.gam, q, other);       // uriir(f)
+  } else {
 #pragma unroll
-    for (int o = -2; o <= 2; ++o) dx[o + 4] = __ldg(dxs + f + o);
-#pragma unroll
-    for (int o = -1; o <= 1; ++o) xx[o + 4] = __ldg(xs + f + o);
-    ppm_cell<D>(P + c + st, N, st, dx, xx, r.gam, qR, tmp);  // uriir(f): L state of cell f+1
-  } else
-#pragma unroll
-  for (int v = 0; v < 9; ++v) {
-    if (v == 5) { qL[v] = 0.0; qR[v] = 0.0; continue; }  // var 6 faces are never read downstream
-    const double* p = P + (size_t)v * N + c;
-    const double um2 = p[-2 * st], um1 = p[-st], u0 = p[0], up1 = p[st], up2 = p[2 * st], up3 = p[3 * st];
-    if (IREC == 6) {
-      qL[v] = mp5_left(um2, um1, u0, up1, up2);
-      qR[v] = mp5_right(um1, u0, up1, up2, up3);
-    } else {
-      qL[v] = weno5_state(um2, um1, u0, up1, up2);
-      qR[v] = weno5_state(up3, up2, up1, u0, um1);
+    for (int v = 0; v < 9; ++v) {
+      if (v == 5) { q[v] = 0.0; continue; }  // var 6 faces are never read downstream
+      // owner cell f + side; the right state reads its stencil mirrored
+      const long long sd = side ? -st : st;
+      const double* p = P + (size_t)v * N + c + side * st;
+      const double a2 = p[-2 * sd], a1 = p[-sd], u0 = p[0], b1 = p[sd], b2 = p[2 * sd];
+      if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? -1.0 : 1.0);
+      else q[v] = weno5_state(a2, a1, u0, b1, b2);
     }
   }
-  if (r.guard & 1) {
-    if (!(qL[0] > 0.0 && qL[4] > 0.0)) load9(P, N, c, qL);
-    if (!(qR[0] > 0.0 && qR[4] > 0.0)) load9(P, N, c + st, qR);
-  }
+  if ((r.guard & 1) && !(q[0] > 0.0 && q[4] > 0.0)) load9(P, N, c + side * st, q);
   Met m;
   if (D == 1) load_met(r.mi, r.nik, r.ik(i, k), m);
   else if (D == 2) load_met(r.mc, r.nik, r.ik(i, k), m);
   else load_met(r.mk, r.nik, r.ik(i, k), m);
   const double gam = r.gam;
-  double uL[9], wL[9], uR[9], wR[9], vpL, vmL, vpR, vmR;
+  double u[9], w[9], vp, vm;
   {
     PS s;
-    pstate(qL, m, gam, s);
-    p2c(s, gam, m.detg, uL);
-    flux<D>(s, gam, m.detg, wL);
-    wavespeed<D>(qL, s, m, gam, vpL, vmL);
+    pstate(q, m, gam, s);
+    const double sr = ent_ratio(s, gam);
+    p2c(s, gam, m.detg, u, sr);
+    flux<D>(s, gam, m.detg, w, sr);
+    wavespeed<D>(q, s, m, gam, vp, vm);
   }
-  {
-    PS s;
-    pstate(qR, m, gam, s);
-    p2c(s, gam, m.detg, uR);
-    flux<D>(s, gam, m.detg, wR);
-    wavespeed<D>(qR, s, m, gam, vpR, vmR);
-  }
+  const unsigned full = 0xffffffffu;
+  const double vpo = __shfl_xor_sync(full, vp, 1), vmo = __shfl_xor_sync(full, vm, 1);
+  const double vpL = side ? vpo : vp, vpR = side ? vp : vpo;
+  const double vmL = side ? vmo : vm, vmR = side ? vm : vmo;
   // calcha.f90:96-120 (cmink uses the R-state plus speed, calcha.f90:107)
   const double cmax = fmax3(0.0, vpR, vpL);
   const double cmin = (D == 3) ? fmin3(0.0, vpR, vmL) : fmin3(0.0, vmR, vmL);
   // hll.f90:83-183
 #pragma unroll
   for (int v = 0; v < 9; ++v) {
-    double w;
-    if (cmin > 0.0) w = wL[v];
+    const double uo = __shfl_xor_sync(full, u[v], 1), wo = __shfl_xor_sync(full, w[v], 1);
+    if (!valid || (v & 1) != side) continue;
+    const double uL = side ? uo : u[v], uR = side ? u[v] : uo;
+    const double wL = side ? wo : w[v], wR = side ? w[v] : wo;
+    double f;
+    if (cmin > 0.0) f = wL;
     else if (cmin <= 0.0 && cmax > 0.0) {
       const double c1 = dmax2(fabs(cmax), fabs(cmin));
-      w = 0.5 * (wL[v] + wR[v] - c1 * (uR[v] - uL[v]));
-    } else if (cmax <= 0.0) w = wR[v];
+      f = 0.5 * (wL + wR - c1 * (uR - uL));
+    } else if (cmax <= 0.0) f = wR;
     else continue;  // NaN speeds: the reference keeps the previous ww
-    if (fabs(w) < 1.0e-40) w = 0.0;
-    if ((r.guard & 2) && v == 5 + D) w = 0.0;  // Toth: no flux of the normal field component
-    F[(size_t)v * N + c] = w;
+    if (fabs(f) < 1.0e-40) f = 0.0;
+    if ((r.guard & 2) && v == 5 + D) f = 0.0;  // Toth: no flux of the normal field component
+    F[(size_t)v * N + c] = f;
   }
 }
 
@@ -651,14 +646,10 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
     double gfl = calgfl(q[1], q[2], q[3], m);
     double vel[4] = {0.0, q[1] * (1. / gfl), q[2] * (1. / gfl), q[3] * (1. / gfl)};
     if (vel[1] < 0.0) {
-      const double alpha1 = 1. / sqrt(-m.gc[0][0]);
-      const double b1 = alpha1 * alpha1 * m.gc[0][1];
+      const double alpha1 = 1. / sqrt(-m.c00);
+      const double b1 = alpha1 * alpha1 * m.c01;
       vel[1] = b1 * (1. / alpha1);
-      double vsq = 0.0;
-#pragma unroll
-      for (int a = 1; a <= 3; ++a)
-#pragma unroll
-        for (int b = 1; b <= 3; ++b) vsq = vsq + m.g[a][b] * vel[a] * vel[b];
+      double vsq = qform3(m, vel[1], vel[2], vel[3]);
       if (vsq >= 1.0) vsq = 1. - 1. / (gflmax * gflmax);
       gfl = 1. / sqrt(1. - vsq);
       q[1] = vel[1] * gfl; q[2] = vel[2] * gfl; q[3] = vel[3] * gfl;
@@ -675,11 +666,7 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
       q[0] = demin;
       q[4] = prmin;
       const double vel[4] = {0.0, 0.0, 0.0, 0.0};
-      double vsq = 0.0;
-#pragma unroll
-      for (int a = 1; a <= 3; ++a)
-#pragma unroll
-        for (int b = 1; b <= 3; ++b) vsq = vsq + m.g[a][b] * vel[a] * vel[b];
+      double vsq = qform3(m, vel[1], vel[2], vel[3]);
       if (vsq >= 1.0) vsq = 1. - 1. / (gflmax * gflmax);
       const double gfl = 1. / sqrt(1. - vsq);
       q[1] = vel[1] * gfl; q[2] = vel[2] * gfl; q[3] = vel[3] * gfl;
@@ -691,11 +678,7 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
     double de = q[0], pr = q[4];
     double gfl = calgfl(q[1], q[2], q[3], m);
     const double vel[4] = {0.0, q[1] * (1. / gfl), q[2] * (1. / gfl), q[3] * (1. / gfl)};
-    double vsq = 0.0;
-#pragma unroll
-    for (int a = 1; a <= 3; ++a)
-#pragma unroll
-      for (int b = 1; b <= 3; ++b) vsq = vsq + (m.g[a][b] + (0.0 * 0.0)) * vel[a] * vel[b];
+    double vsq = qform3(m, vel[1], vel[2], vel[3]);
     if (vsq >= 1.0 || gfl > gflmax) vsq = 1. - 1. / (gflmax * gflmax);
     gfl = 1. / sqrt(1. - vsq);
     double lim[9];
@@ -708,7 +691,7 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
     gfl = s.gfl;
     const double bcon[4] = {0.0, q[6], q[7], q[8]};
     double bcov[4];
-    lower4(bcon, bcov, m.g);
+    lower_g(bcon, bcov, m);
     const double bsq = bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
     const double f105 = (double)1.05f, f005 = (double)0.05f;
     bool capped = false;
@@ -905,7 +888,7 @@ cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s) {
 cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s) {
   const int n = r.imax - 2 * r.nm0 + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b(64, 2, 1);
-  const dim3 g = grid3(n, m, l, b);
+  const dim3 g = grid3(2 * n, m, l, b);  // two lanes per face
   if (r.irec == 5) {
     if (dir == 1) k_flux<1, 5><<<g, b, 0, s>>>(r, P, F);
     else if (dir == 2) k_flux<2, 5><<<g, b, 0, s>>>(r, P, F);

@@ -28,7 +28,7 @@ enum Counter {
 // Everything a kernel needs, by value.  Arrays are structure-of-arrays with
 // the cell index c = (i-1) + imax*((j-1) + jmax*(k-1)) (1-based i, j, k) and
 // variable v at offset v*N.  Metric caches are per (i,k) point
-// q = (i-1) + imax*(k-1), 33 components each (gcov 16, gcon 16, detg).
+// q = (i-1) + imax*(k-1), 18 components each (see Met in rg_device.cuh).
 struct DevRun {
   int imax, jmax, kmax;
   int nm0, nm1;

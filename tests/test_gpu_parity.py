@@ -18,6 +18,16 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
+def flux_err(a, b):
+    """max |a-b| per (variable, direction) relative to the variable's largest
+    flux over all three directions (a direction whose flux vanishes in exact
+    arithmetic may carry round-off residue of the others' size)."""
+    fin = np.isfinite(b)
+    scale = np.abs(np.where(fin, b, 0)).max(axis=(0, 1, 2, 4))[:, None]
+    diff = np.abs(np.where(fin, a - b, 0)).max(axis=(0, 1, 2))
+    return diff / np.maximum(scale, 1e-300)
+
+
 def _pair(gpu_ctx, p, seed=2012):
     o = Oracle(p)
     o.ic_torus(seed=seed)
@@ -72,9 +82,8 @@ def test_calflx_guarded(gpu_ctx, irec):
     r.release()
     n = o.nm1 - 1  # inside the hll range nm0 .. n-nm0 (1-based)
     reg = (slice(n, -n), slice(n, -n), slice(n, -n))
-    for d in range(3):
-        err = field_err(wg[..., d], wo[..., d], reg)
-        assert err.max() < TOL, (d, err)
+    err = flux_err(wg[reg], wo[reg])
+    assert err.max() < TOL, np.unravel_index(err.argmax(), err.shape)
 
 
 def test_calflx_reference_semantics_nan_pattern(gpu_ctx):
@@ -89,11 +98,9 @@ def test_calflx_reference_semantics_nan_pattern(gpu_ctx):
     reg = (slice(n, -n), slice(n, -n), slice(n, -n))
     a, b = wg[reg], wo[reg]
     assert np.array_equal(np.isfinite(a), np.isfinite(b))
-    fin = np.isfinite(b)
-    assert (~fin).any()
-    scale = np.abs(np.where(fin, b, 0)).max(axis=(0, 1, 2))
-    diff = np.abs(np.where(fin, a - b, 0)).max(axis=(0, 1, 2))
-    assert (diff <= TOL * np.maximum(scale, 1e-300)).all()
+    assert (~np.isfinite(b)).any()
+    err = flux_err(a, b)
+    assert err.max() < TOL, np.unravel_index(err.argmax(), err.shape)
 
 
 def test_recov(torus3d):
