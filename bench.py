@@ -184,6 +184,7 @@ def run_gpu(args) -> dict | None:
     ms = max_over_ranks(e0.elapsed_time(e1))
     launches = sum(v["launches"] for v in ctx.profile_read().values())
     st = run.stats()
+    ref_prims = run.prims() if args.mixed else None  # FP64 state after warm-up + timed steps
 
     # end to end through the public API with host buffers (pinned)
     e2e = None
@@ -206,6 +207,43 @@ def run_gpu(args) -> dict | None:
         e2e = {"value": zones * ws * args.e2e_steps / (e_ms * 1e-3), "unit": "zone-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
                "ms_per_step": e_ms / args.e2e_steps, "api": "rg_run_upload_prims + rg_step + rg_run_download_prims"}
+
+    # FP32-mixed run of the same workload: same IC, same number of steps; timed
+    # like the FP64 arm, L1 error of its state against the FP64 state at the end
+    mixed = None
+    if args.mixed:
+        ref_steps = args.warmup + args.steps
+        runm = ctx.admit(dict(p, precision="mixed"))
+        runm.ic_torus(seed=2012 + rank)
+        runm.step(args.warmup)
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        runm.step(args.steps)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        mms = max_over_ranks(m0.elapsed_time(m1))
+        got = runm.prims()
+        mshares = {}
+        if args.prof_steps > 0:
+            ctx.profile(True)
+            runm.step(args.prof_steps)
+            mp = ctx.profile_read()
+            ctx.profile(False)
+            mt = sum(v["ms"] for v in mp.values())
+            mshares = {k: round(v["ms"] / mt, 4) for k, v in mp.items()}
+        runm.release()
+        n = run.nm1
+        sl = (slice(n, -n),) * 3
+        l1 = (np.abs(got[sl] - ref_prims[sl]).sum(axis=(0, 1, 2)) /
+              np.abs(ref_prims[sl]).sum(axis=(0, 1, 2)).clip(1e-300))
+        mixed = {"value": zones * ws * args.steps / (mms * 1e-3), "unit": "zone-updates/s",
+                 "ms_per_step": mms / args.steps, "speedup_vs_fp64": ms / mms,
+                 "l1_rel_vs_fp64": {"rho": float(l1[0]), "p": float(l1[4]), "B1": float(l1[6]),
+                                    "B3": float(l1[8])},
+                 "after_steps": ref_steps, "kernel_share": mshares,
+                 "precision": "FP32 recon/LLF/CT/RK combine (compensated), FP64 recovery/floors/CFL, "
+                              "FP64 fluxes and sources for r < 2 r_H"}
 
     # per-kernel device times (separate pass: CUDA events around every launch on the library stream)
     roofline, shares = None, {}
@@ -245,7 +283,7 @@ def run_gpu(args) -> dict | None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Fishbone-Moncrief torus initial data)",
         "config": dict(config_block(args, p), parallelism=f"replicas x{ws}"),
-        "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+        "e2e": e2e, "mixed": mixed, "gpu_launches": launches, "clocks": clk.summary(),
         "roofline": roofline,
         "kernel_share": shares,
         "recov": {k: st[k] for k in ("recov_nr2", "recov_fail", "recov_carry", "recov_cap")},
@@ -285,6 +323,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--prof-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=1, help="steps in the CPU-baseline sample (0 = skip)")
+    ap.add_argument("--mixed", type=int, default=1, help="also time the FP32-mixed path (1) or not (0)")
     args = ap.parse_args()
     ws, rank, _ = dist_env()
     if args.impl == "reference":

@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libraishin_gpu.so")
 SOURCES = ["rg_kernels.cu", "rg_capi.cu", "rg_geometry.cpp"]
-HEADERS = ["rg_device.cuh", "rg_kernels.cuh", "rg_types.h", "rg_host.h"]
+HEADERS = ["rg_device.cuh", "rg_recon.cuh", "rg_kernels.cuh", "rg_types.h", "rg_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -3,6 +3,7 @@
 // RK3 step driver and the per-routine entry points.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -90,7 +91,7 @@ int check_params(const rg_run_params* p) {
   if (p->ix1 != 1 && p->ix1 != 2) return fail(RG_EINVAL_CONFIG, "ix1 must be 1 or 2");
   if (p->ix2 != 1) return fail(RG_EINVAL_CONFIG, "ix2 must be 1");
   if (p->ix3 != 1 && p->ix3 != 2) return fail(RG_EINVAL_CONFIG, "ix3 must be 1 or 2");
-  if (p->precision != RG_FP64) return fail(RG_EINVAL_CONFIG, "only RG_FP64 is built in this version");
+  if (p->precision != RG_FP64 && p->precision != RG_MIXED) return fail(RG_EINVAL_CONFIG, "unknown precision mode");
   const int nm1 = (p->irec == 5) ? 5 : 4;
   if (p->imax <= 2 * nm1 || p->jmax <= 2 * nm1 || p->kmax <= 2 * nm1)
     return fail(RG_EINVAL_CONFIG, "every extent must exceed 2*nm1 (main.f90:247-254)");
@@ -228,9 +229,10 @@ int bc_launches(const DevRun& r) {
 int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc, double* Pw) {
   const DevRun& d = R->d;
   cudaStream_t s = ctx->stream;
-  RG_CUDA(issue(ctx, K_FLUX1, 1, [&] { return launch_flux(d, 1, Pc, R->b.F[0], s); }));
-  RG_CUDA(issue(ctx, K_FLUX2, 1, [&] { return launch_flux(d, 2, Pc, R->b.F[1], s); }));
-  RG_CUDA(issue(ctx, K_FLUX3, 1, [&] { return launch_flux(d, 3, Pc, R->b.F[2], s); }));
+  const int nf = d.mixed ? 2 : 1;
+  RG_CUDA(issue(ctx, K_FLUX1, nf, [&] { return launch_flux(d, 1, Pc, R->b.F[0], s); }));
+  RG_CUDA(issue(ctx, K_FLUX2, nf, [&] { return launch_flux(d, 2, Pc, R->b.F[1], s); }));
+  RG_CUDA(issue(ctx, K_FLUX3, nf, [&] { return launch_flux(d, 3, Pc, R->b.F[2], s); }));
   RG_CUDA(issue(ctx, K_CT, 1, [&] { return launch_ct(d, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s); }));
   RG_CUDA(issue(ctx, K_UPDATE, 2, [&] {
     return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s);
@@ -341,6 +343,14 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
   d.nm0 = (p->irec == 5) ? 4 : 3;
   d.nm1 = d.nm0 + 1;
   d.irec = p->irec; d.model = p->model; d.guard = p->guard; d.iter = p->iter;
+  d.mixed = (p->precision == RG_MIXED);
+  // cells inside r < 2 r_H keep FP64 in the mixed path (Kerr metrics only)
+  d.i_fp64 = 0;
+  if (p->metric == 303 || p->metric == 403) {
+    const double r2h = 2.0 * (1.0 + std::sqrt(1.0 - p->akm * p->akm));
+    for (int i = 1; i <= p->imax; ++i)
+      if (R->geom.ax[0].x[i] < r2h) d.i_fp64 = i;
+  }
   d.nmax_cfl = d.nm1 * 2 + (d.nm1 - 1);
   d.N = (size_t)p->imax * p->jmax * p->kmax;
   d.nik = (size_t)p->imax * p->kmax;

@@ -308,6 +308,136 @@ __device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, co
   }
 }
 
+// Compensated FP32 accumulation (Kahan/Knuth two-sum, FMA two-product):
+// the running sum keeps its rounding error in a second float.
+struct Acc32 {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float t) {
+    const float x = s + t;
+    const float bb = x - s;
+    c += (s - (x - bb)) + (t - bb);
+    s = x;
+  }
+  // coef * (hi + lo) with the product's rounding error kept (fmaf)
+  __device__ __forceinline__ void add_scaled(float coef, float hi, float lo) {
+    const float p = coef * hi;
+    const float e = fmaf(coef, hi, -p);
+    add(p);
+    c += e + coef * lo;
+  }
+  __device__ __forceinline__ double value() const { return (double)s + (double)c; }
+};
+
+__device__ __forceinline__ void split(double x, float& hi, float& lo) {
+  hi = (float)x;
+  lo = (float)(x - (double)hi);
+}
+
+// Mixed-precision counterpart of stage_rhs: the RK combine runs in FP32 with
+// compensated accumulation (Acc32), the flux divergence in FP32, the
+// geometric source in FP32 outside r < 2 r_H (FP64 inside).  The cell's
+// conserved states P2C(P) are the stored-state stand-ins of the reference's
+// uu/uo arrays and stay FP64, as does the primitive recovery that follows.
+template <int STAGE>
+__device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pn,
+                                const double* __restrict__ Pc, const double* __restrict__ F1,
+                                const double* __restrict__ F2, const double* __restrict__ F3,
+                                const double* __restrict__ CT, double dt, double u[9]) {
+  const size_t N = r.N, c = r.cell(i, j, k), q = r.ik(i, k);
+  const double gam = r.gam;
+  double qc[9];
+  load9(Pc, N, c, qc);
+  PS s;
+  pstate(qc, m, gam, s);
+  double ucur[9];
+  p2c(s, gam, m.detg, ucur);
+  double sf64[4] = {0.0, 0.0, 0.0, 0.0};
+  float sf32[4] = {0.f, 0.f, 0.f, 0.f};
+  const bool fp64_src = (i <= r.i_fp64);
+  {
+    const size_t nik = r.nik;
+    if (fp64_src) {
+      const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
+      double ta = 0.0, tb = 0.0, tc = 0.0, td = 0.0;
+#pragma unroll
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+          const double t = a * s.ucon[mm] * s.ucov[n] + b * (mm == n ? 1.0 : 0.0) - s.bbcon[mm] * s.bbcov[n];
+          ta = ta + t * __ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
+          tb = tb + t * __ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
+          tc = tc + t * __ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
+          td = td + t * __ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
+        }
+      sf64[0] = m.detg * ta; sf64[1] = m.detg * tb; sf64[2] = m.detg * tc; sf64[3] = m.detg * td;
+    } else {
+      const float a = (float)(s.roh + s.bbsq), b = (float)(s.pr + 0.5 * s.bbsq);
+      float ta = 0.f, tb = 0.f, tc = 0.f, td = 0.f;
+#pragma unroll
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+          const float t = a * (float)s.ucon[mm] * (float)s.ucov[n] + (mm == n ? b : 0.f) -
+                          (float)s.bbcon[mm] * (float)s.bbcov[n];
+          ta = ta + t * (float)__ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
+          tb = tb + t * (float)__ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
+          tc = tc + t * (float)__ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
+          td = td + t * (float)__ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
+        }
+      const float dg = (float)m.detg;
+      sf32[0] = dg * ta; sf32[1] = dg * tb; sf32[2] = dg * tc; sf32[3] = dg * td;
+    }
+  }
+  double uo[9];
+  if (STAGE > 1) {
+    double qn[9];
+    load9(Pn, N, c, qn);
+    PS sn;
+    pstate(qn, m, gam, sn);
+    p2c(sn, gam, m.detg, uo);
+  }
+  const float a1 = (float)(dt / __ldg(r.dx1b + i - 1)), a2 = (float)(dt / __ldg(r.dx2b + j - 1)),
+              a3 = (float)(dt / __ldg(r.dx3b + k - 1));
+  const float fdt = (float)dt;
+  // stage weights: U = wo*uo + wc*ucur + wf*(flux divergence + dt*S)
+  const float wo = (STAGE == 1) ? 0.f : (STAGE == 2 ? 0.75f : 1.0f / 3.0f);
+  const float wc = (STAGE == 1) ? 1.f : (STAGE == 2 ? 0.25f : 2.0f / 3.0f);
+  const float wf = wc;
+  const size_t ci = c - 1, cj = c - (size_t)r.imax, ck = c - (size_t)r.imax * r.jmax;
+  auto fd = [&](const double* A, size_t x, size_t xm) { return (float)A[x] - (float)A[xm]; };
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    float d1, d2, d3;
+    if (v == 7) d1 = fd(CT + 2 * N, c, ci);
+    else if (v == 8) d1 = fd(CT + 4 * N, c, ci);
+    else d1 = fd(F1 + (size_t)v * N, c, ci);
+    if (v == 6) d2 = fd(CT, c, cj);
+    else if (v == 8) d2 = fd(CT + 5 * N, c, cj);
+    else d2 = fd(F2 + (size_t)v * N, c, cj);
+    if (v == 6) d3 = fd(CT + 1 * N, c, ck);
+    else if (v == 7) d3 = fd(CT + 3 * N, c, ck);
+    else d3 = fd(F3 + (size_t)v * N, c, ck);
+    Acc32 acc;
+    float hi, lo;
+    if (STAGE > 1) {
+      split(uo[v], hi, lo);
+      acc.add_scaled(wo, hi, lo);
+    }
+    split(ucur[v], hi, lo);
+    acc.add_scaled(wc, hi, lo);
+    acc.add(wf * (-(a1 * d1) - a2 * d2 - a3 * d3));
+    if (v >= 1 && v <= 4) {
+      if (fp64_src) {
+        split(sf64[v - 1] * dt, hi, lo);
+        acc.add_scaled(wf, hi, lo);
+      } else {
+        acc.add(wf * (sf32[v - 1] * fdt));
+      }
+    }
+    u[v] = acc.value();
+  }
+}
+
 __device__ __forceinline__ bool is_interior(const DevRun& r, int i, int j, int k) {
   return i > r.nm1 && i <= r.imax - r.nm1 && j > r.nm1 && j <= r.jmax - r.nm1 && k > r.nm1 && k <= r.kmax - r.nm1;
 }
@@ -320,7 +450,7 @@ __device__ __forceinline__ void queue_carry(const DevRun& r, int i, int j, int k
   else atomicAdd(r.cnt + C_CARRY_OVF, 1ull);
 }
 
-template <int STAGE>
+template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                                                 double* __restrict__ Pw, const double* __restrict__ F1,
                                                 const double* __restrict__ F2, const double* __restrict__ F3,
@@ -340,7 +470,8 @@ __global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restri
   Met m;
   load_met(r.mc, r.nik, r.ik(i, k), m);
   double u[9];
-  stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
+  if (MIX) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
+  else stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
   double qo[9], qn[9];
   load9(Pc, N, c, qo);
   RecovOut o{0.0, false, false, false};
@@ -360,7 +491,7 @@ __global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restri
 // (k, j, i over the interior): each takes the final W of its predecessor cell.
 // One thread; runs only when cells were queued, which the reference data
 // rarely produces.  MODE 0: stage update; MODE 1: recov-only entry point.
-template <int MODE, int STAGE>
+template <int MODE, int STAGE, bool MIX = false>
 __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                             double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                             const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
@@ -390,7 +521,8 @@ __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const doubl
     Met m;
     load_met(r.mc, r.nik, r.ik(i, k), m);
     double u[9], qo[9], qn[9];
-    if (MODE == 0) stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, dt, u);
+    if (MODE == 0 && MIX) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, dt, u);
+    else if (MODE == 0) stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, dt, u);
     else load9(U, r.N, c, u);
     load9(Pc, r.N, c, qo);
     const bool ok = recov_cell(u, qo, qn, m, r.gam, r.iter, r.dmin, r.pmin, r.x1[i - 1], carry, o);
@@ -431,92 +563,107 @@ __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const doubl
 
 // ------------------------------------------------------------- face fluxes
 // Face f+1/2 in direction D over the hll range nm0..n-nm0 in every dimension
-// (hll.f90:83-85).  Two neighbouring threads share a face: the even lane
+// (hll.f90:83-85).  Two neighbouring lanes share a face: the even lane
 // builds the left state from cell f (uriil(f)), the odd lane the right state
 // from cell f+1 (uriir(f), rec.f90:2138); each evaluates its state's conserved
-// variables, flux and wave speeds, and the pair exchanges them by warp shuffle
-// for the LLF flux.  Lanes past the edge of the range work on the last face
-// and store nothing, so every lane takes part in the shuffles.
-template <int D, int IREC>
-__global__ void __launch_bounds__(128) k_flux(DevRun r, const double* __restrict__ P, double* __restrict__ F) {
-  if (!r.scal->active) return;
-  const int nm0 = r.nm0;
-  const int side = threadIdx.x & 1;
-  const int i0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 1) + nm0;
-  const int j0 = blockIdx.y * blockDim.y + threadIdx.y + nm0;
-  const int k0 = blockIdx.z * blockDim.z + threadIdx.z + nm0;
-  const bool valid = i0 <= r.imax - nm0 && j0 <= r.jmax - nm0 && k0 <= r.kmax - nm0;
-  const int i = min(i0, r.imax - nm0), j = min(j0, r.jmax - nm0), k = min(k0, r.kmax - nm0);
+// variables, flux and wave speeds in arithmetic type T, and the pair exchanges
+// them by warp shuffle for the LLF flux.  Lanes past the edge of the range work
+// on the last face and store nothing.  Both lanes of a pair always take the
+// same branch, so the shuffles run on the active mask.
+template <int D, int IREC, typename T>
+__device__ __forceinline__ void face_lane(const DevRun& r, const double* __restrict__ P, double* __restrict__ F,
+                                          int i, int j, int k, int side, bool valid) {
+  const unsigned mask = __activemask();
   const size_t N = r.N, c = r.cell(i, j, k);
   const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.imax : (long long)r.imax * r.jmax);
-  double q[9];
+  T q[9];
   if (IREC == 5) {
     const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;  // owner cell of this lane's state
     const double* dxs = (D == 1) ? r.dx1s : (D == 2 ? r.dx2s : r.dx3s);
     const double* xs = (D == 1) ? r.x1 : (D == 2 ? r.x2 : r.x3);
-    double dx[9], xx[9], other[9];
+    T dx[9], xx[9], other[9];
 #pragma unroll
-    for (int o = -2; o <= 2; ++o) dx[o + 4] = __ldg(dxs + f - 1 + o);
+    for (int o = -2; o <= 2; ++o) dx[o + 4] = T(__ldg(dxs + f - 1 + o));
 #pragma unroll
-    for (int o = -1; o <= 1; ++o) xx[o + 4] = __ldg(xs + f - 1 + o);
-    if (side == 0) ppm_cell<D>(P + c, N, st, dx, xx, r.gam, other, q);  // uriil(f)
-    else ppm_cell<D>(P + c + st, N, st, dx, xx, r.gam, q, other);       // uriir(f)
+    for (int o = -1; o <= 1; ++o) xx[o + 4] = T(__ldg(xs + f - 1 + o));
+    if (side == 0) ppm_cell<D>(P + c, N, st, dx, xx, T(r.gam), other, q);  // uriil(f)
+    else ppm_cell<D>(P + c + st, N, st, dx, xx, T(r.gam), q, other);       // uriir(f)
   } else {
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
-      if (v == 5) { q[v] = 0.0; continue; }  // var 6 faces are never read downstream
+      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       // owner cell f + side; the right state reads its stencil mirrored
       const long long sd = side ? -st : st;
       const double* p = P + (size_t)v * N + c + side * st;
-      const double a2 = p[-2 * sd], a1 = p[-sd], u0 = p[0], b1 = p[sd], b2 = p[2 * sd];
-      if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? -1.0 : 1.0);
+      const T a2 = T(p[-2 * sd]), a1 = T(p[-sd]), u0 = T(p[0]), b1 = T(p[sd]), b2 = T(p[2 * sd]);
+      if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? T(-1) : T(1));
       else q[v] = weno5_state(a2, a1, u0, b1, b2);
     }
   }
-  if ((r.guard & 1) && !(q[0] > 0.0 && q[4] > 0.0)) load9(P, N, c + side * st, q);
-  Met m;
+  if ((r.guard & 1) && !(q[0] > T(0) && q[4] > T(0))) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) q[v] = T(P[(size_t)v * N + c + side * st]);
+  }
+  MetT<T> m;
   if (D == 1) load_met(r.mi, r.nik, r.ik(i, k), m);
   else if (D == 2) load_met(r.mc, r.nik, r.ik(i, k), m);
   else load_met(r.mk, r.nik, r.ik(i, k), m);
-  const double gam = r.gam;
-  double u[9], w[9], vp, vm;
+  const T gam = T(r.gam);
+  T u[9], w[9], vp, vm;
   {
-    PS s;
+    PST<T> s;
     pstate(q, m, gam, s);
-    const double sr = ent_ratio(s, gam);
+    const T sr = ent_ratio(s, gam);
     p2c(s, gam, m.detg, u, sr);
     flux<D>(s, gam, m.detg, w, sr);
     wavespeed<D>(q, s, m, gam, vp, vm);
   }
-  const unsigned full = 0xffffffffu;
-  const double vpo = __shfl_xor_sync(full, vp, 1), vmo = __shfl_xor_sync(full, vm, 1);
-  const double vpL = side ? vpo : vp, vpR = side ? vp : vpo;
-  const double vmL = side ? vmo : vm, vmR = side ? vm : vmo;
+  const T vpo = __shfl_xor_sync(mask, vp, 1), vmo = __shfl_xor_sync(mask, vm, 1);
+  const T vpL = side ? vpo : vp, vpR = side ? vp : vpo;
+  const T vmL = side ? vmo : vm, vmR = side ? vm : vmo;
   // calcha.f90:96-120 (cmink uses the R-state plus speed, calcha.f90:107)
-  const double cmax = fmax3(0.0, vpR, vpL);
-  const double cmin = (D == 3) ? fmin3(0.0, vpR, vmL) : fmin3(0.0, vmR, vmL);
+  const T cmax = fmax3(T(0), vpR, vpL);
+  const T cmin = (D == 3) ? fmin3(T(0), vpR, vmL) : fmin3(T(0), vmR, vmL);
   // hll.f90:83-183
 #pragma unroll
   for (int v = 0; v < 9; ++v) {
-    const double uo = __shfl_xor_sync(full, u[v], 1), wo = __shfl_xor_sync(full, w[v], 1);
+    const T uo = __shfl_xor_sync(mask, u[v], 1), wo = __shfl_xor_sync(mask, w[v], 1);
     if (!valid || (v & 1) != side) continue;
-    const double uL = side ? uo : u[v], uR = side ? u[v] : uo;
-    const double wL = side ? wo : w[v], wR = side ? w[v] : wo;
-    double f;
-    if (cmin > 0.0) f = wL;
-    else if (cmin <= 0.0 && cmax > 0.0) {
-      const double c1 = dmax2(fabs(cmax), fabs(cmin));
-      f = 0.5 * (wL + wR - c1 * (uR - uL));
-    } else if (cmax <= 0.0) f = wR;
+    const T uL = side ? uo : u[v], uR = side ? u[v] : uo;
+    const T wL = side ? wo : w[v], wR = side ? w[v] : wo;
+    T f;
+    if (cmin > T(0)) f = wL;
+    else if (cmin <= T(0) && cmax > T(0)) {
+      const T c1 = dmax2(mabs(cmax), mabs(cmin));
+      f = T(0.5) * (wL + wR - c1 * (uR - uL));
+    } else if (cmax <= T(0)) f = wR;
     else continue;  // NaN speeds: the reference keeps the previous ww
-    if (fabs(f) < 1.0e-40) f = 0.0;
-    if ((r.guard & 2) && v == 5 + D) f = 0.0;  // Toth: no flux of the normal field component
-    F[(size_t)v * N + c] = f;
+    if (mabs(f) < T(1.0e-40)) f = T(0);
+    if ((r.guard & 2) && v == 5 + D) f = T(0);  // Toth: no flux of the normal field component
+    F[(size_t)v * N + c] = double(f);
   }
 }
 
+// Faces with radial index i in [ilo, ihi] (and the hll range in j, k) in
+// arithmetic type T.  The FP64 path launches it once over the whole range;
+// the mixed path launches FP64 for r < 2 r_H (i <= r.i_fp64) and FP32 beyond.
+template <int D, int IREC, typename T>
+__global__ void __launch_bounds__(128) k_flux(DevRun r, const double* __restrict__ P, double* __restrict__ F,
+                                              int ilo, int ihi) {
+  if (!r.scal->active) return;
+  const int nm0 = r.nm0;
+  const int side = threadIdx.x & 1;
+  const int i0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 1) + ilo;
+  const int j0 = blockIdx.y * blockDim.y + threadIdx.y + nm0;
+  const int k0 = blockIdx.z * blockDim.z + threadIdx.z + nm0;
+  const bool valid = i0 <= ihi && j0 <= r.jmax - nm0 && k0 <= r.kmax - nm0;
+  const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(k0, r.kmax - nm0);
+  face_lane<D, IREC, T>(r, P, F, i, j, k, side, valid);
+}
+
 // ---------------------------------------------------------------- flux-CT
-// ct.f90:30-118 on nm1..n-nm1 in every dimension.
+// ct.f90:30-118 on nm1..n-nm1 in every dimension, in arithmetic type T.
+template <typename T>
 __global__ void __launch_bounds__(256) k_ct(DevRun r, const double* __restrict__ F1, const double* __restrict__ F2,
                                             const double* __restrict__ F3, double* __restrict__ CT) {
   if (!r.scal->active) return;
@@ -533,13 +680,20 @@ __global__ void __launch_bounds__(256) k_ct(DevRun r, const double* __restrict__
   const double* fzy = F3 + 7 * N;  // ww(3,8)
   const double* fxz = F1 + 8 * N;  // ww(1,9)
   const double* fyz = F2 + 8 * N;  // ww(2,9)
-  const double e = 1.0 / 8.0;
-  CT[0 * N + c] = e * (2.0 * fyx[c] + fyx[c + di] + fyx[c - di] - fxy[c] - fxy[c + dj] - fxy[c - di] - fxy[c - di + dj]);
-  CT[1 * N + c] = e * (2.0 * fzx[c] + fzx[c + di] + fzx[c - di] - fxz[c] - fxz[c + dk] - fxz[c - di] - fxz[c - di + dk]);
-  CT[2 * N + c] = e * (2.0 * fxy[c] + fxy[c + dj] + fxy[c - dj] - fyx[c] - fyx[c + di] - fyx[c - dj] - fyx[c + di - dj]);
-  CT[3 * N + c] = e * (2.0 * fzy[c] + fzy[c + dj] + fzy[c - dj] - fyz[c] - fyz[c + dk] - fyz[c - dj] - fyz[c - dj + dk]);
-  CT[4 * N + c] = e * (2.0 * fxz[c] + fxz[c + dk] + fxz[c - dk] - fzx[c] - fzx[c + di] - fzx[c - dk] - fzx[c + di - dk]);
-  CT[5 * N + c] = e * (2.0 * fyz[c] + fyz[c + dk] + fyz[c - dk] - fzy[c] - fzy[c + dj] - fzy[c - dk] - fzy[c + dj - dk]);
+  auto L = [](const double* a, size_t x) { return T(a[x]); };
+  const T e = T(1.0) / T(8.0), two = T(2.0);
+  CT[0 * N + c] = double(e * (two * L(fyx, c) + L(fyx, c + di) + L(fyx, c - di) - L(fxy, c) - L(fxy, c + dj) -
+                              L(fxy, c - di) - L(fxy, c - di + dj)));
+  CT[1 * N + c] = double(e * (two * L(fzx, c) + L(fzx, c + di) + L(fzx, c - di) - L(fxz, c) - L(fxz, c + dk) -
+                              L(fxz, c - di) - L(fxz, c - di + dk)));
+  CT[2 * N + c] = double(e * (two * L(fxy, c) + L(fxy, c + dj) + L(fxy, c - dj) - L(fyx, c) - L(fyx, c + di) -
+                              L(fyx, c - dj) - L(fyx, c + di - dj)));
+  CT[3 * N + c] = double(e * (two * L(fzy, c) + L(fzy, c + dj) + L(fzy, c - dj) - L(fyz, c) - L(fyz, c + dk) -
+                              L(fyz, c - dj) - L(fyz, c - dj + dk)));
+  CT[4 * N + c] = double(e * (two * L(fxz, c) + L(fxz, c + dk) + L(fxz, c - dk) - L(fzx, c) - L(fzx, c + di) -
+                              L(fzx, c - dk) - L(fzx, c + di - dk)));
+  CT[5 * N + c] = double(e * (two * L(fyz, c) + L(fyz, c + dk) + L(fyz, c - dk) - L(fzy, c) - L(fzy, c + dj) -
+                              L(fzy, c - dk) - L(fzy, c + dj - dk)));
 }
 
 // ------------------------------------------------------------ boundaries
@@ -885,22 +1039,35 @@ cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s) {
-  const int n = r.imax - 2 * r.nm0 + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
+template <typename T>
+static void launch_flux_t(const DevRun& r, int dir, const double* P, double* F, int ilo, int ihi, cudaStream_t s) {
+  if (ihi < ilo) return;
+  const int n = ihi - ilo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b(64, 2, 1);
   const dim3 g = grid3(2 * n, m, l, b);  // two lanes per face
   if (r.irec == 5) {
-    if (dir == 1) k_flux<1, 5><<<g, b, 0, s>>>(r, P, F);
-    else if (dir == 2) k_flux<2, 5><<<g, b, 0, s>>>(r, P, F);
-    else k_flux<3, 5><<<g, b, 0, s>>>(r, P, F);
+    if (dir == 1) k_flux<1, 5, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    else if (dir == 2) k_flux<2, 5, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    else k_flux<3, 5, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
   } else if (r.irec == 6) {
-    if (dir == 1) k_flux<1, 6><<<g, b, 0, s>>>(r, P, F);
-    else if (dir == 2) k_flux<2, 6><<<g, b, 0, s>>>(r, P, F);
-    else k_flux<3, 6><<<g, b, 0, s>>>(r, P, F);
+    if (dir == 1) k_flux<1, 6, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    else if (dir == 2) k_flux<2, 6, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    else k_flux<3, 6, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
   } else {
-    if (dir == 1) k_flux<1, 7><<<g, b, 0, s>>>(r, P, F);
-    else if (dir == 2) k_flux<2, 7><<<g, b, 0, s>>>(r, P, F);
-    else k_flux<3, 7><<<g, b, 0, s>>>(r, P, F);
+    if (dir == 1) k_flux<1, 7, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    else if (dir == 2) k_flux<2, 7, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    else k_flux<3, 7, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+  }
+}
+
+cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s) {
+  const int lo = r.nm0, hi = r.imax - r.nm0;
+  if (!r.mixed) {
+    launch_flux_t<double>(r, dir, P, F, lo, hi, s);
+  } else {
+    const int split = r.i_fp64 < lo ? lo - 1 : (r.i_fp64 > hi ? hi : r.i_fp64);
+    launch_flux_t<double>(r, dir, P, F, lo, split, s);
+    launch_flux_t<float>(r, dir, P, F, split + 1, hi, s);
   }
   return cudaGetLastError();
 }
@@ -909,24 +1076,33 @@ cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const
                       cudaStream_t s) {
   const int n = r.imax - 2 * r.nm1 + 1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
   const dim3 b(64, 4, 1);
-  k_ct<<<grid3(n, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT);
+  if (r.mixed) k_ct<float><<<grid3(n, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT);
+  else k_ct<double><<<grid3(n, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT);
   return cudaGetLastError();
+}
+
+template <bool MIX>
+static void launch_update_t(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
+                            const double* F1, const double* F2, const double* F3, const double* CT, dim3 g, dim3 b,
+                            cudaStream_t s) {
+  if (stage == 1) {
+    k_update<1, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    k_carry_fix<0, 1, MIX><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  } else if (stage == 2) {
+    k_update<2, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    k_carry_fix<0, 2, MIX><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  } else {
+    k_update<3, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    k_carry_fix<0, 3, MIX><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  }
 }
 
 cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                           const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s) {
   const dim3 b(64, 2, 1);
   const dim3 g = grid3(r.imax, r.jmax, r.kmax, b);
-  if (stage == 1) {
-    k_update<1><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
-    k_carry_fix<0, 1><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  } else if (stage == 2) {
-    k_update<2><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
-    k_carry_fix<0, 2><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  } else {
-    k_update<3><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
-    k_carry_fix<0, 3><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  }
+  if (r.mixed) launch_update_t<true>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, g, b, s);
+  else launch_update_t<false>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, g, b, s);
   return cudaGetLastError();
 }
 

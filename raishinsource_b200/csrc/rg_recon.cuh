@@ -1,0 +1,194 @@
+// rg_recon.cuh -- face reconstruction of rec.f90 (MP5, WENO5, PPM) as device
+// functions templated on the arithmetic type T (see rg_device.cuh).
+#pragma once
+
+namespace rg {
+
+// rec.f90:2346-2370
+template <typename T>
+__device__ __forceinline__ T dmm(T xx, T yy) {
+  return T(0.5) * (sgn1(xx) + sgn1(yy)) * dmin2(mabs(xx), mabs(yy));
+}
+template <typename T>
+__device__ __forceinline__ T dm4(T ww, T xx, T yy, T zz) {
+  T mn = mabs(ww);
+  if (mabs(xx) < mn) mn = mabs(xx);
+  if (mabs(yy) < mn) mn = mabs(yy);
+  if (mabs(zz) < mn) mn = mabs(zz);
+  return T(0.125) * (sgn1(ww) + sgn1(xx)) * mabs(sgn1(ww) + sgn1(yy)) * (sgn1(ww) + sgn1(zz)) * mn;
+}
+
+// rec.f90:2095-2178: MP5 face state of cell 0 from u(-2..+2) given in the
+// order (a2, a1, u0, b1, b2): the left state at +1/2 takes
+// (u-2, u-1, u0, u+1, u+2) and sg = +1; the right state at -1/2 takes the
+// mirrored stencil (u+2, u+1, u0, u-1, u-2) and sg = -1, because the
+// reference's right state flips the signs of the dm4 terms of md and lc
+// (rec.f90:2172-2176).  Negation is exact, so both equal the reference's
+// separate formulas bit for bit, and the two lanes of a face run one code path.
+template <typename T>
+__device__ __forceinline__ T mp5_state(T a2, T a1, T u0, T b1, T b2, T sg) {
+  const T tmp1 = T(1.0) / T(60.0), tmp2 = T(4.0) / T(3.0), alpha = T(4.0), eps1 = T(1.0e-10);
+  const T ul1 = tmp1 * (T(2.) * a2 - T(13.) * a1 + T(47.) * u0 + T(27.) * b1 - T(3.) * b2);
+  const T ulmp = u0 + dmm(b1 - u0, alpha * (u0 - a1));
+  const T t = (ul1 - u0) * (ul1 - ulmp);
+  if (t <= eps1) return ul1;
+  const T dim1 = a2 - T(2.) * a1 + u0;
+  const T di1 = a1 - T(2.) * u0 + b1;
+  const T dip1 = u0 - T(2.) * b1 + b2;
+  const T dm4p = dm4(T(4.) * di1 - dip1, T(4.) * dip1 - di1, di1, dip1);
+  const T dm4m = dm4(T(4.) * di1 - dim1, T(4.) * dim1 - di1, di1, dim1);
+  const T ul = u0 + alpha * (u0 - a1);
+  const T av = T(0.5) * (u0 + b1);
+  const T md = av - (sg * T(0.5)) * dm4p;
+  const T lc = u0 + T(0.5) * (u0 - a1) + (sg * tmp2) * dm4m;
+  const T m1 = fmin3(u0, b1, md), m2 = fmin3(u0, ul, lc);
+  const T m3 = fmax3(u0, b1, md), m4 = fmax3(u0, ul, lc);
+  const T umax = dmax2(m1, m2), umin = dmin2(m3, m4);
+  return ul1 + dmm(umin - ul1, umax - ul1);
+}
+
+// rec.f90:2373-2643 (WENO5-JS); the left state at +1/2 takes
+// (u-2, u-1, u0, u+1, u+2), the right state at -1/2 the mirrored stencil.
+// (13./12.) is a single-precision literal in the reference.
+template <typename T>
+__device__ __forceinline__ T weno5_state(T a2, T a1, T u0, T b1, T b2) {
+  const T cd0 = T(1.0 / 10.0), cd1 = T(6.0 / 10.0), cd2 = T(3.0 / 10.0);
+  const T c00 = T(2.0 / 6.0), c01 = T(-7.0 / 6.0), c02 = T(11.0 / 6.0);
+  const T c10 = T(-1.0 / 6.0), c11 = T(5.0 / 6.0), c12 = T(2.0 / 6.0);
+  const T c20 = T(2.0 / 6.0), c21 = T(5.0 / 6.0), c22 = T(-1.0 / 6.0);
+  const T epsi = T(1.0e-6), c1312 = T((double)(13.0f / 12.0f)), c14 = T(0.25);
+  const T s0 = a2 - T(2.) * a1 + u0, t0 = a2 - T(4.) * a1 + T(3.) * u0;
+  const T s1 = a1 - T(2.) * u0 + b1, t1 = a1 - b1;
+  const T s2 = u0 - T(2.) * b1 + b2, t2 = T(3.) * u0 - T(4.) * b1 + b2;
+  const T be0 = c1312 * (s0 * s0) + c14 * (t0 * t0) + epsi;
+  const T be1 = c1312 * (s1 * s1) + c14 * (t1 * t1) + epsi;
+  const T be2 = c1312 * (s2 * s2) + c14 * (t2 * t2) + epsi;
+  const T w0 = cd0 / (be0 * be0), w1 = cd1 / (be1 * be1), w2 = cd2 / (be2 * be2);
+  const T wt = w0 + w1 + w2;
+  const T o0 = w0 / wt, o1 = w1 / wt, o2 = w2 / wt;
+  const T q0 = c00 * a2 + c01 * a1 + c02 * u0;
+  const T q1 = c10 * a1 + c11 * u0 + c12 * b1;
+  const T q2 = c20 * u0 + c21 * b1 + c22 * b2;
+  return o0 * q0 + o1 * q1 + o2 * q2;
+}
+
+// ------------------------------------------------------------------- PPM
+// rPPM of Marti & Muller (1996) as restated by rec.f90:1261-2058.  The four
+// passes (interp, detect, flaten, monoto) touch only the two face states of
+// one cell each, so both states of cell c follow from the cells c-3..c+3:
+// L = state at c-1/2 (the reference's uriir(c-1)), R = state at c+1/2
+// (uriil(c)).  dx is rec2's shifted dx?b (dummy dx?b(m) = actual dx?b(m-1),
+// rec.f90:58), x the cell centres (contact detection).
+
+// interp Eq. (60)-(61) (rec.f90:1346-1418); the theta direction lacks the
+// factor 2 of r and phi (rec.f90:1414).
+template <typename T>
+__device__ __forceinline__ T ppm_dma(T um, T u0, T up, T dxm, T dx0, T dxp, bool kdir) {
+  const T t1a = dx0 / (dxm + dx0 + dxp);
+  const T t1b = (T(2.0) * dxm + dx0) / (dxp + dx0);
+  const T t1c = (dx0 + T(2.0) * dxp) / (dxm + dx0);
+  const T sp1 = up - u0, sm1 = u0 - um;
+  const T spm1 = sp1 * sm1;
+  const T da = t1a * (t1b * sp1 + t1c * sm1);
+  if (spm1 <= T(0)) return T(0);
+  const T t1 = (da < T(0)) ? T(-1) : T(1);
+  const T t1d = dmin2(mabs(sm1), mabs(sp1));
+  return kdir ? t1 * dmin2(mabs(da), t1d) : t1 * dmin2(mabs(da), T(2.0) * t1d);
+}
+
+// interp Eq. (51) (rec.f90:1422-1468): interface value at c+1/2.
+template <typename T>
+__device__ __forceinline__ T ppm_face(T u0, T u1, T dma0, T dma1, T dxm, T dx0, T dx1, T dx2) {
+  const T t2 = (dx0 / (dx0 + dx1)) * (u1 - u0);
+  const T t3a = T(1.0) / (dxm + dx0 + dx1 + dx2);
+  const T t3b = (T(2.0) * dx1 * dx0) / (dx0 + dx1);
+  const T t3c = ((dxm + dx0) / (T(2.0) * dx0 + dx1)) - ((dx2 + dx1) / (T(2.0) * dx1 + dx0));
+  const T t3 = t3a * t3b * t3c * (u1 - u0);
+  const T t4 = t3a * dx0 * ((dxm + dx0) / (T(2.0) * dx0 + dx1));
+  const T t5 = t3a * dx1 * ((dx1 + dx2) / (dx0 + T(2.0) * dx1));
+  return u0 + t2 + t3 - t4 * dma1 + t5 * dma0;
+}
+
+// Both face states of the cell at p (primitive v at p[v*N], FP64 storage),
+// stride st along direction D; dx[o+4], x[o+4] are the shifted spacing and
+// centre at offset o from the cell.  gam enters the contact test (rec.f90:1623).
+template <int D, typename T>
+__device__ void ppm_cell(const double* __restrict__ p, size_t N, long long st, const T dx[9], const T x[9], T gam,
+                         T L[9], T R[9]) {
+  auto U = [&](int v, int o) { return T(p[(size_t)v * N + o * st]); };
+  auto DX = [&](int o) { return dx[o + 4]; };
+  // detect (rec.f90:1479-1686): contact steepening factor eta on density
+  T eta;
+  {
+    const T eta1 = T(5.0), eta2 = T(0.05), eps1 = T(0.1), ak0 = T(1.0);
+    auto dda = [&](int o) {
+      const T t0a = T(1.0) / (DX(o - 1) + DX(o) + DX(o + 1));
+      const T t0b = (U(0, o + 1) - U(0, o)) / (DX(o + 1) + DX(o));
+      const T t0c = (U(0, o) - U(0, o - 1)) / (DX(o) + DX(o - 1));
+      return t0a * (t0b - t0c);
+    };
+    const T ddp = dda(1), ddm = dda(-1);
+    const T rp = U(0, 1), rm = U(0, -1);
+    const T t1 = ddp * ddm;
+    const T t2 = mabs(rp - rm) - eps1 * dmin2(mabs(rp), mabs(rm));
+    T etatil;
+    if (t1 >= T(0) && t2 <= T(0)) {
+      etatil = T(0);
+    } else {
+      const T t2a = -(ddp - ddm) / (x[5] - x[3]);
+      const T a = x[4] - x[3], b = x[5] - x[4];
+      const T t2b = (a * a * a + b * b * b) / (rp - rm);
+      etatil = t2a * t2b;
+    }
+    eta = dmax2(T(0), dmin2(eta1 * (etatil - eta2), T(1)));
+    const T pp = U(4, 1), pm = U(4, -1);
+    const T t3 = mabs(rp - rm) / dmin2(rp, rm);
+    const T t4 = mabs(pp - pm) / dmin2(pp, pm);
+    if (gam * ak0 * t3 < t4) eta = T(0);
+  }
+  // flaten (rec.f90:1689-1884): shock flattening f2a from p and u^D
+  T f2a;
+  {
+    const T eps2 = T(1.0), omg2 = T(0.52), omg3 = T(10.0);
+    auto f1a = [&](int o) {
+      const T pp1 = U(4, o + 1), pm1 = U(4, o - 1);
+      const T t3a = mabs(pp1 - pm1);
+      const T t1 = eps2 * dmin2(pp1, pm1) - t3a;
+      const T t2 = U(D, o + 1) - U(D, o - 1);
+      const T omg1 = (t1 < T(0) && t2 < T(0)) ? T(1) : T(0);
+      const T t3b = U(4, o + 2) - U(4, o - 2);
+      T t4;
+      if (t3b == T(0)) t4 = (t3a == T(0)) ? -omg2 : T(1.0) - omg2;
+      else t4 = (t3a / t3b) - omg2;
+      return dmin2(T(1), omg1 * dmax2(T(0), t4 * omg3));
+    };
+    const T f1b = (U(4, 1) - U(4, -1) < T(0)) ? f1a(1) : f1a(-1);
+    f2a = dmax2(f1a(0), f1b);
+  }
+#pragma unroll 1
+  for (int v = 0; v < 9; ++v) {
+    if (v == 5) { L[v] = T(0); R[v] = T(0); continue; }  // var 6 faces are never read downstream
+    const T um2 = U(v, -2), um1 = U(v, -1), u0 = U(v, 0), up1 = U(v, 1), up2 = U(v, 2);
+    const T dm = ppm_dma(um2, um1, u0, DX(-2), DX(-1), DX(0), D == 3);
+    const T d0 = ppm_dma(um1, u0, up1, DX(-1), DX(0), DX(1), D == 3);
+    const T dp = ppm_dma(u0, up1, up2, DX(0), DX(1), DX(2), D == 3);
+    T l = ppm_face(um1, u0, dm, d0, DX(-2), DX(-1), DX(0), DX(1));
+    T r = ppm_face(u0, up1, d0, dp, DX(-1), DX(0), DX(1), DX(2));
+    if (v == 0) {
+      r = r * (T(1.0) - eta) + (up1 - T(0.5) * dp) * eta;
+      l = l * (T(1.0) - eta) + (um1 + T(0.5) * dm) * eta;
+    }
+    r = u0 * f2a + r * (T(1.0) - f2a);
+    l = u0 * f2a + l * (T(1.0) - f2a);
+    // monoto (rec.f90:1887-2056)
+    if ((r - u0) * (l - u0) >= T(0)) { r = u0; l = u0; }
+    const T t3 = T(6.0) * (r - l) * (u0 - T(0.5) * (r + l));
+    const T t4 = (r - l) * (r - l);
+    if (t3 > t4) l = T(3.0) * u0 - T(2.0) * r;
+    if (-t3 > t4) r = T(3.0) * u0 - T(2.0) * l;
+    L[v] = l;
+    R[v] = r;
+  }
+}
+
+}  // namespace rg

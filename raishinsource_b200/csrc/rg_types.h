@@ -33,6 +33,8 @@ struct DevRun {
   int imax, jmax, kmax;
   int nm0, nm1;
   int irec, model, guard, iter;
+  int mixed;             // 1: FP32 reconstruction/fluxes/CT/RK combine (RG_MIXED)
+  int i_fp64;            // radial cells 1..i_fp64 (r < 2 r_H) keep FP64 in the mixed path
   int nmax_cfl;          // nm1*2 + (nm1-1) (cdtcfl.f90:38)
   size_t N;              // cells
   size_t nik;            // (i,k) points
