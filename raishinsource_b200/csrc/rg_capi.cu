@@ -111,9 +111,12 @@ int check_params(const rg_run_params* p) {
 size_t footprint_bytes(const rg_run_params* p) {
   const size_t N = (size_t)p->imax * p->jmax * p->kmax;
   const size_t nik = (size_t)p->imax * p->kmax;
-  const size_t state = (3 * 9 + 3 * 9 + 6 + 2 * 9 + 9) * N * sizeof(double);
+  const size_t state = (3 * 9 + 3 * 9 + 6 + 2 * 9 + 9 + 9) * N * sizeof(double);
   const size_t geom = (3 * kMetComps + 64) * nik * sizeof(double) + 16 * (size_t)(p->imax + p->jmax + p->kmax) * sizeof(double);
-  return state + geom + sizeof(Scal) + C_NCOUNTERS * 8 + kCarryCap * sizeof(int);
+  size_t mixed = 0;
+  if (p->precision == RG_MIXED)  // P32, F32 x3, CT32; FP32 metric caches and Christoffels
+    mixed = (9 + 27 + 6) * N * sizeof(float) + (3 * kMetComps + 64) * nik * sizeof(float);
+  return state + geom + mixed + sizeof(Scal) + C_NCOUNTERS * 8 + kCarryCap * sizeof(int);
 }
 
 Run* find(rg_ctx* ctx, int id) {
@@ -143,6 +146,14 @@ std::vector<double> shifted(const std::vector<double>& v, int n) {
   for (int m = 2; m <= n; ++m) o[m - 1] = v[m - 1];
   o[0] = v[1];
   return o;
+}
+
+// The per-routine entry points compute in FP64 whatever the run's precision.
+DevRun fp64_view(const Run* R) {
+  DevRun d = R->d;
+  d.mixed = 0;
+  d.P32 = nullptr;
+  return d;
 }
 
 int set_time(rg_ctx* ctx, Run* R, double t0) {
@@ -229,12 +240,12 @@ int bc_launches(const DevRun& r) {
 int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc, double* Pw) {
   const DevRun& d = R->d;
   cudaStream_t s = ctx->stream;
-  const int nf = d.mixed ? 2 : 1;
+  const int nf = n_flux_launches(d);
   RG_CUDA(issue(ctx, K_FLUX1, nf, [&] { return launch_flux(d, 1, Pc, R->b.F[0], s); }));
   RG_CUDA(issue(ctx, K_FLUX2, nf, [&] { return launch_flux(d, 2, Pc, R->b.F[1], s); }));
   RG_CUDA(issue(ctx, K_FLUX3, nf, [&] { return launch_flux(d, 3, Pc, R->b.F[2], s); }));
-  RG_CUDA(issue(ctx, K_CT, 1, [&] { return launch_ct(d, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s); }));
-  RG_CUDA(issue(ctx, K_UPDATE, 2, [&] {
+  RG_CUDA(issue(ctx, K_CT, n_ct_launches(d), [&] { return launch_ct(d, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s); }));
+  RG_CUDA(issue(ctx, K_UPDATE, n_update_launches(d), [&] {
     return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s);
   }));
   RG_CUDA(issue(ctx, K_BC, bc_launches(d), [&] { return launch_bc(d, Pw, Pn, s); }));
@@ -344,6 +355,7 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
   d.nm1 = d.nm0 + 1;
   d.irec = p->irec; d.model = p->model; d.guard = p->guard; d.iter = p->iter;
   d.mixed = (p->precision == RG_MIXED);
+  d.gkind = (p->gam == 4.0 / 3.0) ? 1 : (p->gam == 5.0 / 3.0 ? 2 : 0);
   // cells inside r < 2 r_H keep FP64 in the mixed path (Kerr metrics only)
   d.i_fp64 = 0;
   if (p->metric == 303 || p->metric == 403) {
@@ -379,6 +391,11 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
   R->b.stage2 = static_cast<double*>(ptr);
   if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
   R->aos = static_cast<double*>(ptr);
+  if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
+  d.Un = static_cast<double*>(ptr);
+  if ((rc = dalloc(R, &ptr, 2 * (size_t)p->imax * sizeof(double)))) return bail(rc);
+  d.fl_de = static_cast<double*>(ptr);
+  d.fl_pr = d.fl_de + p->imax;
   if ((rc = dalloc(R, &ptr, sizeof(Scal)))) return bail(rc);
   d.scal = static_cast<Scal*>(ptr);
   if ((rc = dalloc(R, &ptr, C_NCOUNTERS * sizeof(unsigned long long)))) return bail(rc);
@@ -406,6 +423,38 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
   if ((rc = upload(shifted(G.ax[0].dxb, p->imax), &d.dx1s, R, s))) return bail(rc);
   if ((rc = upload(shifted(G.ax[1].dxb, p->jmax), &d.dx2s, R, s))) return bail(rc);
   if ((rc = upload(shifted(G.ax[2].dxb, p->kmax), &d.dx3s, R, s))) return bail(rc);
+  // the caches and floor tables are this run's own allocations: fill their derived parts
+  if (launch_geom_derive(d, const_cast<double*>(d.mc), const_cast<double*>(d.mi), const_cast<double*>(d.mk),
+                         const_cast<double*>(d.fl_de), const_cast<double*>(d.fl_pr), s) != cudaSuccess)
+    return bail(fail(RG_ECUDA, "geometry setup kernel failed"));
+  if (d.mixed) {
+    const size_t nik = d.nik;
+    float* f = nullptr;
+    auto falloc = [&](size_t n) -> int {
+      void* q = nullptr;
+      int e = dalloc(R, &q, n * sizeof(float));
+      f = static_cast<float*>(q);
+      return e;
+    };
+    if ((rc = falloc(9 * N))) return bail(rc);
+    d.P32 = f;
+    for (int k = 0; k < 3; ++k) {
+      if ((rc = falloc(9 * N))) return bail(rc);
+      d.F32[k] = f;
+      if (cudaMemsetAsync(f, 0, 9 * N * sizeof(float), s) != cudaSuccess) return bail(RG_ECUDA);
+    }
+    if ((rc = falloc(6 * N))) return bail(rc);
+    d.CT32 = f;
+    if (cudaMemsetAsync(f, 0, 6 * N * sizeof(float), s) != cudaSuccess) return bail(RG_ECUDA);
+    const double* src[4] = {d.mc, d.mi, d.mk, d.chr};
+    const float** dst[4] = {&d.mc32, &d.mi32, &d.mk32, &d.chr32};
+    for (int a = 0; a < 4; ++a) {
+      const size_t n = (a < 3 ? (size_t)kMetComps : (size_t)64) * nik;
+      if ((rc = falloc(n))) return bail(rc);
+      if (launch_to_f32(src[a], f, n, s) != cudaSuccess) return bail(fail(RG_ECUDA, "FP32 cache setup failed"));
+      *dst[a] = f;
+    }
+  }
   if ((rc = set_time(ctx, R, 0.0))) return bail(rc);
   if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(RG_ECUDA, "setup failed"));
   const int id = ctx->next_id++;
@@ -431,6 +480,7 @@ int rg_run_ic_torus(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin,
   torus_ic(R->p, R->geom, seed, amp, rin, rmax, beta, kappa, P);
   R->cur = 0;
   RG_CUDA(cudaMemcpyAsync(R->b.P[0], P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (R->d.P32) RG_CUDA(launch_to_f32(R->b.P[0], R->d.P32, 9 * R->d.N, ctx->stream));
   int rc = set_time(ctx, R, 0.0);
   if (rc) return rc;
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -444,6 +494,7 @@ int rg_run_upload_prims(rg_ctx* ctx, int run, const double* uri, double t0) {
   R->cur = 0;
   int rc = to_soa(ctx, R, uri, R->b.P[0]);
   if (rc) return rc;
+  if (R->d.P32) RG_CUDA(launch_to_f32(R->b.P[0], R->d.P32, 9 * R->d.N, ctx->stream));
   return set_time(ctx, R, t0);
 }
 
@@ -515,14 +566,14 @@ int rg_caluu1(rg_ctx* ctx, int run, const double* uri, double* uu) {
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   int rc = to_soa(ctx, R, uri, R->b.stage);
   if (rc) return rc;
-  RG_CUDA(launch_p2c(R->d, R->b.stage, R->b.stage2, ctx->stream));
+  RG_CUDA(launch_p2c(fp64_view(R), R->b.stage, R->b.stage2, ctx->stream));
   return from_soa(ctx, R, R->b.stage2, uu);
 }
 
 int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
-  const DevRun& d = R->d;
+  const DevRun d = fp64_view(R);
   const size_t N = d.N;
   int rc = to_soa(ctx, R, uri, R->b.stage);
   if (rc) return rc;
@@ -566,7 +617,7 @@ int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri) {
   int rc = to_soa(ctx, R, uu, R->b.stage);
   if (rc) return rc;
   if ((rc = to_soa(ctx, R, uri, R->b.stage2))) return rc;
-  RG_CUDA(launch_recov_only(R->d, R->b.stage, R->b.stage2, R->b.F[0], ctx->stream));
+  RG_CUDA(launch_recov_only(fp64_view(R), R->b.stage, R->b.stage2, R->b.F[0], ctx->stream));
   return from_soa(ctx, R, R->b.F[0], uri);
 }
 
@@ -580,7 +631,7 @@ int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl) {
   const double one = 1.0;
   std::memcpy(&sc.dtcfl_bits, &one, sizeof(double));
   RG_CUDA(cudaMemcpyAsync(R->d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
-  RG_CUDA(launch_cfl(R->d, R->b.stage, ctx->stream));
+  RG_CUDA(launch_cfl(fp64_view(R), R->b.stage, ctx->stream));
   RG_CUDA(cudaMemcpyAsync(&sc, R->d.scal, sizeof(Scal), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
   std::memcpy(dtcfl, &sc.dtcfl_bits, sizeof(double));
@@ -596,8 +647,9 @@ int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio) {
   Scal sc{};
   sc.active = 1;
   RG_CUDA(cudaMemcpyAsync(R->d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
-  RG_CUDA(launch_bc(R->d, R->b.stage, R->b.stage2, ctx->stream));
-  RG_CUDA(launch_floor(R->d, R->b.stage, ctx->stream));
+  const DevRun d = fp64_view(R);
+  RG_CUDA(launch_bc(d, R->b.stage, R->b.stage2, ctx->stream));
+  RG_CUDA(launch_floor(d, R->b.stage, ctx->stream));
   return from_soa(ctx, R, R->b.stage, uri);
 }
 
@@ -668,7 +720,7 @@ extern "C" int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, dou
     g_static_scal_addr[ctx->device] = static_cast<Scal*>(b);
   }
   double* ct = g_static_ct_addr[ctx->device];
-  DevRun d = R->d;
+  DevRun d = fp64_view(R);
   d.scal = g_static_scal_addr[ctx->device];  // the run's own time state is not touched
   cudaStream_t s = ctx->stream;
   // The arrays keep the previous call's contents: clear them first.

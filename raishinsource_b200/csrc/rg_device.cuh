@@ -46,20 +46,30 @@ __device__ __forceinline__ T dmax2(T a, T b) { return (b > a) ? b : a; }
 // host checks this at admission).  gcov is symmetric; gcon, an LU inverse
 // (coord.f90:1504), is not symmetric to the last bit and keeps its full 3x3
 // block.  Sums below run over the nonzero terms in the reference's order.
+// The last eight fields are functions of the others that the reference
+// recomputes at every use (lapse, shift, cal3met's gcon3a diagonal,
+// coord.f90:970-1013, and 1/sqrt(-g)); k_met_derive evaluates them once per
+// point with the same expressions, so using them changes no result.
 template <typename T>
 struct MetT {
   T g00, g01, g02, g11, g12, g22, g33;                 // gcov
   T c00, c01, c02, c10, c11, c12, c20, c21, c22, c33;  // gcon
   T detg;                                              // sqrt(-g)
+  T al;                                                // alpha = 1/sqrt(-g^00)
+  T ial;                                               // 1/alpha
+  T be1, be2;                                          // beta^r, beta^phi = alpha^2 g^0i
+  T g3_11, g3_22, g3_33;                               // g^dd + (beta^d/alpha)^2
+  T idetg;                                             // 1/sqrt(-g)
 };
 using Met = MetT<double>;
-constexpr int kMetComps = 18;
 
 // Metric cache layout: per (i,k) point q, component c at c*nik + q, in the
-// order of the MetT fields (always stored in FP64).
-template <typename T>
-__device__ __forceinline__ void load_met(const double* __restrict__ base, size_t nik, size_t q, MetT<T>& m) {
-  const double* b = base + q;
+// order of the MetT fields (FP64, with FP32 copies for the mixed path's FP32
+// kernels).  Components a kernel does
+// not use are never loaded (dead loads are removed by the compiler).
+template <typename T, typename S>
+__device__ __forceinline__ void load_met(const S* __restrict__ base, size_t nik, size_t q, MetT<T>& m) {
+  const S* b = base + q;
   m.g00 = T(__ldg(b + 0 * nik)); m.g01 = T(__ldg(b + 1 * nik)); m.g02 = T(__ldg(b + 2 * nik));
   m.g11 = T(__ldg(b + 3 * nik)); m.g12 = T(__ldg(b + 4 * nik)); m.g22 = T(__ldg(b + 5 * nik));
   m.g33 = T(__ldg(b + 6 * nik));
@@ -68,6 +78,51 @@ __device__ __forceinline__ void load_met(const double* __restrict__ base, size_t
   m.c20 = T(__ldg(b + 13 * nik)); m.c21 = T(__ldg(b + 14 * nik)); m.c22 = T(__ldg(b + 15 * nik));
   m.c33 = T(__ldg(b + 16 * nik));
   m.detg = T(__ldg(b + 17 * nik));
+  m.al = T(__ldg(b + 18 * nik)); m.ial = T(__ldg(b + 19 * nik));
+  m.be1 = T(__ldg(b + 20 * nik)); m.be2 = T(__ldg(b + 21 * nik));
+  m.g3_11 = T(__ldg(b + 22 * nik)); m.g3_22 = T(__ldg(b + 23 * nik)); m.g3_33 = T(__ldg(b + 24 * nik));
+  m.idetg = T(__ldg(b + 25 * nik));
+}
+
+// The derived fields of one point from its base fields: calucon's
+// alpha1/b1/b2 (physfunc.f90:58-66), calcha4*'s gcon3a(d,d) via cal3met
+// (calcha.f90:400-410, coord.f90:990-1005) and recov1a's 1/detg.
+__device__ __forceinline__ void met_derive(const double base[kMetBase], double out[kMetComps - kMetBase]) {
+  const double alpha1 = 1. / sqrt(-base[7]);
+  const double b1 = alpha1 * alpha1 * base[8];
+  const double b2 = alpha1 * alpha1 * base[9];
+  const double on1 = b1 / alpha1, on2 = b2 / alpha1, on3 = 0.0 / alpha1;
+  out[0] = alpha1;
+  out[1] = 1. / alpha1;
+  out[2] = b1;
+  out[3] = b2;
+  out[4] = base[11] + (on1 * on1);
+  out[5] = base[15] + (on2 * on2);
+  out[6] = base[16] + (on3 * on3);
+  out[7] = 1. / base[17];
+}
+
+// x**gam for the adiabatic indices of the reference's setups: 4/3
+// (pram.f90:40) as x*cbrt(x) and 5/3 as x*cbrt(x)^2, otherwise pow.  The
+// cube-root forms agree with pow to a few ulp at a fraction of its cost.
+// Negative or NaN x keeps pow's result (NaN), as in the reference, where a
+// reconstructed negative density makes the entropy variable NaN.
+// kind: 1 for gam == 4/3, 2 for gam == 5/3 (bitwise), 0 otherwise.
+__device__ __forceinline__ double pow_gam(double x, double gam, int kind) {
+  if (kind == 0 || !(x >= 0.0)) return pow(x, gam);
+  const double c = cbrt(x);
+  return kind == 1 ? x * c : x * c * c;
+}
+__device__ __forceinline__ float pow_gam(float x, float gam, int kind) {
+  if (kind == 0 || !(x >= 0.f)) return powf(x, gam);
+  const float c = cbrtf(x);
+  return kind == 1 ? x * c : x * c * c;
+}
+// x**(gam-1): cbrt(x) for 4/3, cbrt(x)^2 for 5/3.
+__device__ __forceinline__ double pow_gam1(double x, double gam, int kind) {
+  if (kind == 0 || !(x >= 0.0)) return pow(x, gam - 1.);
+  const double c = cbrt(x);
+  return kind == 1 ? c : c * c;
 }
 
 // sum_{a,b=1..3} g_ab x_a x_b over the nonzero terms in (a,b) order
@@ -113,15 +168,12 @@ __device__ __forceinline__ T calgfl(const T u1, const T u2, const T u3, const Me
   return msqrt(T(1) + utsq);
 }
 
-// physfunc.f90:45-78
+// physfunc.f90:45-78 (alpha1, b1, b2 and 1/alpha1 from the metric cache)
 template <typename T>
 __device__ __forceinline__ void calucon(T u1, T u2, T u3, T gfl, const MetT<T>& m, T ucon[4]) {
-  const T alpha1 = T(1) / msqrt(-m.c00);
-  const T b1 = alpha1 * alpha1 * m.c01;
-  const T b2 = alpha1 * alpha1 * m.c02;
-  ucon[0] = gfl * (T(1) / alpha1);
-  ucon[1] = u1 - gfl * b1 * (T(1) / alpha1);
-  ucon[2] = u2 - gfl * b2 * (T(1) / alpha1);
+  ucon[0] = gfl * m.ial;
+  ucon[1] = u1 - gfl * m.be1 * m.ial;
+  ucon[2] = u2 - gfl * m.be2 * m.ial;
   ucon[3] = u3;  // beta^theta = 0
 }
 
@@ -154,7 +206,7 @@ __device__ __forceinline__ void pstate(const T q[9], const MetT<T>& m, T gam, PS
 
 // p / rho^Gamma of a state (caluu.f90:303, calflx.f90:474), computed once per state.
 template <typename T>
-__device__ __forceinline__ T ent_ratio(const PST<T>& s, T gam) { return s.pr / mpow(s.de, gam); }
+__device__ __forceinline__ T ent_ratio(const PST<T>& s, T gam, int gkind) { return s.pr / pow_gam(s.de, gam, gkind); }
 
 // caluu.f90:92-118: sqrt(-g) (rho u^t, T^t_i, T^t_t + rho u^t, s u^t, B^i).
 // delta(0,n) is the literal identity of caldelta (physfunc.f90:122-158).
@@ -171,8 +223,8 @@ __device__ __forceinline__ void p2c(const PST<T>& s, T gam, T detg, T u[9], T sr
   for (int n = 0; n < 9; ++n) u[n] = detg * u[n];
 }
 template <typename T>
-__device__ __forceinline__ void p2c(const PST<T>& s, T gam, T detg, T u[9]) {
-  p2c(s, gam, detg, u, ent_ratio(s, gam));
+__device__ __forceinline__ void p2c(const PST<T>& s, T gam, int gkind, T detg, T u[9]) {
+  p2c(s, gam, detg, u, ent_ratio(s, gam, gkind));
 }
 
 // calflx.f90:391-795, direction D (1 = r, 2 = phi, 3 = theta).  The induction
@@ -201,11 +253,9 @@ __device__ __forceinline__ void flux(const PST<T>& s, T gam, T detg, T w[9], T s
 // spatial metrics: gcov3a = gcov + 0*0, gcon3a(D,D) = gcon(D,D) + (beta^D/alpha)^2.
 template <int D, typename T>
 __device__ __forceinline__ void wavespeed(const T q[9], const PST<T>& s, const MetT<T>& m, T gam, T& vfp, T& vfm) {
-  const T alpha1 = T(1) / msqrt(-m.c00);
-  const T betad = (D == 1) ? alpha1 * alpha1 * m.c01 : (D == 2 ? alpha1 * alpha1 * m.c02 : T(0));
-  const T oncon_d = betad / alpha1;
-  const T gcdd = (D == 1) ? m.c11 : (D == 2 ? m.c22 : m.c33);
-  const T gc3dd = gcdd + (oncon_d * oncon_d);
+  const T alpha1 = m.al;
+  const T betad = (D == 1) ? m.be1 : (D == 2 ? m.be2 : T(0));
+  const T gc3dd = (D == 1) ? m.g3_11 : (D == 2 ? m.g3_22 : m.g3_33);
   const T vcon[4] = {T(0), q[1] * (T(1) / s.gfl), q[2] * (T(1) / s.gfl), q[3] * (T(1) / s.gfl)};
   const T vsq = qform3(m, vcon[1], vcon[2], vcon[3]);
   const T cssq = gam * s.pr / s.roh;

@@ -187,10 +187,10 @@ void metric_at(const rg_run_params& p, double r, double th, double th_mks, Mat g
 // Returns false if an entry coupling theta to (t,r,phi) is nonzero or gcov is
 // not symmetric, which the compact kernels do not represent.
 bool store_met(std::vector<double>& dst, size_t nik, size_t q, const Mat g, const Mat gc) {
-  const double v[kMetComps] = {g[0][0], g[0][1], g[0][2], g[1][1], g[1][2], g[2][2], g[3][3],
+  const double v[kMetBase] = {g[0][0], g[0][1], g[0][2], g[1][1], g[1][2], g[2][2], g[3][3],
                                gc[0][0], gc[0][1], gc[0][2], gc[1][0], gc[1][1], gc[1][2],
                                gc[2][0], gc[2][1], gc[2][2], gc[3][3], sqrt_minus_det(g)};
-  for (int c = 0; c < kMetComps; ++c) dst[(size_t)c * nik + q] = v[c];
+  for (int c = 0; c < kMetBase; ++c) dst[(size_t)c * nik + q] = v[c];
   bool ok = g[1][0] == g[0][1] && g[2][0] == g[0][2] && g[2][1] == g[1][2];
   for (int a = 0; a < 3; ++a) ok = ok && g[a][3] == 0.0 && g[3][a] == 0.0 && gc[a][3] == 0.0 && gc[3][a] == 0.0;
   return ok;
@@ -573,7 +573,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
     for (int j = 1; j <= jmax; ++j)
       for (int i = 2; i <= imax - 1; ++i) {
         auto A = [&](int ii, int kk) { return apot[cidx(ii, j, kk)]; };
-        const double dg = G.mc[(size_t)(kMetComps - 1) * nik + (size_t)(i - 1) + (size_t)imax * (k - 1)];
+        const double dg = G.mc[(size_t)(kMetBase - 1) * nik + (size_t)(i - 1) + (size_t)imax * (k - 1)];
         const double c1 = 0.5 * (A(i + 1, k + 1) + A(i, k + 1) - A(i + 1, k) - A(i, k));
         const double h3 = mks ? 0.5 * (X3.xb[k + 1] + X3.xb[k]) - 0.5 * (X3.xb[k] + X3.xb[k - 1])
                               : 0.5 * (X3.x[k + 1] + X3.x[k]) - 0.5 * (X3.x[k] + X3.x[k - 1]);

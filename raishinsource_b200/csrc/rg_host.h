@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../include/raishin_gpu.h"
+#include "rg_types.h"
 
 namespace rg {
 
@@ -13,7 +14,6 @@ struct Axis {
   std::vector<double> x, xa, xb, xab, dx, dxb;
 };
 
-constexpr int kMetComps = 18;  // compact metric per point (rg_device.cuh, Met)
 
 struct HostGeom {
   Axis ax[3];                      // i = r, j = phi, k = theta

@@ -43,25 +43,25 @@ constexpr int kRescaleCap = 1000;  // the reference's "go to 95" loop (recov.f90
 // non-negative root and no carried-in W is given: the reference then keeps W
 // from the previous cell of its loop (recov.f90:810-815), which the caller
 // resolves in loop order.
-__device__ bool recov_cell(const double u[9], const double q[9], double out[9], const Met& m, double gam,
-                           int iter, double dmin, double pmin, double x1i, const double* wg_carry, RecovOut& res) {
+__device__ bool recov_cell(const double u[9], const double q[9], double out[9], const Met& m, double gam, int gkind,
+                           int iter, double demin_i, double prmin_i, const double* wg_carry, RecovOut& res) {
   const double safty = 1.0e-4, saftybig = 1.0e5, dv = 1.0e-2;
   const double gam1 = gam / (gam - 1.0), gam2 = 1.0 / gam1;
-  const double detg1 = m.detg;
+  const double idetg1 = m.idetg;  // 1. / detg1
   double delta = 1.0, deltaend = 1.e-7;
   int irecov = 0;
-  const double alpha1 = 1. / sqrt(-m.c00);
-  const double dro = alpha1 * u[0] * (1. / detg1);
+  const double alpha1 = m.al;
+  const double dro = alpha1 * u[0] * idetg1;
   double qcov[4], qcon[4], bcon[4], bcov[4], oncov[4], oncon[4];
-  qcov[0] = alpha1 * (u[4] - u[0]) * (1. / detg1);
-  qcov[1] = alpha1 * u[1] * (1. / detg1);
-  qcov[2] = alpha1 * u[2] * (1. / detg1);
-  qcov[3] = alpha1 * u[3] * (1. / detg1);
-  const double gss = alpha1 * u[5] * (1. / detg1);
+  qcov[0] = alpha1 * (u[4] - u[0]) * idetg1;
+  qcov[1] = alpha1 * u[1] * idetg1;
+  qcov[2] = alpha1 * u[2] * idetg1;
+  qcov[3] = alpha1 * u[3] * idetg1;
+  const double gss = alpha1 * u[5] * idetg1;
   bcon[0] = 0.0;
-  bcon[1] = alpha1 * u[6] * (1. / detg1);
-  bcon[2] = alpha1 * u[7] * (1. / detg1);
-  bcon[3] = alpha1 * u[8] * (1. / detg1);
+  bcon[1] = alpha1 * u[6] * idetg1;
+  bcon[2] = alpha1 * u[7] * idetg1;
+  bcon[3] = alpha1 * u[8] * idetg1;
   double ro = q[0], pp = q[4];
   double util[4] = {0.0, q[1], q[2], q[3]};
   lower_g(bcon, bcov, m);
@@ -207,8 +207,8 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
         gfsq = gf * gf;
         ro = dro * (1. / gf);
         pp = (gss * (1. / gf)) * pow(ro, gam - 1.);
-        if (ro < 0.0) ro = dmin * pow(x1i, -1.5);
-        if (pp < 0.0) pp = (gam - 1.) * pmin * pow(x1i, -2.5);
+        if (ro < 0.0) ro = demin_i;
+        if (pp < 0.0) pp = prmin_i;
         const double roh = ro + gam1 * pp;
         wg = fabs(gfsq * roh);
 #pragma unroll
@@ -227,14 +227,14 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
   // recov.f90:1174-1216 (the uu(6) rewrite is overwritten by caluu1 and is not kept)
   if (irecov == 0) {
     out[0] = ro; out[1] = util[1]; out[2] = util[2]; out[3] = util[3]; out[4] = pp;
-    out[5] = ro * pp / pow(ro, gam - 1.);
+    out[5] = ro * pp / pow_gam1(ro, gam, gkind);
   } else {
     out[0] = q[0]; out[1] = q[1]; out[2] = q[2]; out[3] = q[3]; out[4] = q[4];
-    out[5] = q[0] * q[4] / pow(q[0], gam);
+    out[5] = q[0] * q[4] / pow_gam(q[0], gam, gkind);
   }
-  out[6] = u[6] * (1. / detg1);
-  out[7] = u[7] * (1. / detg1);
-  out[8] = u[8] * (1. / detg1);
+  out[6] = u[6] * idetg1;
+  out[7] = u[7] * idetg1;
+  out[8] = u[8] * idetg1;
   return true;
 }
 
@@ -254,7 +254,11 @@ __device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, co
   PS s;
   pstate(qc, m, gam, s);
   double ucur[9];
-  p2c(s, gam, m.detg, ucur);
+  p2c(s, gam, r.gkind, m.detg, ucur);
+  // U^n = P2C(P^n) is this stage's ucur in stage 1; stages 2 and 3 read it back
+  if (STAGE == 1)
+#pragma unroll
+    for (int v = 0; v < 9; ++v) r.Un[(size_t)v * N + c] = ucur[v];
   // geometric source (calsf.f90:6-151): S_nu = sqrt(-g) T^m_n Gamma^n_{nu m}
   double sf[4];
   {
@@ -274,13 +278,7 @@ __device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, co
     sf[0] = m.detg * ta; sf[1] = m.detg * tb; sf[2] = m.detg * tc; sf[3] = m.detg * td;
   }
   double uo[9];
-  if (STAGE > 1) {
-    double qn[9];
-    load9(Pn, N, c, qn);
-    PS sn;
-    pstate(qn, m, gam, sn);
-    p2c(sn, gam, m.detg, uo);
-  }
+  if (STAGE > 1) load9(r.Un, N, c, uo);
   const double a1 = dt / __ldg(r.dx1b + i - 1), a2 = dt / __ldg(r.dx2b + j - 1), a3 = dt / __ldg(r.dx3b + k - 1);
   const size_t ci = c - 1, cj = c - (size_t)r.imax, ck = c - (size_t)r.imax * r.jmax;
 #pragma unroll
@@ -333,16 +331,16 @@ __device__ __forceinline__ void split(double x, float& hi, float& lo) {
   lo = (float)(x - (double)hi);
 }
 
-// Mixed-precision counterpart of stage_rhs: the RK combine runs in FP32 with
-// compensated accumulation (Acc32), the flux divergence in FP32, the
-// geometric source in FP32 outside r < 2 r_H (FP64 inside).  The cell's
-// conserved states P2C(P) are the stored-state stand-ins of the reference's
-// uu/uo arrays and stay FP64, as does the primitive recovery that follows.
+// Mixed-precision counterpart of stage_rhs for cells beyond r = 2 r_H: the
+// flux divergence (FP32 face fluxes and flux-CT values), the geometric source
+// (FP32 Christoffel cache, FP32 copy of the cell's 4-vectors) and the RK
+// combine run in FP32; the combine accumulates with compensation (Acc32), so
+// the conserved state keeps the FP64 precision of its inputs U^n and
+// P2C(P).  Those inputs, the stored-state stand-ins of the reference's uu/uo
+// arrays, stay FP64, as does the primitive recovery that follows.
 template <int STAGE>
-__device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pn,
-                                const double* __restrict__ Pc, const double* __restrict__ F1,
-                                const double* __restrict__ F2, const double* __restrict__ F3,
-                                const double* __restrict__ CT, double dt, double u[9]) {
+__device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pc,
+                                double dt, double u[9]) {
   const size_t N = r.N, c = r.cell(i, j, k), q = r.ik(i, k);
   const double gam = r.gam;
   double qc[9];
@@ -350,51 +348,32 @@ __device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met&
   PS s;
   pstate(qc, m, gam, s);
   double ucur[9];
-  p2c(s, gam, m.detg, ucur);
-  double sf64[4] = {0.0, 0.0, 0.0, 0.0};
-  float sf32[4] = {0.f, 0.f, 0.f, 0.f};
-  const bool fp64_src = (i <= r.i_fp64);
+  p2c(s, gam, r.gkind, m.detg, ucur);
+  if (STAGE == 1)
+#pragma unroll
+    for (int v = 0; v < 9; ++v) r.Un[(size_t)v * N + c] = ucur[v];
+  float sf[4];
   {
     const size_t nik = r.nik;
-    if (fp64_src) {
-      const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
-      double ta = 0.0, tb = 0.0, tc = 0.0, td = 0.0;
+    const float a = (float)(s.roh + s.bbsq), b = (float)(s.pr + 0.5 * s.bbsq);
+    float uc[4], ul[4], bc[4], bl[4];
 #pragma unroll
-      for (int n = 0; n < 4; ++n)
-#pragma unroll
-        for (int mm = 0; mm < 4; ++mm) {
-          const double t = a * s.ucon[mm] * s.ucov[n] + b * (mm == n ? 1.0 : 0.0) - s.bbcon[mm] * s.bbcov[n];
-          ta = ta + t * __ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
-          tb = tb + t * __ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
-          tc = tc + t * __ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
-          td = td + t * __ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
-        }
-      sf64[0] = m.detg * ta; sf64[1] = m.detg * tb; sf64[2] = m.detg * tc; sf64[3] = m.detg * td;
-    } else {
-      const float a = (float)(s.roh + s.bbsq), b = (float)(s.pr + 0.5 * s.bbsq);
-      float ta = 0.f, tb = 0.f, tc = 0.f, td = 0.f;
-#pragma unroll
-      for (int n = 0; n < 4; ++n)
-#pragma unroll
-        for (int mm = 0; mm < 4; ++mm) {
-          const float t = a * (float)s.ucon[mm] * (float)s.ucov[n] + (mm == n ? b : 0.f) -
-                          (float)s.bbcon[mm] * (float)s.bbcov[n];
-          ta = ta + t * (float)__ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
-          tb = tb + t * (float)__ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
-          tc = tc + t * (float)__ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
-          td = td + t * (float)__ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
-        }
-      const float dg = (float)m.detg;
-      sf32[0] = dg * ta; sf32[1] = dg * tb; sf32[2] = dg * tc; sf32[3] = dg * td;
+    for (int n = 0; n < 4; ++n) {
+      uc[n] = (float)s.ucon[n]; ul[n] = (float)s.ucov[n]; bc[n] = (float)s.bbcon[n]; bl[n] = (float)s.bbcov[n];
     }
-  }
-  double uo[9];
-  if (STAGE > 1) {
-    double qn[9];
-    load9(Pn, N, c, qn);
-    PS sn;
-    pstate(qn, m, gam, sn);
-    p2c(sn, gam, m.detg, uo);
+    float ta = 0.f, tb = 0.f, tc = 0.f, td = 0.f;
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const float t = a * uc[mm] * ul[n] + (mm == n ? b : 0.f) - bc[mm] * bl[n];
+        ta = ta + t * __ldg(r.chr32 + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
+        tb = tb + t * __ldg(r.chr32 + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
+        tc = tc + t * __ldg(r.chr32 + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
+        td = td + t * __ldg(r.chr32 + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
+      }
+    const float dg = (float)m.detg;
+    sf[0] = dg * ta; sf[1] = dg * tb; sf[2] = dg * tc; sf[3] = dg * td;
   }
   const float a1 = (float)(dt / __ldg(r.dx1b + i - 1)), a2 = (float)(dt / __ldg(r.dx2b + j - 1)),
               a3 = (float)(dt / __ldg(r.dx3b + k - 1));
@@ -404,7 +383,11 @@ __device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met&
   const float wc = (STAGE == 1) ? 1.f : (STAGE == 2 ? 0.25f : 2.0f / 3.0f);
   const float wf = wc;
   const size_t ci = c - 1, cj = c - (size_t)r.imax, ck = c - (size_t)r.imax * r.jmax;
-  auto fd = [&](const double* A, size_t x, size_t xm) { return (float)A[x] - (float)A[xm]; };
+  const float* F1 = r.F32[0];
+  const float* F2 = r.F32[1];
+  const float* F3 = r.F32[2];
+  const float* CT = r.CT32;
+  auto fd = [&](const float* A, size_t x, size_t xm) { return A[x] - A[xm]; };
 #pragma unroll
   for (int v = 0; v < 9; ++v) {
     float d1, d2, d3;
@@ -420,20 +403,14 @@ __device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met&
     Acc32 acc;
     float hi, lo;
     if (STAGE > 1) {
-      split(uo[v], hi, lo);
+      split(r.Un[(size_t)v * N + c], hi, lo);
       acc.add_scaled(wo, hi, lo);
     }
     split(ucur[v], hi, lo);
     acc.add_scaled(wc, hi, lo);
-    acc.add(wf * (-(a1 * d1) - a2 * d2 - a3 * d3));
-    if (v >= 1 && v <= 4) {
-      if (fp64_src) {
-        split(sf64[v - 1] * dt, hi, lo);
-        acc.add_scaled(wf, hi, lo);
-      } else {
-        acc.add(wf * (sf32[v - 1] * fdt));
-      }
-    }
+    float inc = -(a1 * d1) - a2 * d2 - a3 * d3;
+    if (v >= 1 && v <= 4) inc = inc + sf[v - 1] * fdt;
+    acc.add(wf * inc);
     u[v] = acc.value();
   }
 }
@@ -450,15 +427,18 @@ __device__ __forceinline__ void queue_carry(const DevRun& r, int i, int j, int k
   else atomicAdd(r.cnt + C_CARRY_OVF, 1ull);
 }
 
+// One stage of every cell with radial index in [ilo, ihi]: interior cells get
+// the RK combine (FP64, or MIX = mixed precision for the cells beyond
+// r = 2 r_H) and recov1a; ghost cells copy their primitives through.
 template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                                                 double* __restrict__ Pw, const double* __restrict__ F1,
                                                 const double* __restrict__ F2, const double* __restrict__ F3,
-                                                const double* __restrict__ CT) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+                                                const double* __restrict__ CT, int ilo, int ihi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + ilo;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-  if (i > r.imax || j > r.jmax || k > r.kmax) return;
+  if (i > ihi || j > r.jmax || k > r.kmax) return;
   const size_t N = r.N, c = r.cell(i, j, k);
   // A finished run (time > tmax) copies its state through the stage so that the
   // host-side buffer rotation stays valid without a host synchronisation.
@@ -470,12 +450,12 @@ __global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restri
   Met m;
   load_met(r.mc, r.nik, r.ik(i, k), m);
   double u[9];
-  if (MIX) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
+  if (MIX) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pc, r.scal->dt, u);
   else stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
   double qo[9], qn[9];
   load9(Pc, N, c, qo);
   RecovOut o{0.0, false, false, false};
-  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.iter, r.dmin, r.pmin, __ldg(r.x1 + i - 1), nullptr, o);
+  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, __ldg(r.fl_de + i - 1), __ldg(r.fl_pr + i - 1), nullptr, o);
   if (!ok) {
     queue_carry(r, i, j, k);
   } else {
@@ -491,7 +471,7 @@ __global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restri
 // (k, j, i over the interior): each takes the final W of its predecessor cell.
 // One thread; runs only when cells were queued, which the reference data
 // rarely produces.  MODE 0: stage update; MODE 1: recov-only entry point.
-template <int MODE, int STAGE, bool MIX = false>
+template <int MODE, int STAGE>
 __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                             double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                             const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
@@ -521,11 +501,11 @@ __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const doubl
     Met m;
     load_met(r.mc, r.nik, r.ik(i, k), m);
     double u[9], qo[9], qn[9];
-    if (MODE == 0 && MIX) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, dt, u);
+    if (MODE == 0 && r.mixed && i > r.i_fp64) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pc, dt, u);
     else if (MODE == 0) stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, dt, u);
     else load9(U, r.N, c, u);
     load9(Pc, r.N, c, qo);
-    const bool ok = recov_cell(u, qo, qn, m, r.gam, r.iter, r.dmin, r.pmin, r.x1[i - 1], carry, o);
+    const bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, r.fl_de[i - 1], r.fl_pr[i - 1], carry, o);
     if (ok) {
       wg_out = o.wg;
       if (write)
@@ -569,10 +549,30 @@ __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const doubl
 // variables, flux and wave speeds in arithmetic type T, and the pair exchanges
 // them by warp shuffle for the LLF flux.  Lanes past the edge of the range work
 // on the last face and store nothing.  Both lanes of a pair always take the
-// same branch, so the shuffles run on the active mask.
-template <int D, int IREC, typename T>
-__device__ __forceinline__ void face_lane(const DevRun& r, const double* __restrict__ P, double* __restrict__ F,
-                                          int i, int j, int k, int side, bool valid) {
+// same branch, so the shuffles run on the active mask.  S is the storage type
+// of the primitives, metric cache and fluxes (double, or float for the FP32
+// half of the mixed path, which then reads and writes no FP64 array).  Fcopy,
+// if given, receives an FP32 copy of the fluxes of faces i <= icopy (the FP64
+// faces next to the FP32 region of the mixed path).
+template <int D, typename S>
+__device__ __forceinline__ const S* met_of(const DevRun& r);
+template <>
+__device__ __forceinline__ const double* met_of<1, double>(const DevRun& r) { return r.mi; }
+template <>
+__device__ __forceinline__ const double* met_of<2, double>(const DevRun& r) { return r.mc; }
+template <>
+__device__ __forceinline__ const double* met_of<3, double>(const DevRun& r) { return r.mk; }
+template <>
+__device__ __forceinline__ const float* met_of<1, float>(const DevRun& r) { return r.mi32; }
+template <>
+__device__ __forceinline__ const float* met_of<2, float>(const DevRun& r) { return r.mc32; }
+template <>
+__device__ __forceinline__ const float* met_of<3, float>(const DevRun& r) { return r.mk32; }
+
+template <int D, int IREC, typename T, typename S>
+__device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__ P, S* __restrict__ F,
+                                          float* __restrict__ Fcopy, int icopy, int i, int j, int k, int side,
+                                          bool valid) {
   const unsigned mask = __activemask();
   const size_t N = r.N, c = r.cell(i, j, k);
   const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.imax : (long long)r.imax * r.jmax);
@@ -594,7 +594,7 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const double* __restr
       if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       // owner cell f + side; the right state reads its stencil mirrored
       const long long sd = side ? -st : st;
-      const double* p = P + (size_t)v * N + c + side * st;
+      const S* p = P + (size_t)v * N + c + side * st;
       const T a2 = T(p[-2 * sd]), a1 = T(p[-sd]), u0 = T(p[0]), b1 = T(p[sd]), b2 = T(p[2 * sd]);
       if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? T(-1) : T(1));
       else q[v] = weno5_state(a2, a1, u0, b1, b2);
@@ -605,15 +605,13 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const double* __restr
     for (int v = 0; v < 9; ++v) q[v] = T(P[(size_t)v * N + c + side * st]);
   }
   MetT<T> m;
-  if (D == 1) load_met(r.mi, r.nik, r.ik(i, k), m);
-  else if (D == 2) load_met(r.mc, r.nik, r.ik(i, k), m);
-  else load_met(r.mk, r.nik, r.ik(i, k), m);
+  load_met(met_of<D, S>(r), r.nik, r.ik(i, k), m);
   const T gam = T(r.gam);
   T u[9], w[9], vp, vm;
   {
     PST<T> s;
     pstate(q, m, gam, s);
-    const T sr = ent_ratio(s, gam);
+    const T sr = ent_ratio(s, gam, r.gkind);
     p2c(s, gam, m.detg, u, sr);
     flux<D>(s, gam, m.detg, w, sr);
     wavespeed<D>(q, s, m, gam, vp, vm);
@@ -624,6 +622,7 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const double* __restr
   // calcha.f90:96-120 (cmink uses the R-state plus speed, calcha.f90:107)
   const T cmax = fmax3(T(0), vpR, vpL);
   const T cmin = (D == 3) ? fmin3(T(0), vpR, vmL) : fmin3(T(0), vmR, vmL);
+  const bool copy = Fcopy != nullptr && i <= icopy;
   // hll.f90:83-183
 #pragma unroll
   for (int v = 0; v < 9; ++v) {
@@ -640,16 +639,18 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const double* __restr
     else continue;  // NaN speeds: the reference keeps the previous ww
     if (mabs(f) < T(1.0e-40)) f = T(0);
     if ((r.guard & 2) && v == 5 + D) f = T(0);  // Toth: no flux of the normal field component
-    F[(size_t)v * N + c] = double(f);
+    F[(size_t)v * N + c] = S(f);
+    if (copy) Fcopy[(size_t)v * N + c] = float(f);
   }
 }
 
 // Faces with radial index i in [ilo, ihi] (and the hll range in j, k) in
-// arithmetic type T.  The FP64 path launches it once over the whole range;
-// the mixed path launches FP64 for r < 2 r_H (i <= r.i_fp64) and FP32 beyond.
-template <int D, int IREC, typename T>
-__global__ void __launch_bounds__(128) k_flux(DevRun r, const double* __restrict__ P, double* __restrict__ F,
-                                              int ilo, int ihi) {
+// arithmetic type T on storage S.  The FP64 path launches it once over the
+// whole range; the mixed path launches FP64 for r < 2 r_H (faces i <=
+// i_fp64 + 1, copied to FP32 up to i_fp64) and FP32 beyond.
+template <int D, int IREC, typename T, typename S>
+__global__ void __launch_bounds__(128) k_flux(DevRun r, const S* __restrict__ P, S* __restrict__ F,
+                                              float* __restrict__ Fcopy, int icopy, int ilo, int ihi) {
   if (!r.scal->active) return;
   const int nm0 = r.nm0;
   const int side = threadIdx.x & 1;
@@ -658,42 +659,51 @@ __global__ void __launch_bounds__(128) k_flux(DevRun r, const double* __restrict
   const int k0 = blockIdx.z * blockDim.z + threadIdx.z + nm0;
   const bool valid = i0 <= ihi && j0 <= r.jmax - nm0 && k0 <= r.kmax - nm0;
   const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(k0, r.kmax - nm0);
-  face_lane<D, IREC, T>(r, P, F, i, j, k, side, valid);
+  face_lane<D, IREC, T, S>(r, P, F, Fcopy, icopy, i, j, k, side, valid);
 }
 
 // ---------------------------------------------------------------- flux-CT
-// ct.f90:30-118 on nm1..n-nm1 in every dimension, in arithmetic type T.
-template <typename T>
-__global__ void __launch_bounds__(256) k_ct(DevRun r, const double* __restrict__ F1, const double* __restrict__ F2,
-                                            const double* __restrict__ F3, double* __restrict__ CT) {
+// ct.f90:30-118 on nm1..n-nm1 in every dimension (edges with i in [ilo, ihi]),
+// in arithmetic type T on flux storage S.  CTcopy, if given, receives an FP32
+// copy (the FP64 edges next to the FP32 region of the mixed path).
+template <typename T, typename S>
+__global__ void __launch_bounds__(256) k_ct(DevRun r, const S* __restrict__ F1, const S* __restrict__ F2,
+                                            const S* __restrict__ F3, S* __restrict__ CT,
+                                            float* __restrict__ CTcopy, int ilo, int ihi) {
   if (!r.scal->active) return;
   const int nm1 = r.nm1;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + nm1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + ilo;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + nm1;
   const int k = blockIdx.z * blockDim.z + threadIdx.z + nm1;
-  if (i > r.imax - nm1 || j > r.jmax - nm1 || k > r.kmax - nm1) return;
+  if (i > ihi || j > r.jmax - nm1 || k > r.kmax - nm1) return;
   const size_t N = r.N, c = r.cell(i, j, k);
   const size_t di = 1, dj = (size_t)r.imax, dk = (size_t)r.imax * r.jmax;
-  const double* fyx = F2 + 6 * N;  // ww(2,7)
-  const double* fzx = F3 + 6 * N;  // ww(3,7)
-  const double* fxy = F1 + 7 * N;  // ww(1,8)
-  const double* fzy = F3 + 7 * N;  // ww(3,8)
-  const double* fxz = F1 + 8 * N;  // ww(1,9)
-  const double* fyz = F2 + 8 * N;  // ww(2,9)
-  auto L = [](const double* a, size_t x) { return T(a[x]); };
+  const S* fyx = F2 + 6 * N;  // ww(2,7)
+  const S* fzx = F3 + 6 * N;  // ww(3,7)
+  const S* fxy = F1 + 7 * N;  // ww(1,8)
+  const S* fzy = F3 + 7 * N;  // ww(3,8)
+  const S* fxz = F1 + 8 * N;  // ww(1,9)
+  const S* fyz = F2 + 8 * N;  // ww(2,9)
+  auto L = [](const S* a, size_t x) { return T(a[x]); };
   const T e = T(1.0) / T(8.0), two = T(2.0);
-  CT[0 * N + c] = double(e * (two * L(fyx, c) + L(fyx, c + di) + L(fyx, c - di) - L(fxy, c) - L(fxy, c + dj) -
-                              L(fxy, c - di) - L(fxy, c - di + dj)));
-  CT[1 * N + c] = double(e * (two * L(fzx, c) + L(fzx, c + di) + L(fzx, c - di) - L(fxz, c) - L(fxz, c + dk) -
-                              L(fxz, c - di) - L(fxz, c - di + dk)));
-  CT[2 * N + c] = double(e * (two * L(fxy, c) + L(fxy, c + dj) + L(fxy, c - dj) - L(fyx, c) - L(fyx, c + di) -
-                              L(fyx, c - dj) - L(fyx, c + di - dj)));
-  CT[3 * N + c] = double(e * (two * L(fzy, c) + L(fzy, c + dj) + L(fzy, c - dj) - L(fyz, c) - L(fyz, c + dk) -
-                              L(fyz, c - dj) - L(fyz, c - dj + dk)));
-  CT[4 * N + c] = double(e * (two * L(fxz, c) + L(fxz, c + dk) + L(fxz, c - dk) - L(fzx, c) - L(fzx, c + di) -
-                              L(fzx, c - dk) - L(fzx, c + di - dk)));
-  CT[5 * N + c] = double(e * (two * L(fyz, c) + L(fyz, c + dk) + L(fyz, c - dk) - L(fzy, c) - L(fzy, c + dj) -
-                              L(fzy, c - dk) - L(fzy, c + dj - dk)));
+  T o[6];
+  o[0] = e * (two * L(fyx, c) + L(fyx, c + di) + L(fyx, c - di) - L(fxy, c) - L(fxy, c + dj) - L(fxy, c - di) -
+              L(fxy, c - di + dj));
+  o[1] = e * (two * L(fzx, c) + L(fzx, c + di) + L(fzx, c - di) - L(fxz, c) - L(fxz, c + dk) - L(fxz, c - di) -
+              L(fxz, c - di + dk));
+  o[2] = e * (two * L(fxy, c) + L(fxy, c + dj) + L(fxy, c - dj) - L(fyx, c) - L(fyx, c + di) - L(fyx, c - dj) -
+              L(fyx, c + di - dj));
+  o[3] = e * (two * L(fzy, c) + L(fzy, c + dj) + L(fzy, c - dj) - L(fyz, c) - L(fyz, c + dk) - L(fyz, c - dj) -
+              L(fyz, c - dj + dk));
+  o[4] = e * (two * L(fxz, c) + L(fxz, c + dk) + L(fxz, c - dk) - L(fzx, c) - L(fzx, c + di) - L(fzx, c - dk) -
+              L(fzx, c + di - dk));
+  o[5] = e * (two * L(fyz, c) + L(fyz, c + dk) + L(fyz, c - dk) - L(fzy, c) - L(fzy, c + dj) - L(fzy, c - dk) -
+              L(fzy, c + dj - dk));
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    CT[(size_t)a * N + c] = S(o[a]);
+    if (CTcopy) CTcopy[(size_t)a * N + c] = float(o[a]);
+  }
 }
 
 // ------------------------------------------------------------ boundaries
@@ -794,15 +804,13 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
   load9(P, N, c, q);
   Met m;
   load_met(r.mc, r.nik, r.ik(i, k), m);
-  const double gam = r.gam, rr = __ldg(r.x1 + i - 1);
+  const double gam = r.gam;
   if (r.model >= 7 && r.model <= 20 && i > r.imax - r.nm1) {
     const double gflmax = 10.0;
     double gfl = calgfl(q[1], q[2], q[3], m);
     double vel[4] = {0.0, q[1] * (1. / gfl), q[2] * (1. / gfl), q[3] * (1. / gfl)};
     if (vel[1] < 0.0) {
-      const double alpha1 = 1. / sqrt(-m.c00);
-      const double b1 = alpha1 * alpha1 * m.c01;
-      vel[1] = b1 * (1. / alpha1);
+      vel[1] = m.be1 * m.ial;  // beta^r / alpha
       double vsq = qform3(m, vel[1], vel[2], vel[3]);
       if (vsq >= 1.0) vsq = 1. - 1. / (gflmax * gflmax);
       gfl = 1. / sqrt(1. - vsq);
@@ -811,8 +819,8 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
   }
   if (r.model >= 7 && r.model <= 15) {
     const double epsilon = 1.e-2, gflmax = 10.0;
-    const double demin = r.dmin * pow(rr, -1.5);
-    const double prmin = (gam - 1.) * r.pmin * pow(rr, -2.5);
+    const double demin = __ldg(r.fl_de + i - 1);
+    const double prmin = __ldg(r.fl_pr + i - 1);
     const double dthe = 1.0 * (1. + epsilon) * demin;
     const double dthe1 = 1.0 * (1. + epsilon) * prmin;
     const double bsq = q[6] * q[6] + q[7] * q[7] + q[8] * q[8];
@@ -860,8 +868,8 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
     if (capped) atomicAdd(r.cnt + C_FLOORCAP, 1ull);
     if (de != q[0]) q[0] = de;
     else if (pr != q[4]) q[4] = pr;
-    const double demin = r.dmin * pow(rr, -1.5);
-    const double prmin = (gam - 1.) * r.pmin * pow(rr, -2.5);
+    const double demin = __ldg(r.fl_de + i - 1);
+    const double prmin = __ldg(r.fl_pr + i - 1);
     const double bbromax = 50.0, bbprmax = 2.e3, prromax = 1.e6;
     if (pr < prmin) q[4] = prmin;
     if (pr > r.pmax) q[4] = r.pmax;
@@ -875,6 +883,15 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
   }
 #pragma unroll
   for (int v = 0; v < 6; ++v) P[(size_t)v * N + c] = q[v];
+  if (r.P32)  // FP32 copy of the final primitives for the next stage's FP32 faces
+#pragma unroll
+    for (int v = 0; v < 9; ++v) r.P32[(size_t)v * N + c] = (float)q[v];
+}
+
+// FP32 copy of a primitive array (mixed runs, after initial data or upload).
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+  const size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x < n) b[x] = (float)a[x];
 }
 
 // ------------------------------------------------------------------- CFL
@@ -966,7 +983,7 @@ __global__ void __launch_bounds__(128) k_recov(DevRun r, const double* __restric
   load9(U, N, c, u);
   load9(Pc, N, c, qo);
   RecovOut o{0.0, false, false, false};
-  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.iter, r.dmin, r.pmin, __ldg(r.x1 + i - 1), nullptr, o);
+  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, __ldg(r.fl_de + i - 1), __ldg(r.fl_pr + i - 1), nullptr, o);
   if (!ok) queue_carry(r, i, j, k);
   else
 #pragma unroll
@@ -989,7 +1006,7 @@ __global__ void __launch_bounds__(128) k_p2c(DevRun r, const double* __restrict_
   load_met(r.mc, r.nik, r.ik(i, k), m);
   PS s;
   pstate(q, m, r.gam, s);
-  p2c(s, r.gam, m.detg, u);
+  p2c(s, r.gam, r.gkind, m.detg, u);
 #pragma unroll
   for (int v = 0; v < 9; ++v) U[(size_t)v * N + c] = u[v];
 }
@@ -1010,6 +1027,27 @@ __global__ void k_soa_to_aos(const double* __restrict__ s, double* __restrict__ 
 __global__ void k_fill(double* p, double v, size_t n) {
   const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c < n) p[c] = v;
+}
+
+// Derived metric fields (met_derive) of every point of the three caches and
+// the radial floor profiles of atmosphere1a/pminmax2b (correction.f90:897-898).
+__global__ void k_geom_derive(DevRun r, double* mc, double* mi, double* mk, double* fl_de, double* fl_pr) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < r.nik) {
+    double* caches[3] = {mc, mi, mk};
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) {
+      double base[kMetBase], d[kMetComps - kMetBase];
+      for (int c = 0; c < kMetBase; ++c) base[c] = caches[a][(size_t)c * r.nik + q];
+      met_derive(base, d);
+      for (int c = 0; c < kMetComps - kMetBase; ++c) caches[a][(size_t)(kMetBase + c) * r.nik + q] = d[c];
+    }
+  }
+  if (q < (size_t)r.imax) {
+    const double rr = r.x1[q];
+    fl_de[q] = r.dmin * pow(rr, -1.5);
+    fl_pr[q] = (r.gam - 1.) * r.pmin * pow(rr, -2.5);
+  }
 }
 
 inline dim3 grid3(int nx, int ny, int nz, dim3 b) {
@@ -1039,70 +1077,111 @@ cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <typename T>
-static void launch_flux_t(const DevRun& r, int dir, const double* P, double* F, int ilo, int ihi, cudaStream_t s) {
+template <typename T, typename S>
+static void launch_flux_t(const DevRun& r, int dir, const S* P, S* F, float* Fcopy, int icopy, int ilo, int ihi,
+                          cudaStream_t s) {
   if (ihi < ilo) return;
   const int n = ihi - ilo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b(64, 2, 1);
   const dim3 g = grid3(2 * n, m, l, b);  // two lanes per face
   if (r.irec == 5) {
-    if (dir == 1) k_flux<1, 5, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
-    else if (dir == 2) k_flux<2, 5, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
-    else k_flux<3, 5, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    if (dir == 1) k_flux<1, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+    else if (dir == 2) k_flux<2, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+    else k_flux<3, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
   } else if (r.irec == 6) {
-    if (dir == 1) k_flux<1, 6, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
-    else if (dir == 2) k_flux<2, 6, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
-    else k_flux<3, 6, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    if (dir == 1) k_flux<1, 6, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+    else if (dir == 2) k_flux<2, 6, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+    else k_flux<3, 6, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
   } else {
-    if (dir == 1) k_flux<1, 7, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
-    else if (dir == 2) k_flux<2, 7, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
-    else k_flux<3, 7, T><<<g, b, 0, s>>>(r, P, F, ilo, ihi);
+    if (dir == 1) k_flux<1, 7, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+    else if (dir == 2) k_flux<2, 7, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+    else k_flux<3, 7, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
   }
+}
+
+// Radial index of the last FP64 cell of a mixed run, clamped to [lo-1, hi].
+static int fp64_split(const DevRun& r, int lo, int hi) {
+  return r.i_fp64 < lo ? lo - 1 : (r.i_fp64 > hi ? hi : r.i_fp64);
 }
 
 cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s) {
   const int lo = r.nm0, hi = r.imax - r.nm0;
   if (!r.mixed) {
-    launch_flux_t<double>(r, dir, P, F, lo, hi, s);
+    launch_flux_t<double, double>(r, dir, P, F, nullptr, 0, lo, hi, s);
   } else {
-    const int split = r.i_fp64 < lo ? lo - 1 : (r.i_fp64 > hi ? hi : r.i_fp64);
-    launch_flux_t<double>(r, dir, P, F, lo, split, s);
-    launch_flux_t<float>(r, dir, P, F, split + 1, hi, s);
+    // FP64 faces up to i_fp64 + 1 (flux-CT of the last FP64 edges reads them),
+    // copied to FP32 up to i_fp64; FP32 faces from i_fp64 + 1 on.
+    const int split = fp64_split(r, lo, hi);
+    if (split >= lo)
+      launch_flux_t<double, double>(r, dir, P, F, r.F32[dir - 1], split, lo, split < hi ? split + 1 : hi, s);
+    launch_flux_t<float, float>(r, dir, r.P32, r.F32[dir - 1], nullptr, 0, split + 1, hi, s);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
                       cudaStream_t s) {
-  const int n = r.imax - 2 * r.nm1 + 1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
+  const int lo = r.nm1, hi = r.imax - r.nm1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
   const dim3 b(64, 4, 1);
-  if (r.mixed) k_ct<float><<<grid3(n, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT);
-  else k_ct<double><<<grid3(n, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT);
+  if (!r.mixed) {
+    k_ct<double, double><<<grid3(hi - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, nullptr, lo, hi);
+  } else {
+    const int split = fp64_split(r, lo, hi);
+    if (split >= lo)
+      k_ct<double, double><<<grid3(split - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, r.CT32, lo, split);
+    if (split < hi)
+      k_ct<float, float><<<grid3(hi - split, m, l, b), b, 0, s>>>(r, r.F32[0], r.F32[1], r.F32[2], r.CT32,
+                                                                     nullptr, split + 1, hi);
+  }
   return cudaGetLastError();
 }
 
 template <bool MIX>
 static void launch_update_t(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
-                            const double* F1, const double* F2, const double* F3, const double* CT, dim3 g, dim3 b,
-                            cudaStream_t s) {
-  if (stage == 1) {
-    k_update<1, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
-    k_carry_fix<0, 1, MIX><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  } else if (stage == 2) {
-    k_update<2, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
-    k_carry_fix<0, 2, MIX><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  } else {
-    k_update<3, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
-    k_carry_fix<0, 3, MIX><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  }
+                            const double* F1, const double* F2, const double* F3, const double* CT, int ilo,
+                            int ihi, cudaStream_t s) {
+  if (ihi < ilo) return;
+  const dim3 b(64, 2, 1);
+  const dim3 g = grid3(ihi - ilo + 1, r.jmax, r.kmax, b);
+  if (stage == 1) k_update<1, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
+  else if (stage == 2) k_update<2, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
+  else k_update<3, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
 }
 
 cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                           const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s) {
-  const dim3 b(64, 2, 1);
-  const dim3 g = grid3(r.imax, r.jmax, r.kmax, b);
-  if (r.mixed) launch_update_t<true>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, g, b, s);
-  else launch_update_t<false>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, g, b, s);
+  if (!r.mixed) {
+    launch_update_t<false>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, 1, r.imax, s);
+  } else {
+    const int split = fp64_split(r, 1, r.imax);
+    launch_update_t<false>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, 1, split, s);
+    launch_update_t<true>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, split + 1, r.imax, s);
+  }
+  if (stage == 1) k_carry_fix<0, 1><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  else if (stage == 2) k_carry_fix<0, 2><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  else k_carry_fix<0, 3><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  return cudaGetLastError();
+}
+
+// Launches issued by launch_flux (per direction), launch_ct and launch_update.
+int n_flux_launches(const DevRun& r) {
+  if (!r.mixed) return 1;
+  const int lo = r.nm0, hi = r.imax - r.nm0, split = fp64_split(r, lo, hi);
+  return (split >= lo) + (split < hi);
+}
+int n_ct_launches(const DevRun& r) {
+  if (!r.mixed) return 1;
+  const int lo = r.nm1, hi = r.imax - r.nm1, split = fp64_split(r, lo, hi);
+  return (split >= lo) + (split < hi);
+}
+int n_update_launches(const DevRun& r) {
+  if (!r.mixed) return 2;
+  const int split = fp64_split(r, 1, r.imax);
+  return (split >= 1) + (split < r.imax) + 1;
+}
+
+cudaError_t launch_to_f32(const double* a, float* b, size_t n, cudaStream_t s) {
+  k_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, b, n);
   return cudaGetLastError();
 }
 
@@ -1153,6 +1232,12 @@ cudaError_t launch_aos_to_soa(const double* aos, double* soa, size_t N, cudaStre
 }
 cudaError_t launch_soa_to_aos(const double* soa, double* aos, size_t N, cudaStream_t s) {
   k_soa_to_aos<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(soa, aos, N);
+  return cudaGetLastError();
+}
+cudaError_t launch_geom_derive(const DevRun& r, double* mc, double* mi, double* mk, double* fl_de, double* fl_pr,
+                               cudaStream_t s) {
+  const size_t n = r.nik > (size_t)r.imax ? r.nik : (size_t)r.imax;
+  k_geom_derive<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(r, mc, mi, mk, fl_de, fl_pr);
   return cudaGetLastError();
 }
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s) {

@@ -32,5 +32,12 @@ cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t
 cudaError_t launch_aos_to_soa(const double* aos, double* soa, size_t N, cudaStream_t s);
 cudaError_t launch_soa_to_aos(const double* soa, double* aos, size_t N, cudaStream_t s);
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s);
+int n_flux_launches(const DevRun& r);
+int n_ct_launches(const DevRun& r);
+int n_update_launches(const DevRun& r);
+cudaError_t launch_to_f32(const double* a, float* b, size_t n, cudaStream_t s);
+// derived metric fields of the three caches and the radial floor profiles (run setup)
+cudaError_t launch_geom_derive(const DevRun& r, double* mc, double* mi, double* mk, double* fl_de, double* fl_pr,
+                               cudaStream_t s);
 
 }  // namespace rg

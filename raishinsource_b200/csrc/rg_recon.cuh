@@ -109,11 +109,11 @@ __device__ __forceinline__ T ppm_face(T u0, T u1, T dma0, T dma1, T dxm, T dx0, 
   return u0 + t2 + t3 - t4 * dma1 + t5 * dma0;
 }
 
-// Both face states of the cell at p (primitive v at p[v*N], FP64 storage),
+// Both face states of the cell at p (primitive v at p[v*N], storage type S),
 // stride st along direction D; dx[o+4], x[o+4] are the shifted spacing and
 // centre at offset o from the cell.  gam enters the contact test (rec.f90:1623).
-template <int D, typename T>
-__device__ void ppm_cell(const double* __restrict__ p, size_t N, long long st, const T dx[9], const T x[9], T gam,
+template <int D, typename T, typename S>
+__device__ void ppm_cell(const S* __restrict__ p, size_t N, long long st, const T dx[9], const T x[9], T gam,
                          T L[9], T R[9]) {
   auto U = [&](int v, int o) { return T(p[(size_t)v * N + o * st]); };
   auto DX = [&](int o) { return dx[o + 4]; };

@@ -6,9 +6,20 @@
 
 #include "../../include/raishin_gpu.h"
 
+#ifdef __CUDACC__
+#define RG_HD __host__ __device__
+#else
+#define RG_HD
+#endif
+
 namespace rg {
 
 constexpr int NV = 9;
+
+// Metric cache components per (i,k) point: the host stores the first
+// kMetBase (gcov, gcon blocks, sqrt(-g)); k_met_derive fills the rest.
+constexpr int kMetBase = 18;
+constexpr int kMetComps = 26;
 
 // Device scalars of a run (one small block of device memory).
 struct Scal {
@@ -34,6 +45,7 @@ struct DevRun {
   int nm0, nm1;
   int irec, model, guard, iter;
   int mixed;             // 1: FP32 reconstruction/fluxes/CT/RK combine (RG_MIXED)
+  int gkind;             // x**gam form: 1 gam == 4/3, 2 gam == 5/3 (cube roots), 0 pow
   int i_fp64;            // radial cells 1..i_fp64 (r < 2 r_H) keep FP64 in the mixed path
   int nmax_cfl;          // nm1*2 + (nm1-1) (cdtcfl.f90:38)
   size_t N;              // cells
@@ -49,6 +61,17 @@ struct DevRun {
   const double* dx3b;
   const double* x2;      // phi centres (PPM contact detection)
   const double* x3;      // theta centres
+  const double* fl_de;   // density floor dmin * x1(i)**(-1.5) (correction.f90:897), index i-1
+  const double* fl_pr;   // pressure floor (gam-1) * pmin * x1(i)**(-2.5) (correction.f90:898), index i-1
+  double* Un;            // conserved variables of the step's initial primitives (9*N), written in stage 1
+  // FP32 arrays of the mixed path (null for FP64 runs)
+  const float* mc32;     // FP32 copies of the metric caches
+  const float* mi32;
+  const float* mk32;
+  const float* chr32;    // FP32 copy of the Christoffel symbols
+  float* P32;            // FP32 copy of the current primitives (written by the floor pass)
+  float* F32[3];         // FP32 face fluxes per direction, 9*N each
+  float* CT32;           // FP32 flux-CT values, 6*N
   const double* dx1s;    // rec2's shifted dx1b: dummy dx1b(i) = actual dx1b(i-1), index i-1
   const double* dx2s;
   const double* dx3s;
@@ -58,10 +81,10 @@ struct DevRun {
   int* carry_list;       // interior cells queued for the W carry fix-up
   int carry_cap;
 
-  __host__ __device__ size_t cell(int i, int j, int k) const {
+  RG_HD size_t cell(int i, int j, int k) const {
     return (size_t)(i - 1) + (size_t)imax * ((size_t)(j - 1) + (size_t)jmax * (size_t)(k - 1));
   }
-  __host__ __device__ size_t ik(int i, int k) const { return (size_t)(i - 1) + (size_t)imax * (size_t)(k - 1); }
+  RG_HD size_t ik(int i, int k) const { return (size_t)(i - 1) + (size_t)imax * (size_t)(k - 1); }
 };
 
 }  // namespace rg
