@@ -1,14 +1,26 @@
-"""Benchmark: zone-updates/s of the FP64 GRMHD update on one B200 (and N replicas).
+"""Benchmark: zone-updates/s of the GRMHD update on one B200 (and N replicas).
 
-Workload (default): the 3D Fishbone-Moncrief torus of the reference's
-configuration 1: 256 (r) x 128 (theta) x 128 (phi) cells including ghosts,
-modified Kerr-Schild (a = 0.9375), MP5 + HLLE(LLF) + flux-CT + RK3, CFL 0.4,
-FP64, with the positivity fallback on (guard bit 1; with reference semantics
-MP5 drives face densities negative at the torus surface and the entropy flux
-turns NaN).  One step = one full RK3 step over all interior cells; a zone-
-update is one interior cell advanced by one step.  Data are synthetic (the
-torus is generated, seeded); the state (~0.3 GB per copy) exceeds the 126 MB
-L2, so no flush is needed between steps.
+Headline workload: the 3D Fishbone-Moncrief torus of 256 (r) x 128 (theta) x
+128 (phi) cells including ghosts, modified Kerr-Schild (a = 0.9375), MP5 +
+HLLE(LLF) + flux-CT + RK3, CFL 0.4, FP64, with the positivity fallback on
+(guard bit 1; with reference semantics MP5 drives face densities negative at
+the torus surface and the entropy flux turns NaN).  One step = one full RK3
+step over all interior cells; a zone-update is one interior cell advanced by
+one step.  Data are synthetic (seeded torus initial data); the state (~0.3 GB
+per copy) exceeds the 126 MB L2, so no flush is needed between steps.
+
+Extra sections of the same JSON line (N = 1 only; each 0 flag skips one):
+  mixed          FP32-mixed vs FP64 on the 384 x 192 x 192 torus: both timed
+                 over --mixed-steps steps from the same initial data, L1/Linf
+                 errors of rho, p and B and the error of the horizon mass and
+                 energy accretion rates of the mixed state against the FP64
+                 state after those steps.
+  torus2d        the 2D torus (256 x 256, phi slab) in FP64, 1000 steps.
+  batched_tubes  1024 seeded 1D RMHD Riemann tubes of 400-3200 cells run to
+                 t = 0.4 in one batch (rg_step_batch), FP64 and FP32-mixed.
+  serving        a seeded Poisson stream of 2D tori (grids 128^2..512^2, half
+                 FP64, half mixed, 2000 steps each) served with continuous
+                 batching: p50/p99 latency and aggregate zone-updates/s.
 
 Arms:
   default            GPU arm through the C ABI (value = device-resident steps;
@@ -184,7 +196,6 @@ def run_gpu(args) -> dict | None:
     ms = max_over_ranks(e0.elapsed_time(e1))
     launches = sum(v["launches"] for v in ctx.profile_read().values())
     st = run.stats()
-    ref_prims = run.prims() if args.mixed else None  # FP64 state after warm-up + timed steps
 
     # end to end through the public API with host buffers (pinned)
     e2e = None
@@ -207,43 +218,6 @@ def run_gpu(args) -> dict | None:
         e2e = {"value": zones * ws * args.e2e_steps / (e_ms * 1e-3), "unit": "zone-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
                "ms_per_step": e_ms / args.e2e_steps, "api": "rg_run_upload_prims + rg_step + rg_run_download_prims"}
-
-    # FP32-mixed run of the same workload: same IC, same number of steps; timed
-    # like the FP64 arm, L1 error of its state against the FP64 state at the end
-    mixed = None
-    if args.mixed:
-        ref_steps = args.warmup + args.steps
-        runm = ctx.admit(dict(p, precision="mixed"))
-        runm.ic_torus(seed=2012 + rank)
-        runm.step(args.warmup)
-        torch.cuda.synchronize()
-        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        m0.record(stream)
-        runm.step(args.steps)
-        m1.record(stream)
-        torch.cuda.synchronize()
-        mms = max_over_ranks(m0.elapsed_time(m1))
-        got = runm.prims()
-        mshares = {}
-        if args.prof_steps > 0:
-            ctx.profile(True)
-            runm.step(args.prof_steps)
-            mp = ctx.profile_read()
-            ctx.profile(False)
-            mt = sum(v["ms"] for v in mp.values())
-            mshares = {k: round(v["ms"] / mt, 4) for k, v in mp.items()}
-        runm.release()
-        n = run.nm1
-        sl = (slice(n, -n),) * 3
-        l1 = (np.abs(got[sl] - ref_prims[sl]).sum(axis=(0, 1, 2)) /
-              np.abs(ref_prims[sl]).sum(axis=(0, 1, 2)).clip(1e-300))
-        mixed = {"value": zones * ws * args.steps / (mms * 1e-3), "unit": "zone-updates/s",
-                 "ms_per_step": mms / args.steps, "speedup_vs_fp64": ms / mms,
-                 "l1_rel_vs_fp64": {"rho": float(l1[0]), "p": float(l1[4]), "B1": float(l1[6]),
-                                    "B3": float(l1[8])},
-                 "after_steps": ref_steps, "kernel_share": mshares,
-                 "precision": "FP32 recon/LLF/CT/RK combine (compensated), FP64 recovery/floors/CFL, "
-                              "FP64 fluxes and sources for r < 2 r_H"}
 
     # per-kernel device times (separate pass: CUDA events around every launch on the library stream)
     roofline, shares = None, {}
@@ -271,6 +245,16 @@ def run_gpu(args) -> dict | None:
                     "bytes_per_unit": BYTES_PER_UNIT[top], "units_per_launch": u, "ms_per_launch": per_launch_ms,
                     "note": "FP64-pipe bound path: HBM fraction of algorithmic bytes, see profiles/"}
     run.release()
+    extra = {}
+    if ws == 1:
+        if args.mixed_steps > 0:
+            extra["mixed"] = section_mixed(ctx, args)
+        if args.torus2d_steps > 0:
+            extra["torus2d"] = section_torus2d(ctx, args)
+        if args.tubes > 0:
+            extra["batched_tubes"] = section_tubes(ctx, args)
+        if args.serve_requests > 0:
+            extra["serving"] = section_serving(ctx, args)
     ctx.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
@@ -283,12 +267,157 @@ def run_gpu(args) -> dict | None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Fishbone-Moncrief torus initial data)",
         "config": dict(config_block(args, p), parallelism=f"replicas x{ws}"),
-        "e2e": e2e, "mixed": mixed, "gpu_launches": launches, "clocks": clk.summary(),
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         "roofline": roofline,
         "kernel_share": shares,
         "recov": {k: st[k] for k in ("recov_nr2", "recov_fail", "recov_carry", "recov_cap")},
     }
+    line.update(extra)
     return line
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _rel_errs(got, ref, n):
+    """Interior L1 (sum |a-b| / sum |b|) and Linf (max |a-b| / max |b|) per variable."""
+    import numpy as np
+    sl = (slice(n, -n),) * 3
+    a, b = got[sl], ref[sl]
+    d = np.abs(a - b)
+    l1 = d.sum(axis=(0, 1, 2)) / np.abs(b).sum(axis=(0, 1, 2)).clip(1e-300)
+    linf = d.max(axis=(0, 1, 2)) / np.abs(b).max(axis=(0, 1, 2)).clip(1e-300)
+    names = {"rho": 0, "p": 4, "B1": 6, "B2": 7, "B3": 8}
+    return ({k: float(l1[v]) for k, v in names.items()}, {k: float(linf[v]) for k, v in names.items()})
+
+
+def section_mixed(ctx, args) -> dict:
+    """FP64 and FP32-mixed runs of the same torus from the same initial data."""
+    import torch
+    from raishinsource_b200 import config
+    nr, nth, nph = (int(x) for x in args.mixed_grid.split(","))
+    p = dict(config.torus(nr=nr, nth=nth, nph=nph), guard=args.guard)
+    zones = config.interior_cells(p)
+    stream = torch.cuda.current_stream()
+    out = {"workload": f"fm_torus_3d_{nr}x{nth}x{nph}_mp5", "steps": args.mixed_steps, "interior_cells": zones}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        r = ctx.admit(dict(p, precision=prec))
+        r.ic_torus(seed=2012)
+        r.step(3)  # first use of every kernel; counted in the comparison below
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record(stream)
+        r.step(args.mixed_steps - 3)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = r.stats()
+        states[prec] = (r.prims(), r.horizon_flux(), st)
+        out[prec] = {"value": zones * (args.mixed_steps - 3) / (ms * 1e-3), "unit": "zone-updates/s",
+                     "ms_per_step": ms / (args.mixed_steps - 3), "time": st["time"],
+                     "recov_nr2": st["recov_nr2"], "recov_fail": st["recov_fail"]}
+        r.release()
+    (a, (ma, ea), _), (b, (mb, eb), _) = states["mixed"], states["fp64"]
+    l1, linf = _rel_errs(a, b, config.ghost_widths(p["irec"])[1])
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["l1_rel_mixed_vs_fp64"] = l1
+    out["linf_rel_mixed_vs_fp64"] = linf
+    out["horizon"] = {"mdot_fp64": mb, "mdot_mixed": ma, "edot_fp64": eb, "edot_mixed": ea,
+                      "mdot_rel_err": abs(ma - mb) / max(abs(mb), 1e-300),
+                      "edot_rel_err": abs(ea - eb) / max(abs(eb), 1e-300)}
+    out["precision"] = ("FP32 reconstruction, LLF fluxes, flux-CT and RK combine (compensated accumulation) "
+                        "beyond 2 r_H; FP64 recovery, floors, CFL, metric and sources inside 2 r_H")
+    return out
+
+
+def section_torus2d(ctx, args) -> dict:
+    import torch
+    from raishinsource_b200 import config
+    p = dict(config.torus(nr=256, nth=256), guard=args.guard)
+    zones = config.interior_cells(p)
+    r = ctx.admit(p)
+    r.ic_torus(seed=2012)
+    r.step(5)
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    stream = torch.cuda.current_stream()
+    e0.record(stream)
+    r.step(args.torus2d_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    r.release()
+    return {"workload": "fm_torus_2d_256x256_mp5_fp64 (phi slab of 9 stored as one plane)", "steps": args.torus2d_steps,
+            "value": zones * args.torus2d_steps / (ms * 1e-3), "unit": "zone-updates/s",
+            "ms_per_step": ms / args.torus2d_steps}
+
+
+def section_tubes(ctx, args) -> dict:
+    """Seeded Riemann tubes in one batch, run to t = tmax, FP64 and mixed."""
+    import numpy as np
+    import torch
+    from raishinsource_b200 import config
+    rng = np.random.default_rng(2012)
+    lengths = rng.integers(400, 3201, size=args.tubes)
+    out = {"tubes": args.tubes, "lengths": [int(lengths.min()), int(lengths.max())], "tmax": args.tube_tmax}
+    finals = {}
+    for prec in ("fp64", "mixed"):
+        runs = []
+        for t, n in enumerate(lengths):
+            r = ctx.admit(config.tube(n=int(n), tmax=args.tube_tmax, precision=prec))
+            r.ic_tube(seed=2012, tube=t)
+            runs.append(r)
+        stream = torch.cuda.current_stream()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0, e1 = _events()
+        e0.record(stream)
+        chunk, steps, done_at = 64, 0, {}
+        while True:
+            st = ctx.step_batch(runs, chunk, stats=True)
+            steps += chunk
+            now = time.perf_counter() - t0
+            for k, x in enumerate(st):
+                if k not in done_at and x["time"] > args.tube_tmax:
+                    done_at[k] = now
+            if len(done_at) == len(runs):
+                break
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        zu = sum(x["steps"] * int(n) for x, n in zip(st, lengths))
+        info = ctx.batch_info(runs)
+        lat = np.array(sorted(done_at.values()))
+        out[prec] = {"value": zu / (ms * 1e-3), "unit": "zone-updates/s", "zone_updates": int(zu),
+                     "batch_steps": steps, "wall_ms": ms, "p50_run_latency_s": float(np.percentile(lat, 50)),
+                     "p99_run_latency_s": float(np.percentile(lat, 99)), "tuned": info,
+                     "floor_caps": int(sum(x["floor_cap"] for x in st))}
+        finals[prec] = [r.prims()[4, 4, :, 0] for r in runs]  # rho along the tube
+        for r in runs:
+            r.release()
+    num = sum(np.abs(a - b).sum() for a, b in zip(finals["mixed"], finals["fp64"]))
+    den = sum(np.abs(b).sum() for b in finals["fp64"])
+    out["l1_rel_rho_mixed_vs_fp64"] = float(num / den)
+    return out
+
+
+def section_serving(ctx, args) -> dict:
+    from raishinsource_b200 import serving
+    import torch
+    reqs = serving.poisson_stream(args.serve_requests, rate=args.serve_rate, seed=2012, steps=args.serve_steps)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(args.serve_budget_gb * 2**30, 0.8 * free))
+    srv = serving.Server(ctx, mem_budget=budget, max_runs=64, tick_steps=50)
+    res = srv.serve(reqs)
+    srv.close()
+    res.pop("done")
+    res.update({"arrival_rate_per_s": args.serve_rate, "steps_per_request": args.serve_steps,
+                "mem_budget_gb": budget / 2**30, "unit": "zone-updates/s",
+                "grids": [128, 256, 384, 512], "mix": "half FP64, half FP32-mixed"})
+    return res
 
 
 def time_reference(args, steps: int, label_cores=None) -> dict:
@@ -323,7 +452,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--prof-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=1, help="steps in the CPU-baseline sample (0 = skip)")
-    ap.add_argument("--mixed", type=int, default=1, help="also time the FP32-mixed path (1) or not (0)")
+    ap.add_argument("--mixed-steps", type=int, default=1000, help="steps of the FP64-vs-mixed section (0 = skip)")
+    ap.add_argument("--mixed-grid", default="384,192,192", help="imax,kmax,jmax of the mixed section")
+    ap.add_argument("--torus2d-steps", type=int, default=1000, help="steps of the 2D torus section (0 = skip)")
+    ap.add_argument("--tubes", type=int, default=1024, help="Riemann tubes of the batched section (0 = skip)")
+    ap.add_argument("--tube-tmax", type=float, default=0.4)
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving section (0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serve-steps", type=int, default=2000)
+    ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="device memory budget for admission")
     args = ap.parse_args()
     ws, rank, _ = dist_env()
     if args.impl == "reference":

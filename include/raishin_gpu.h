@@ -58,7 +58,17 @@ typedef struct rg_run_params {
                     bit 2: zero flux of the normal B component before flux-CT (Toth 2000),
                     which the reference's LLF term breaks (hll.f90:109).  Not in the reference. */
   int precision; /* rg_precision */
+  int flags;     /* RG_FLAG_* bits */
 } rg_run_params;
+
+/* rg_run_params.flags.  A direction of extent 2*nm1+1 (one interior cell)
+ * whose ghost fills copy that cell (periodic or copy codes) and on which the
+ * metric does not depend (phi; theta in Minkowski space) holds one state along
+ * it: the reference's 2D phi slab and the transverse directions of a 1D tube.
+ * The library stores such a direction as one plane and computes its interior
+ * cell only, with results equal to computing every cell; uploaded primitives
+ * must then be uniform along it.  RG_FLAG_FULL computes every cell instead. */
+#define RG_FLAG_FULL 1
 
 typedef struct rg_step_stats {
   long long steps;        /* full RK3 steps taken */
@@ -91,6 +101,18 @@ int rg_ctx_set_stream(rg_ctx* ctx, void* stream);
  * allocates the device state.  RG_ENOMEM_ADMIT if it does not fit. */
 int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id);
 int rg_run_release(rg_ctx* ctx, int run);
+/* Admission in two parts, for schedulers that prepare runs on other threads
+ * while their context keeps the GPU busy: rg_prep_create checks the
+ * parameters and computes the grid, metric and Christoffel symbols on the
+ * host (no context, no GPU; any thread), rg_prep_ic_torus adds the torus
+ * initial data of rg_run_ic_torus, and rg_run_admit_prep allocates the run on
+ * the context and uploads both (the run then starts at time 0).  The
+ * preparation stays valid for further admissions until rg_prep_destroy. */
+typedef struct rg_prep rg_prep;
+int rg_prep_create(const rg_run_params* p, rg_prep** out);
+int rg_prep_ic_torus(rg_prep* prep, uint64_t seed, double amp, double rin, double rmax, double beta, double kappa);
+int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id);
+int rg_prep_destroy(rg_prep* prep);
 /* Device bytes a run with these parameters needs (admission by footprint). */
 int rg_run_footprint(const rg_run_params* p, size_t* bytes);
 
@@ -99,15 +121,38 @@ int rg_run_footprint(const rg_run_params* p, size_t* bytes);
  * uniform keyed by (seed, cell).  Also sets time = 0 (main.f90:530-548). */
 int rg_run_ic_torus(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin, double rmax,
                     double beta, double kappa);
+/* Initial data: seeded 1D RMHD Riemann problem number `tube` in the pattern
+ * of mdshoctub (mdgrmhd.f90:56-118): a left state for i <= imax/2 and a right
+ * state beyond, drawn from a counter-based uniform keyed by (seed, tube):
+ * rho log-uniform in [0.1, 10], p log-uniform in [0.01, 100], |v| <= 0.9,
+ * B^x in [0, 5] shared by both sides, B^y, B^z in [-5, 5].  Sets time = 0. */
+int rg_run_ic_tube(rg_ctx* ctx, int run, uint64_t seed, uint64_t tube);
 /* Host <-> device primitives, layout a(nv,i,j,k).  Upload also sets time = t0. */
 int rg_run_upload_prims(rg_ctx* ctx, int run, const double* uri, double t0);
 int rg_run_download_prims(rg_ctx* ctx, int run, double* uri);
 
 /* Advance nsteps full RK3 steps of main.f90:586-1147 on the device (CFL
  * reduction, three stages, ghost fill, floors).  Stops early once the loop-top
- * time exceeds tmax.  Asynchronous on the context stream unless stats != NULL. */
+ * time exceeds tmax.  Asynchronous on the context stream unless stats != NULL.
+ * A run with a slab direction steps as a batch of one (rg_step_batch). */
 int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats);
 int rg_run_stats(rg_ctx* ctx, int run, rg_step_stats* stats);
+
+/* Advance nruns runs together by nsteps full RK3 steps.  The runs must have a
+ * slab direction (2D phi slabs, 1D tubes; see RG_FLAG_FULL); runs that share
+ * reconstruction, precision and slab class form one batch, whose step is one
+ * launch per kernel kind over a per-run tile table (persistent grid), captured
+ * once in a CUDA graph and replayed each step.  The first call for a set of
+ * runs tunes the tile width and grid size on trial steps from a snapshot of
+ * the runs' state, which it restores.  Each run's result equals its result
+ * stepped alone.  stats, if given, receives nruns records.  Replaces the
+ * reference's one-run-per-job time loop (main.f90:586-1151) for ensembles. */
+int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_stats* stats);
+/* The tuned shape of the batch of exactly these runs: block width of the cell
+ * kernels, persistent blocks per SM (0: one block per tile), launches per
+ * step and the step time measured by the tuner (ms). */
+int rg_batch_info(rg_ctx* ctx, const int* runs, int nruns, int* width, int* grid_factor, int* launches,
+                  double* tuned_ms);
 
 /* Kernel timing: rg_profile(ctx, 1) clears the counters and brackets every
  * following launch of rg_step with CUDA events on the context stream;
@@ -131,6 +176,15 @@ int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri);
 int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl);
 /* bnd4 + infchk + atmosphere1a + pminmax2b (bnd.f90, correction.f90) on uri in/out */
 int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio);
+
+/* Accretion rates through the inner edge of the interior (the radial face
+ * nm1+1/2, just outside the horizon for the torus grids): mdot = -sum of the
+ * radial flux of sqrt(-g) rho u^r over the interior (phi, theta) faces times
+ * dx2*dx3, edot the same of the energy variable sqrt(-g)(T^r_t + rho u^r)
+ * (calflx.f90:391-528), from FP64 fluxes of the run's current primitives.
+ * The reference has no such diagnostic; it is how the mixed-precision path's
+ * effect on the accretion is measured. */
+int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot);
 
 /* Allocation-free variant of rg_calflx, for callers that cannot call
  * cudaMalloc when they need the fluxes (code running inside a CUDA stream

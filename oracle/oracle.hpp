@@ -143,5 +143,7 @@ void mdtorus1(State& s, uint64_t seed, double amp, double rin, double rmax, doub
               double kappa);
 double callfish(double akm, double rmax);
 double ic_uniform(uint64_t seed, uint64_t idx);
+void tube_states(uint64_t seed, uint64_t tube, double gam, double q[2][9]);
+void mdtube(State& s, uint64_t seed, uint64_t tube);
 
 }  // namespace orc

@@ -43,6 +43,11 @@ void orc_ic_torus(void* h, unsigned long long seed, double amp, double rin, doub
   orc::mdtorus1(*s, seed, amp, rin, rmax, beta, kappa);
 }
 
+// seeded Riemann tube (pattern of mdshoctub, mdgrmhd.f90:56-118)
+void orc_ic_tube(void* h, unsigned long long seed, unsigned long long tube) {
+  orc::mdtube(*static_cast<State*>(h), seed, tube);
+}
+
 void orc_set_prims(void* h, const double* uri) {
   State* s = static_cast<State*>(h);
   std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));

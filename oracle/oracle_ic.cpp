@@ -118,8 +118,11 @@ void mdtorus1(State& s, uint64_t seed, double amp, double rin, double rmax, doub
           q[5] = pr * (1.0 / std::pow(de, gam - 1.));
         }
       }
-  // normalise to rho_max = 1 and perturb p (mdgrmhd.f90:1198-1320)
+  // normalise to rho_max = 1 and perturb p (mdgrmhd.f90:1198-1320).  In a 2D
+  // phi slab (jmax = 2*nm1+1) the draw is keyed by the (r, theta) cell of the
+  // interior phi index: the slab then holds one axisymmetric state.
   const double rhomax1a = rhomax1;
+  const bool phi_slab = (jmax == 2 * s.nm1 + 1);
   for (int k = 1; k <= kmax; ++k)
     for (int j = 1; j <= jmax; ++j)
       for (int i = 1; i <= imax; ++i) {
@@ -132,7 +135,7 @@ void mdtorus1(State& s, uint64_t seed, double amp, double rin, double rmax, doub
           double* q = &u[s.a(1, i, j, k)];
           double de = q[0] * (1.0 / rhomax1a);
           double pr = q[4] * (1.0 / rhomax1a);
-          const double r01 = ic_uniform(seed, (uint64_t)c);
+          const double r01 = ic_uniform(seed, (uint64_t)(phi_slab ? s.cell(i, s.nm1 + 1, k) : c));
           pr = pr * (1.0 + amp * (r01 - 0.5));
           if (de <= rhomin1) { de = rhomin1; q[1] = 0.0; q[2] = 0.0; q[3] = 0.0; pr = prmin1; }
           if (pr <= prmin1) { de = rhomin1; q[1] = 0.0; q[2] = 0.0; q[3] = 0.0; pr = prmin1; }
@@ -212,6 +215,51 @@ void mdtorus1(State& s, uint64_t seed, double amp, double rin, double rmax, doub
     u[NV * c + 7] = u[NV * c + 7] * bnorm;
     u[NV * c + 8] = u[NV * c + 8] * bnorm;
   }
+}
+
+// Seeded 1D RMHD Riemann problem in the pattern of mdshoctub
+// (mdgrmhd.f90:56-118): the left state fills i <= imax/2, the right state the
+// rest, in every cell (ghosts included); util is the spatial 4-velocity
+// gamma*v (Minkowski) and uri(6) = p / rho**(gam-1).  The two states are drawn
+// with ic_uniform keyed by (seed, 16*tube + field): field 0 the shared B^x in
+// [0, 5]; per side s (base 1 + 7s) rho log-uniform in [0.1, 10], p
+// log-uniform in [0.01, 100], v^x, v^y, v^z uniform in [-0.9, 0.9] (scaled
+// down to |v| = 0.9 when larger), B^y and B^z uniform in [-5, 5].
+void tube_states(uint64_t seed, uint64_t tube, double gam, double q[2][9]) {
+  auto U = [&](int f) { return ic_uniform(seed, 16 * tube + (uint64_t)f); };
+  const double bx = 5.0 * U(0);
+  for (int sd = 0; sd < 2; ++sd) {
+    const int b = 1 + 7 * sd;
+    const double de = std::pow(10.0, -1.0 + 2.0 * U(b));
+    const double pr = std::pow(10.0, -2.0 + 4.0 * U(b + 1));
+    double v[3] = {0.9 * (2.0 * U(b + 2) - 1.0), 0.9 * (2.0 * U(b + 3) - 1.0), 0.9 * (2.0 * U(b + 4) - 1.0)};
+    const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (vv > 0.81) {
+      const double f = 0.9 / std::sqrt(vv);
+      v[0] *= f; v[1] *= f; v[2] *= f;
+    }
+    const double g = 1.0 / std::sqrt(1.0 - (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    q[sd][0] = de;
+    q[sd][1] = g * v[0];
+    q[sd][2] = g * v[1];
+    q[sd][3] = g * v[2];
+    q[sd][4] = pr;
+    q[sd][5] = pr * (1. / std::pow(de, gam - 1.));
+    q[sd][6] = bx;
+    q[sd][7] = 5.0 * (2.0 * U(b + 5) - 1.0);
+    q[sd][8] = 5.0 * (2.0 * U(b + 6) - 1.0);
+  }
+}
+
+void mdtube(State& s, uint64_t seed, uint64_t tube) {
+  double q[2][9];
+  tube_states(seed, tube, s.p.gam, q);
+  for (int k = 1; k <= s.kmax; ++k)
+    for (int j = 1; j <= s.jmax; ++j)
+      for (int i = 1; i <= s.imax; ++i) {
+        const double* src = q[i <= s.imax / 2 ? 0 : 1];
+        for (int n = 1; n <= NV; ++n) s.uri[s.a(n, i, j, k)] = src[n - 1];
+      }
 }
 
 }  // namespace orc

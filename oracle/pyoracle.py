@@ -53,6 +53,7 @@ def _lib():
         lib.orc_nm1.restype = C.c_int
         lib.orc_ic_torus.argtypes = [P, C.c_ulonglong, C.c_double, C.c_double, C.c_double, C.c_double,
                                      C.c_double]
+        lib.orc_ic_tube.argtypes = [P, C.c_ulonglong, C.c_ulonglong]
         for f in ("orc_set_prims", "orc_get_prims", "orc_get_cons"):
             getattr(lib, f).argtypes = [P, D]
         lib.orc_init_cons.argtypes = [P]
@@ -119,6 +120,10 @@ class Oracle:
 
     def ic_torus(self, seed=2012, amp=0.04, rin=6.0, rmax=12.0, beta=100.0, kappa=1e-3):
         self.lib.orc_ic_torus(self.h, seed, amp, rin, rmax, beta, kappa)
+
+    def ic_tube(self, seed=2012, tube=0):
+        """Seeded 1D Riemann problem (left state for i <= imax/2, pattern of mdshoctub)."""
+        self.lib.orc_ic_tube(self.h, seed, tube)
 
     def set_prims(self, uri: np.ndarray):
         uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)

@@ -26,8 +26,9 @@ STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA"
 
 #: every entry point include/raishin_gpu.h declares
 EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
-           "rg_run_footprint", "rg_run_ic_torus", "rg_run_upload_prims", "rg_run_download_prims", "rg_step",
-           "rg_run_stats", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calflx_static")
+           "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
+           "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_step",
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_run_horizon_flux", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -49,6 +50,7 @@ class RunParams(C.Structure):
         ("ibc", (C.c_int * 9) * 6),
         ("guard", C.c_int),
         ("precision", C.c_int),
+        ("flags", C.c_int),
     ]
 
 
@@ -84,13 +86,21 @@ def load(path: str = LIB_PATH):
     lib.rg_ctx_set_stream.argtypes = [P, P]
     lib.rg_run_admit.argtypes = [P, C.POINTER(RunParams), C.POINTER(C.c_int)]
     lib.rg_run_release.argtypes = [P, I]
+    lib.rg_prep_create.argtypes = [C.POINTER(RunParams), C.POINTER(C.c_void_p)]
+    lib.rg_prep_ic_torus.argtypes = [P, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+    lib.rg_run_admit_prep.argtypes = [P, P, C.POINTER(C.c_int)]
+    lib.rg_prep_destroy.argtypes = [P]
     lib.rg_run_footprint.argtypes = [C.POINTER(RunParams), C.POINTER(C.c_size_t)]
     lib.rg_run_ic_torus.argtypes = [P, I, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double]
+    lib.rg_run_ic_tube.argtypes = [P, I, C.c_uint64, C.c_uint64]
     lib.rg_run_upload_prims.argtypes = [P, I, C.c_void_p, C.c_double]
     lib.rg_run_download_prims.argtypes = [P, I, C.c_void_p]
     lib.rg_step.argtypes = [P, I, I, C.POINTER(StepStats)]
     lib.rg_run_stats.argtypes = [P, I, C.POINTER(StepStats)]
+    lib.rg_step_batch.argtypes = [P, C.POINTER(C.c_int), I, I, C.POINTER(StepStats)]
+    lib.rg_batch_info.argtypes = [P, C.POINTER(C.c_int), I, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.rg_profile.argtypes = [P, I]
     lib.rg_profile_read.argtypes = [P, D, C.POINTER(C.c_longlong), I]
     lib.rg_caluu1.argtypes = [P, I, D, D]
@@ -99,6 +109,7 @@ def load(path: str = LIB_PATH):
     lib.rg_cdtcfl.argtypes = [P, I, D, D]
     lib.rg_bnd_floor.argtypes = [P, I, D, D]
     lib.rg_calflx_static.argtypes = [P, I, P, P]
+    lib.rg_run_horizon_flux.argtypes = [P, I, D, D]
     _lib = lib
     return lib
 
@@ -117,6 +128,8 @@ def make_params(p: dict) -> RunParams:
                     o.ibc[s][m] = int(p["ibc"][s][m])
         elif name == "guard":
             o.guard = int(p.get("guard", 0))
+        elif name == "flags":
+            o.flags = int(p.get("flags", 0))
         elif name == "precision":
             o.precision = {"fp64": 0, "mixed": 1}[p.get("precision", "fp64")]
         else:
@@ -173,6 +186,25 @@ class Context:
     def admit(self, params: dict) -> "Run":
         return Run(self, params)
 
+    def admit_prep(self, prep: Prep) -> "Run":
+        """Admit a prepared run (geometry and initial data computed by Prep)."""
+        return Run(self, prep.params, prep)
+
+    def step_batch(self, runs, n: int = 1, stats: bool = False):
+        """Advance several runs together (rg_step_batch); with stats, one dict per run."""
+        ids = (C.c_int * len(runs))(*[r.id for r in runs])
+        st = (StepStats * len(runs))() if stats else None
+        _check(self.lib, self.lib.rg_step_batch(self.h, ids, len(runs), int(n), st))
+        return [x.as_dict() for x in st] if stats else None
+
+    def batch_info(self, runs) -> dict:
+        """Tuned shape of the batch of exactly these runs."""
+        ids = (C.c_int * len(runs))(*[r.id for r in runs])
+        w, f, nl, ms = C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0)
+        _check(self.lib, self.lib.rg_batch_info(self.h, ids, len(runs), C.byref(w), C.byref(f), C.byref(nl),
+                                                C.byref(ms)))
+        return {"width": w.value, "grid_per_sm": f.value, "launches_per_step": nl.value, "tuned_ms_per_step": ms.value}
+
     def __enter__(self):
         return self
 
@@ -180,15 +212,46 @@ class Context:
         self.close()
 
 
+class Prep:
+    """Host-side preparation of a run (rg_prep_*): geometry and, optionally,
+    torus initial data, computed without a context on any thread."""
+
+    def __init__(self, params: dict):
+        self.lib = load()
+        self.params = dict(params)
+        self._p = make_params(params)
+        h = C.c_void_p()
+        _check(self.lib, self.lib.rg_prep_create(C.byref(self._p), C.byref(h)))
+        self.h = h
+
+    def ic_torus(self, seed=2012, amp=0.04, rin=6.0, rmax=12.0, beta=100.0, kappa=1e-3):
+        _check(self.lib, self.lib.rg_prep_ic_torus(self.h, seed, amp, rin, rmax, beta, kappa))
+        return self
+
+    def close(self):
+        if self.h:
+            self.lib.rg_prep_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Run:
     """One admitted run: device-resident state of one grid."""
 
-    def __init__(self, ctx: Context, params: dict):
+    def __init__(self, ctx: Context, params: dict, prep: "Prep | None" = None):
         self.ctx, self.lib = ctx, ctx.lib
         self.params = dict(params)
         self._p = make_params(params)
         rid = C.c_int(0)
-        _check(self.lib, self.lib.rg_run_admit(ctx.h, C.byref(self._p), C.byref(rid)))
+        if prep is None:
+            _check(self.lib, self.lib.rg_run_admit(ctx.h, C.byref(self._p), C.byref(rid)))
+        else:
+            _check(self.lib, self.lib.rg_run_admit_prep(ctx.h, prep.h, C.byref(rid)))
         self.id = rid.value
         self.shape = (params["kmax"], params["jmax"], params["imax"], 9)
         self.nm0, self.nm1 = ghost_widths(params["irec"])
@@ -204,6 +267,10 @@ class Run:
     # initial data / state transfer
     def ic_torus(self, seed=2012, amp=0.04, rin=6.0, rmax=12.0, beta=100.0, kappa=1e-3):
         _check(self.lib, self.lib.rg_run_ic_torus(self.ctx.h, self.id, seed, amp, rin, rmax, beta, kappa))
+
+    def ic_tube(self, seed=2012, tube=0):
+        """Seeded 1D Riemann problem (left state for i <= imax/2, pattern of mdshoctub)."""
+        _check(self.lib, self.lib.rg_run_ic_tube(self.ctx.h, self.id, seed, tube))
 
     def upload_prims(self, uri, t0: float = 0.0):
         uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
@@ -262,6 +329,12 @@ class Run:
         """Allocation-free flux call on caller-owned device buffers (raw device
         pointers): d_prims 9*N SoA primitives in, d_ww 27*N fluxes out."""
         _check(self.lib, self.lib.rg_calflx_static(self.ctx.h, self.id, C.c_void_p(d_prims), C.c_void_p(d_ww)))
+
+    def horizon_flux(self) -> tuple[float, float]:
+        """(mdot, edot) through the inner edge of the interior (rg_run_horizon_flux)."""
+        m, e = C.c_double(0), C.c_double(0)
+        _check(self.lib, self.lib.rg_run_horizon_flux(self.ctx.h, self.id, C.byref(m), C.byref(e)))
+        return m.value, e.value
 
     def bnd_floor(self, uri, urio) -> np.ndarray:
         out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)

@@ -19,6 +19,9 @@ PI = 3.14159265358979323  # pram.f90:30
 # reconstruction selectors (pram.f90:73 / rec.f90:61-112)
 IREC_PPM, IREC_MP5, IREC_WENO5 = 5, 6, 7
 
+# rg_run_params.flags: compute every cell of a slab direction instead of one plane
+FLAG_FULL = 1
+
 # boundary codes (bnd.f90:398-413)
 BC_PERIODIC, BC_COPY, BC_ANTISYM, BC_SYM, BC_OUTFLOW18 = 1, 5, 12, 14, 18
 
@@ -69,7 +72,10 @@ def tube(n: int = 400, irec: int = IREC_MP5, cfl: float = 0.4, tmax: float = 0.4
          precision: str = "fp64") -> dict:
     """1D RMHD shock tube in Minkowski space (metric 1, model 2): x in [1, 2]
     (cell centres, ghosts included; x > 0 because the floors use x**-1.5),
-    Gamma = 5/3, copy boundaries in x and a periodic 2*nm1+1 slab in y and z."""
+    Gamma = 5/3, copy boundaries in x and a 2*nm1+1 slab with copy
+    boundaries in y and z.  (With periodic y and z the reference's
+    single-rank periodic fill never refreshes the cells that are ghosts in
+    both, bnd.f90:50-70/160-180/272-292, and flux-CT reads them.)"""
     _, nm1 = ghost_widths(irec)
     imax = int(n) + 2 * nm1
     w = 2 * nm1 + 1
@@ -79,7 +85,7 @@ def tube(n: int = 400, irec: int = IREC_MP5, cfl: float = 0.4, tmax: float = 0.4
         xmin=1.0, xmax=2.0, ymin=0.0, ymax=(w - 1) * dx, zmin=0.0, zmax=(w - 1) * dx,
         R0=0.0, hslope=0.5, akm=0.0, gam=5.0 / 3.0, cfl=cfl, dmin=1.0e-4, pmin=1.0e-6, pmax=1.0e6,
         tmax=tmax, dtmin=1.0e-9,
-        ibc=[[5] * 9, [5] * 9, [1] * 9, [1] * 9, [1] * 9, [1] * 9], precision=precision,
+        ibc=[[5] * 9] * 6, precision=precision,
     )
 
 

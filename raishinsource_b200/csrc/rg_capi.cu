@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <map>
 #include <string>
 #include <vector>
@@ -37,8 +38,12 @@ constexpr int kCarryCap = 1 << 16;
 struct Run {
   rg_run_params p{};
   DevRun d{};
-  DevBufs b{};
-  double* aos = nullptr;   // 9*N staging buffer in the reference layout
+  DevBufs b{};             // stored-layout buffers of the step (stage/stage2 unused)
+  DevBufs fb{};            // full-layout buffers of the per-routine entry points (allocated on first use)
+  bool fb_ready = false;
+  double* aos = nullptr;   // 9*Nfull staging buffer in the reference layout (allocated on first use)
+  int* bad = nullptr;      // device flag: uploaded data not uniform along a slab direction
+  size_t nfull = 0;        // imax*jmax*kmax
   int cur = 0;             // index of P^n in b.P
   std::vector<void*> allocs;
   size_t bytes = 0;
@@ -47,13 +52,32 @@ struct Run {
 
 }  // namespace
 
+// Host-side preparation of a run (geometry, initial data), built without a context.
+struct rg_prep {
+  rg_run_params p{};
+  HostGeom geom;
+  std::vector<double> ic;  // full-layout SoA primitives, empty if none
+};
+
 // Kernel kinds timed by the profiling mode (rg_profile).
 enum Kind { K_CFL = 0, K_FLUX1, K_FLUX2, K_FLUX3, K_CT, K_UPDATE, K_BC, K_FLOOR, K_SCALAR, K_NKINDS };
+
+// A batched step of one class of runs: its tile plan, the tuned launch
+// shape and the CUDA graph of one step.
+struct BatchEntry {
+  std::vector<int> ids;        // member runs, sorted
+  BatchPlan* plan = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int width = 128, grid_factor = 0;
+  double tuned_ms = 0.0;       // step time of the chosen shape
+};
 
 struct rg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   std::map<int, Run*> runs;
+  std::map<std::vector<int>, BatchEntry*> batches;
+  std::map<long long, std::pair<int, int>> tuned;  // batch class -> (width, grid factor) chosen by the tuner
   int next_id = 1;
   long long launches[K_NKINDS] = {};   // kernel launches issued, per kind
   bool prof = false;                   // bracket every launch with CUDA events
@@ -108,10 +132,50 @@ int check_params(const rg_run_params* p) {
   return RG_OK;
 }
 
+// A direction that holds one interior cell, whose ghost fills copy that cell
+// (periodic or copy codes for every variable on both sides) and on which the
+// metric does not depend (phi always; theta only in Minkowski space) keeps the
+// same state in all its cells after each ghost fill, provided every other
+// direction's boundary codes are physical ones (bnd.f90:384-1058), whose
+// passes cover all columns: the single-rank periodic pass covers only columns
+// with interior transverse indices (bnd.f90:50-70, 160-180, 272-292), so with
+// two periodic directions the cells that are ghosts in both are never
+// refreshed.  Such a direction is stored as one plane.
+bool all_physical(const rg_run_params* p, int dir) {
+  for (int sd = 2 * (dir - 1); sd <= 2 * (dir - 1) + 1; ++sd)
+    for (int v = 0; v < 9; ++v)
+      if (p->ibc[sd][v] == 1 || p->ibc[sd][v] == 0) return false;
+  return true;
+}
+
+bool slab_direction(const rg_run_params* p, int dir, int nm1) {
+  const int n = dir == 2 ? p->jmax : p->kmax;
+  if (n != 2 * nm1 + 1) return false;
+  if (dir == 3 && p->metric != 1) return false;
+  for (int sd = 2 * (dir - 1); sd <= 2 * (dir - 1) + 1; ++sd)
+    for (int v = 0; v < 9; ++v)
+      if (p->ibc[sd][v] != 1 && p->ibc[sd][v] != 5) return false;
+  for (int e = 1; e <= 3; ++e)
+    if (e != dir && !all_physical(p, e)) return false;
+  return true;
+}
+
+size_t stored_cells(const rg_run_params* p) {
+  const int nm1 = (p->irec == 5) ? 5 : 4;
+  const bool full = (p->flags & RG_FLAG_FULL) != 0;
+  const size_t jpl = (!full && slab_direction(p, 2, nm1)) ? 1 : (size_t)p->jmax;
+  const size_t kpl = (!full && slab_direction(p, 3, nm1)) ? 1 : (size_t)p->kmax;
+  return (size_t)p->imax * jpl * kpl;
+}
+
+// Device bytes of a run's step state, geometry and FP32 copies (the
+// per-routine entry points' full-layout buffers are allocated on first use).
 size_t footprint_bytes(const rg_run_params* p) {
-  const size_t N = (size_t)p->imax * p->jmax * p->kmax;
-  const size_t nik = (size_t)p->imax * p->kmax;
-  const size_t state = (3 * 9 + 3 * 9 + 6 + 2 * 9 + 9 + 9) * N * sizeof(double);
+  const size_t N = stored_cells(p);
+  const int nm1 = (p->irec == 5) ? 5 : 4;
+  const bool kslab = !(p->flags & RG_FLAG_FULL) && slab_direction(p, 3, nm1);
+  const size_t nik = (size_t)p->imax * (kslab ? 1 : p->kmax);
+  const size_t state = (3 * 9 + 3 * 9 + 6 + 9) * N * sizeof(double);
   const size_t geom = (3 * kMetComps + 64) * nik * sizeof(double) + 16 * (size_t)(p->imax + p->jmax + p->kmax) * sizeof(double);
   size_t mixed = 0;
   if (p->precision == RG_MIXED)  // P32, F32 x3, CT32; FP32 metric caches and Christoffels
@@ -148,12 +212,59 @@ std::vector<double> shifted(const std::vector<double>& v, int n) {
   return o;
 }
 
-// The per-routine entry points compute in FP64 whatever the run's precision.
-DevRun fp64_view(const Run* R) {
+// The per-routine entry points compute in FP64 on the reference's full
+// array layout, whatever the run's precision and slab directions.
+DevRun full_view(const Run* R) {
   DevRun d = R->d;
   d.mixed = 0;
   d.P32 = nullptr;
+  d.jfix = d.kfix = 0;
+  d.jpl = d.jmax;
+  d.kpl = d.kmax;
+  d.sj = (size_t)d.imax;
+  d.sk = (size_t)d.imax * d.jmax;
+  d.N = R->nfull;
+  d.Un = nullptr;
   return d;
+}
+
+// Full-layout work buffers of the per-routine entry points, allocated on first use.
+int full_bufs(Run* R, cudaStream_t s, DevBufs** out) {
+  if (!R->fb_ready) {
+    const size_t N = R->nfull;
+    void* p = nullptr;
+    int rc;
+    for (int k = 0; k < 3; ++k) {
+      if ((rc = dalloc(R, &p, 9 * N * sizeof(double)))) return rc;
+      R->fb.F[k] = static_cast<double*>(p);
+      if (cudaMemsetAsync(p, 0, 9 * N * sizeof(double), s) != cudaSuccess) return fail(RG_ECUDA, "memset failed");
+    }
+    if ((rc = dalloc(R, &p, 6 * N * sizeof(double)))) return rc;
+    R->fb.CT = static_cast<double*>(p);
+    if (cudaMemsetAsync(p, 0, 6 * N * sizeof(double), s) != cudaSuccess) return fail(RG_ECUDA, "memset failed");
+    if ((rc = dalloc(R, &p, 9 * N * sizeof(double)))) return rc;
+    R->fb.stage = static_cast<double*>(p);
+    if ((rc = dalloc(R, &p, 9 * N * sizeof(double)))) return rc;
+    R->fb.stage2 = static_cast<double*>(p);
+    R->fb_ready = true;
+  }
+  *out = &R->fb;
+  return RG_OK;
+}
+
+// Values of a full-layout SoA array (v*Nfull + full cell) at the stored cells of d.
+std::vector<double> stored_from_full(const DevRun& d, const std::vector<double>& full, size_t nfull) {
+  if (!d.jfix && !d.kfix) return full;
+  std::vector<double> out(9 * d.N);
+  for (int k = 1; k <= d.kmax; ++k) {
+    if (d.kfix && k != d.kfix) continue;
+    for (int j = 1; j <= d.jmax; ++j) {
+      if (d.jfix && j != d.jfix) continue;
+      for (int i = 1; i <= d.imax; ++i)
+        for (int v = 0; v < 9; ++v) out[(size_t)v * d.N + d.cell(i, j, k)] = full[(size_t)v * nfull + d.cell_full(i, j, k)];
+    }
+  }
+  return out;
 }
 
 int set_time(rg_ctx* ctx, Run* R, double t0) {
@@ -168,17 +279,42 @@ int set_time(rg_ctx* ctx, Run* R, double t0) {
   return RG_OK;
 }
 
-int to_soa(rg_ctx* ctx, Run* R, const double* host_aos, double* dev_soa) {
-  const size_t N = R->d.N;
-  RG_CUDA(cudaMemcpyAsync(R->aos, host_aos, 9 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  RG_CUDA(launch_aos_to_soa(R->aos, dev_soa, N, ctx->stream));
+int ensure_aos(Run* R) {
+  if (R->aos) return RG_OK;
+  void* p = nullptr;
+  int rc = dalloc(R, &p, 9 * R->nfull * sizeof(double));
+  if (rc) return rc;
+  R->aos = static_cast<double*>(p);
   return RG_OK;
 }
 
-int from_soa(rg_ctx* ctx, Run* R, const double* dev_soa, double* host_aos) {
-  const size_t N = R->d.N;
-  RG_CUDA(launch_soa_to_aos(dev_soa, R->aos, N, ctx->stream));
-  RG_CUDA(cudaMemcpyAsync(host_aos, R->aos, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+// Host reference-layout array -> device SoA in the layout of view v (the run's
+// stored layout, or the full layout of the per-routine entry points).  With
+// check, data that are not uniform along a slab direction are refused.
+int to_soa(rg_ctx* ctx, Run* R, const double* host_aos, double* dev_soa, const DevRun& v, bool check) {
+  int rc = ensure_aos(R);
+  if (rc) return rc;
+  RG_CUDA(cudaMemcpyAsync(R->aos, host_aos, 9 * R->nfull * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  const bool slab = v.jfix || v.kfix;
+  if (check && slab) RG_CUDA(cudaMemsetAsync(R->bad, 0, sizeof(int), ctx->stream));
+  RG_CUDA(launch_aos_to_soa(v, R->aos, dev_soa, (check && slab) ? R->bad : nullptr, ctx->stream));
+  if (check && slab) {
+    int bad = 0;
+    RG_CUDA(cudaMemcpyAsync(&bad, R->bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (bad)
+      return fail(RG_EINVAL_CONFIG,
+                  "primitives differ along a slab direction (the run stores one plane of it); admit the run "
+                  "with flags bit 0 (RG_FLAG_FULL) to compute every cell");
+  }
+  return RG_OK;
+}
+
+int from_soa(rg_ctx* ctx, Run* R, const double* dev_soa, double* host_aos, const DevRun& v) {
+  int rc = ensure_aos(R);
+  if (rc) return rc;
+  RG_CUDA(launch_soa_to_aos(v, dev_soa, R->aos, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(host_aos, R->aos, 9 * R->nfull * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
   return RG_OK;
 }
@@ -222,20 +358,6 @@ int drain_events(rg_ctx* ctx) {
   return RG_OK;
 }
 
-int bc_launches(const DevRun& r) {
-  int n = 0;
-  for (int side0 = 0; side0 <= 4; side0 += 2) {
-    bool per = false, phys = false;
-    for (int sd = side0; sd <= side0 + 1; ++sd)
-      for (int v = 0; v < 9; ++v) {
-        per = per || r.ibc[sd][v] == 1;
-        phys = phys || (r.ibc[sd][v] != 1 && r.ibc[sd][v] != 0);
-      }
-    n += per + phys;
-  }
-  return n;
-}
-
 // One RK3 stage (main.f90:807-911 / 919-1032 / 1043-1147).
 int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc, double* Pw) {
   const DevRun& d = R->d;
@@ -248,7 +370,7 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
   RG_CUDA(issue(ctx, K_UPDATE, n_update_launches(d), [&] {
     return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s);
   }));
-  RG_CUDA(issue(ctx, K_BC, bc_launches(d), [&] { return launch_bc(d, Pw, Pn, s); }));
+  RG_CUDA(issue(ctx, K_BC, n_bc_launches(d), [&] { return launch_bc(d, Pw, Pn, s); }));
   RG_CUDA(issue(ctx, K_FLOOR, 1, [&] { return launch_floor(d, Pw, s); }));
   return RG_OK;
 }
@@ -272,6 +394,193 @@ int read_stats(rg_ctx* ctx, Run* R, rg_step_stats* st) {
   st->dt = sc.dt;
   if (c[C_CARRY_OVF]) return fail(RG_EOVERFLOW, "W-carry list overflowed");
   if (c[C_CAP] || c[C_FLOORCAP]) return fail(RG_ENR_CAP, "a capped rescale loop was hit");
+  return RG_OK;
+}
+
+void free_batch(BatchEntry* E) {
+  if (E->graph) cudaGraphExecDestroy(E->graph);
+  batch_destroy(E->plan);
+  delete E;
+}
+
+// Forget every batch a run belongs to (its buffers are about to be freed).
+void drop_batches(rg_ctx* ctx, int run) {
+  for (auto it = ctx->batches.begin(); it != ctx->batches.end();) {
+    if (std::find(it->first.begin(), it->first.end(), run) != it->first.end()) {
+      free_batch(it->second);
+      it = ctx->batches.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+// Runs of one batch class share reconstruction, precision and slab class.
+long long batch_class(const Run* R) {
+  const DevRun& d = R->d;
+  return (long long)d.irec * 1000 + d.mixed * 100 + (d.jfix ? 10 : 0) + (d.kfix ? 1 : 0);
+}
+
+int kind_of(const BatchPlan* B, int idx) {
+  int dir = 0;
+  switch (batch_launch_kind(B, idx, &dir)) {
+    case 1: return K_CFL;
+    case 3: return K_FLUX1 + dir - 1;
+    case 4: return K_CT;
+    case 5: case 6: return K_UPDATE;
+    case 7: case 8: return K_BC;
+    case 9: return K_FLOOR;
+    default: return K_SCALAR;
+  }
+}
+
+// Device state of the member runs that a trial step changes: P^n, its FP32
+// copy, the scalar block and the counters.
+struct Snapshot {
+  std::vector<void*> bufs;
+  int save(std::vector<Run*>& rs, cudaStream_t s) {
+    for (Run* R : rs) {
+      const DevRun& d = R->d;
+      const size_t sizes[4] = {9 * d.N * sizeof(double), d.P32 ? 9 * d.N * sizeof(float) : 0, sizeof(Scal),
+                               C_NCOUNTERS * sizeof(unsigned long long)};
+      const void* srcs[4] = {R->b.P[R->cur], d.P32, d.scal, d.cnt};
+      for (int a = 0; a < 4; ++a) {
+        void* p = nullptr;
+        if (sizes[a]) {
+          if (cudaMalloc(&p, sizes[a]) != cudaSuccess) return fail(RG_ENOMEM_ADMIT, "autotune snapshot");
+          if (cudaMemcpyAsync(p, srcs[a], sizes[a], cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return fail(RG_ECUDA, "autotune snapshot copy");
+        }
+        bufs.push_back(p);
+      }
+    }
+    return RG_OK;
+  }
+  int restore(std::vector<Run*>& rs, cudaStream_t s) {
+    size_t a = 0;
+    for (Run* R : rs) {
+      const DevRun& d = R->d;
+      const size_t sizes[4] = {9 * d.N * sizeof(double), d.P32 ? 9 * d.N * sizeof(float) : 0, sizeof(Scal),
+                               C_NCOUNTERS * sizeof(unsigned long long)};
+      void* dsts[4] = {R->b.P[R->cur], d.P32, d.scal, d.cnt};
+      for (int k = 0; k < 4; ++k, ++a)
+        if (sizes[k] && cudaMemcpyAsync(dsts[k], bufs[a], sizes[k], cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+          return fail(RG_ECUDA, "autotune restore copy");
+    }
+    return RG_OK;
+  }
+  ~Snapshot() {
+    for (void* p : bufs) cudaFree(p);
+  }
+};
+
+// Build, tune and capture the batched step of runs of one class.  The tuner
+// times candidate persistent grid sizes (one block per tile, or 2, 4 or 8
+// blocks per SM, over tiles of 128 cells along i) on trial steps that start
+// from a snapshot of the runs' state, restores the state and keeps the
+// fastest; the grid size changes which block handles a tile, never a cell's
+// arithmetic.  The chosen size is kept per batch class for later batches of
+// the context, and the one-step launch sequence is captured once in a CUDA
+// graph.
+int capture_batch(BatchEntry* E);
+
+int make_batch(rg_ctx* ctx, std::vector<Run*>& rs, const std::vector<int>& ids, BatchEntry** out) {
+  cudaStream_t s = ctx->stream;
+  std::vector<DevRun> dr;
+  for (Run* R : rs) dr.push_back(R->d);
+  const long long cls = batch_class(rs[0]);
+  auto tk = ctx->tuned.find(cls);
+  if (tk != ctx->tuned.end()) {  // shape already tuned for this class (e.g. a serving batch that changed members)
+    BatchEntry* E = new BatchEntry();
+    E->ids = ids;
+    if (batch_build(dr, tk->second.first, &E->plan)) {
+      delete E;
+      return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
+    }
+    E->width = tk->second.first;
+    E->grid_factor = tk->second.second;
+    batch_set_grid(E->plan, E->grid_factor);
+    const int rc = capture_batch(E);
+    if (rc) return rc;
+    *out = E;
+    return RG_OK;
+  }
+  Snapshot snap;
+  int rc = snap.save(rs, s);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  RG_CUDA(cudaEventCreate(&e0));
+  RG_CUDA(cudaEventCreate(&e1));
+  BatchEntry* E = new BatchEntry();
+  E->ids = ids;
+  double best = 1e30;
+  const int widths[1] = {128}, factors[4] = {0, 2, 4, 8};
+  for (int w : widths) {
+    BatchPlan* P = nullptr;
+    if (batch_build(dr, w, &P)) {
+      delete E;
+      return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
+    }
+    int keep_factor = -1;
+    for (int f : factors) {
+      batch_set_grid(P, f);
+      float ms = 0.f;
+      for (int rep = 0; rep < 3; ++rep) {  // one warm-up step, two timed
+        if (rep == 1) RG_CUDA(cudaEventRecord(e0, s));
+        RG_CUDA(batch_step(P, s));
+      }
+      RG_CUDA(cudaEventRecord(e1, s));
+      RG_CUDA(cudaEventSynchronize(e1));
+      RG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if ((rc = snap.restore(rs, s))) return rc;
+      if (ms < best) {
+        best = ms;
+        keep_factor = f;
+      }
+    }
+    if (keep_factor >= 0) {
+      if (E->plan) batch_destroy(E->plan);
+      E->plan = P;
+      E->width = w;
+      E->grid_factor = keep_factor;
+      E->tuned_ms = best / 2.0;
+      batch_set_grid(P, keep_factor);
+    } else {
+      batch_destroy(P);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  RG_CUDA(cudaStreamSynchronize(s));
+  ctx->tuned[cls] = {E->width, E->grid_factor};
+  const int crc = capture_batch(E);
+  if (crc) return crc;
+  *out = E;
+  return RG_OK;
+}
+
+int capture_batch(BatchEntry* E) {
+  // one step captured as a graph (the rotation is read on the device, so it replays for every step)
+  // (captured on a private stream: the context stream may be the legacy default stream)
+  cudaGraph_t g = nullptr;
+  cudaStream_t cs = nullptr;
+  RG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  RG_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t ce = batch_step(E->plan, cs);
+  const cudaError_t ee = cudaStreamEndCapture(cs, &g);
+  cudaStreamDestroy(cs);
+  if (ce != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    free_batch(E);
+    return fail(RG_ECUDA, "capturing the batched step failed");
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&E->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    E->graph = nullptr;
+    free_batch(E);
+    return fail(RG_ECUDA, "instantiating the batched step graph failed");
+  }
   return RG_OK;
 }
 
@@ -302,6 +611,7 @@ int rg_ctx_destroy(rg_ctx* ctx) {
   if (!ctx) return RG_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->batches) free_batch(kv.second);
   for (auto& kv : ctx->runs) free_run(kv.second);
   for (auto& pe : ctx->pending) ctx->pool.push_back(pe.second.first), ctx->pool.push_back(pe.second.second);
   for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
@@ -332,10 +642,45 @@ int rg_run_footprint(const rg_run_params* p, size_t* bytes) {
   return RG_OK;
 }
 
-int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
-  if (!ctx || !run_id) return fail(RG_EINVAL_CONFIG, "null argument");
+int rg_prep_create(const rg_run_params* p, rg_prep** out) {
+  if (!out) return fail(RG_EINVAL_CONFIG, "null argument");
   int rc = check_params(p);
   if (rc) return rc;
+  rg_prep* P = new rg_prep();
+  P->p = *p;
+  build_geometry(*p, P->geom);
+  if (!P->geom.compact_ok) {
+    delete P;
+    return fail(RG_EINVAL_CONFIG, "metric couples theta to (t,r,phi): not representable by the compact cache");
+  }
+  *out = P;
+  return RG_OK;
+}
+
+int rg_prep_ic_torus(rg_prep* P, uint64_t seed, double amp, double rin, double rmax, double beta, double kappa) {
+  if (!P) return fail(RG_EINVAL_CONFIG, "null preparation");
+  torus_ic(P->p, P->geom, seed, amp, rin, rmax, beta, kappa, P->ic);
+  return RG_OK;
+}
+
+int rg_prep_destroy(rg_prep* P) {
+  delete P;
+  return RG_OK;
+}
+
+int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
+  rg_prep* P = nullptr;
+  int rc = rg_prep_create(p, &P);
+  if (rc) return rc;
+  rc = rg_run_admit_prep(ctx, P, run_id);
+  delete P;
+  return rc;
+}
+
+int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
+  if (!ctx || !run_id || !prep) return fail(RG_EINVAL_CONFIG, "null argument");
+  const rg_run_params* p = &prep->p;
+  int rc = RG_OK;
   RG_CUDA(cudaSetDevice(ctx->device));
   size_t free_b = 0, total_b = 0;
   RG_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -344,11 +689,7 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
     return fail(RG_ENOMEM_ADMIT, "run footprint " + std::to_string(need) + " B exceeds free device memory");
   Run* R = new Run();
   R->p = *p;
-  build_geometry(*p, R->geom);
-  if (!R->geom.compact_ok) {
-    delete R;
-    return fail(RG_EINVAL_CONFIG, "metric couples theta to (t,r,phi): not representable by the compact cache");
-  }
+  R->geom = prep->geom;
   DevRun& d = R->d;
   d.imax = p->imax; d.jmax = p->jmax; d.kmax = p->kmax;
   d.nm0 = (p->irec == 5) ? 4 : 3;
@@ -364,8 +705,17 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
       if (R->geom.ax[0].x[i] < r2h) d.i_fp64 = i;
   }
   d.nmax_cfl = d.nm1 * 2 + (d.nm1 - 1);
-  d.N = (size_t)p->imax * p->jmax * p->kmax;
-  d.nik = (size_t)p->imax * p->kmax;
+  const bool full = (p->flags & RG_FLAG_FULL) != 0;
+  d.jfix = (!full && slab_direction(p, 2, d.nm1)) ? d.nm1 + 1 : 0;
+  d.kfix = (!full && slab_direction(p, 3, d.nm1)) ? d.nm1 + 1 : 0;
+  d.jpl = d.jfix ? 1 : p->jmax;
+  d.kpl = d.kfix ? 1 : p->kmax;
+  d.sj = d.jfix ? 0 : (size_t)p->imax;
+  d.sk = d.kfix ? 0 : (size_t)p->imax * d.jpl;
+  d.N = (size_t)p->imax * d.jpl * d.kpl;
+  R->nfull = (size_t)p->imax * p->jmax * p->kmax;
+  d.kmet = d.kfix;
+  d.nik = (size_t)p->imax * (d.kfix ? 1 : p->kmax);
   d.gam = p->gam; d.cfl = p->cfl; d.dmin = p->dmin; d.pmin = p->pmin; d.pmax = p->pmax; d.tmax = p->tmax;
   std::memcpy(d.ibc, p->ibc, sizeof(d.ibc));
   d.carry_cap = kCarryCap;
@@ -380,19 +730,21 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
   for (int k = 0; k < 3; ++k) {
     if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
     R->b.P[k] = static_cast<double*>(ptr);
+    d.P[k] = R->b.P[k];
     if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
     R->b.F[k] = static_cast<double*>(ptr);
   }
   if ((rc = dalloc(R, &ptr, 6 * N * sizeof(double)))) return bail(rc);
   R->b.CT = static_cast<double*>(ptr);
-  if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
-  R->b.stage = static_cast<double*>(ptr);
-  if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
-  R->b.stage2 = static_cast<double*>(ptr);
-  if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
-  R->aos = static_cast<double*>(ptr);
+  for (int k = 0; k < 3; ++k) d.F[k] = R->b.F[k];
+  d.CT = R->b.CT;
   if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
   d.Un = static_cast<double*>(ptr);
+  if ((rc = dalloc(R, &ptr, sizeof(int)))) return bail(rc);
+  R->bad = static_cast<int*>(ptr);
+  if (!d.jfix && !d.kfix) {  // the full layout is the stored one: share the step's flux buffers
+    R->fb.F[0] = R->b.F[0]; R->fb.F[1] = R->b.F[1]; R->fb.F[2] = R->b.F[2]; R->fb.CT = R->b.CT;
+  }
   if ((rc = dalloc(R, &ptr, 2 * (size_t)p->imax * sizeof(double)))) return bail(rc);
   d.fl_de = static_cast<double*>(ptr);
   d.fl_pr = d.fl_de + p->imax;
@@ -409,10 +761,20 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
   }
   if (cudaMemsetAsync(R->b.CT, 0, 6 * N * sizeof(double), s) != cudaSuccess) return bail(RG_ECUDA);
   const HostGeom& G = R->geom;
-  if ((rc = upload(G.mc, &d.mc, R, s))) return bail(rc);
-  if ((rc = upload(G.mi, &d.mi, R, s))) return bail(rc);
-  if ((rc = upload(G.mk, &d.mk, R, s))) return bail(rc);
-  if ((rc = upload(G.chr, &d.chr, R, s))) return bail(rc);
+  // a theta slab keeps the metric row of its computed index only (the metric is uniform there)
+  auto row = [&](const std::vector<double>& v, int comps) {
+    if (!d.kfix) return v;
+    std::vector<double> o((size_t)comps * d.nik);
+    const size_t full = (size_t)p->imax * p->kmax;
+    for (int c = 0; c < comps; ++c)
+      for (int i = 1; i <= p->imax; ++i)
+        o[(size_t)c * d.nik + (size_t)(i - 1)] = v[(size_t)c * full + (size_t)(i - 1) + (size_t)p->imax * (d.kfix - 1)];
+    return o;
+  };
+  if ((rc = upload(row(G.mc, kMetComps), &d.mc, R, s))) return bail(rc);
+  if ((rc = upload(row(G.mi, kMetComps), &d.mi, R, s))) return bail(rc);
+  if ((rc = upload(row(G.mk, kMetComps), &d.mk, R, s))) return bail(rc);
+  if ((rc = upload(row(G.chr, 64), &d.chr, R, s))) return bail(rc);
   std::vector<double> t;
   if ((rc = upload(zero_based(G.ax[0].x, p->imax), &d.x1, R, s))) return bail(rc);
   if ((rc = upload(zero_based(G.ax[0].dxb, p->imax), &d.dx1b, R, s))) return bail(rc);
@@ -456,6 +818,13 @@ int rg_run_admit(rg_ctx* ctx, const rg_run_params* p, int* run_id) {
     }
   }
   if ((rc = set_time(ctx, R, 0.0))) return bail(rc);
+  if (!prep->ic.empty()) {  // initial data computed with the preparation
+    const std::vector<double> Ps = stored_from_full(d, prep->ic, R->nfull);
+    if (cudaMemcpyAsync(R->b.P[0], Ps.data(), Ps.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return bail(fail(RG_ECUDA, "initial data upload failed"));
+    if (d.P32 && launch_to_f32(R->b.P[0], d.P32, 9 * d.N, s) != cudaSuccess)
+      return bail(fail(RG_ECUDA, "initial data upload failed"));
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(RG_ECUDA, "setup failed"));
   const int id = ctx->next_id++;
   ctx->runs[id] = R;
@@ -467,6 +836,7 @@ int rg_run_release(rg_ctx* ctx, int run) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   cudaStreamSynchronize(ctx->stream);
+  drop_batches(ctx, run);
   free_run(R);
   ctx->runs.erase(run);
   return RG_OK;
@@ -478,9 +848,34 @@ int rg_run_ic_torus(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin,
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   std::vector<double> P;
   torus_ic(R->p, R->geom, seed, amp, rin, rmax, beta, kappa, P);
+  const std::vector<double> Ps = stored_from_full(R->d, P, R->nfull);
+  R->cur = 0;
+  RG_CUDA(cudaMemcpyAsync(R->b.P[0], Ps.data(), Ps.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (R->d.P32) RG_CUDA(launch_to_f32(R->b.P[0], R->d.P32, 9 * R->d.N, ctx->stream));
+  int rc = set_time(ctx, R, 0.0);
+  if (rc) return rc;
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+int rg_run_ic_tube(rg_ctx* ctx, int run, uint64_t seed, uint64_t tube) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  const DevRun& d = R->d;
+  double q[2][9];
+  tube_states(seed, tube, d.gam, q);
+  std::vector<double> P(9 * d.N);
+  for (int k = 1; k <= d.kmax; ++k) {
+    if (d.kfix && k != d.kfix) continue;
+    for (int j = 1; j <= d.jmax; ++j) {
+      if (d.jfix && j != d.jfix) continue;
+      for (int i = 1; i <= d.imax; ++i)
+        for (int v = 0; v < 9; ++v) P[(size_t)v * d.N + d.cell(i, j, k)] = q[i <= d.imax / 2 ? 0 : 1][v];
+    }
+  }
   R->cur = 0;
   RG_CUDA(cudaMemcpyAsync(R->b.P[0], P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  if (R->d.P32) RG_CUDA(launch_to_f32(R->b.P[0], R->d.P32, 9 * R->d.N, ctx->stream));
+  if (d.P32) RG_CUDA(launch_to_f32(R->b.P[0], d.P32, 9 * d.N, ctx->stream));
   int rc = set_time(ctx, R, 0.0);
   if (rc) return rc;
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -492,7 +887,7 @@ int rg_run_upload_prims(rg_ctx* ctx, int run, const double* uri, double t0) {
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!uri) return fail(RG_EINVAL_CONFIG, "null array");
   R->cur = 0;
-  int rc = to_soa(ctx, R, uri, R->b.P[0]);
+  int rc = to_soa(ctx, R, uri, R->b.P[0], R->d, true);
   if (rc) return rc;
   if (R->d.P32) RG_CUDA(launch_to_f32(R->b.P[0], R->d.P32, 9 * R->d.N, ctx->stream));
   return set_time(ctx, R, t0);
@@ -502,12 +897,16 @@ int rg_run_download_prims(rg_ctx* ctx, int run, double* uri) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!uri) return fail(RG_EINVAL_CONFIG, "null array");
-  return from_soa(ctx, R, R->b.P[R->cur], uri);
+  return from_soa(ctx, R, R->b.P[R->cur], uri, R->d);
 }
 
 int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  // A run with a slab direction steps as a batch of one: it then runs the same
+  // compiled kernels alone as in any batch, so its results do not depend on
+  // the company it keeps, and its step is replayed from a CUDA graph.
+  if (R->d.jfix || R->d.kfix) return rg_step_batch(ctx, &run, 1, nsteps, stats);
   cudaStream_t s = ctx->stream;
   for (int n = 0; n < nsteps; ++n) {
     double* Pn = R->b.P[R->cur];
@@ -528,6 +927,78 @@ int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats) {
     if (rc) return rc;
   }
   if (stats) return read_stats(ctx, R, stats);
+  return RG_OK;
+}
+
+int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_stats* stats) {
+  if (!ctx || !runs || nruns <= 0) return fail(RG_EINVAL_CONFIG, "empty batch");
+  std::map<long long, std::vector<int>> groups;
+  for (int a = 0; a < nruns; ++a) {
+    Run* R = find(ctx, runs[a]);
+    if (!R) return fail(RG_ENOTFOUND, "unknown run in batch");
+    if (!R->d.jfix && !R->d.kfix)
+      return fail(RG_EINVAL_CONFIG, "batched steps take runs with a slab direction (2D phi slabs, 1D tubes)");
+    groups[batch_class(R)].push_back(runs[a]);
+  }
+  std::vector<BatchEntry*> es;
+  for (auto& kv : groups) {
+    std::vector<int> ids = kv.second;
+    std::sort(ids.begin(), ids.end());
+    if (std::adjacent_find(ids.begin(), ids.end()) != ids.end())
+      return fail(RG_EINVAL_CONFIG, "a run appears twice in the batch");
+    auto it = ctx->batches.find(ids);
+    if (it == ctx->batches.end()) {
+      std::vector<Run*> rs;
+      for (int id : ids) rs.push_back(find(ctx, id));
+      BatchEntry* E = nullptr;
+      int rc = make_batch(ctx, rs, ids, &E);
+      if (rc) return rc;
+      it = ctx->batches.emplace(ids, E).first;
+    }
+    es.push_back(it->second);
+  }
+  cudaStream_t s = ctx->stream;
+  for (int n = 0; n < nsteps; ++n)
+    for (BatchEntry* E : es) {
+      const int nl = batch_launch_count(E->plan);
+      if (!ctx->prof) {
+        RG_CUDA(cudaGraphLaunch(E->graph, s));
+        for (int a = 0; a < nl; ++a) ctx->launches[kind_of(E->plan, a)] += 1;
+      } else {
+        for (int a = 0; a < nl; ++a) RG_CUDA(issue(ctx, kind_of(E->plan, a), 1, [&] { return batch_issue(E->plan, a, s); }));
+      }
+    }
+  for (int a = 0; a < nruns; ++a) {
+    Run* R = find(ctx, runs[a]);
+    R->cur = (R->cur + nsteps) % 3;
+  }
+  if (ctx->prof) {
+    int rc = drain_events(ctx);
+    if (rc) return rc;
+  }
+  if (stats) {
+    int worst = RG_OK;
+    for (int a = 0; a < nruns; ++a) {
+      const int rc = read_stats(ctx, find(ctx, runs[a]), stats + a);
+      if (rc == RG_ECUDA) return rc;
+      if (rc && !worst) worst = rc;
+    }
+    return worst;
+  }
+  return RG_OK;
+}
+
+int rg_batch_info(rg_ctx* ctx, const int* runs, int nruns, int* width, int* grid_factor, int* launches,
+                  double* tuned_ms) {
+  if (!ctx || !runs || nruns <= 0) return fail(RG_EINVAL_CONFIG, "empty batch");
+  std::vector<int> ids(runs, runs + nruns);
+  std::sort(ids.begin(), ids.end());
+  auto it = ctx->batches.find(ids);
+  if (it == ctx->batches.end()) return fail(RG_ENOTFOUND, "no batch of exactly these runs has been stepped");
+  if (width) *width = it->second->width;
+  if (grid_factor) *grid_factor = it->second->grid_factor;
+  if (launches) *launches = batch_launch_count(it->second->plan);
+  if (tuned_ms) *tuned_ms = it->second->tuned_ms;
   return RG_OK;
 }
 
@@ -564,29 +1035,34 @@ int rg_run_stats(rg_ctx* ctx, int run, rg_step_stats* stats) {
 int rg_caluu1(rg_ctx* ctx, int run, const double* uri, double* uu) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
-  int rc = to_soa(ctx, R, uri, R->b.stage);
-  if (rc) return rc;
-  RG_CUDA(launch_p2c(fp64_view(R), R->b.stage, R->b.stage2, ctx->stream));
-  return from_soa(ctx, R, R->b.stage2, uu);
+  if (!uri || !uu) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
+  RG_CUDA(launch_p2c(d, B->stage, B->stage2, ctx->stream));
+  return from_soa(ctx, R, B->stage2, uu, d);
 }
 
 int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
-  const DevRun d = fp64_view(R);
+  if (!uri || !ww) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
   const size_t N = d.N;
-  int rc = to_soa(ctx, R, uri, R->b.stage);
-  if (rc) return rc;
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
   Scal sc{};
   sc.active = 1;
   RG_CUDA(cudaMemcpyAsync(d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
-  for (int dir = 1; dir <= 3; ++dir) RG_CUDA(launch_flux(d, dir, R->b.stage, R->b.F[dir - 1], ctx->stream));
-  RG_CUDA(launch_ct(d, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, ctx->stream));
+  for (int dir = 1; dir <= 3; ++dir) RG_CUDA(launch_flux(d, dir, B->stage, B->F[dir - 1], ctx->stream));
+  RG_CUDA(launch_ct(d, B->F[0], B->F[1], B->F[2], B->CT, ctx->stream));
   std::vector<double> F(27 * N), CT(6 * N);
   for (int dir = 0; dir < 3; ++dir)
-    RG_CUDA(cudaMemcpyAsync(F.data() + (size_t)dir * 9 * N, R->b.F[dir], 9 * N * sizeof(double),
+    RG_CUDA(cudaMemcpyAsync(F.data() + (size_t)dir * 9 * N, B->F[dir], 9 * N * sizeof(double),
                             cudaMemcpyDeviceToHost, ctx->stream));
-  RG_CUDA(cudaMemcpyAsync(CT.data(), R->b.CT, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(CT.data(), B->CT, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
   const int nm1 = d.nm1;
   for (int k = 1; k <= d.kmax; ++k)
@@ -611,28 +1087,81 @@ int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
   return RG_OK;
 }
 
+int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!mdot || !edot) return fail(RG_EINVAL_CONFIG, "null output");
+  const DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc) return rc;
+  // the run's current primitives in the full layout
+  RG_CUDA(launch_soa_to_aos(R->d, R->b.P[R->cur], B->stage2, ctx->stream));
+  int* nobad = nullptr;
+  RG_CUDA(launch_aos_to_soa(d, B->stage2, B->stage, nobad, ctx->stream));
+  Scal sc{};
+  sc.active = 1;
+  // fluxes on scratch scalar state: the run's own time state is left alone
+  Scal* tmp = nullptr;
+  RG_CUDA(cudaMalloc(&tmp, sizeof(Scal)));
+  DevRun dv = d;
+  dv.scal = tmp;
+  RG_CUDA(cudaMemcpyAsync(tmp, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
+  RG_CUDA(launch_flux(dv, 1, B->stage, B->F[0], ctx->stream));
+  // radial face nm1+1/2 (the inner edge of the interior): F1 of rho u^r and of the energy variable
+  const int i = d.nm1;
+  std::vector<double> f0((size_t)d.jmax * d.kmax), f4((size_t)d.jmax * d.kmax);
+  // in the full layout the faces (i, j, k) of fixed i lie imax values apart
+  const size_t rows = (size_t)d.jmax * d.kmax, pitch = (size_t)d.imax * sizeof(double);
+  RG_CUDA(cudaMemcpy2DAsync(f0.data(), sizeof(double), B->F[0] + d.cell(i, 1, 1), pitch, sizeof(double), rows,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaMemcpy2DAsync(f4.data(), sizeof(double), B->F[0] + 4 * d.N + d.cell(i, 1, 1), pitch, sizeof(double),
+                            rows, cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  cudaFree(tmp);
+  const Axis& X2 = R->geom.ax[1];
+  const Axis& X3 = R->geom.ax[2];
+  double m = 0.0, e = 0.0;
+  for (int k = d.nm1 + 1; k <= d.kmax - d.nm1; ++k)
+    for (int j = d.nm1 + 1; j <= d.jmax - d.nm1; ++j) {
+      const size_t o = (size_t)(j - 1) + (size_t)d.jmax * (k - 1);
+      const double area = X2.dx[j] * X3.dx[k];
+      m += f0[o] * area;
+      e += f4[o] * area;
+    }
+  *mdot = -m;
+  *edot = -e;
+  return RG_OK;
+}
+
 int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
-  int rc = to_soa(ctx, R, uu, R->b.stage);
-  if (rc) return rc;
-  if ((rc = to_soa(ctx, R, uri, R->b.stage2))) return rc;
-  RG_CUDA(launch_recov_only(fp64_view(R), R->b.stage, R->b.stage2, R->b.F[0], ctx->stream));
-  return from_soa(ctx, R, R->b.F[0], uri);
+  if (!uu || !uri) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uu, B->stage, d, false))) return rc;
+  if ((rc = to_soa(ctx, R, uri, B->stage2, d, false))) return rc;
+  RG_CUDA(launch_recov_only(d, B->stage, B->stage2, B->F[0], ctx->stream));
+  return from_soa(ctx, R, B->F[0], uri, d);
 }
 
 int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
-  int rc = to_soa(ctx, R, uri, R->b.stage);
-  if (rc) return rc;
+  if (!uri || !dtcfl) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
   Scal sc{};
   sc.active = 1;
   const double one = 1.0;
   std::memcpy(&sc.dtcfl_bits, &one, sizeof(double));
-  RG_CUDA(cudaMemcpyAsync(R->d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
-  RG_CUDA(launch_cfl(fp64_view(R), R->b.stage, ctx->stream));
-  RG_CUDA(cudaMemcpyAsync(&sc, R->d.scal, sizeof(Scal), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
+  RG_CUDA(launch_cfl(d, B->stage, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(&sc, d.scal, sizeof(Scal), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
   std::memcpy(dtcfl, &sc.dtcfl_bits, sizeof(double));
   return RG_OK;
@@ -641,16 +1170,18 @@ int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl) {
 int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
-  int rc = to_soa(ctx, R, uri, R->b.stage);
-  if (rc) return rc;
-  if ((rc = to_soa(ctx, R, urio, R->b.stage2))) return rc;
+  if (!uri || !urio) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
+  if ((rc = to_soa(ctx, R, urio, B->stage2, d, false))) return rc;
   Scal sc{};
   sc.active = 1;
-  RG_CUDA(cudaMemcpyAsync(R->d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
-  const DevRun d = fp64_view(R);
-  RG_CUDA(launch_bc(d, R->b.stage, R->b.stage2, ctx->stream));
-  RG_CUDA(launch_floor(d, R->b.stage, ctx->stream));
-  return from_soa(ctx, R, R->b.stage, uri);
+  RG_CUDA(cudaMemcpyAsync(d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
+  RG_CUDA(launch_bc(d, B->stage, B->stage2, ctx->stream));
+  RG_CUDA(launch_floor(d, B->stage, ctx->stream));
+  return from_soa(ctx, R, B->stage, uri, d);
 }
 
 }  // extern "C"
@@ -702,7 +1233,7 @@ extern "C" int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, dou
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!d_prims || !d_ww) return fail(RG_EINVAL_CONFIG, "null device buffer");
-  const size_t N = R->d.N;
+  const size_t N = R->nfull;
   if (N > kStaticMaxCells)
     return fail(RG_EINVAL_CONFIG, "rg_calflx_static: grid of " + std::to_string(N) +
                                       " cells exceeds the static scratch maximum of " +
@@ -720,7 +1251,7 @@ extern "C" int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, dou
     g_static_scal_addr[ctx->device] = static_cast<Scal*>(b);
   }
   double* ct = g_static_ct_addr[ctx->device];
-  DevRun d = fp64_view(R);
+  DevRun d = full_view(R);
   d.scal = g_static_scal_addr[ctx->device];  // the run's own time state is not touched
   cudaStream_t s = ctx->stream;
   // The arrays keep the previous call's contents: clear them first.

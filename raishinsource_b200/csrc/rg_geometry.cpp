@@ -455,6 +455,39 @@ double fm_ell(double a, double r) {
 
 }  // namespace
 
+// Seeded 1D RMHD Riemann problem in the pattern of mdshoctub
+// (mdgrmhd.f90:56-118): state[0] fills i <= imax/2, state[1] the rest.  The
+// states are drawn with uniform01 keyed by (seed, 16*tube + field): field 0
+// the shared B^x in [0, 5]; per side s (fields 1+7s ..) rho log-uniform in
+// [0.1, 10], p log-uniform in [0.01, 100], v^x, v^y, v^z uniform in
+// [-0.9, 0.9] (scaled down to |v| = 0.9 when larger), B^y, B^z uniform in
+// [-5, 5].  Primitives: util = gamma*v (Minkowski), uri(6) = p/rho**(gam-1).
+void tube_states(uint64_t seed, uint64_t tube, double gam, double state[2][9]) {
+  auto U = [&](int f) { return uniform01(seed, 16 * tube + (uint64_t)f); };
+  const double bx = 5.0 * U(0);
+  for (int side = 0; side < 2; ++side) {
+    const int f0 = 1 + 7 * side;
+    const double rho = std::pow(10.0, -1.0 + 2.0 * U(f0));
+    const double pg = std::pow(10.0, -2.0 + 4.0 * U(f0 + 1));
+    double v[3];
+    for (int a = 0; a < 3; ++a) v[a] = 0.9 * (2.0 * U(f0 + 2 + a) - 1.0);
+    const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (v2 > 0.81) {
+      const double scale = 0.9 / std::sqrt(v2);
+      for (double& x : v) x *= scale;
+    }
+    const double lor = 1.0 / std::sqrt(1.0 - (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    double* q = state[side];
+    q[0] = rho;
+    for (int a = 0; a < 3; ++a) q[1 + a] = lor * v[a];
+    q[4] = pg;
+    q[5] = pg * (1. / std::pow(rho, gam - 1.));
+    q[6] = bx;
+    q[7] = 5.0 * (2.0 * U(f0 + 5) - 1.0);
+    q[8] = 5.0 * (2.0 * U(f0 + 6) - 1.0);
+  }
+}
+
 void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double amp, double rin, double rmax,
               double beta, double kappa, std::vector<double>& P) {
   const int imax = p.imax, jmax = p.jmax, kmax = p.kmax;
@@ -535,7 +568,11 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
           at(5, i, j, k) = pr * (1.0 / std::pow(de, gam - 1.));
         }
       }
-  // normalise rho_max to 1, perturb p (mdgrmhd.f90:1198-1320)
+  // normalise rho_max to 1, perturb p (mdgrmhd.f90:1198-1320).  In a 2D phi
+  // slab (jmax = 2*nm1+1) the draw is keyed by the (r, theta) cell of the
+  // interior phi index, so that the slab holds one axisymmetric state.
+  const int nm1_ic = (p.irec == 5) ? 5 : 4;
+  const bool phi_slab = (jmax == 2 * nm1_ic + 1);
   for (int k = 1; k <= kmax; ++k)
     for (int j = 1; j <= jmax; ++j)
       for (int i = 1; i <= imax; ++i) {
@@ -545,7 +582,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
           const double rmin1 = p.dmin * std::pow(r, -1.5), pmin1 = p.pmin * (gam - 1.) * std::pow(r, -2.5);
           double de = at(0, i, j, k) * (1.0 / rhomax);
           double pr = at(4, i, j, k) * (1.0 / rhomax);
-          pr = pr * (1.0 + amp * (uniform01(seed, c) - 0.5));
+          pr = pr * (1.0 + amp * (uniform01(seed, phi_slab ? cidx(i, nm1_ic + 1, k) : c) - 0.5));
           if (de <= rmin1 || pr <= pmin1) {
             de = rmin1;
             pr = pmin1;

@@ -29,4 +29,7 @@ void build_geometry(const rg_run_params& p, HostGeom& g);
 void torus_ic(const rg_run_params& p, const HostGeom& g, uint64_t seed, double amp, double rin, double rmax,
               double beta, double kappa, std::vector<double>& prim);
 
+// Left/right primitive states of the seeded Riemann tube `tube` (mdshoctub pattern).
+void tube_states(uint64_t seed, uint64_t tube, double gam, double state[2][9]);
+
 }  // namespace rg

@@ -11,6 +11,10 @@
 // All state is FP64 structure-of-arrays; a step never synchronises the host.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <functional>
+#include <vector>
+
 #include "rg_device.cuh"
 #include "rg_kernels.cuh"
 
@@ -27,6 +31,16 @@ __device__ __forceinline__ void count_event(const DevRun& r, int which, bool fla
 __device__ __forceinline__ void load9(const double* __restrict__ P, size_t N, size_t c, double q[9]) {
 #pragma unroll
   for (int v = 0; v < 9; ++v) q[v] = P[(size_t)v * N + c];
+}
+
+// j and k of this thread for a kernel whose j (k) range starts at lo: the
+// slab index when the direction is a slab (one stored plane), otherwise from
+// the grid's y (z) coordinate.
+__device__ __forceinline__ int jidx(const DevRun& r, int lo, uint3 bid) {
+  return r.jfix ? r.jfix : (int)(bid.y * blockDim.y + threadIdx.y) + lo;
+}
+__device__ __forceinline__ int kidx(const DevRun& r, int lo, uint3 bid) {
+  return r.kfix ? r.kfix : (int)(bid.z * blockDim.z + threadIdx.z) + lo;
 }
 
 // ----------------------------------------------------------------- recov1a
@@ -280,7 +294,7 @@ __device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, co
   double uo[9];
   if (STAGE > 1) load9(r.Un, N, c, uo);
   const double a1 = dt / __ldg(r.dx1b + i - 1), a2 = dt / __ldg(r.dx2b + j - 1), a3 = dt / __ldg(r.dx3b + k - 1);
-  const size_t ci = c - 1, cj = c - (size_t)r.imax, ck = c - (size_t)r.imax * r.jmax;
+  const size_t ci = c - 1, cj = c - r.sj, ck = c - r.sk;
 #pragma unroll
   for (int v = 0; v < 9; ++v) {
     // flux-CT replaces ww(2,7) ww(3,7) ww(1,8) ww(3,8) ww(1,9) ww(2,9) (ct.f90:98-109)
@@ -382,7 +396,7 @@ __device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met&
   const float wo = (STAGE == 1) ? 0.f : (STAGE == 2 ? 0.75f : 1.0f / 3.0f);
   const float wc = (STAGE == 1) ? 1.f : (STAGE == 2 ? 0.25f : 2.0f / 3.0f);
   const float wf = wc;
-  const size_t ci = c - 1, cj = c - (size_t)r.imax, ck = c - (size_t)r.imax * r.jmax;
+  const size_t ci = c - 1, cj = c - r.sj, ck = c - r.sk;
   const float* F1 = r.F32[0];
   const float* F2 = r.F32[1];
   const float* F3 = r.F32[2];
@@ -427,17 +441,21 @@ __device__ __forceinline__ void queue_carry(const DevRun& r, int i, int j, int k
   else atomicAdd(r.cnt + C_CARRY_OVF, 1ull);
 }
 
+#ifndef RG_UPDATE_MINB
+#define RG_UPDATE_MINB 3
+#endif
+
 // One stage of every cell with radial index in [ilo, ihi]: interior cells get
 // the RK combine (FP64, or MIX = mixed precision for the cells beyond
 // r = 2 r_H) and recov1a; ghost cells copy their primitives through.
 template <int STAGE, bool MIX>
-__global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
+__device__ __forceinline__ void update_body(const DevRun& r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                                                 double* __restrict__ Pw, const double* __restrict__ F1,
                                                 const double* __restrict__ F2, const double* __restrict__ F3,
-                                                const double* __restrict__ CT, int ilo, int ihi) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + ilo;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+                                                const double* __restrict__ CT, int ilo, int ihi, const uint3 bid) {
+  const int i = bid.x * blockDim.x + threadIdx.x + ilo;
+  const int j = jidx(r, 1, bid);
+  const int k = kidx(r, 1, bid);
   if (i > ihi || j > r.jmax || k > r.kmax) return;
   const size_t N = r.N, c = r.cell(i, j, k);
   // A finished run (time > tmax) copies its state through the stage so that the
@@ -466,16 +484,21 @@ __global__ void __launch_bounds__(128) k_update(DevRun r, const double* __restri
   count_event(r, C_FAIL, ok && o.fail);
   count_event(r, C_CAP, ok && o.cap);
 }
+template <int STAGE, bool MIX>
+__global__ void __launch_bounds__(128, RG_UPDATE_MINB) k_update(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
+                                                double* __restrict__ Pw, const double* __restrict__ F1,
+                                                const double* __restrict__ F2, const double* __restrict__ F3,
+                                                const double* __restrict__ CT, int ilo, int ihi) { update_body<STAGE, MIX>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi, blockIdx); }
 
 // Resolve cells queued by k_update / k_recov in the reference's loop order
 // (k, j, i over the interior): each takes the final W of its predecessor cell.
 // One thread; runs only when cells were queued, which the reference data
 // rarely produces.  MODE 0: stage update; MODE 1: recov-only entry point.
 template <int MODE, int STAGE>
-__global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
-                            double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
-                            const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void carry_fix_body(const DevRun& r, const double* __restrict__ Pn, const double* __restrict__ Pc,
+                               double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
+                               const double* __restrict__ F3, const double* __restrict__ CT,
+                               const double* __restrict__ U) {
   if (MODE == 0 && !r.scal->active) return;
   int n = r.scal->carry_count;
   if (n <= 0) return;
@@ -540,6 +563,12 @@ __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const doubl
   }
   r.scal->carry_count = 0;
 }
+template <int MODE, int STAGE>
+__global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
+                            double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
+                            const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) carry_fix_body<MODE, STAGE>(r, Pn, Pc, Pw, F1, F2, F3, CT, U);
+}
 
 // ------------------------------------------------------------- face fluxes
 // Face f+1/2 in direction D over the hll range nm0..n-nm0 in every dimension
@@ -575,7 +604,7 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
                                           bool valid) {
   const unsigned mask = __activemask();
   const size_t N = r.N, c = r.cell(i, j, k);
-  const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.imax : (long long)r.imax * r.jmax);
+  const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.sj : (long long)r.sk);
   T q[9];
   if (IREC == 5) {
     const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;  // owner cell of this lane's state
@@ -644,40 +673,49 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
   }
 }
 
+// Resident blocks of 128 threads per SM the FP64 face kernel is compiled for
+// (registers per thread <= 65536 / (128 * blocks), in steps of 8).
+#ifndef RG_FLUX_MINB64
+#define RG_FLUX_MINB64 5
+#endif
+
 // Faces with radial index i in [ilo, ihi] (and the hll range in j, k) in
 // arithmetic type T on storage S.  The FP64 path launches it once over the
 // whole range; the mixed path launches FP64 for r < 2 r_H (faces i <=
 // i_fp64 + 1, copied to FP32 up to i_fp64) and FP32 beyond.
 template <int D, int IREC, typename T, typename S>
-__global__ void __launch_bounds__(128) k_flux(DevRun r, const S* __restrict__ P, S* __restrict__ F,
-                                              float* __restrict__ Fcopy, int icopy, int ilo, int ihi) {
+__device__ __forceinline__ void flux_body(const DevRun& r, const S* __restrict__ P, S* __restrict__ F,
+                                              float* __restrict__ Fcopy, int icopy, int ilo, int ihi, const uint3 bid) {
   if (!r.scal->active) return;
   const int nm0 = r.nm0;
   const int side = threadIdx.x & 1;
-  const int i0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 1) + ilo;
-  const int j0 = blockIdx.y * blockDim.y + threadIdx.y + nm0;
-  const int k0 = blockIdx.z * blockDim.z + threadIdx.z + nm0;
+  const int i0 = (int)((bid.x * blockDim.x + threadIdx.x) >> 1) + ilo;
+  const int j0 = jidx(r, nm0, bid);
+  const int k0 = kidx(r, nm0, bid);
   const bool valid = i0 <= ihi && j0 <= r.jmax - nm0 && k0 <= r.kmax - nm0;
   const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(k0, r.kmax - nm0);
   face_lane<D, IREC, T, S>(r, P, F, Fcopy, icopy, i, j, k, side, valid);
 }
+template <int D, int IREC, typename T, typename S>
+__global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_flux(DevRun r, const S* __restrict__ P, S* __restrict__ F,
+                                              float* __restrict__ Fcopy, int icopy, int ilo, int ihi) { flux_body<D, IREC, T, S>(r, P, F, Fcopy, icopy, ilo, ihi, blockIdx); }
 
 // ---------------------------------------------------------------- flux-CT
 // ct.f90:30-118 on nm1..n-nm1 in every dimension (edges with i in [ilo, ihi]),
 // in arithmetic type T on flux storage S.  CTcopy, if given, receives an FP32
 // copy (the FP64 edges next to the FP32 region of the mixed path).
 template <typename T, typename S>
-__global__ void __launch_bounds__(256) k_ct(DevRun r, const S* __restrict__ F1, const S* __restrict__ F2,
+__device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F1, const S* __restrict__ F2,
                                             const S* __restrict__ F3, S* __restrict__ CT,
-                                            float* __restrict__ CTcopy, int ilo, int ihi) {
+                                            float* __restrict__ CTcopy, int ilo, int ihi, const uint3 bid) {
   if (!r.scal->active) return;
   const int nm1 = r.nm1;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + ilo;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + nm1;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + nm1;
+  const int i = bid.x * blockDim.x + threadIdx.x + ilo;
+  const int j = jidx(r, nm1, bid);
+  const int k = kidx(r, nm1, bid);
   if (i > ihi || j > r.jmax - nm1 || k > r.kmax - nm1) return;
   const size_t N = r.N, c = r.cell(i, j, k);
-  const size_t di = 1, dj = (size_t)r.imax, dk = (size_t)r.imax * r.jmax;
+  const size_t di = 1, dj = r.sj, dk = r.sk;
   const S* fyx = F2 + 6 * N;  // ww(2,7)
   const S* fzx = F3 + 6 * N;  // ww(3,7)
   const S* fxy = F1 + 7 * N;  // ww(1,8)
@@ -705,8 +743,19 @@ __global__ void __launch_bounds__(256) k_ct(DevRun r, const S* __restrict__ F1, 
     if (CTcopy) CTcopy[(size_t)a * N + c] = float(o[a]);
   }
 }
+template <typename T, typename S>
+__global__ void __launch_bounds__(256) k_ct(DevRun r, const S* __restrict__ F1, const S* __restrict__ F2,
+                                            const S* __restrict__ F3, S* __restrict__ CT,
+                                            float* __restrict__ CTcopy, int ilo, int ihi) { ct_body<T, S>(r, F1, F2, F3, CT, CTcopy, ilo, ihi, blockIdx); }
 
 // ------------------------------------------------------------ boundaries
+// Transverse indices of a column of direction D: (j,k) for D = 1, (i,k) for
+// D = 2, (i,j) for D = 3; a slab direction contributes its fixed index.
+template <int D>
+__device__ __forceinline__ int col_fix1(const DevRun& r) { return D == 1 ? r.jfix : 0; }
+template <int D>
+__device__ __forceinline__ int col_fix2(const DevRun& r) { return D == 3 ? r.jfix : r.kfix; }
+
 // Layer n (1-based) along direction D of column (t1, t2).
 template <int D>
 __device__ __forceinline__ size_t col_cell(const DevRun& r, int t1, int t2, int n) {
@@ -718,13 +767,13 @@ __device__ __forceinline__ size_t col_cell(const DevRun& r, int t1, int t2, int 
 // bnd.f90:45-70, 156-180, 266-292: single-rank periodic copy for columns whose
 // transverse indices are interior.
 template <int D>
-__global__ void k_bc_periodic(DevRun r, double* __restrict__ P) {
+__device__ __forceinline__ void bc_periodic_body(const DevRun& r, double* __restrict__ P, const uint3 bid) {
   if (!r.scal->active) return;
   const int nm1 = r.nm1;
   const int n1 = (D == 1) ? r.jmax : r.imax;
   const int n2 = (D == 3) ? r.jmax : r.kmax;
-  const int t1 = blockIdx.x * blockDim.x + threadIdx.x + nm1 + 1;
-  const int t2 = blockIdx.y * blockDim.y + threadIdx.y + nm1 + 1;
+  const int t1 = col_fix1<D>(r) ? col_fix1<D>(r) : (int)(bid.x * blockDim.x + threadIdx.x) + nm1 + 1;
+  const int t2 = col_fix2<D>(r) ? col_fix2<D>(r) : (int)(bid.y * blockDim.y + threadIdx.y) + nm1 + 1;
   if (t1 > n1 - nm1 || t2 > n2 - nm1) return;
   const int len = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
   const int ib0 = 1 + nm1, ib1 = len - nm1;
@@ -738,15 +787,17 @@ __global__ void k_bc_periodic(DevRun r, double* __restrict__ P) {
       }
     }
 }
+template <int D>
+__global__ void k_bc_periodic(DevRun r, double* __restrict__ P) { bc_periodic_body<D>(r, P, blockIdx); }
 
 // bnd.f90:384-1058: physical boundary codes for every column of direction D.
 template <int D>
-__global__ void k_bc_phys(DevRun r, double* __restrict__ P, const double* __restrict__ Po) {
+__device__ __forceinline__ void bc_phys_body(const DevRun& r, double* __restrict__ P, const double* __restrict__ Po, const uint3 bid) {
   if (!r.scal->active) return;
   const int n1 = (D == 1) ? r.jmax : r.imax;
   const int n2 = (D == 3) ? r.jmax : r.kmax;
-  const int t1 = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int t2 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int t1 = col_fix1<D>(r) ? col_fix1<D>(r) : (int)(bid.x * blockDim.x + threadIdx.x) + 1;
+  const int t2 = col_fix2<D>(r) ? col_fix2<D>(r) : (int)(bid.y * blockDim.y + threadIdx.y) + 1;
   if (t1 > n1 || t2 > n2) return;
   const int nm1 = r.nm1;
   const int L = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
@@ -787,17 +838,19 @@ __global__ void k_bc_phys(DevRun r, double* __restrict__ P, const double* __rest
     }
   }
 }
+template <int D>
+__global__ void k_bc_phys(DevRun r, double* __restrict__ P, const double* __restrict__ Po) { bc_phys_body<D>(r, P, Po, blockIdx); }
 
 // ----------------------------------------------------------------- floors
 // infchk (bnd.f90:1636-1824, outer radial ghosts), atmosphere1a
 // (correction.f90:226-447) and pminmax2b (correction.f90:744-999) over every
 // cell, in place.  pminmax2b stores rho alone when its rescale loop changed rho
 // (the "elseif" at correction.f90:887-893).
-__global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P) {
+__device__ __forceinline__ void floor_body(const DevRun& r, double* __restrict__ P, const uint3 bid) {
   if (!r.scal->active) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  const int i = bid.x * blockDim.x + threadIdx.x + 1;
+  const int j = jidx(r, 1, bid);
+  const int k = kidx(r, 1, bid);
   if (i > r.imax || j > r.jmax || k > r.kmax) return;
   const size_t N = r.N, c = r.cell(i, j, k);
   double q[9];
@@ -887,6 +940,7 @@ __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P)
 #pragma unroll
     for (int v = 0; v < 9; ++v) r.P32[(size_t)v * N + c] = (float)q[v];
 }
+__global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P) { floor_body(r, P, blockIdx); }
 
 // FP32 copy of a primitive array (mixed runs, after initial data or upload).
 __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
@@ -898,11 +952,11 @@ __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, si
 // cdtcfl4 (cdtcfl.f90:2-129) with calcha4 (calcha.f90:129-367) over
 // is1+1..ie1-1 (every dimension); min over cells, then over blocks with an
 // atomicMin on the bit pattern (positive doubles order like their bits).
-__global__ void __launch_bounds__(128) k_cfl(DevRun r, const double* __restrict__ P) {
+__device__ __forceinline__ void cfl_body(const DevRun& r, const double* __restrict__ P, const uint3 bid) {
   if (!r.scal->active) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+  const int i = bid.x * blockDim.x + threadIdx.x + 2;
+  const int j = jidx(r, 2, bid);
+  const int k = kidx(r, 2, bid);
   double dtc = 1.0;
   if (i <= r.imax - 1 && j <= r.jmax - 1 && k <= r.kmax - 1) {
     const size_t c = r.cell(i, j, k);
@@ -942,34 +996,39 @@ __global__ void __launch_bounds__(128) k_cfl(DevRun r, const double* __restrict_
     if (t == 0 && x > 0.0) atomicMin(&r.scal->dtcfl_bits, (unsigned long long)__double_as_longlong(x));
   }
 }
+__global__ void __launch_bounds__(128) k_cfl(DevRun r, const double* __restrict__ P) { cfl_body(r, P, blockIdx); }
 
-__global__ void k_step_begin(DevRun r) {
+__device__ __forceinline__ void step_begin_body(const DevRun& r) {
   Scal* s = r.scal;
   if (!s->active) return;
   s->time = s->timeh;  // main.f90:617-620
   if (s->time > r.tmax) { s->active = 0; return; }
   s->dtcfl_bits = (unsigned long long)__double_as_longlong(1.0);
 }
-
-__global__ void k_dt(DevRun r) {
+__device__ __forceinline__ void dt_body(const DevRun& r) {
   Scal* s = r.scal;
   if (!s->active) return;
   const double dtcfl = __longlong_as_double((long long)s->dtcfl_bits);
   s->dt = r.cfl * dtcfl;  // main.f90:763
   s->timeh = s->time + s->dt;
 }
-
-__global__ void k_step_end(DevRun r) {
-  if (!r.scal->active) return;
-  atomicAdd(r.cnt + C_STEPS, 1ull);
+// The buffer rotation advances every step (a finished run copies its state
+// through the stages), the step count only while the run is active.
+__device__ __forceinline__ void step_end_body(const DevRun& r) {
+  Scal* s = r.scal;
+  s->cur = (s->cur + 1) % 3;
+  if (s->active) atomicAdd(r.cnt + C_STEPS, 1ull);
 }
+__global__ void k_step_begin(DevRun r) { step_begin_body(r); }
+__global__ void k_dt(DevRun r) { dt_body(r); }
+__global__ void k_step_end(DevRun r) { step_end_body(r); }
 
 // ------------------------------------------------- per-routine entry points
 __global__ void __launch_bounds__(128) k_recov(DevRun r, const double* __restrict__ U, const double* __restrict__ Pc,
                                                double* __restrict__ Pw) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  const int j = jidx(r, 1, blockIdx);
+  const int k = kidx(r, 1, blockIdx);
   if (i > r.imax || j > r.jmax || k > r.kmax) return;
   const size_t N = r.N, c = r.cell(i, j, k);
   if (!is_interior(r, i, j, k)) {
@@ -996,8 +1055,8 @@ __global__ void __launch_bounds__(128) k_recov(DevRun r, const double* __restric
 // caluu1 (caluu.f90:2-126) on every cell
 __global__ void __launch_bounds__(128) k_p2c(DevRun r, const double* __restrict__ P, double* __restrict__ U) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  const int j = jidx(r, 1, blockIdx);
+  const int k = kidx(r, 1, blockIdx);
   if (i > r.imax || j > r.jmax || k > r.kmax) return;
   const size_t N = r.N, c = r.cell(i, j, k);
   double q[9], u[9];
@@ -1011,18 +1070,41 @@ __global__ void __launch_bounds__(128) k_p2c(DevRun r, const double* __restrict_
   for (int v = 0; v < 9; ++v) U[(size_t)v * N + c] = u[v];
 }
 
-// a(nv, cell) <-> SoA
-__global__ void k_aos_to_soa(const double* __restrict__ a, double* __restrict__ s, size_t N) {
-  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= N) return;
+// a(nv, cell) of the reference's full array <-> stored SoA.  Upload reads the
+// stored cells' values and flags (bad != 0) any full-array cell whose value
+// differs from the stored cell it maps to: a slab direction holds one plane,
+// so its data must be uniform along it.  Download writes every full cell.
+__global__ void k_aos_to_soa(DevRun r, const double* __restrict__ a, double* __restrict__ s, int* bad) {
+  const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t nfull = (size_t)r.imax * r.jmax * r.kmax;
+  if (f >= nfull) return;
+  const int i = (int)(f % r.imax) + 1;
+  const int j = (int)((f / r.imax) % r.jmax) + 1;
+  const int k = (int)(f / ((size_t)r.imax * r.jmax)) + 1;
+  const bool owner = (!r.jfix || j == r.jfix) && (!r.kfix || k == r.kfix);
+  const size_t c = r.cell(i, j, k);
+  if (owner) {
 #pragma unroll
-  for (int v = 0; v < 9; ++v) s[(size_t)v * N + c] = a[9 * c + v];
+    for (int v = 0; v < 9; ++v) s[(size_t)v * r.N + c] = a[9 * f + v];
+  } else if (bad) {
+    const size_t o = r.cell_full(i, r.jfix ? r.jfix : j, r.kfix ? r.kfix : k);
+    bool same = true;
+#pragma unroll
+    for (int v = 0; v < 9; ++v)
+      same = same && (__double_as_longlong(a[9 * f + v]) == __double_as_longlong(a[9 * o + v]));
+    if (!same) atomicOr(bad, 1);
+  }
 }
-__global__ void k_soa_to_aos(const double* __restrict__ s, double* __restrict__ a, size_t N) {
-  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= N) return;
+__global__ void k_soa_to_aos(DevRun r, const double* __restrict__ s, double* __restrict__ a) {
+  const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t nfull = (size_t)r.imax * r.jmax * r.kmax;
+  if (f >= nfull) return;
+  const int i = (int)(f % r.imax) + 1;
+  const int j = (int)((f / r.imax) % r.jmax) + 1;
+  const int k = (int)(f / ((size_t)r.imax * r.jmax)) + 1;
+  const size_t c = r.cell(i, j, k);
 #pragma unroll
-  for (int v = 0; v < 9; ++v) a[9 * c + v] = s[(size_t)v * N + c];
+  for (int v = 0; v < 9; ++v) a[9 * f + v] = s[(size_t)v * r.N + c];
 }
 __global__ void k_fill(double* p, double v, size_t n) {
   const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1054,6 +1136,16 @@ inline dim3 grid3(int nx, int ny, int nz, dim3 b) {
   return dim3((unsigned)((nx + (int)b.x - 1) / (int)b.x), (unsigned)((ny + (int)b.y - 1) / (int)b.y),
               (unsigned)((nz + (int)b.z - 1) / (int)b.z));
 }
+// Block shape and grid of a cell kernel over (nx, ny, nz): a slab direction
+// has one index, so its block and grid extent fold to 1 (its threads move to x).
+inline dim3 sblock(const DevRun& r, dim3 b) {
+  if (r.jfix) { b.x *= b.y; b.y = 1; }
+  if (r.kfix) { b.x *= b.z; b.z = 1; }
+  return b;
+}
+inline dim3 sgrid(const DevRun& r, int nx, int ny, int nz, dim3 b) {
+  return grid3(nx, r.jfix ? 1 : ny, r.kfix ? 1 : nz, b);
+}
 
 }  // namespace
 
@@ -1072,8 +1164,8 @@ cudaError_t launch_step_end(const DevRun& r, cudaStream_t s) {
 }
 
 cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s) {
-  const dim3 b(64, 2, 1);
-  k_cfl<<<grid3(r.imax - 2, r.jmax - 2, r.kmax - 2, b), b, 0, s>>>(r, P);
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  k_cfl<<<sgrid(r, r.imax - 2, r.jmax - 2, r.kmax - 2, b), b, 0, s>>>(r, P);
   return cudaGetLastError();
 }
 
@@ -1082,8 +1174,8 @@ static void launch_flux_t(const DevRun& r, int dir, const S* P, S* F, float* Fco
                           cudaStream_t s) {
   if (ihi < ilo) return;
   const int n = ihi - ilo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
-  const dim3 b(64, 2, 1);
-  const dim3 g = grid3(2 * n, m, l, b);  // two lanes per face
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 g = sgrid(r, 2 * n, m, l, b);  // two lanes per face
   if (r.irec == 5) {
     if (dir == 1) k_flux<1, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
     else if (dir == 2) k_flux<2, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
@@ -1122,16 +1214,16 @@ cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cu
 cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
                       cudaStream_t s) {
   const int lo = r.nm1, hi = r.imax - r.nm1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
-  const dim3 b(64, 4, 1);
+  const dim3 b = sblock(r, dim3(64, 4, 1));
   if (!r.mixed) {
-    k_ct<double, double><<<grid3(hi - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, nullptr, lo, hi);
+    k_ct<double, double><<<sgrid(r, hi - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, nullptr, lo, hi);
   } else {
     const int split = fp64_split(r, lo, hi);
     if (split >= lo)
-      k_ct<double, double><<<grid3(split - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, r.CT32, lo, split);
+      k_ct<double, double><<<sgrid(r, split - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, r.CT32, lo, split);
     if (split < hi)
-      k_ct<float, float><<<grid3(hi - split, m, l, b), b, 0, s>>>(r, r.F32[0], r.F32[1], r.F32[2], r.CT32,
-                                                                     nullptr, split + 1, hi);
+      k_ct<float, float><<<sgrid(r, hi - split, m, l, b), b, 0, s>>>(r, r.F32[0], r.F32[1], r.F32[2], r.CT32,
+                                                                         nullptr, split + 1, hi);
   }
   return cudaGetLastError();
 }
@@ -1141,8 +1233,8 @@ static void launch_update_t(const DevRun& r, int stage, const double* Pn, const 
                             const double* F1, const double* F2, const double* F3, const double* CT, int ilo,
                             int ihi, cudaStream_t s) {
   if (ihi < ilo) return;
-  const dim3 b(64, 2, 1);
-  const dim3 g = grid3(ihi - ilo + 1, r.jmax, r.kmax, b);
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 g = sgrid(r, ihi - ilo + 1, r.jmax, r.kmax, b);
   if (stage == 1) k_update<1, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
   else if (stage == 2) k_update<2, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
   else k_update<3, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
@@ -1194,44 +1286,82 @@ static bool any_code(const DevRun& r, int side0, bool periodic) {
   return false;
 }
 
+// Columns (n1 x n2) of a boundary pass; a transverse slab direction has one column.
+static void bc_shape(int n1, int n2, bool fix1, bool fix2, dim3& g, dim3& b) {
+  b = dim3(fix1 ? 1 : (fix2 ? 128 : 32), fix2 ? 1 : (fix1 ? 128 : 4), 1);
+  g = grid3(fix1 ? 1 : n1, fix2 ? 1 : n2, 1, b);
+}
+
+int n_bc_launches(const DevRun& r) {
+  int n = 0;
+  for (int d = 0; d < 3; ++d) {
+    const bool slab = (d == 1 && r.jfix) || (d == 2 && r.kfix);  // ghost fill of a slab plane is a no-op
+    if (slab) continue;
+    n += any_code(r, 2 * d, true) + any_code(r, 2 * d, false);
+  }
+  return n;
+}
+
 cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t s) {
-  const dim3 b(32, 4, 1);
   const int nm1 = r.nm1;
-  // periodic passes on interior columns (bndpefb4), then physical passes on all columns (bndryfb4)
-  if (any_code(r, 0, true)) k_bc_periodic<1><<<grid3(r.jmax - 2 * nm1, r.kmax - 2 * nm1, 1, b), b, 0, s>>>(r, P);
-  if (any_code(r, 2, true)) k_bc_periodic<2><<<grid3(r.imax - 2 * nm1, r.kmax - 2 * nm1, 1, b), b, 0, s>>>(r, P);
-  if (any_code(r, 4, true)) k_bc_periodic<3><<<grid3(r.imax - 2 * nm1, r.jmax - 2 * nm1, 1, b), b, 0, s>>>(r, P);
-  if (any_code(r, 0, false)) k_bc_phys<1><<<grid3(r.jmax, r.kmax, 1, b), b, 0, s>>>(r, P, Po);
-  if (any_code(r, 2, false)) k_bc_phys<2><<<grid3(r.imax, r.kmax, 1, b), b, 0, s>>>(r, P, Po);
-  if (any_code(r, 4, false)) k_bc_phys<3><<<grid3(r.imax, r.jmax, 1, b), b, 0, s>>>(r, P, Po);
+  const bool jf = r.jfix != 0, kf = r.kfix != 0;
+  dim3 g, b;
+  // periodic passes on interior columns (bndpefb4), then physical passes on all
+  // columns (bndryfb4); a slab direction's own passes copy its plane onto itself
+  if (any_code(r, 0, true)) {
+    bc_shape(r.jmax - 2 * nm1, r.kmax - 2 * nm1, jf, kf, g, b);
+    k_bc_periodic<1><<<g, b, 0, s>>>(r, P);
+  }
+  if (!jf && any_code(r, 2, true)) {
+    bc_shape(r.imax - 2 * nm1, r.kmax - 2 * nm1, false, kf, g, b);
+    k_bc_periodic<2><<<g, b, 0, s>>>(r, P);
+  }
+  if (!kf && any_code(r, 4, true)) {
+    bc_shape(r.imax - 2 * nm1, r.jmax - 2 * nm1, false, jf, g, b);
+    k_bc_periodic<3><<<g, b, 0, s>>>(r, P);
+  }
+  if (any_code(r, 0, false)) {
+    bc_shape(r.jmax, r.kmax, jf, kf, g, b);
+    k_bc_phys<1><<<g, b, 0, s>>>(r, P, Po);
+  }
+  if (!jf && any_code(r, 2, false)) {
+    bc_shape(r.imax, r.kmax, false, kf, g, b);
+    k_bc_phys<2><<<g, b, 0, s>>>(r, P, Po);
+  }
+  if (!kf && any_code(r, 4, false)) {
+    bc_shape(r.imax, r.jmax, false, jf, g, b);
+    k_bc_phys<3><<<g, b, 0, s>>>(r, P, Po);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s) {
-  const dim3 b(64, 2, 1);
-  k_floor<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P);
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  k_floor<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P);
   return cudaGetLastError();
 }
 
 cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s) {
-  const dim3 b(64, 2, 1);
-  k_recov<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  k_recov<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
   k_carry_fix<1, 1><<<1, 1, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
   return cudaGetLastError();
 }
 
 cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s) {
-  const dim3 b(64, 2, 1);
-  k_p2c<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P, U);
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  k_p2c<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P, U);
   return cudaGetLastError();
 }
 
-cudaError_t launch_aos_to_soa(const double* aos, double* soa, size_t N, cudaStream_t s) {
-  k_aos_to_soa<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(aos, soa, N);
+cudaError_t launch_aos_to_soa(const DevRun& r, const double* aos, double* soa, int* bad, cudaStream_t s) {
+  const size_t n = (size_t)r.imax * r.jmax * r.kmax;
+  k_aos_to_soa<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(r, aos, soa, bad);
   return cudaGetLastError();
 }
-cudaError_t launch_soa_to_aos(const double* soa, double* aos, size_t N, cudaStream_t s) {
-  k_soa_to_aos<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(soa, aos, N);
+cudaError_t launch_soa_to_aos(const DevRun& r, const double* soa, double* aos, cudaStream_t s) {
+  const size_t n = (size_t)r.imax * r.jmax * r.kmax;
+  k_soa_to_aos<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(r, soa, aos);
   return cudaGetLastError();
 }
 cudaError_t launch_geom_derive(const DevRun& r, double* mc, double* mi, double* mk, double* fl_de, double* fl_pr,
@@ -1244,5 +1374,7 @@ cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s) {
   k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, v, n);
   return cudaGetLastError();
 }
+
+#include "rg_batch.cuh"
 
 }  // namespace rg

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "rg_types.h"
 
 namespace rg {
@@ -29,15 +31,28 @@ cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s);
 // per-routine entry points
 cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s);
 cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s);
-cudaError_t launch_aos_to_soa(const double* aos, double* soa, size_t N, cudaStream_t s);
-cudaError_t launch_soa_to_aos(const double* soa, double* aos, size_t N, cudaStream_t s);
+// reference layout a(nv,i,j,k) of the full array <-> the run's stored SoA
+// (bad, if given, is set non-zero when the data are not uniform along a slab direction)
+cudaError_t launch_aos_to_soa(const DevRun& r, const double* aos, double* soa, int* bad, cudaStream_t s);
+cudaError_t launch_soa_to_aos(const DevRun& r, const double* soa, double* aos, cudaStream_t s);
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s);
 int n_flux_launches(const DevRun& r);
 int n_ct_launches(const DevRun& r);
 int n_update_launches(const DevRun& r);
+int n_bc_launches(const DevRun& r);
 cudaError_t launch_to_f32(const double* a, float* b, size_t n, cudaStream_t s);
 // derived metric fields of the three caches and the radial floor profiles (run setup)
 cudaError_t launch_geom_derive(const DevRun& r, double* mc, double* mi, double* mk, double* fl_de, double* fl_pr,
                                cudaStream_t s);
+
+// Batched steps of runs of one class (rg_batch.cuh).
+struct BatchPlan;
+int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out);
+void batch_destroy(BatchPlan* B);
+int batch_launch_count(const BatchPlan* B);
+void batch_set_grid(BatchPlan* B, int factor);
+cudaError_t batch_issue(const BatchPlan* B, int idx, cudaStream_t s);
+cudaError_t batch_step(const BatchPlan* B, cudaStream_t s);
+int batch_launch_kind(const BatchPlan* B, int idx, int* dir);
 
 }  // namespace rg

@@ -29,6 +29,8 @@ struct Scal {
   double timeh;                   // time + dt
   int active;                     // 0 once time > tmax: every kernel of the step returns early
   int carry_count;                // cells queued for the loop-order W carry fix-up
+  int cur;                        // index of P^n among the run's three primitive buffers
+  int pad;
 };
 
 // Counters (device, atomically accumulated).
@@ -37,19 +39,30 @@ enum Counter {
 };
 
 // Everything a kernel needs, by value.  Arrays are structure-of-arrays with
-// the cell index c = (i-1) + imax*((j-1) + jmax*(k-1)) (1-based i, j, k) and
-// variable v at offset v*N.  Metric caches are per (i,k) point
-// q = (i-1) + imax*(k-1), 18 components each (see Met in rg_device.cuh).
+// the cell index c = (i-1) + sj*(j-1) + sk*(k-1) (1-based i, j, k; sj = imax,
+// sk = imax*jmax unless a direction is a slab) and variable v at offset v*N.
+// Metric caches are per (i,k) point q = (i-1) + imax*(k-1), kMetComps
+// components each (see MetT in rg_device.cuh).
 struct DevRun {
-  int imax, jmax, kmax;
+  int imax, jmax, kmax;  // logical extents incl. ghosts (the reference's array bounds)
+  // Slab directions.  A direction of extent 2*nm1+1 (one interior cell) whose
+  // boundaries copy the interior cell (periodic or copy codes) and on which the
+  // metric does not depend holds the same state in every one of its cells after
+  // each ghost fill: the reference's 2D phi slab and the transverse directions
+  // of a 1D tube.  Such a direction is stored as a single plane; kernels compute
+  // only its interior index jfix/kfix and read neighbours in it at stride 0.
+  int jfix, kfix;        // the computed index of a slab direction, 0 otherwise
+  int kmet;              // metric caches hold one theta row (a theta slab), 0 otherwise
+  int jpl, kpl;          // stored planes in j and k (1 along a slab direction)
+  size_t sj, sk;         // storage strides of j and k neighbours (0 along a slab direction)
   int nm0, nm1;
   int irec, model, guard, iter;
   int mixed;             // 1: FP32 reconstruction/fluxes/CT/RK combine (RG_MIXED)
   int gkind;             // x**gam form: 1 gam == 4/3, 2 gam == 5/3 (cube roots), 0 pow
   int i_fp64;            // radial cells 1..i_fp64 (r < 2 r_H) keep FP64 in the mixed path
   int nmax_cfl;          // nm1*2 + (nm1-1) (cdtcfl.f90:38)
-  size_t N;              // cells
-  size_t nik;            // (i,k) points
+  size_t N;              // stored cells (imax * jpl * kpl)
+  size_t nik;            // (i,k) points of the metric caches (imax for a theta slab)
   double gam, cfl, dmin, pmin, pmax, tmax;
   const double* mc;      // metric at cell centres (also the phi faces)
   const double* mi;      // metric at the r faces x1a(i)
@@ -76,15 +89,24 @@ struct DevRun {
   const double* dx2s;
   const double* dx3s;
   int ibc[6][9];
+  double* P[3];          // the run's rotating primitive buffers (P^n = P[scal->cur])
+  double* F[3];          // FP64 face fluxes per direction
+  double* CT;            // FP64 flux-CT values
   Scal* scal;
   unsigned long long* cnt;
   int* carry_list;       // interior cells queued for the W carry fix-up
   int carry_cap;
 
   RG_HD size_t cell(int i, int j, int k) const {
+    return (size_t)(i - 1) + sj * (size_t)(j - 1) + sk * (size_t)(k - 1);
+  }
+  // index of cell (i,j,k) in the reference's full array (imax*jmax*kmax cells)
+  RG_HD size_t cell_full(int i, int j, int k) const {
     return (size_t)(i - 1) + (size_t)imax * ((size_t)(j - 1) + (size_t)jmax * (size_t)(k - 1));
   }
-  RG_HD size_t ik(int i, int k) const { return (size_t)(i - 1) + (size_t)imax * (size_t)(k - 1); }
+  // metric-cache point of (i, k); a theta slab (Minkowski only, so the metric
+  // is the same at every k) keeps one row, also in the full-layout view
+  RG_HD size_t ik(int i, int k) const { return (size_t)(i - 1) + (kmet ? 0 : (size_t)imax * (size_t)(k - 1)); }
 };
 
 }  // namespace rg

@@ -217,3 +217,41 @@ def test_mixed_precision_tracks_fp64(gpu_ctx, irec):
     l1 = _l1(a, b, config.ghost_widths(irec)[1])
     assert l1[0] < 1e-5, l1
     assert l1[[4, 6, 8]].max() < 1e-4, l1
+
+
+def test_slab_2d_equals_full_compute(gpu_ctx):
+    """The 2D phi slab (jmax = 2*nm1+1) is stored as one plane; stepping it
+    gives the primitives of computing all jmax planes (RG_FLAG_FULL) to the
+    per-step bound (the two are separately compiled kernels, so FMA
+    contraction may differ in the last bit)."""
+    p = dict(config.torus(nr=64, nth=48), guard=1)
+    rs = gpu_ctx.admit(p)
+    rf = gpu_ctx.admit(dict(p, flags=config.FLAG_FULL))
+    rs.ic_torus(seed=11)
+    rf.ic_torus(seed=11)
+    ss = rs.step(5, stats=True)
+    sf = rf.step(5, stats=True)
+    a, b = rs.prims(), rf.prims()
+    rs.release()
+    rf.release()
+    assert ss["time"] == pytest.approx(sf["time"], rel=1e-13)
+    err = field_err(a, b)
+    assert err.max() < 1e-12, err
+    # every phi plane of the download is the stored plane
+    assert (a == a[:, 4:5]).all()
+
+
+def test_slab_rejects_nonuniform_upload(gpu_ctx):
+    from raishinsource_b200.capi import RgError
+    p = dict(config.torus(nr=40, nth=40), guard=1)
+    o = Oracle(p)
+    o.ic_torus(seed=3)
+    u = o.prims()
+    r = gpu_ctx.admit(p)
+    r.upload_prims(u)  # uniform along phi: accepted
+    u2 = u.copy()
+    u2[:, 0, :, 0] *= 1.01  # one phi ghost plane differs
+    with pytest.raises(RgError) as e:
+        r.upload_prims(u2)
+    r.release()
+    assert e.value.code == 1
