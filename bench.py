@@ -122,6 +122,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, device: str = "cuda") -> float:
+    """The maximum of x over the ranks of the default process group (x itself
+    without one): replicas are timed by their slowest rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -172,13 +184,6 @@ def run_gpu(args) -> dict | None:
     def barrier():
         if ws > 1:
             torch.distributed.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
 
     # warm-up (also the first use of every kernel)
     run.step(args.warmup)
@@ -247,14 +252,15 @@ def run_gpu(args) -> dict | None:
     run.release()
     extra = {}
     if ws == 1:
-        if args.mixed_steps > 0:
-            extra["mixed"] = section_mixed(ctx, args)
-        if args.torus2d_steps > 0:
-            extra["torus2d"] = section_torus2d(ctx, args)
-        if args.tubes > 0:
-            extra["batched_tubes"] = section_tubes(ctx, args)
-        if args.serve_requests > 0:
-            extra["serving"] = section_serving(ctx, args)
+        sections = (("mixed", args.mixed_steps, section_mixed), ("torus2d", args.torus2d_steps, section_torus2d),
+                    ("batched_tubes", args.tubes, section_tubes), ("serving", args.serve_requests, section_serving))
+        for name, n, fn in sections:
+            if n > 0:
+                t = time.perf_counter()
+                extra[name] = fn(ctx, args)
+                extra[name]["section_wall_s"] = time.perf_counter() - t
+                print(f"[bench] section {name} done in {extra[name]['section_wall_s']:.1f} s", file=sys.stderr,
+                      flush=True)
     ctx.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
@@ -362,12 +368,15 @@ def section_tubes(ctx, args) -> dict:
     from raishinsource_b200 import config
     rng = np.random.default_rng(2012)
     lengths = rng.integers(400, 3201, size=args.tubes)
-    out = {"tubes": args.tubes, "lengths": [int(lengths.min()), int(lengths.max())], "tmax": args.tube_tmax}
+    out = {"tubes": args.tubes, "lengths": [int(lengths.min()), int(lengths.max())], "tmax": args.tube_tmax,
+           "timed_steps": "to t = tmax" if args.tube_steps <= 0 else args.tube_steps,
+           "note": ("zone-updates/s counts interior cells of active tubes; latencies are the wall time at which a "
+                    "tube passed tmax, null unless all tubes finished in the timed steps")}
     finals = {}
     for prec in ("fp64", "mixed"):
         runs = []
         for t, n in enumerate(lengths):
-            r = ctx.admit(config.tube(n=int(n), tmax=args.tube_tmax, precision=prec))
+            r = ctx.admit(dict(config.tube(n=int(n), tmax=args.tube_tmax, precision=prec), guard=args.guard))
             r.ic_tube(seed=2012, tube=t)
             runs.append(r)
         stream = torch.cuda.current_stream()
@@ -375,13 +384,16 @@ def section_tubes(ctx, args) -> dict:
         t0 = time.perf_counter()
         e0, e1 = _events()
         e0.record(stream)
-        chunk, steps, done_at = 64, 0, {}
-        while True:
-            st = ctx.step_batch(runs, chunk, stats=True)
+        # every tube ends within imax steps (dt >= cfl*dx once speeds are clipped to 1); by default only the
+        # first --tube-steps steps are timed (see the section notes)
+        chunk, steps, done_at = 32, 0, {}
+        cap = 2 * (int(lengths.max()) + 16) if args.tube_steps <= 0 else args.tube_steps
+        while steps < cap:
+            st = ctx.step_batch(runs, chunk, stats=True, strict=False)
             steps += chunk
             now = time.perf_counter() - t0
             for k, x in enumerate(st):
-                if k not in done_at and x["time"] > args.tube_tmax:
+                if k not in done_at and not (x["time"] <= args.tube_tmax):
                     done_at[k] = now
             if len(done_at) == len(runs):
                 break
@@ -390,17 +402,24 @@ def section_tubes(ctx, args) -> dict:
         ms = e0.elapsed_time(e1)
         zu = sum(x["steps"] * int(n) for x, n in zip(st, lengths))
         info = ctx.batch_info(runs)
-        lat = np.array(sorted(done_at.values()))
+        lat = np.array(sorted(done_at.values())) if len(done_at) == len(runs) else None
         out[prec] = {"value": zu / (ms * 1e-3), "unit": "zone-updates/s", "zone_updates": int(zu),
-                     "batch_steps": steps, "wall_ms": ms, "p50_run_latency_s": float(np.percentile(lat, 50)),
-                     "p99_run_latency_s": float(np.percentile(lat, 99)), "tuned": info,
-                     "floor_caps": int(sum(x["floor_cap"] for x in st))}
-        finals[prec] = [r.prims()[4, 4, :, 0] for r in runs]  # rho along the tube
+                     "batch_steps": steps, "wall_ms": ms,
+                     "p50_run_latency_s": None if lat is None else float(np.percentile(lat, 50)),
+                     "p99_run_latency_s": None if lat is None else float(np.percentile(lat, 99)), "tuned": info,
+                     "capped_rescale_loops": {"recov_w": int(sum(x["recov_cap"] for x in st)),
+                                              "pminmax2b": int(sum(x["floor_cap"] for x in st))},
+                     "recov_fail": int(sum(x["recov_fail"] for x in st)),
+                     "recov_nr2": int(sum(x["recov_nr2"] for x in st)),
+                     "unfinished_tubes": len(runs) - len(done_at)}
+        finals[prec] = [r.stored_prims()[0, 0, 0, :] for r in runs]  # rho along the tube
         for r in runs:
             r.release()
-    num = sum(np.abs(a - b).sum() for a, b in zip(finals["mixed"], finals["fp64"]))
-    den = sum(np.abs(b).sum() for b in finals["fp64"])
-    out["l1_rel_rho_mixed_vs_fp64"] = float(num / den)
+    fin = [np.isfinite(a).all() and np.isfinite(b).all() for a, b in zip(finals["mixed"], finals["fp64"])]
+    num = sum(np.abs(a - b).sum() for a, b, f in zip(finals["mixed"], finals["fp64"], fin) if f)
+    den = sum(np.abs(b).sum() for b, f in zip(finals["fp64"], fin) if f)
+    out["l1_rel_rho_mixed_vs_fp64"] = float(num / den) if den > 0 else None
+    out["nonfinite_tubes"] = int(len(fin) - sum(fin))
     return out
 
 
@@ -457,6 +476,8 @@ def main():
     ap.add_argument("--torus2d-steps", type=int, default=1000, help="steps of the 2D torus section (0 = skip)")
     ap.add_argument("--tubes", type=int, default=1024, help="Riemann tubes of the batched section (0 = skip)")
     ap.add_argument("--tube-tmax", type=float, default=0.4)
+    ap.add_argument("--tube-steps", type=int, default=96,
+                    help="batch steps timed in the tube section (0 = run every tube to tmax)")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving section (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--serve-steps", type=int, default=2000)

@@ -131,6 +131,14 @@ int rg_run_ic_tube(rg_ctx* ctx, int run, uint64_t seed, uint64_t tube);
 int rg_run_upload_prims(rg_ctx* ctx, int run, const double* uri, double t0);
 int rg_run_download_prims(rg_ctx* ctx, int run, double* uri);
 
+/* The run's stored layout (a slab direction holds one plane): ncells stored
+ * cells, jplanes and kplanes stored planes in j and k; rg_run_download_stored
+ * copies the primitives as stored, variable v of stored cell
+ * c = (i-1) + imax*((j-1) + jplanes*(k-1)) at v*ncells + c (9*ncells doubles),
+ * j and k counted within the stored planes. */
+int rg_run_layout(rg_ctx* ctx, int run, size_t* ncells, int* jplanes, int* kplanes);
+int rg_run_download_stored(rg_ctx* ctx, int run, double* soa);
+
 /* Advance nsteps full RK3 steps of main.f90:586-1147 on the device (CFL
  * reduction, three stages, ghost fill, floors).  Stops early once the loop-top
  * time exceeds tmax.  Asynchronous on the context stream unless stats != NULL.
@@ -176,6 +184,18 @@ int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri);
 int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl);
 /* bnd4 + infchk + atmosphere1a + pminmax2b (bnd.f90, correction.f90) on uri in/out */
 int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio);
+
+/* Restart files byte-compatible with store1 / restar2 (restar.f90:5-88,
+ * 273-346) for one rank: gfortran sequential unformatted records (4-byte
+ * lengths) (myrank = 0, nd), (it0, ih0), (time), then per cell in (k, j, i)
+ * order uu, u0, uri, uri0 (9 doubles each).  rg_run_store writes the run's
+ * current primitives, their conserved variables (caluu1) and the initial state
+ * uri0 (NULL: the current primitives) with its conserved variables;
+ * rg_run_restore reads a file of this grid, uploads uri with time = the
+ * stored time (icres = 1, main.f90:560-571) and returns it0, ih0, nd and,
+ * if uri0 is not NULL, the stored initial primitives. */
+int rg_run_store(rg_ctx* ctx, int run, const char* path, int it0, int ih0, int nd, const double* uri0);
+int rg_run_restore(rg_ctx* ctx, int run, const char* path, int* it0, int* ih0, int* nd, double* uri0);
 
 /* Accretion rates through the inner edge of the interior (the radial face
  * nm1+1/2, just outside the horizon for the torus grids): mdot = -sum of the

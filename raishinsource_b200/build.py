@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libraishin_gpu.so")
 SOURCES = ["rg_kernels.cu", "rg_capi.cu", "rg_geometry.cpp"]
-HEADERS = ["rg_device.cuh", "rg_recon.cuh", "rg_kernels.cuh", "rg_types.h", "rg_host.h"]
+HEADERS = ["rg_device.cuh", "rg_recon.cuh", "rg_kernels.cuh", "rg_batch.cuh", "rg_types.h", "rg_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,7 +40,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     tmp = LIB + ".tmp%d" % os.getpid()
     fmad = "false" if os.environ.get("RG_FMAD", "1") == "0" else "true"
     cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", f"--fmad={fmad}", "-shared",
-           "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-o", tmp, *srcs]
+           "-Xcompiler", "-fPIC,-ffp-contract=off,-O2,-fopenmp", "-o", tmp, *srcs, "-lgomp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -27,8 +27,8 @@ STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA"
 #: every entry point include/raishin_gpu.h declares
 EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
-           "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_step",
-           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_run_horizon_flux", "rg_calflx_static")
+           "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -97,6 +97,8 @@ def load(path: str = LIB_PATH):
     lib.rg_run_upload_prims.argtypes = [P, I, C.c_void_p, C.c_double]
     lib.rg_run_download_prims.argtypes = [P, I, C.c_void_p]
     lib.rg_step.argtypes = [P, I, I, C.POINTER(StepStats)]
+    lib.rg_run_layout.argtypes = [P, I, C.POINTER(C.c_size_t), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.rg_run_download_stored.argtypes = [P, I, C.c_void_p]
     lib.rg_run_stats.argtypes = [P, I, C.POINTER(StepStats)]
     lib.rg_step_batch.argtypes = [P, C.POINTER(C.c_int), I, I, C.POINTER(StepStats)]
     lib.rg_batch_info.argtypes = [P, C.POINTER(C.c_int), I, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -110,6 +112,9 @@ def load(path: str = LIB_PATH):
     lib.rg_bnd_floor.argtypes = [P, I, D, D]
     lib.rg_calflx_static.argtypes = [P, I, P, P]
     lib.rg_run_horizon_flux.argtypes = [P, I, D, D]
+    lib.rg_run_store.argtypes = [P, I, C.c_char_p, I, I, I, C.c_void_p]
+    lib.rg_run_restore.argtypes = [P, I, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.c_void_p]
     _lib = lib
     return lib
 
@@ -190,11 +195,15 @@ class Context:
         """Admit a prepared run (geometry and initial data computed by Prep)."""
         return Run(self, prep.params, prep)
 
-    def step_batch(self, runs, n: int = 1, stats: bool = False):
-        """Advance several runs together (rg_step_batch); with stats, one dict per run."""
+    def step_batch(self, runs, n: int = 1, stats: bool = False, strict: bool = True):
+        """Advance several runs together (rg_step_batch); with stats, one dict per run.
+        With strict=False a capped rescale loop (RG_ENR_CAP, counted in the stats)
+        does not raise."""
         ids = (C.c_int * len(runs))(*[r.id for r in runs])
         st = (StepStats * len(runs))() if stats else None
-        _check(self.lib, self.lib.rg_step_batch(self.h, ids, len(runs), int(n), st))
+        rc = self.lib.rg_step_batch(self.h, ids, len(runs), int(n), st)
+        if not (rc == 4 and not strict):
+            _check(self.lib, rc)
         return [x.as_dict() for x in st] if stats else None
 
     def batch_info(self, runs) -> dict:
@@ -285,6 +294,15 @@ class Run:
         _check(self.lib, self.lib.rg_run_download_prims(self.ctx.h, self.id, out.ctypes.data))
         return out
 
+    def stored_prims(self) -> np.ndarray:
+        """Primitives as stored on the device, shape (9, kplanes, jplanes, imax):
+        a slab direction has one plane (rg_run_download_stored)."""
+        n, jp, kp = C.c_size_t(0), C.c_int(0), C.c_int(0)
+        _check(self.lib, self.lib.rg_run_layout(self.ctx.h, self.id, C.byref(n), C.byref(jp), C.byref(kp)))
+        out = np.empty((9, kp.value, jp.value, self.params["imax"]), dtype=np.float64)
+        _check(self.lib, self.lib.rg_run_download_stored(self.ctx.h, self.id, out.ctypes.data))
+        return out
+
     def download_prims_ptr(self, host_ptr: int):
         _check(self.lib, self.lib.rg_run_download_prims(self.ctx.h, self.id, C.c_void_p(host_ptr)))
 
@@ -329,6 +347,22 @@ class Run:
         """Allocation-free flux call on caller-owned device buffers (raw device
         pointers): d_prims 9*N SoA primitives in, d_ww 27*N fluxes out."""
         _check(self.lib, self.lib.rg_calflx_static(self.ctx.h, self.id, C.c_void_p(d_prims), C.c_void_p(d_ww)))
+
+    def store(self, path: str, it0: int = 0, ih0: int = 0, nd: int = 0, uri0=None):
+        """Write a restart file in the store1 layout (rg_run_store)."""
+        ptr = None
+        if uri0 is not None:
+            uri0 = np.ascontiguousarray(uri0, dtype=np.float64).reshape(self.shape)
+            ptr = uri0.ctypes.data
+        _check(self.lib, self.lib.rg_run_store(self.ctx.h, self.id, os.fsencode(path), it0, ih0, nd, ptr))
+
+    def restore(self, path: str) -> dict:
+        """Read a restart file of this grid (rg_run_restore); returns it0, ih0, nd and uri0."""
+        it0, ih0, nd = C.c_int(0), C.c_int(0), C.c_int(0)
+        uri0 = self.zeros()
+        _check(self.lib, self.lib.rg_run_restore(self.ctx.h, self.id, os.fsencode(path), C.byref(it0), C.byref(ih0),
+                                                 C.byref(nd), uri0.ctypes.data))
+        return {"it0": it0.value, "ih0": ih0.value, "nd": nd.value, "uri0": uri0}
 
     def horizon_flux(self) -> tuple[float, float]:
         """(mdot, edot) through the inner edge of the interior (rg_run_horizon_flux)."""

@@ -91,6 +91,15 @@ struct CarryB {
   }
 };
 
+template <int STAGE>
+struct StragB {
+  __device__ void operator()(const DevRun& r, const Tile& t) const {
+    double *Pn, *Pc, *Pw;
+    stage_ptrs(r, STAGE, Pn, Pc, Pw);
+    straggler_body<STAGE>(r, Pn, Pc, Pw, r.F[0], r.F[1], r.F[2], r.CT, make_uint3(t.bx, 0, 0));
+  }
+};
+
 template <int D, bool PERIODIC>
 struct BcB {
   int stage;
@@ -135,7 +144,7 @@ struct ScalarB {
 // ------------------------------------------------------------- host side
 // One launch of a batched step: the kernel to run and its tile range.
 enum BKind {
-  BK_BEGIN, BK_CFL, BK_DT, BK_FLUX, BK_CT, BK_UPDATE, BK_CARRY, BK_BCPER, BK_BCPHYS, BK_FLOOR, BK_END
+  BK_BEGIN, BK_CFL, BK_DT, BK_FLUX, BK_CT, BK_UPDATE, BK_CARRY, BK_BCPER, BK_BCPHYS, BK_FLOOR, BK_END, BK_STRAG
 };
 struct BLaunch {
   int kind;
@@ -272,6 +281,11 @@ int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
       });
     }
     L.fp32 = 0;
+    L.kind = BK_STRAG;
+    L.block = dim3(128, 1, 1);
+    plan_append(*B, T, L, runs, [&](int a, const DevRun& r, std::vector<Tile>& t) {
+      if (r.strag_list) add_tiles(t, a, dim3((unsigned)((r.strag_cap + 127) / 128), 1, 1), 0, 0, 0);
+    });
     L.kind = BK_CARRY;
     L.block = dim3(32, 1, 1);
     plan_append(*B, T, L, runs, one);
@@ -413,6 +427,10 @@ cudaError_t batch_issue(const BatchPlan* B, int idx, cudaStream_t s) {
       if (L.stage == 1) return L.fp32 ? go_update<1, true>(B, L, s) : go_update<1, false>(B, L, s);
       if (L.stage == 2) return L.fp32 ? go_update<2, true>(B, L, s) : go_update<2, false>(B, L, s);
       return L.fp32 ? go_update<3, true>(B, L, s) : go_update<3, false>(B, L, s);
+    case BK_STRAG:
+      if (L.stage == 1) return kb_go<StragB<1>, 128, 1>(B, L, StragB<1>{}, s);
+      if (L.stage == 2) return kb_go<StragB<2>, 128, 1>(B, L, StragB<2>{}, s);
+      return kb_go<StragB<3>, 128, 1>(B, L, StragB<3>{}, s);
     case BK_CARRY:
       if (L.stage == 1) return kb_go<CarryB<1>, 32, 1>(B, L, CarryB<1>{}, s);
       if (L.stage == 2) return kb_go<CarryB<2>, 32, 1>(B, L, CarryB<2>{}, s);

@@ -55,6 +55,8 @@ struct Run {
 // Host-side preparation of a run (geometry, initial data), built without a context.
 struct rg_prep {
   rg_run_params p{};
+  int krow = 0;        // geometry of one theta row (theta slab)
+  bool plane = false;  // initial data of the interior phi plane only (phi slab)
   HostGeom geom;
   std::vector<double> ic;  // full-layout SoA primitives, empty if none
 };
@@ -160,6 +162,10 @@ bool slab_direction(const rg_run_params* p, int dir, int nm1) {
   return true;
 }
 
+// Capacity of a run's list of deferred recoveries (cells per stage whose
+// Newton-Raphson passes kDeferIter iterations; a few per 10^4 in practice).
+int straggler_cap(size_t N) { return (int)std::max<size_t>(1024, std::min<size_t>(N / 64, (size_t)1 << 20)); }
+
 size_t stored_cells(const rg_run_params* p) {
   const int nm1 = (p->irec == 5) ? 5 : 4;
   const bool full = (p->flags & RG_FLAG_FULL) != 0;
@@ -180,7 +186,7 @@ size_t footprint_bytes(const rg_run_params* p) {
   size_t mixed = 0;
   if (p->precision == RG_MIXED)  // P32, F32 x3, CT32; FP32 metric caches and Christoffels
     mixed = (9 + 27 + 6) * N * sizeof(float) + (3 * kMetComps + 64) * nik * sizeof(float);
-  return state + geom + mixed + sizeof(Scal) + C_NCOUNTERS * 8 + kCarryCap * sizeof(int);
+  return state + geom + mixed + sizeof(Scal) + C_NCOUNTERS * 8 + (kCarryCap + straggler_cap(N)) * sizeof(int);
 }
 
 Run* find(rg_ctx* ctx, int id) {
@@ -430,6 +436,7 @@ int kind_of(const BatchPlan* B, int idx) {
     case 5: case 6: return K_UPDATE;
     case 7: case 8: return K_BC;
     case 9: return K_FLOOR;
+    case 11: return K_UPDATE;
     default: return K_SCALAR;
   }
 }
@@ -648,7 +655,11 @@ int rg_prep_create(const rg_run_params* p, rg_prep** out) {
   if (rc) return rc;
   rg_prep* P = new rg_prep();
   P->p = *p;
-  build_geometry(*p, P->geom);
+  const int nm1 = (p->irec == 5) ? 5 : 4;
+  const bool full = (p->flags & RG_FLAG_FULL) != 0;
+  P->krow = (!full && slab_direction(p, 3, nm1)) ? nm1 + 1 : 0;  // theta slab: one metric row
+  P->plane = !full && slab_direction(p, 2, nm1);                   // phi slab: one initial-data plane
+  build_geometry(*p, P->geom, P->krow);
   if (!P->geom.compact_ok) {
     delete P;
     return fail(RG_EINVAL_CONFIG, "metric couples theta to (t,r,phi): not representable by the compact cache");
@@ -659,7 +670,8 @@ int rg_prep_create(const rg_run_params* p, rg_prep** out) {
 
 int rg_prep_ic_torus(rg_prep* P, uint64_t seed, double amp, double rin, double rmax, double beta, double kappa) {
   if (!P) return fail(RG_EINVAL_CONFIG, "null preparation");
-  torus_ic(P->p, P->geom, seed, amp, rin, rmax, beta, kappa, P->ic);
+  if (P->krow) return fail(RG_EINVAL_CONFIG, "torus initial data needs a Kerr metric (this run is a Minkowski slab)");
+  torus_ic(P->p, P->geom, seed, amp, rin, rmax, beta, kappa, P->ic, P->plane);
   return RG_OK;
 }
 
@@ -754,6 +766,9 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   d.cnt = static_cast<unsigned long long*>(ptr);
   if ((rc = dalloc(R, &ptr, kCarryCap * sizeof(int)))) return bail(rc);
   d.carry_list = static_cast<int*>(ptr);
+  d.strag_cap = straggler_cap(N);
+  if ((rc = dalloc(R, &ptr, (size_t)d.strag_cap * sizeof(int)))) return bail(rc);
+  d.strag_list = static_cast<int*>(ptr);
   if (cudaMemsetAsync(d.cnt, 0, C_NCOUNTERS * sizeof(unsigned long long), s) != cudaSuccess) return bail(RG_ECUDA);
   for (int k = 0; k < 3; ++k) {
     if (cudaMemsetAsync(R->b.P[k], 0, 9 * N * sizeof(double), s) != cudaSuccess) return bail(RG_ECUDA);
@@ -761,20 +776,12 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   }
   if (cudaMemsetAsync(R->b.CT, 0, 6 * N * sizeof(double), s) != cudaSuccess) return bail(RG_ECUDA);
   const HostGeom& G = R->geom;
-  // a theta slab keeps the metric row of its computed index only (the metric is uniform there)
-  auto row = [&](const std::vector<double>& v, int comps) {
-    if (!d.kfix) return v;
-    std::vector<double> o((size_t)comps * d.nik);
-    const size_t full = (size_t)p->imax * p->kmax;
-    for (int c = 0; c < comps; ++c)
-      for (int i = 1; i <= p->imax; ++i)
-        o[(size_t)c * d.nik + (size_t)(i - 1)] = v[(size_t)c * full + (size_t)(i - 1) + (size_t)p->imax * (d.kfix - 1)];
-    return o;
-  };
-  if ((rc = upload(row(G.mc, kMetComps), &d.mc, R, s))) return bail(rc);
-  if ((rc = upload(row(G.mi, kMetComps), &d.mi, R, s))) return bail(rc);
-  if ((rc = upload(row(G.mk, kMetComps), &d.mk, R, s))) return bail(rc);
-  if ((rc = upload(row(G.chr, 64), &d.chr, R, s))) return bail(rc);
+  // (a theta slab's geometry holds the one metric row of its computed index)
+  if (G.nik != d.nik) return bail(fail(RG_EINVAL_CONFIG, "geometry prepared for another slab layout"));
+  if ((rc = upload(G.mc, &d.mc, R, s))) return bail(rc);
+  if ((rc = upload(G.mi, &d.mi, R, s))) return bail(rc);
+  if ((rc = upload(G.mk, &d.mk, R, s))) return bail(rc);
+  if ((rc = upload(G.chr, &d.chr, R, s))) return bail(rc);
   std::vector<double> t;
   if ((rc = upload(zero_based(G.ax[0].x, p->imax), &d.x1, R, s))) return bail(rc);
   if ((rc = upload(zero_based(G.ax[0].dxb, p->imax), &d.dx1b, R, s))) return bail(rc);
@@ -847,7 +854,8 @@ int rg_run_ic_torus(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin,
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   std::vector<double> P;
-  torus_ic(R->p, R->geom, seed, amp, rin, rmax, beta, kappa, P);
+  if (R->d.kmet) return fail(RG_EINVAL_CONFIG, "torus initial data needs a Kerr metric (this run is a Minkowski slab)");
+  torus_ic(R->p, R->geom, seed, amp, rin, rmax, beta, kappa, P, R->d.jfix != 0);
   const std::vector<double> Ps = stored_from_full(R->d, P, R->nfull);
   R->cur = 0;
   RG_CUDA(cudaMemcpyAsync(R->b.P[0], Ps.data(), Ps.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -898,6 +906,24 @@ int rg_run_download_prims(rg_ctx* ctx, int run, double* uri) {
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!uri) return fail(RG_EINVAL_CONFIG, "null array");
   return from_soa(ctx, R, R->b.P[R->cur], uri, R->d);
+}
+
+int rg_run_layout(rg_ctx* ctx, int run, size_t* ncells, int* jplanes, int* kplanes) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (ncells) *ncells = R->d.N;
+  if (jplanes) *jplanes = R->d.jpl;
+  if (kplanes) *kplanes = R->d.kpl;
+  return RG_OK;
+}
+
+int rg_run_download_stored(rg_ctx* ctx, int run, double* soa) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!soa) return fail(RG_EINVAL_CONFIG, "null array");
+  RG_CUDA(cudaMemcpyAsync(soa, R->b.P[R->cur], 9 * R->d.N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
 }
 
 int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats) {
@@ -1085,6 +1111,76 @@ int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
           }
       }
   return RG_OK;
+}
+
+// ------------------------------------------------------------ restart files
+// store1 / restar2 (restar.f90:5-88, 273-346) write and read one rank's state
+// as gfortran sequential unformatted records (a 4-byte length before and
+// after each record): (myrank, nd), (it0, ih0), (time), then for every cell in
+// (k, j, i) order four records of nv = 9 doubles: uu, u0, uri, uri0.
+namespace {
+
+bool put_record(FILE* f, const void* data, uint32_t n) {
+  return fwrite(&n, 4, 1, f) == 1 && (n == 0 || fwrite(data, n, 1, f) == 1) && fwrite(&n, 4, 1, f) == 1;
+}
+bool get_record(FILE* f, void* data, uint32_t n) {
+  uint32_t a = 0, b = 0;
+  if (fread(&a, 4, 1, f) != 1 || a != n) return false;
+  if (n && fread(data, n, 1, f) != 1) return false;
+  return fread(&b, 4, 1, f) == 1 && b == n;
+}
+
+}  // namespace
+
+int rg_run_store(rg_ctx* ctx, int run, const char* path, int it0, int ih0, int nd, const double* uri0) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!path) return fail(RG_EINVAL_CONFIG, "null path");
+  const size_t nf = R->nfull;
+  std::vector<double> uri(9 * nf), uu(9 * nf), u0(9 * nf), p0;
+  int rc = rg_run_download_prims(ctx, run, uri.data());
+  if (rc) return rc;
+  if ((rc = rg_caluu1(ctx, run, uri.data(), uu.data()))) return rc;
+  const double* pr0 = uri0 ? uri0 : uri.data();
+  if ((rc = rg_caluu1(ctx, run, pr0, u0.data()))) return rc;
+  rg_step_stats st{};
+  Scal sc{};
+  RG_CUDA(cudaMemcpyAsync(&sc, R->d.scal, sizeof(Scal), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  (void)st;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(RG_EINVAL_CONFIG, std::string("cannot open ") + path);
+  const int32_t h1[2] = {0, nd}, h2[2] = {it0, ih0};
+  const double time = sc.timeh;
+  bool ok = put_record(f, h1, 8) && put_record(f, h2, 8) && put_record(f, &time, 8);
+  for (size_t c = 0; ok && c < nf; ++c)
+    ok = put_record(f, &uu[9 * c], 72) && put_record(f, &u0[9 * c], 72) && put_record(f, &uri[9 * c], 72) &&
+         put_record(f, &pr0[9 * c], 72);
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? RG_OK : fail(RG_EINVAL_CONFIG, std::string("write failed: ") + path);
+}
+
+int rg_run_restore(rg_ctx* ctx, int run, const char* path, int* it0, int* ih0, int* nd, double* uri0) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!path) return fail(RG_EINVAL_CONFIG, "null path");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(RG_EINVAL_CONFIG, std::string("cannot open ") + path);
+  const size_t nf = R->nfull;
+  int32_t h1[2], h2[2];
+  double time = 0.0;
+  std::vector<double> uri(9 * nf), rec(9);
+  bool ok = get_record(f, h1, 8) && get_record(f, h2, 8) && get_record(f, &time, 8);
+  for (size_t c = 0; ok && c < nf; ++c) {
+    ok = get_record(f, rec.data(), 72) && get_record(f, rec.data(), 72) && get_record(f, &uri[9 * c], 72) &&
+         get_record(f, uri0 ? uri0 + 9 * c : rec.data(), 72);
+  }
+  std::fclose(f);
+  if (!ok) return fail(RG_EINVAL_CONFIG, std::string("not a restart file of this grid: ") + path);
+  if (it0) *it0 = h2[0];
+  if (ih0) *ih0 = h2[1];
+  if (nd) *nd = h1[1];
+  return rg_run_upload_prims(ctx, run, uri.data(), time);  // restart at timeh (main.f90:560-571)
 }
 
 int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot) {

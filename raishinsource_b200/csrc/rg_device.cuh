@@ -118,6 +118,12 @@ __device__ __forceinline__ float pow_gam(float x, float gam, int kind) {
   const float c = cbrtf(x);
   return kind == 1 ? x * c : x * c * c;
 }
+// x**(1-gam) for x > 0: 1/cbrt(x) for 4/3, 1/cbrt(x)^2 for 5/3.
+__device__ __forceinline__ double pow_1mgam(double x, double gam, int kind) {
+  if (kind == 0 || !(x > 0.0)) return pow(x, 1. - gam);
+  const double c = rcbrt(x);
+  return kind == 1 ? c : c * c;
+}
 // x**(gam-1): cbrt(x) for 4/3, cbrt(x)^2 for 5/3.
 __device__ __forceinline__ double pow_gam1(double x, double gam, int kind) {
   if (kind == 0 || !(x >= 0.0)) return pow(x, gam - 1.);

@@ -245,13 +245,14 @@ static void make_axis(int n, double lo, double hi, int kind, bool is_x1, bool is
   ax.dxb[1] = ax.dxb[2];
 }
 
-void build_geometry(const rg_run_params& p, HostGeom& G) {
+void build_geometry(const rg_run_params& p, HostGeom& G, int krow) {
   const bool mks = (p.metric == 403);
   make_axis(p.imax, p.xmin, p.xmax, p.ix1, true, false, mks, p.R0, p.hslope, G.ax[0]);
   make_axis(p.jmax, p.ymin, p.ymax, 1, false, false, mks, p.R0, p.hslope, G.ax[1]);
   make_axis(p.kmax, p.zmin, p.zmax, p.ix3, false, true, mks, p.R0, p.hslope, G.ax[2]);
   const int imax = p.imax, kmax = p.kmax;
-  const size_t nik = (size_t)imax * kmax;
+  // krow > 0: one theta row (a theta slab in Minkowski space, where every row is the same)
+  const size_t nik = (size_t)imax * (krow > 0 ? 1 : kmax);
   G.nik = nik;
   G.mc.assign(kMetComps * nik, 0.0);
   G.mi.assign(kMetComps * nik, 0.0);
@@ -260,16 +261,23 @@ void build_geometry(const rg_run_params& p, HostGeom& G) {
   G.chr.assign(64 * nik, 0.0);
   const Axis& X1 = G.ax[0];
   const Axis& X3 = G.ax[2];
-  for (int k = 1; k <= kmax; ++k)
-    for (int i = 1; i <= imax; ++i) {
-      const size_t q = (size_t)(i - 1) + (size_t)imax * (k - 1);
+  // every (i, k) point is independent: OpenMP over points (bit-identical to a serial loop)
+  const int k0 = (krow > 0 ? krow : 1), nk = (krow > 0 ? 1 : kmax);
+  bool ok = true;
+#pragma omp parallel for schedule(static) reduction(&& : ok) if ((long long)nk * imax > 4096)
+  for (long long pt = 0; pt < (long long)nk * imax; ++pt) {
+      const int k = k0 + (int)(pt / imax), i = 1 + (int)(pt % imax);
+      const size_t q = (size_t)(i - 1) + (krow > 0 ? 0 : (size_t)imax * (k - 1));
       Mat g, gc;
       metric_at(p, X1.x[i], X3.x[k], X3.xb[k], g, gc);
-      G.compact_ok &= store_met(G.mc, nik, q, g, gc);
+      ok = store_met(G.mc, nik, q, g, gc) && ok;
       metric_at(p, X1.xa[i], X3.x[k], X3.xb[k], g, gc);
-      G.compact_ok &= store_met(G.mi, nik, q, g, gc);
+      ok = store_met(G.mi, nik, q, g, gc) && ok;
       metric_at(p, X1.x[i], X3.xa[k], X3.xb[k], g, gc);  // hfac at the centre theta_MKS (coord.f90:96-98)
-      G.compact_ok &= store_met(G.mk, nik, q, g, gc);
+      ok = store_met(G.mk, nik, q, g, gc) && ok;
+      // Minkowski: the central differences of the constant metric vanish exactly,
+      // so every Christoffel symbol is 0 (the array is zero-initialised)
+      if (p.metric == 1) continue;
       // Christoffel symbols by central differences, delta = 1e-5 (coord.f90:1134-1317)
       const double delta = 1.0e-5, small = 1.e-12;
       double r0 = X1.x[i], th0 = X3.x[k], thm = X3.xb[k];
@@ -311,6 +319,7 @@ void build_geometry(const rg_run_params& p, HostGeom& G) {
             G.chr[(size_t)(l + 4 * m + 16 * n) * nik + q] = gcon[l][0] * low[0][m][n] + gcon[l][1] * low[1][m][n] +
                                                             gcon[l][2] * low[2][m][n] + gcon[l][3] * low[3][m][n];
     }
+  G.compact_ok = ok;
 }
 
 }  // namespace rg
@@ -489,8 +498,13 @@ void tube_states(uint64_t seed, uint64_t tube, double gam, double state[2][9]) {
 }
 
 void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double amp, double rin, double rmax,
-              double beta, double kappa, std::vector<double>& P) {
+              double beta, double kappa, std::vector<double>& P, bool plane_only) {
   const int imax = p.imax, jmax = p.jmax, kmax = p.kmax;
+  // Every phi plane of the torus is the same except for the perturbation,
+  // which a 2D phi slab keys by its interior plane: a run that stores the slab
+  // as one plane needs only that plane (the others stay zero).
+  const int nm1_pl = (p.irec == 5) ? 5 : 4;
+  const int jlo = plane_only ? nm1_pl + 1 : 1, jhi = plane_only ? nm1_pl + 1 : jmax;
   const size_t N = (size_t)imax * jmax * kmax, nik = G.nik;
   const double gam = p.gam, a = p.akm;
   const Axis& X1 = G.ax[0];
@@ -505,7 +519,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
   std::vector<double> lnh(N, 0.0), apot(N, 0.0);
   // floor atmosphere everywhere (mdgrmhd.f90:964-1021)
   for (int k = 1; k <= kmax; ++k)
-    for (int j = 1; j <= jmax; ++j)
+    for (int j = jlo; j <= jhi; ++j)
       for (int i = 1; i <= imax; ++i) {
         const double r = X1.x[i];
         const double de = p.dmin * std::pow(r, -1.5), pr = p.pmin * (gam - 1.) * std::pow(r, -2.5);
@@ -523,7 +537,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
                       2.0 * a * rin * ell * (1.0 / al);
   double rhomax = 0.0;
   for (int k = 1; k <= kmax; ++k)
-    for (int j = 1; j <= jmax; ++j)
+    for (int j = jlo; j <= jhi; ++j)
       for (int i = 1; i <= imax; ++i) {
         const double r = X1.x[i], th = X3.x[k];
         double sth = std::sin(th);
@@ -574,7 +588,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
   const int nm1_ic = (p.irec == 5) ? 5 : 4;
   const bool phi_slab = (jmax == 2 * nm1_ic + 1);
   for (int k = 1; k <= kmax; ++k)
-    for (int j = 1; j <= jmax; ++j)
+    for (int j = jlo; j <= jhi; ++j)
       for (int i = 1; i <= imax; ++i) {
         const double r = X1.x[i], th = X3.x[k];
         const size_t c = cidx(i, j, k);
@@ -595,19 +609,19 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
       }
   // A_phi ~ max(<rho> - 0.2, 0) at cell corners (mdgrmhd.f90:1335-1368)
   for (int k = 2; k <= kmax; ++k)
-    for (int j = 1; j <= jmax; ++j)
+    for (int j = jlo; j <= jhi; ++j)
       for (int i = 2; i <= imax; ++i) {
         const double av = 0.25 * (at(0, i, j, k) + at(0, i - 1, j, k) + at(0, i, j, k - 1) + at(0, i - 1, j, k - 1));
         const double a1 = (av != 0.0) ? ((av * (1. / 1.0)) - 0.2) : 0.0;
         if (a1 > 0.0) apot[cidx(i, j, k)] = a1;
       }
-  for (int j = 1; j <= jmax; ++j)
+  for (int j = jlo; j <= jhi; ++j)
     for (int i = 1; i <= imax; ++i) apot[cidx(i, j, 1)] = apot[cidx(i, j, 2)];
   for (int k = 1; k <= kmax; ++k)
-    for (int j = 1; j <= jmax; ++j) apot[cidx(1, j, k)] = apot[cidx(2, j, k)];
+    for (int j = jlo; j <= jhi; ++j) apot[cidx(1, j, k)] = apot[cidx(2, j, k)];
   const bool mks = (p.metric == 403);
   for (int k = 2; k <= kmax - 1; ++k)
-    for (int j = 1; j <= jmax; ++j)
+    for (int j = jlo; j <= jhi; ++j)
       for (int i = 2; i <= imax - 1; ++i) {
         auto A = [&](int ii, int kk) { return apot[cidx(ii, j, kk)]; };
         const double dg = G.mc[(size_t)(kMetBase - 1) * nik + (size_t)(i - 1) + (size_t)imax * (k - 1)];
@@ -620,20 +634,20 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
         at(6, i, j, k) = (c1 != 0.0) ? -(c1 * (1.0 / (h3 * dg))) : 0.0;
         at(8, i, j, k) = (c3 != 0.0) ? c3 * (1.0 / (h1 * dg)) : 0.0;
       }
-  for (int j = 1; j <= jmax; ++j)
+  for (int j = jlo; j <= jhi; ++j)
     for (int i = 1; i <= imax; ++i) {
       at(6, i, j, 1) = at(6, i, j, 2); at(6, i, j, kmax) = at(6, i, j, kmax - 1);
       at(8, i, j, 1) = at(8, i, j, 2); at(8, i, j, kmax) = at(8, i, j, kmax - 1);
     }
   for (int k = 1; k <= kmax; ++k)
-    for (int j = 1; j <= jmax; ++j) {
+    for (int j = jlo; j <= jhi; ++j) {
       at(6, 1, j, k) = at(6, 2, j, k); at(6, imax, j, k) = at(6, imax - 1, j, k);
       at(8, 1, j, k) = at(8, 2, j, k); at(8, imax, j, k) = at(8, imax - 1, j, k);
     }
   // scale B to the target minimum plasma beta (mdgrmhd.f90:1424-1540)
   double beta_min = 1.e5;
   for (int k = 1; k <= kmax; ++k)
-    for (int j = 1; j <= jmax; ++j)
+    for (int j = jlo; j <= jhi; ++j)
       for (int i = 1; i <= imax; ++i) {
         const size_t q = (size_t)(i - 1) + (size_t)imax * (k - 1);
         Mat g, gc;

@@ -23,11 +23,12 @@ struct HostGeom {
   std::vector<double> chr;         // 64 components per point, SoA
 };
 
-void build_geometry(const rg_run_params& p, HostGeom& g);
+// krow > 0 computes the single theta row krow (theta slab in Minkowski space).
+void build_geometry(const rg_run_params& p, HostGeom& g, int krow = 0);
 
 // mdtorus1 (mdgrmhd.f90:879-1654) into SoA primitives prim[v*N + c].
 void torus_ic(const rg_run_params& p, const HostGeom& g, uint64_t seed, double amp, double rin, double rmax,
-              double beta, double kappa, std::vector<double>& prim);
+              double beta, double kappa, std::vector<double>& prim, bool plane_only = false);
 
 // Left/right primitive states of the seeded Riemann tube `tube` (mdshoctub pattern).
 void tube_states(uint64_t seed, uint64_t tube, double gam, double state[2][9]);

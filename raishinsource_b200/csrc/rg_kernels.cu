@@ -47,6 +47,7 @@ __device__ __forceinline__ int kidx(const DevRun& r, int lo, uint3 bid) {
 struct RecovOut {
   double wg;
   bool nr2, fail, cap;
+  bool deferred;  // the iteration passed `defer` steps unconverged: nothing written, redo without limit
 };
 
 constexpr int kRescaleCap = 1000;  // the reference's "go to 95" loop (recov.f90:823-850) is unbounded
@@ -58,7 +59,8 @@ constexpr int kRescaleCap = 1000;  // the reference's "go to 95" loop (recov.f90
 // from the previous cell of its loop (recov.f90:810-815), which the caller
 // resolves in loop order.
 __device__ bool recov_cell(const double u[9], const double q[9], double out[9], const Met& m, double gam, int gkind,
-                           int iter, double demin_i, double prmin_i, const double* wg_carry, RecovOut& res) {
+                           int iter, double demin_i, double prmin_i, const double* wg_carry, RecovOut& res,
+                           int defer = 0x7fffffff) {
   const double safty = 1.0e-4, saftybig = 1.0e5, dv = 1.0e-2;
   const double gam1 = gam / (gam - 1.0), gam2 = 1.0 / gam1;
   const double idetg1 = m.idetg;  // 1. / detg1
@@ -128,9 +130,28 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
     const double vsqo = vsq;
     double xxn = wg, yyn = vsq;
     // 2D Newton-Raphson on (W, v^2) (recov.f90:877-960)
+    // Brent's cycle detection on the iterate (xxn, yyn), compared bit for bit:
+    // the step is a function of the iterate alone, so once an iterate repeats
+    // while the current step is still above the tolerance, every later step
+    // repeats a step already found too large and the reference's loop runs to
+    // iter without converging.  Its outcome (irecov = 1) is taken at once; the
+    // 2D iterate is not used after a failure.
+    long long cyc_x = __double_as_longlong(xxn), cyc_y = __double_as_longlong(yyn);
+    int cyc_pow = 1, cyc_lam = 0;
     for (int nnn = 1; nnn <= iter; ++nnn) {
       if (!(fabs(delta) >= deltaend && irecov == 0)) break;
       if (nnn == iter) { irecov = 1; break; }
+      if (nnn > 1 && __double_as_longlong(xxn) == cyc_x && __double_as_longlong(yyn) == cyc_y) {
+        irecov = 1;
+        break;
+      }
+      if (++cyc_lam == cyc_pow) {
+        cyc_x = __double_as_longlong(xxn);
+        cyc_y = __double_as_longlong(yyn);
+        cyc_pow <<= 1;
+        cyc_lam = 0;
+      }
+      if (nnn > defer) { res.deferred = true; return true; }
       wg = xxn;
       vsq = yyn;
       wsq = wg * wg;
@@ -185,23 +206,44 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
       deltaend = 1.e-6;
       irecov = 0;
       xxn = vsqo;
+      // Cycle detection as in the 2D iteration; here the last iterate's W is
+      // kept on failure (the carried-in guess of a following cell), so on a
+      // repeat the loop counter advances by whole cycles and the remaining
+      // (fewer than one cycle of) iterations run as in the reference.
+      long long cyc_s = __double_as_longlong(xxn);
+      int cyc_pow2 = 1, cyc_lam2 = 0, cyc_at = 1;
+      bool cyc_on = true;
+      const double dro_g1 = pow(dro, gam - 1.);  // loop-invariant factor of dW/dv^2
       for (int nnn = 1; nnn <= iter; ++nnn) {
         if (!(fabs(delta) >= deltaend && irecov == 0)) break;
         if (nnn == iter) { irecov = 1; break; }
+        if (cyc_on && nnn > 1 && __double_as_longlong(xxn) == cyc_s) {
+          const int L = nnn - cyc_at;  // the iterate at the start of iteration cyc_at recurred
+          nnn += ((iter - nnn) / L) * L;
+          cyc_on = false;
+          if (nnn == iter) { irecov = 1; break; }
+        }
+        if (cyc_on && ++cyc_lam2 == cyc_pow2) {
+          cyc_s = __double_as_longlong(xxn);
+          cyc_at = nnn;
+          cyc_pow2 <<= 1;
+          cyc_lam2 = 0;
+        }
+        if (nnn > defer) { res.deferred = true; return true; }
         vsq = xxn;
         double gtmp = 1. - vsq;
         if (gtmp < 0.0 || gtmp < safty) { gtmp = safty; vsq = 1. - gtmp; }
         gf = 1. / sqrt(gtmp);
         gfsq = gf * gf;
         ro = dro * (1. / gf);
-        pp = (gss / dro) * pow(ro, gam);
+        pp = (gss / dro) * pow_gam(ro, gam, gkind);
         const double roh = ro + gam1 * pp;
         wg = fabs(gfsq * roh);
         wsq = wg * wg;
         const double w3 = wsq * wg;
-        const double dgfdvsq = 0.5 * pow(gtmp, -1.5);
+        const double dgfdvsq = 0.5 * (gfsq * gf);  // 0.5 gtmp^-1.5 with gf = gtmp^-1/2
         const double dwdvsq =
-            dro * dgfdvsq + gam1 * gss * pow(dro, gam - 1.) * (2. - gam) * pow(gf, 1. - gam) * dgfdvsq;
+            dro * dgfdvsq + gam1 * gss * dro_g1 * (2. - gam) * pow_1mgam(gf, gam, gkind) * dgfdvsq;
         const double f = qtsq - vsq * (wg + bsq) * (wg + bsq) + (qdotbsq * (bsq + 2. * wg)) / wsq;
         const double ta = -((wg + bsq) * (wg + bsq));
         const double tb = -(2. * vsq * (wg + bsq));
@@ -220,7 +262,7 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
         gf = 1. / sqrt(gtmp);
         gfsq = gf * gf;
         ro = dro * (1. / gf);
-        pp = (gss * (1. / gf)) * pow(ro, gam - 1.);
+        pp = (gss * (1. / gf)) * pow_gam1(ro, gam, gkind);
         if (ro < 0.0) ro = demin_i;
         if (pp < 0.0) pp = prmin_i;
         const double roh = ro + gam1 * pp;
@@ -441,6 +483,24 @@ __device__ __forceinline__ void queue_carry(const DevRun& r, int i, int j, int k
   else atomicAdd(r.cnt + C_CARRY_OVF, 1ull);
 }
 
+// Divergence-aware recovery: a cell whose Newton-Raphson has not converged
+// after kDeferIter iterations (the usual count is 2-10; the reference allows
+// `iter` = 5000 per loop) is queued instead of holding its warp, and the
+// straggler pass recomputes the queued cells from scratch, packed one per
+// thread, so a slow cell costs one thread's time rather than 32.  The result
+// is the same as the undeferred computation.
+constexpr int kDeferIter = 64;
+
+// Queue a deferred cell; false if the list is full (the caller then finishes it in place).
+__device__ __forceinline__ bool queue_straggler(const DevRun& r, int i, int j, int k) {
+  const int ni = r.imax - 2 * r.nm1, nj = r.jmax - 2 * r.nm1;
+  const int lin = (i - r.nm1 - 1) + ni * ((j - r.nm1 - 1) + nj * (k - r.nm1 - 1));
+  const int slot = atomicAdd(&r.scal->strag_count, 1);
+  if (slot >= r.strag_cap) return false;
+  r.strag_list[slot] = lin;
+  return true;
+}
+
 #ifndef RG_UPDATE_MINB
 #define RG_UPDATE_MINB 3
 #endif
@@ -473,7 +533,13 @@ __device__ __forceinline__ void update_body(const DevRun& r, const double* __res
   double qo[9], qn[9];
   load9(Pc, N, c, qo);
   RecovOut o{0.0, false, false, false};
-  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, __ldg(r.fl_de + i - 1), __ldg(r.fl_pr + i - 1), nullptr, o);
+  const double dei = __ldg(r.fl_de + i - 1), pri = __ldg(r.fl_pr + i - 1);
+  bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, dei, pri, nullptr, o, r.strag_list ? kDeferIter : 0x7fffffff);
+  if (o.deferred) {
+    if (queue_straggler(r, i, j, k)) return;
+    o = RecovOut{0.0, false, false, false};
+    ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, dei, pri, nullptr, o);
+  }
   if (!ok) {
     queue_carry(r, i, j, k);
   } else {
@@ -483,6 +549,50 @@ __device__ __forceinline__ void update_body(const DevRun& r, const double* __res
   count_event(r, C_NR2, ok && o.nr2);
   count_event(r, C_FAIL, ok && o.fail);
   count_event(r, C_CAP, ok && o.cap);
+}
+
+// The straggler pass: slot t of the run's list, recomputed without deferral
+// (stage combine, source, then recov1a), in the reference's arithmetic.
+template <int STAGE>
+__device__ __forceinline__ void straggler_body(const DevRun& r, const double* __restrict__ Pn,
+                                               const double* __restrict__ Pc, double* __restrict__ Pw,
+                                               const double* __restrict__ F1, const double* __restrict__ F2,
+                                               const double* __restrict__ F3, const double* __restrict__ CT,
+                                               const uint3 bid) {
+  if (!r.scal->active) return;
+  const int t = bid.x * blockDim.x + threadIdx.x;
+  const int n = min(r.scal->strag_count, r.strag_cap);
+  if (t >= n) return;
+  const int lin = r.strag_list[t];
+  const int ni = r.imax - 2 * r.nm1, nj = r.jmax - 2 * r.nm1;
+  const int i = lin % ni + r.nm1 + 1, j = (lin / ni) % nj + r.nm1 + 1, k = lin / (ni * nj) + r.nm1 + 1;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  Met m;
+  load_met(r.mc, r.nik, r.ik(i, k), m);
+  double u[9], qo[9], qn[9];
+  if (r.mixed && i > r.i_fp64) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pc, r.scal->dt, u);
+  else stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
+  load9(Pc, N, c, qo);
+  RecovOut o{0.0, false, false, false};
+  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, __ldg(r.fl_de + i - 1), __ldg(r.fl_pr + i - 1),
+                             nullptr, o);
+  if (!ok) {
+    queue_carry(r, i, j, k);
+  } else {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = qn[v];
+  }
+  count_event(r, C_NR2, ok && o.nr2);
+  count_event(r, C_FAIL, ok && o.fail);
+  count_event(r, C_CAP, ok && o.cap);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(128) k_straggler(DevRun r, const double* __restrict__ Pn,
+                                                   const double* __restrict__ Pc, double* __restrict__ Pw,
+                                                   const double* __restrict__ F1, const double* __restrict__ F2,
+                                                   const double* __restrict__ F3, const double* __restrict__ CT) {
+  straggler_body<STAGE>(r, Pn, Pc, Pw, F1, F2, F3, CT, blockIdx);
 }
 template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(128, RG_UPDATE_MINB) k_update(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
@@ -499,6 +609,7 @@ __device__ void carry_fix_body(const DevRun& r, const double* __restrict__ Pn, c
                                double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                                const double* __restrict__ F3, const double* __restrict__ CT,
                                const double* __restrict__ U) {
+  if (MODE == 0) r.scal->strag_count = 0;  // the straggler pass of this stage has run
   if (MODE == 0 && !r.scal->active) return;
   int n = r.scal->carry_count;
   if (n <= 0) return;
@@ -1249,6 +1360,12 @@ cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const do
     launch_update_t<false>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, 1, split, s);
     launch_update_t<true>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, split + 1, r.imax, s);
   }
+  if (r.strag_list) {
+    const unsigned gs = (unsigned)((r.strag_cap + 127) / 128);
+    if (stage == 1) k_straggler<1><<<gs, 128, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    else if (stage == 2) k_straggler<2><<<gs, 128, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+    else k_straggler<3><<<gs, 128, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
+  }
   if (stage == 1) k_carry_fix<0, 1><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
   else if (stage == 2) k_carry_fix<0, 2><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
   else k_carry_fix<0, 3><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
@@ -1267,9 +1384,10 @@ int n_ct_launches(const DevRun& r) {
   return (split >= lo) + (split < hi);
 }
 int n_update_launches(const DevRun& r) {
-  if (!r.mixed) return 2;
+  const int extra = 1 + (r.strag_list ? 1 : 0);  // carry fix, straggler pass
+  if (!r.mixed) return 1 + extra;
   const int split = fp64_split(r, 1, r.imax);
-  return (split >= 1) + (split < r.imax) + 1;
+  return (split >= 1) + (split < r.imax) + extra;
 }
 
 cudaError_t launch_to_f32(const double* a, float* b, size_t n, cudaStream_t s) {

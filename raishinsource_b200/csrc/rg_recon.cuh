@@ -4,10 +4,18 @@
 
 namespace rg {
 
-// rec.f90:2346-2370
+// rec.f90:2346-2370.  dmm = 0.5*(sign(1,x)+sign(1,y))*min(|x|,|y|) and
+// dm4 = 0.125*(sw+sx)*|sw+sy|*(sw+sz)*min(|w|,|x|,|y|,|z|) (s = sign(1,.);
+// note the reference's abs covers only the middle factor, so dm4 is +min
+// when all four signs agree, whatever that sign).  The sign factors are
+// +-1 or a signed zero, so the products are evaluated here as selects on the
+// sign bits: the same values bit for bit (signed zeros and NaN included) with
+// the FP64 arithmetic reduced to the min and one multiply.
 template <typename T>
 __device__ __forceinline__ T dmm(T xx, T yy) {
-  return T(0.5) * (sgn1(xx) + sgn1(yy)) * dmin2(mabs(xx), mabs(yy));
+  const T mn = dmin2(mabs(xx), mabs(yy));
+  // same signs: 0.5*(+-2)*mn = +-mn; otherwise 0.5*(+0)*mn = +0 (or NaN)
+  return (signbit(xx) == signbit(yy)) ? copysign(mn, xx) : T(0) * mn;
 }
 template <typename T>
 __device__ __forceinline__ T dm4(T ww, T xx, T yy, T zz) {
@@ -15,7 +23,14 @@ __device__ __forceinline__ T dm4(T ww, T xx, T yy, T zz) {
   if (mabs(xx) < mn) mn = mabs(xx);
   if (mabs(yy) < mn) mn = mabs(yy);
   if (mabs(zz) < mn) mn = mabs(zz);
-  return T(0.125) * (sgn1(ww) + sgn1(xx)) * mabs(sgn1(ww) + sgn1(yy)) * (sgn1(ww) + sgn1(zz)) * mn;
+  const bool nw = signbit(ww);
+  const bool az = nw != signbit(xx), bz = nw != signbit(yy), cz = nw != signbit(zz);
+  if (!az && !bz && !cz) return mn;  // 0.125 * (2 sw) * 2 * (2 sw) = +1
+  // a zero factor: the product ((0.125*A)*B)*C*mn is a zero with the sign of
+  // A times the sign of C, where A = sw+sx and C = sw+sz are +0 when their
+  // signs differ and 2 sw otherwise (B = |sw+sy| >= 0 keeps the sign)
+  const bool neg = (!az && nw) != (!cz && nw);
+  return (neg ? T(-0.0) : T(0)) * mn;
 }
 
 // rec.f90:2095-2178: MP5 face state of cell 0 from u(-2..+2) given in the

@@ -30,7 +30,7 @@ struct Scal {
   int active;                     // 0 once time > tmax: every kernel of the step returns early
   int carry_count;                // cells queued for the loop-order W carry fix-up
   int cur;                        // index of P^n among the run's three primitive buffers
-  int pad;
+  int strag_count;                // cells whose primitive recovery was deferred this stage
 };
 
 // Counters (device, atomically accumulated).
@@ -96,6 +96,8 @@ struct DevRun {
   unsigned long long* cnt;
   int* carry_list;       // interior cells queued for the W carry fix-up
   int carry_cap;
+  int* strag_list;       // interior cells whose Newton-Raphson passed kDeferIter iterations
+  int strag_cap;
 
   RG_HD size_t cell(int i, int j, int k) const {
     return (size_t)(i - 1) + sj * (size_t)(j - 1) + sk * (size_t)(k - 1);

@@ -100,7 +100,7 @@ class Server:
         prep.ic_torus(**req.ic)
         return prep
 
-    def serve(self, requests: list[Request], clock=time.perf_counter) -> dict:
+    def serve(self, requests: list[Request], clock=time.perf_counter, max_wall_s: float = 3600.0) -> dict:
         reqs = sorted(requests, key=lambda r: r.arrival)
         t0 = clock()
         nxt = 0                                  # next request to arrive
@@ -112,6 +112,9 @@ class Server:
         busy = 0.0
         while len(done) < len(reqs):
             now = clock() - t0
+            if now > max_wall_s:
+                raise RuntimeError(f"serving did not finish within {max_wall_s} s "
+                                   f"({len(done)} of {len(reqs)} requests done)")
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
                 r = reqs[nxt]
                 waiting.append((r, self.pool.submit(self._prepare, r), footprint(r.params)))

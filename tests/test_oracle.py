@@ -154,3 +154,27 @@ def test_thread_count_independence(monkeypatch):
         r = subprocess.run([sys.executable, "-c", code % ROOT], capture_output=True, env=env, check=True)
         outs.append(r.stdout)
     assert outs[0] == outs[1]
+
+
+def test_periodic_transverse_corners_stay_stale():
+    """With periodic boundaries in both transverse directions of a 1D tube,
+    the single-rank periodic fill (bnd.f90:50-70, 160-180, 272-292) covers
+    only columns whose transverse indices are interior, so the cells that are
+    ghosts in both directions keep their old values; with copy boundaries
+    (the tube setup used here) every transverse cell equals the interior one."""
+    from raishinsource_b200 import config as cfg
+    p = cfg.tube(n=60)
+    per = dict(p, ibc=[[5] * 9, [5] * 9, [1] * 9, [1] * 9, [1] * 9, [1] * 9])
+    for params, uniform in ((per, False), (p, True)):
+        o = Oracle(params)
+        o.ic_tube(seed=3, tube=1)
+        ic = o.prims()
+        o.init_cons()
+        o.step(2)
+        u = o.prims()  # (k, j, i, v)
+        line = u[4, 4]
+        same = all(np.array_equal(u[k, j], line) for k in range(9) for j in range(9))
+        assert same == uniform
+        if not uniform:
+            # a corner ghost (j and k both ghosts) still holds the initial data
+            assert np.array_equal(u[0, 0], ic[0, 0]) and not np.array_equal(line, ic[4, 4])
