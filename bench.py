@@ -59,6 +59,9 @@ FALLBACK_HBM_GBS = 6650.0
 #  cfl:     per cell: read 9                                 -> 9 * 8
 BYTES_PER_UNIT = {"flux_r": 136, "flux_phi": 136, "flux_theta": 136, "update": 480, "flux_ct": 96,
                   "floors": 120, "cfl": 72}
+# DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one launch divided by
+# its units) on the 192x96x96 torus, whose state already exceeds the L2
+DRAM_BYTES_PER_UNIT = {"update": 471.0, "flux_r": 113.0, "flux_phi": 120.0, "flux_theta": 122.0}
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -234,7 +237,8 @@ def run_gpu(args) -> dict | None:
         total = sum(v["ms"] for v in prof.values())
         shares = {k: round(v["ms"] / total, 4) for k, v in prof.items()}
         top = max((k for k in prof if k in BYTES_PER_UNIT), key=lambda k: prof[k]["ms"])
-        n_launch = prof[top]["launches"] / (2 if top == "update" else 1)
+        # one update per stage comprises the cell kernel, the straggler pass and the W-carry pass
+        n_launch = 3 * args.prof_steps if top == "update" else prof[top]["launches"]
         nm0, nm1 = run.nm0, run.nm1
         faces = (p["imax"] - 2 * nm0 + 1) * (p["jmax"] - 2 * nm0 + 1) * (p["kmax"] - 2 * nm0 + 1)
         units = {"update": zones,
@@ -245,8 +249,12 @@ def run_gpu(args) -> dict | None:
         per_launch_ms = prof[top]["ms"] / max(n_launch, 1)
         peak, peak_kind = measured_peaks()
         achieved = BYTES_PER_UNIT[top] * u / (per_launch_ms * 1e-3) / 1e9
+        traffic = DRAM_BYTES_PER_UNIT.get(top)
         roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
-                    "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                    "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None if traffic is None else traffic * u,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on the "
+                                      "192x96x96 torus, scaled by the units of one launch",
                     "bytes_per_unit": BYTES_PER_UNIT[top], "units_per_launch": u, "ms_per_launch": per_launch_ms,
                     "note": "FP64-pipe bound path: HBM fraction of algorithmic bytes, see profiles/"}
     run.release()

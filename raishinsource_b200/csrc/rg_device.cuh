@@ -21,6 +21,15 @@ __device__ __forceinline__ double mabs(double x) { return fabs(x); }
 __device__ __forceinline__ float mabs(float x) { return fabsf(x); }
 __device__ __forceinline__ double sgn1(double x) { return copysign(1.0, x); }
 __device__ __forceinline__ float sgn1(float x) { return copysignf(1.0f, x); }
+// Division in the arithmetic type: exact IEEE division in FP64 (the
+// reference's arithmetic); in the FP32 half of the mixed path the fast
+// approximate division (at most 2 ulp), whose error is far below that of the
+// FP32 arithmetic around it.
+__device__ __forceinline__ double mdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float mdiv(float a, float b) { return __fdividef(a, b); }
+template <typename T>
+__device__ __forceinline__ T mrcp(T x) { return mdiv(T(1), x); }
+
 template <typename T>
 __device__ __forceinline__ T fmax3(T a, T b, T c) {
   T r = a;
@@ -203,16 +212,16 @@ __device__ __forceinline__ void pstate(const T q[9], const MetT<T>& m, T gam, PS
   lower_g(s.ucon, s.ucov, m);
   // physfunc.f90:81-100
   s.bbcon[0] = s.b1 * s.ucov[1] + s.b2 * s.ucov[2] + s.b3 * s.ucov[3];
-  s.bbcon[1] = (s.b1 + s.bbcon[0] * s.ucon[1]) * (T(1) / s.ucon[0]);
-  s.bbcon[2] = (s.b2 + s.bbcon[0] * s.ucon[2]) * (T(1) / s.ucon[0]);
-  s.bbcon[3] = (s.b3 + s.bbcon[0] * s.ucon[3]) * (T(1) / s.ucon[0]);
+  s.bbcon[1] = (s.b1 + s.bbcon[0] * s.ucon[1]) * mrcp(s.ucon[0]);
+  s.bbcon[2] = (s.b2 + s.bbcon[0] * s.ucon[2]) * mrcp(s.ucon[0]);
+  s.bbcon[3] = (s.b3 + s.bbcon[0] * s.ucon[3]) * mrcp(s.ucon[0]);
   lower_g(s.bbcon, s.bbcov, m);
   s.bbsq = s.bbcon[0] * s.bbcov[0] + s.bbcon[1] * s.bbcov[1] + s.bbcon[2] * s.bbcov[2] + s.bbcon[3] * s.bbcov[3];
 }
 
 // p / rho^Gamma of a state (caluu.f90:303, calflx.f90:474), computed once per state.
 template <typename T>
-__device__ __forceinline__ T ent_ratio(const PST<T>& s, T gam, int gkind) { return s.pr / pow_gam(s.de, gam, gkind); }
+__device__ __forceinline__ T ent_ratio(const PST<T>& s, T gam, int gkind) { return mdiv(s.pr, pow_gam(s.de, gam, gkind)); }
 
 // caluu.f90:92-118: sqrt(-g) (rho u^t, T^t_i, T^t_t + rho u^t, s u^t, B^i).
 // delta(0,n) is the literal identity of caldelta (physfunc.f90:122-158).
@@ -248,7 +257,7 @@ __device__ __forceinline__ void flux(const PST<T>& s, T gam, T detg, T w[9], T s
 #pragma unroll
   for (int m = 1; m <= 3; ++m) {
     if (m == D) w[5 + m] = T(0);
-    else w[5 + m] = (ud * (T(1) / s.ucon[0])) * bc[m] - (s.ucon[m] * (T(1) / s.ucon[0])) * bc[D];
+    else w[5 + m] = (ud * mrcp(s.ucon[0])) * bc[m] - (s.ucon[m] * mrcp(s.ucon[0])) * bc[D];
   }
 #pragma unroll
   for (int n = 0; n < 9; ++n) w[n] = detg * w[n];
@@ -262,16 +271,16 @@ __device__ __forceinline__ void wavespeed(const T q[9], const PST<T>& s, const M
   const T alpha1 = m.al;
   const T betad = (D == 1) ? m.be1 : (D == 2 ? m.be2 : T(0));
   const T gc3dd = (D == 1) ? m.g3_11 : (D == 2 ? m.g3_22 : m.g3_33);
-  const T vcon[4] = {T(0), q[1] * (T(1) / s.gfl), q[2] * (T(1) / s.gfl), q[3] * (T(1) / s.gfl)};
+  const T vcon[4] = {T(0), q[1] * mrcp(s.gfl), q[2] * mrcp(s.gfl), q[3] * mrcp(s.gfl)};
   const T vsq = qform3(m, vcon[1], vcon[2], vcon[3]);
-  const T cssq = gam * s.pr / s.roh;
-  const T vasq = s.bbsq * (T(1) / (s.roh + s.bbsq));
+  const T cssq = mdiv(gam * s.pr, s.roh);
+  const T vasq = s.bbsq * mrcp(s.roh + s.bbsq);
   const T omsq = vasq + cssq * (T(1) - vasq);
   const T f1 = vcon[D] * (T(1) - omsq);
   const T f2 = T(1) - vsq * omsq;
   const T f3 = omsq * (T(1) - vsq) * ((T(1) - vsq * omsq) * gc3dd - (T(1) - omsq) * vcon[D] * vcon[D]);
-  vfp = (f1 + msqrt(f3)) * (T(1) / f2);
-  vfm = (f1 - msqrt(f3)) * (T(1) / f2);
+  vfp = (f1 + msqrt(f3)) * mrcp(f2);
+  vfm = (f1 - msqrt(f3)) * mrcp(f2);
   vfp = alpha1 * vfp - betad;
   vfm = alpha1 * vfm - betad;
   if (mabs(vfp) > T(1)) vfp = T(1);
