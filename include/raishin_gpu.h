@@ -146,11 +146,12 @@ int rg_run_download_stored(rg_ctx* ctx, int run, double* soa);
 int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats);
 int rg_run_stats(rg_ctx* ctx, int run, rg_step_stats* stats);
 
-/* Advance nruns runs together by nsteps full RK3 steps.  The runs must have a
- * slab direction (2D phi slabs, 1D tubes; see RG_FLAG_FULL); runs that share
- * reconstruction, precision and slab class form one batch, whose step is one
- * launch per kernel kind over a per-run tile table (persistent grid), captured
- * once in a CUDA graph and replayed each step.  The first call for a set of
+/* Advance nruns runs together by nsteps full RK3 steps.  Runs that share
+ * reconstruction, precision and slab class (see RG_FLAG_FULL) form one batch,
+ * whose step is one launch per kernel kind over a per-run tile table
+ * (persistent grid), captured once in a CUDA graph and replayed each step.
+ * Meant for many small runs (2D slabs, 1D tubes); a large 3D run alone is
+ * faster through rg_step.  The first call for a set of
  * runs tunes the tile width and grid size on trial steps from a snapshot of
  * the runs' state, which it restores.  Each run's result equals its result
  * stepped alone.  stats, if given, receives nruns records.  Replaces the

@@ -79,7 +79,8 @@ struct rg_ctx {
   cudaStream_t stream = nullptr;
   std::map<int, Run*> runs;
   std::map<std::vector<int>, BatchEntry*> batches;
-  std::map<long long, std::pair<int, int>> tuned;  // batch class -> (width, grid factor) chosen by the tuner
+  struct Tuned { int width, grid_factor; double ms; };
+  std::map<long long, Tuned> tuned;  // batch class -> shape chosen by the tuner and its step time
   int next_id = 1;
   long long launches[K_NKINDS] = {};   // kernel launches issued, per kind
   bool prof = false;                   // bracket every launch with CUDA events
@@ -500,12 +501,13 @@ int make_batch(rg_ctx* ctx, std::vector<Run*>& rs, const std::vector<int>& ids, 
   if (tk != ctx->tuned.end()) {  // shape already tuned for this class (e.g. a serving batch that changed members)
     BatchEntry* E = new BatchEntry();
     E->ids = ids;
-    if (batch_build(dr, tk->second.first, &E->plan)) {
+    if (batch_build(dr, tk->second.width, &E->plan)) {
       delete E;
       return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
     }
-    E->width = tk->second.first;
-    E->grid_factor = tk->second.second;
+    E->width = tk->second.width;
+    E->grid_factor = tk->second.grid_factor;
+    E->tuned_ms = tk->second.ms;
     batch_set_grid(E->plan, E->grid_factor);
     const int rc = capture_batch(E);
     if (rc) return rc;
@@ -559,7 +561,7 @@ int make_batch(rg_ctx* ctx, std::vector<Run*>& rs, const std::vector<int>& ids, 
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   RG_CUDA(cudaStreamSynchronize(s));
-  ctx->tuned[cls] = {E->width, E->grid_factor};
+  ctx->tuned[cls] = {E->width, E->grid_factor, E->tuned_ms};
   const int crc = capture_batch(E);
   if (crc) return crc;
   *out = E;
@@ -962,8 +964,6 @@ int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_s
   for (int a = 0; a < nruns; ++a) {
     Run* R = find(ctx, runs[a]);
     if (!R) return fail(RG_ENOTFOUND, "unknown run in batch");
-    if (!R->d.jfix && !R->d.kfix)
-      return fail(RG_EINVAL_CONFIG, "batched steps take runs with a slab direction (2D phi slabs, 1D tubes)");
     groups[batch_class(R)].push_back(runs[a]);
   }
   std::vector<BatchEntry*> es;

@@ -130,3 +130,19 @@ def test_batch_membership_change_and_release(gpu_ctx):
     assert np.array_equal(solo.prims(), rs[2].prims())
     for r in (rs[0], rs[2], solo):
         r.release()
+
+
+def test_tube_mixed_tracks_fp64(gpu_ctx):
+    """FP32-mixed tubes (Minkowski: no FP64 region) stay close to FP64 over 40 steps."""
+    ps = [dict(config.tube(n=300), guard=1), dict(config.tube(n=300, precision="mixed"), guard=1)]
+    rs = [gpu_ctx.admit(p) for p in ps]
+    for r in rs:
+        r.ic_tube(seed=2012, tube=4)
+    for r in rs:
+        r.step(40)
+    a, b = rs[1].stored_prims()[:, 0, 0, :], rs[0].stored_prims()[:, 0, 0, :]
+    for r in rs:
+        r.release()
+    l1 = np.abs(a - b).sum(axis=1) / np.abs(b).sum(axis=1).clip(1e-300)
+    assert np.isfinite(a).all()
+    assert l1[0] < 1e-4, l1

@@ -255,3 +255,43 @@ def test_slab_rejects_nonuniform_upload(gpu_ctx):
         r.upload_prims(u2)
     r.release()
     assert e.value.code == 1
+
+
+@pytest.mark.parametrize("irec", [config.IREC_PPM, config.IREC_WENO5])
+def test_step_2d_slab_ppm_weno5(gpu_ctx, irec):
+    """2D phi slab (stored as one plane; PPM needs nm1 = 5, jmax = 11) against
+    the oracle, which computes every phi cell."""
+    p = dict(config.torus(nr=56, nth=48, irec=irec), guard=1)
+    errs, _ = _step_err(gpu_ctx, p, 2, seed=21)
+    assert errs.max() < TOL, errs
+
+
+def test_admission_refuses_oversize_footprint(gpu_ctx):
+    """A run whose device footprint exceeds free memory is refused before any
+    allocation (RG_ENOMEM_ADMIT)."""
+    from raishinsource_b200.capi import RgError, footprint
+    import torch
+    free, _ = torch.cuda.mem_get_info()
+    p = config.torus(nr=1536, nth=1024, nph=1024)
+    assert footprint(p) > free
+    with pytest.raises(RgError) as e:
+        gpu_ctx.admit(p)
+    assert e.value.code == 2
+
+
+def test_thousand_steps_l1_ppm(gpu_ctx):
+    """1000 steps without re-synchronisation (PPM, reference semantics, 2D
+    torus 64x64): L1 of rho, p and B against the oracle stays below 1e-10."""
+    p = config.torus(nr=64, nth=64, irec=config.IREC_PPM)
+    o = Oracle(p)
+    o.ic_torus(seed=4)
+    o.init_cons()
+    r = gpu_ctx.admit(p)
+    r.upload_prims(o.prims())
+    o.step(1000)
+    st = r.step(1000, stats=True)
+    got, want = r.prims(), o.prims()
+    r.release()
+    assert st["steps"] == 1000
+    l1 = _l1(got, want, o.nm1)
+    assert l1[[0, 4, 6, 7, 8]].max() < 1e-10, l1
