@@ -185,6 +185,18 @@ int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri);
 int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl);
 /* bnd4 + infchk + atmosphere1a + pminmax2b (bnd.f90, correction.f90) on uri in/out */
 int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio);
+/* caltenr + calsf (calsf.f90:6-151) on every cell: sf(2:5,i,j,k), 4 doubles
+ * per cell */
+int rg_calsf(rg_ctx* ctx, int run, const double* uri, double* sf);
+/* One RK3 stage of rkt.f90 on the interior (is1+nm1..ie1-nm1 in each
+ * direction) with akap?b = dt/dx?b (main.f90:766-779): stage 1 = rk2fst +
+ * rk2adsff, unew = uh from ucur = uu; stage 2 = rk3snd + rk3adsfs, unew = us
+ * from uo and ucur = uh; stage 3 = rk3trd + rk3adsft, unew = un from uo and
+ * ucur = us (rkt.f90:2-42, 91-180, 183-215, 253-320).  ww(3,nv,i,j,k) with flux-CT
+ * applied (rg_calflx), sf(2:5,i,j,k) (rg_calsf); uo may be NULL in stage 1;
+ * unew is in/out (cells outside the interior keep their values). */
+int rg_rkt(rg_ctx* ctx, int run, int stage, double dt, const double* ww, const double* uo, const double* ucur,
+           const double* sf, double* unew);
 
 /* Restart files byte-compatible with store1 / restar2 (restar.f90:5-88,
  * 273-346) for one rank: gfortran sequential unformatted records (4-byte

@@ -128,7 +128,7 @@ void rec2(State& s);
 void calcha(State& s);
 void hlle(State& s);
 void fluxct(State& s);
-void calsf_all(State& s);
+void calsf_all(State& s, bool every_cell = false);
 void rkstage(State& s, int stage);
 void recov1a(State& s, std::vector<double>& uu);
 void bnd4(State& s);

@@ -118,6 +118,33 @@ void orc_recov(void* h, double* uu, double* uri) {
   std::memcpy(uri, s->uri.data(), s->uri.size() * sizeof(double));
 }
 
+// caltenr + calsf on every cell of the given primitives; sf(2:5,i,j,k) out
+void orc_calsf(void* h, const double* uri, double* sf) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  orc::calsf_all(*s, true);
+  std::memcpy(sf, s->sf.data(), s->sf.size() * sizeof(double));
+}
+
+// One RK3 stage (rkstage) with the given dt, ww, sf and conserved inputs:
+// stage 1 uh from uu = ucur; stage 2 us from uo and uh = ucur; stage 3 un from
+// uo and us = ucur.  unew is in/out (cells outside the interior keep theirs).
+void orc_rkt(void* h, int stage, double dt, const double* ww, const double* uo, const double* ucur,
+             const double* sf, double* unew) {
+  State* s = static_cast<State*>(h);
+  const size_t n = s->uu.size();
+  s->dt = dt;
+  std::memcpy(s->ww.data(), ww, s->ww.size() * sizeof(double));
+  std::memcpy(s->sf.data(), sf, s->sf.size() * sizeof(double));
+  std::vector<double>& in = (stage == 1) ? s->uu : (stage == 2 ? s->uh : s->us);
+  std::vector<double>& out = (stage == 1) ? s->uh : (stage == 2 ? s->us : s->un);
+  std::memcpy(in.data(), ucur, n * sizeof(double));
+  if (stage > 1) std::memcpy(s->uo.data(), uo, n * sizeof(double));
+  std::memcpy(out.data(), unew, n * sizeof(double));
+  orc::rkstage(*s, stage);
+  std::memcpy(unew, out.data(), n * sizeof(double));
+}
+
 // cdtcfl4 on the given primitives
 double orc_cdtcfl(void* h, const double* uri) {
   State* s = static_cast<State*>(h);

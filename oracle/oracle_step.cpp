@@ -636,15 +636,16 @@ void fluxct(State& s) {
       }
 }
 
-// calsf.f90:6-151 (T^m_n at the cell and S_nu = sqrt(-g) T^m_n Gamma^n_{nu m});
-// computed on the interior only, the only cells that read sf (rkt.f90).
-void calsf_all(State& s) {
+// calsf.f90:6-151 (T^m_n at the cell and S_nu = sqrt(-g) T^m_n Gamma^n_{nu m}).
+// The step computes it on the interior only, the only cells that read sf
+// (rkt.f90); every_cell covers the reference's whole loop range.
+void calsf_all(State& s, bool every_cell) {
   const double gam = s.p.gam;
-  const int nm1 = s.nm1;
+  const int lo = every_cell ? 0 : s.nm1;
 #pragma omp parallel for schedule(static)
-  for (int k = nm1 + 1; k <= s.kmax - nm1; ++k)
-    for (int j = nm1 + 1; j <= s.jmax - nm1; ++j)
-      for (int i = nm1 + 1; i <= s.imax - nm1; ++i) {
+  for (int k = lo + 1; k <= s.kmax - lo; ++k)
+    for (int j = lo + 1; j <= s.jmax - lo; ++j)
+      for (int i = lo + 1; i <= s.imax - lo; ++i) {
         const size_t q = s.ik(i, k);
         PS ps;
         pstate(&s.uri[s.a(1, i, j, k)], s.gcov[q], s.gcon[q], gam, ps);

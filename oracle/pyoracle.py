@@ -70,6 +70,8 @@ def _lib():
         lib.orc_cdtcfl.argtypes = [P, D]
         lib.orc_cdtcfl.restype = C.c_double
         lib.orc_bnd_floor.argtypes = [P, D, D]
+        lib.orc_calsf.argtypes = [P, D, D]
+        lib.orc_rkt.argtypes = [P, C.c_int, C.c_double, D, D, D, D, D]
         lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
         lib.orc_get_array.restype = C.c_longlong
         _LIB = lib
@@ -176,6 +178,23 @@ class Oracle:
         uri = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
         self.lib.orc_recov(self.h, _ptr(uu), _ptr(uri))
         return uu, uri
+
+    def calsf(self, uri) -> np.ndarray:
+        """sf(2:5,i,j,k) of every cell, shape (kmax, jmax, imax, 4)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = np.zeros(self.shape[:3] + (4,), dtype=np.float64)
+        self.lib.orc_calsf(self.h, _ptr(uri), _ptr(out))
+        return out
+
+    def rkt(self, stage: int, dt: float, ww, uo, ucur, sf, unew) -> np.ndarray:
+        """One RK3 stage of rkt.f90; returns the updated copy of unew."""
+        ww = np.ascontiguousarray(ww, dtype=np.float64).reshape(self.shape + (3,))
+        ucur = np.ascontiguousarray(ucur, dtype=np.float64).reshape(self.shape)
+        sf = np.ascontiguousarray(sf, dtype=np.float64).reshape(self.shape[:3] + (4,))
+        uo = ucur if uo is None else np.ascontiguousarray(uo, dtype=np.float64).reshape(self.shape)
+        out = np.array(unew, dtype=np.float64, order="C").reshape(self.shape)
+        self.lib.orc_rkt(self.h, stage, dt, _ptr(ww), _ptr(uo), _ptr(ucur), _ptr(sf), _ptr(out))
+        return out
 
     def cdtcfl(self, uri) -> float:
         uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)

@@ -28,7 +28,7 @@ STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA"
 EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
-           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -69,14 +69,18 @@ _lib = None
 def load(path: str = LIB_PATH):
     """Load the CUDA library (building it first if the .so is absent or stale).
 
-    RAISHIN_GPU_LIB names an already built variant of the library to load
-    instead (e.g. the uncontracted RG_FMAD=0 build)."""
+    RAISHIN_GPU_LIB=exact loads the uncontracted variant
+    (libraishin_gpu_exact.so) instead; any other value is the path of a
+    library to load."""
     global _lib
     if _lib is not None:
         return _lib
     from . import build as _build
     path = os.environ.get("RAISHIN_GPU_LIB", path)
-    path = _build.build() if path == LIB_PATH else path
+    if path == LIB_PATH:
+        path = _build.build()
+    elif path == "exact":
+        path = _build.build(variants=("exact",))
     lib = C.CDLL(path)
     P, D, I = C.c_void_p, C.POINTER(C.c_double), C.c_int
     lib.rg_last_error.restype = C.c_char_p
@@ -110,6 +114,8 @@ def load(path: str = LIB_PATH):
     lib.rg_recov.argtypes = [P, I, D, D]
     lib.rg_cdtcfl.argtypes = [P, I, D, D]
     lib.rg_bnd_floor.argtypes = [P, I, D, D]
+    lib.rg_calsf.argtypes = [P, I, D, D]
+    lib.rg_rkt.argtypes = [P, I, I, C.c_double, D, D, D, D, D]
     lib.rg_calflx_static.argtypes = [P, I, P, P]
     lib.rg_run_horizon_flux.argtypes = [P, I, D, D]
     lib.rg_run_store.argtypes = [P, I, C.c_char_p, I, I, I, C.c_void_p]
@@ -335,6 +341,27 @@ class Run:
         uu = np.ascontiguousarray(uu, dtype=np.float64).reshape(self.shape)
         out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
         _check(self.lib, self.lib.rg_recov(self.ctx.h, self.id, _dptr(uu), _dptr(out)))
+        return out
+
+    def calsf(self, uri) -> np.ndarray:
+        """sf(2:5,i,j,k) as shape (kmax, jmax, imax, 4)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = np.zeros(self.shape[:3] + (4,), dtype=np.float64)
+        _check(self.lib, self.lib.rg_calsf(self.ctx.h, self.id, _dptr(uri), _dptr(out)))
+        return out
+
+    def rkt(self, stage: int, dt: float, ww, uo, ucur, sf, unew) -> np.ndarray:
+        """One RK3 stage (rg_rkt); returns the updated copy of unew."""
+        ww = np.ascontiguousarray(ww, dtype=np.float64).reshape(self.shape + (3,))
+        ucur = np.ascontiguousarray(ucur, dtype=np.float64).reshape(self.shape)
+        sf = np.ascontiguousarray(sf, dtype=np.float64).reshape(self.shape[:3] + (4,))
+        out = np.array(unew, dtype=np.float64, order="C").reshape(self.shape)
+        uo_p = None
+        if uo is not None:
+            uo = np.ascontiguousarray(uo, dtype=np.float64).reshape(self.shape)
+            uo_p = _dptr(uo)
+        _check(self.lib, self.lib.rg_rkt(self.ctx.h, self.id, stage, dt, _dptr(ww), uo_p, _dptr(ucur), _dptr(sf),
+                                         _dptr(out)))
         return out
 
     def cdtcfl(self, uri) -> float:

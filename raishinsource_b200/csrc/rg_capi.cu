@@ -42,6 +42,7 @@ struct Run {
   DevBufs fb{};            // full-layout buffers of the per-routine entry points (allocated on first use)
   bool fb_ready = false;
   double* aos = nullptr;   // 9*Nfull staging buffer in the reference layout (allocated on first use)
+  double* unew = nullptr;  // 9*Nfull output of rg_rkt (allocated on first use)
   int* bad = nullptr;      // device flag: uploaded data not uniform along a slab direction
   size_t nfull = 0;        // imax*jmax*kmax
   int cur = 0;             // index of P^n in b.P
@@ -710,7 +711,11 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   d.nm1 = d.nm0 + 1;
   d.irec = p->irec; d.model = p->model; d.guard = p->guard; d.iter = p->iter;
   d.mixed = (p->precision == RG_MIXED);
+#ifdef RG_EXACT_ARITH
+  d.gkind = 0;  // every power through pow(), as the reference writes it
+#else
   d.gkind = (p->gam == 4.0 / 3.0) ? 1 : (p->gam == 5.0 / 3.0 ? 2 : 0);
+#endif
   // cells inside r < 2 r_H keep FP64 in the mixed path (Kerr metrics only)
   d.i_fp64 = 0;
   if (p->metric == 303 || p->metric == 403) {
@@ -1113,6 +1118,60 @@ int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
   return RG_OK;
 }
 
+int rg_calsf(rg_ctx* ctx, int run, const double* uri, double* sf) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!uri || !sf) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  const size_t N = d.N;
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
+  RG_CUDA(launch_calsf(d, B->stage, B->CT, ctx->stream));
+  std::vector<double> S(4 * N);
+  RG_CUDA(cudaMemcpyAsync(S.data(), B->CT, 4 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (size_t c = 0; c < N; ++c)
+    for (int n = 0; n < 4; ++n) sf[4 * c + n] = S[(size_t)n * N + c];
+  return RG_OK;
+}
+
+int rg_rkt(rg_ctx* ctx, int run, int stage, double dt, const double* ww, const double* uo, const double* ucur,
+           const double* sf, double* unew) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (stage < 1 || stage > 3) return fail(RG_EINVAL_CONFIG, "stage must be 1, 2 or 3");
+  if (!ww || !ucur || !sf || !unew || (stage > 1 && !uo)) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  const size_t N = d.N;
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc) return rc;
+  if (!R->unew) {
+    void* p = nullptr;
+    if ((rc = dalloc(R, &p, 9 * N * sizeof(double)))) return rc;
+    R->unew = static_cast<double*>(p);
+  }
+  // ww(3,nv,i,j,k) and sf(2:5,i,j,k) to planes (host side: this entry point
+  // serves per-routine swap-in and parity, not the step)
+  std::vector<double> W(9 * N), S(4 * N);
+  for (int dir = 0; dir < 3; ++dir) {
+    for (size_t c = 0; c < N; ++c)
+      for (int v = 0; v < 9; ++v) W[(size_t)v * N + c] = ww[dir + 3 * (v + 9 * c)];
+    RG_CUDA(cudaMemcpyAsync(B->F[dir], W.data(), 9 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));  // W is refilled for the next direction
+  }
+  for (size_t c = 0; c < N; ++c)
+    for (int n = 0; n < 4; ++n) S[(size_t)n * N + c] = sf[4 * c + n];
+  RG_CUDA(cudaMemcpyAsync(B->CT, S.data(), 4 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = to_soa(ctx, R, ucur, B->stage, d, false))) return rc;
+  if (stage > 1 && (rc = to_soa(ctx, R, uo, B->stage2, d, false))) return rc;
+  if ((rc = to_soa(ctx, R, unew, R->unew, d, false))) return rc;
+  RG_CUDA(launch_rkt(d, stage, B->F[0], B->F[1], B->F[2], stage > 1 ? B->stage2 : nullptr, B->stage, B->CT, R->unew,
+                     dt, ctx->stream));
+  return from_soa(ctx, R, R->unew, unew, d);
+}
+
 // ------------------------------------------------------------ restart files
 // store1 / restar2 (restar.f90:5-88, 273-346) write and read one rank's state
 // as gfortran sequential unformatted records (a 4-byte length before and
@@ -1143,11 +1202,9 @@ int rg_run_store(rg_ctx* ctx, int run, const char* path, int it0, int ih0, int n
   if ((rc = rg_caluu1(ctx, run, uri.data(), uu.data()))) return rc;
   const double* pr0 = uri0 ? uri0 : uri.data();
   if ((rc = rg_caluu1(ctx, run, pr0, u0.data()))) return rc;
-  rg_step_stats st{};
   Scal sc{};
   RG_CUDA(cudaMemcpyAsync(&sc, R->d.scal, sizeof(Scal), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
-  (void)st;
   FILE* f = std::fopen(path, "wb");
   if (!f) return fail(RG_EINVAL_CONFIG, std::string("cannot open ") + path);
   const int32_t h1[2] = {0, nd}, h2[2] = {it0, ih0};

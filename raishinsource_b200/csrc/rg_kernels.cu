@@ -295,6 +295,46 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
 }
 
 // ------------------------------------------------------------ stage update
+// calsf.f90:107-151 with caltenr's T^m_n (calsf.f90:6-104): the source
+// S_nu = sqrt(-g) sum_{n,m} T^m_n Gamma^n_{nu m} of one cell from its
+// 4-vectors and the Christoffel cache at metric point q, summed in the
+// reference's (n, m) order; sf[0..3] = sf(2:5) (nu = 1, 2, 3, 0).
+__device__ __forceinline__ void geom_source(const DevRun& r, const PS& s, size_t q, double detg, double sf[4]) {
+  const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
+  double ta = 0.0, tb = 0.0, tc = 0.0, td = 0.0;
+  const size_t nik = r.nik;
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int mm = 0; mm < 4; ++mm) {
+      const double t = a * s.ucon[mm] * s.ucov[n] + b * (mm == n ? 1.0 : 0.0) - s.bbcon[mm] * s.bbcov[n];
+      ta = ta + t * __ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
+      tb = tb + t * __ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
+      tc = tc + t * __ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
+      td = td + t * __ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
+    }
+  sf[0] = detg * ta; sf[1] = detg * tb; sf[2] = detg * tc; sf[3] = detg * td;
+}
+
+// rk2fst (rkt.f90:2-42), rk3snd (rkt.f90:91-134) and rk3trd (rkt.f90:137-180)
+// for one variable: uo = U^n, uc = the stage input (uu, uh or us), a? = dt/dx?b
+// and d? the flux differences; (1./3.) and (2./3.) are single-precision
+// literals in the reference.
+template <int STAGE>
+__device__ __forceinline__ double rk_combine(double uo, double uc, double a1, double d1, double a2, double d2,
+                                             double a3, double d3) {
+  if (STAGE == 1) return uc - a1 * d1 - a2 * d2 - a3 * d3;
+  if (STAGE == 2) return (3.0 * uo + uc) * 0.25 + (-(a1 * d1) - a2 * d2 - a3 * d3) * 0.25;
+  return (uo + 2. * uc) * (double)(1.0f / 3.0f) + (-(a1 * d1) - a2 * d2 - a3 * d3) * (double)(2.0f / 3.0f);
+}
+// rk2adsff / rk3adsfs / rk3adsft (rkt.f90:183-215, 253-320) for one of variables 2-5.
+template <int STAGE>
+__device__ __forceinline__ double rk_add_source(double u, double sf, double dt) {
+  if (STAGE == 1) return u + sf * dt;
+  if (STAGE == 2) return u + sf * dt * 0.25;
+  return u + sf * dt * (double)(2.0f / 3.0f);
+}
+
 // Conserved state after the RK combine and source (rkt.f90:2-320) of one
 // interior cell.  U = P2C(P) always holds in the reference (caluu1 runs after
 // every stage, main.f90:899), so the stage inputs uu/uo/uh/us are recomputed
@@ -317,22 +357,7 @@ __device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, co
     for (int v = 0; v < 9; ++v) r.Un[(size_t)v * N + c] = ucur[v];
   // geometric source (calsf.f90:6-151): S_nu = sqrt(-g) T^m_n Gamma^n_{nu m}
   double sf[4];
-  {
-    const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
-    double ta = 0.0, tb = 0.0, tc = 0.0, td = 0.0;
-    const size_t nik = r.nik;
-#pragma unroll
-    for (int n = 0; n < 4; ++n)
-#pragma unroll
-      for (int mm = 0; mm < 4; ++mm) {
-        const double t = a * s.ucon[mm] * s.ucov[n] + b * (mm == n ? 1.0 : 0.0) - s.bbcon[mm] * s.bbcov[n];
-        ta = ta + t * __ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
-        tb = tb + t * __ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
-        tc = tc + t * __ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
-        td = td + t * __ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
-      }
-    sf[0] = m.detg * ta; sf[1] = m.detg * tb; sf[2] = m.detg * tc; sf[3] = m.detg * td;
-  }
+  geom_source(r, s, q, m.detg, sf);
   double uo[9];
   if (STAGE > 1) load9(r.Un, N, c, uo);
   const double a1 = dt / __ldg(r.dx1b + i - 1), a2 = dt / __ldg(r.dx2b + j - 1), a3 = dt / __ldg(r.dx3b + k - 1);
@@ -350,16 +375,10 @@ __device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, co
     if (v == 6) d3 = CT[1 * N + c] - CT[1 * N + ck];
     else if (v == 7) d3 = CT[3 * N + c] - CT[3 * N + ck];
     else d3 = F3[(size_t)v * N + c] - F3[(size_t)v * N + ck];
-    if (STAGE == 1) u[v] = ucur[v] - a1 * d1 - a2 * d2 - a3 * d3;
-    else if (STAGE == 2) u[v] = (3.0 * uo[v] + ucur[v]) * 0.25 + (-(a1 * d1) - a2 * d2 - a3 * d3) * 0.25;
-    else u[v] = (uo[v] + 2. * ucur[v]) * (double)(1.0f / 3.0f) + (-(a1 * d1) - a2 * d2 - a3 * d3) * (double)(2.0f / 3.0f);
+    u[v] = rk_combine<STAGE>(STAGE > 1 ? uo[v] : 0.0, ucur[v], a1, d1, a2, d2, a3, d3);
   }
 #pragma unroll
-  for (int v = 1; v <= 4; ++v) {
-    if (STAGE == 1) u[v] = u[v] + sf[v - 1] * dt;
-    else if (STAGE == 2) u[v] = u[v] + sf[v - 1] * dt * 0.25;
-    else u[v] = u[v] + sf[v - 1] * dt * (double)(2.0f / 3.0f);
-  }
+  for (int v = 1; v <= 4; ++v) u[v] = rk_add_source<STAGE>(u[v], sf[v - 1], dt);
 }
 
 // Compensated FP32 accumulation (Kahan/Knuth two-sum, FMA two-product):
@@ -1181,6 +1200,55 @@ __global__ void __launch_bounds__(128) k_p2c(DevRun r, const double* __restrict_
   for (int v = 0; v < 9; ++v) U[(size_t)v * N + c] = u[v];
 }
 
+// caltenr + calsf (calsf.f90:6-151) on every cell: sf(2:5) as four planes
+// SF[n*N + c].
+__global__ void __launch_bounds__(128) k_calsf(DevRun r, const double* __restrict__ P, double* __restrict__ SF) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = jidx(r, 1, blockIdx);
+  const int k = kidx(r, 1, blockIdx);
+  if (i > r.imax || j > r.jmax || k > r.kmax) return;
+  const size_t N = r.N, c = r.cell(i, j, k), q = r.ik(i, k);
+  double p[9];
+  load9(P, N, c, p);
+  Met m;
+  load_met(r.mc, r.nik, q, m);
+  PS s;
+  pstate(p, m, r.gam, s);
+  double sf[4];
+  geom_source(r, s, q, m.detg, sf);
+#pragma unroll
+  for (int n = 0; n < 4; ++n) SF[(size_t)n * N + c] = sf[n];
+}
+
+// One RK stage of rkt.f90 (rk2fst, rk3snd or rk3trd, then the matching
+// rk*ads*) on the interior: W[d] holds ww(d, m) of cell c at m*N + c (flux-CT
+// already applied), Uo = uo (stages 2 and 3), Uc = the stage input (uu, uh or
+// us), SF = sf(2:5) as four planes; Unew keeps its values outside the interior.
+template <int STAGE>
+__global__ void __launch_bounds__(128) k_rkt(DevRun r, const double* __restrict__ W1, const double* __restrict__ W2,
+                                             const double* __restrict__ W3, const double* __restrict__ Uo,
+                                             const double* __restrict__ Uc, const double* __restrict__ SF,
+                                             double* __restrict__ Unew, double dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = jidx(r, 1, blockIdx);
+  const int k = kidx(r, 1, blockIdx);
+  if (i > r.imax || j > r.jmax || k > r.kmax || !is_interior(r, i, j, k)) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  const size_t ci = c - 1, cj = c - r.sj, ck = c - r.sk;
+  const double a1 = dt / __ldg(r.dx1b + i - 1), a2 = dt / __ldg(r.dx2b + j - 1), a3 = dt / __ldg(r.dx3b + k - 1);
+  double u[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    const size_t o = (size_t)v * N;
+    const double d1 = W1[o + c] - W1[o + ci], d2 = W2[o + c] - W2[o + cj], d3 = W3[o + c] - W3[o + ck];
+    u[v] = rk_combine<STAGE>(STAGE > 1 ? Uo[o + c] : 0.0, Uc[o + c], a1, d1, a2, d2, a3, d3);
+  }
+#pragma unroll
+  for (int v = 1; v <= 4; ++v) u[v] = rk_add_source<STAGE>(u[v], SF[(size_t)(v - 1) * N + c], dt);
+#pragma unroll
+  for (int v = 0; v < 9; ++v) Unew[(size_t)v * N + c] = u[v];
+}
+
 // a(nv, cell) of the reference's full array <-> stored SoA.  Upload reads the
 // stored cells' values and flags (bad != 0) any full-array cell whose value
 // differs from the stored cell it maps to: a slab direction holds one plane,
@@ -1469,6 +1537,22 @@ cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Po
 cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s) {
   const dim3 b = sblock(r, dim3(64, 2, 1));
   k_p2c<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P, U);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStream_t s) {
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  k_calsf<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P, SF);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rkt(const DevRun& r, int stage, const double* W1, const double* W2, const double* W3,
+                       const double* Uo, const double* Uc, const double* SF, double* Unew, double dt, cudaStream_t s) {
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 g = sgrid(r, r.imax, r.jmax, r.kmax, b);
+  if (stage == 1) k_rkt<1><<<g, b, 0, s>>>(r, W1, W2, W3, Uo, Uc, SF, Unew, dt);
+  else if (stage == 2) k_rkt<2><<<g, b, 0, s>>>(r, W1, W2, W3, Uo, Uc, SF, Unew, dt);
+  else k_rkt<3><<<g, b, 0, s>>>(r, W1, W2, W3, Uo, Uc, SF, Unew, dt);
   return cudaGetLastError();
 }
 

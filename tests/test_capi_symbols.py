@@ -20,14 +20,15 @@ def test_header_declares_entry_points():
 
 
 def test_library_exports_every_declared_symbol():
+    """Both variants (product and uncontracted) export the whole ABI."""
     from raishinsource_b200 import build
     from raishinsource_b200.capi import EXPORTS
-    path = build.build()
-    lib = ctypes.CDLL(path)
     syms = declared_symbols()
     assert sorted(EXPORTS) == syms
-    for s in syms:
-        assert hasattr(lib, s), s
+    for variant in build.VARIANTS:
+        lib = ctypes.CDLL(build.build(variants=(variant,)))
+        for s in syms:
+            assert hasattr(lib, s), (variant, s)
 
 
 def test_footprint_and_param_checks_run_on_cpu():

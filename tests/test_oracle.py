@@ -178,3 +178,37 @@ def test_periodic_transverse_corners_stay_stale():
         if not uniform:
             # a corner ghost (j and k both ghosts) still holds the initial data
             assert np.array_equal(u[0, 0], ic[0, 0]) and not np.array_equal(line, ic[4, 4])
+
+
+def test_rkt_stage_combinations_and_literals(torus_small):
+    """rkt.f90 with zero fluxes and sources: stage 1 returns uu, stage 2
+    (3 uo + uh)/4, stage 3 (uo + 2 us) times the single-precision (1./3.)
+    (rkt.f90:169); cells outside the interior keep unew."""
+    _, o = torus_small
+    rng = np.random.default_rng(3)
+    shape = o.prims().shape
+    ww = np.zeros(shape + (3,))
+    sf = np.zeros(shape[:3] + (4,))
+    uo, uc, unew = (rng.standard_normal(shape) for _ in range(3))
+    n = o.nm1
+    inner = (slice(n, -n), slice(n, -n), slice(n, -n))
+    third = float(np.float32(1.0) / np.float32(3.0))
+    want = {1: uc, 2: (3.0 * uo + uc) * 0.25, 3: (uo + 2.0 * uc) * third}
+    for stage in (1, 2, 3):
+        got = o.rkt(stage, 0.1, ww, uo, uc, sf, unew)
+        assert np.array_equal(got[inner], want[stage][inner])
+        outside = np.ones(shape[:3], dtype=bool)
+        outside[inner] = False
+        assert np.array_equal(got[outside], unew[outside])
+
+
+def test_calsf_covers_every_cell(torus_small):
+    """caltenr + calsf run over the reference's whole loop range (calsf.f90:121-123):
+    the ghost cells get finite, nonzero sources too."""
+    _, o = torus_small
+    sf = o.calsf(o.prims())
+    assert np.isfinite(sf).all()
+    n = o.nm1
+    ghosts = np.ones(sf.shape[:3], dtype=bool)
+    ghosts[n:-n, n:-n, n:-n] = False
+    assert (np.abs(sf[ghosts]).max(axis=1) > 0).mean() > 0.5
