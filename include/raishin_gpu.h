@@ -219,6 +219,19 @@ int rg_run_restore(rg_ctx* ctx, int run, const char* path, int* it0, int* ih0, i
  * effect on the accretion is measured. */
 int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot);
 
+/* Derived quantities of the output converter (convert_vtk2dn1.f90:254-371,
+ * with transmks2ks1 / transks2bl1, convert_vtk2dn1.f90:1399-1554) from the
+ * run's current primitives, 7 doubles per point: the Lorentz factors of the
+ * Boyer-Lindquist ZAMO (gfa) and of the static observer at infinity (gfb),
+ * b^2, the Bernoulli parameter -h u_t, and the BL velocity u^i + gfa
+ * beta^i/alpha (i = r, phi, theta); inside r_H gfa = gfb = 1 and the velocity
+ * is 0.  jslice = 0: every cell, out[7*((i-1) + imax*((j-1) + jmax*(k-1))) + f];
+ * jslice = j: the meridional plane at phi index j (the converter's 2D cut),
+ * out[7*((i-1) + imax*(k-1)) + f], only that plane crossing to the host.
+ * Kerr metrics (303, 403) only.  Replaces the per-rank files read by the
+ * converter; the VTK writing itself stays with the caller. */
+int rg_run_derived(rg_ctx* ctx, int run, int jslice, double* out);
+
 /* Allocation-free variant of rg_calflx, for callers that cannot call
  * cudaMalloc when they need the fluxes (code running inside a CUDA stream
  * capture, or a host program whose device memory comes only from its own pool).

@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle.so")
-SOURCES = ["oracle_geom.cpp", "oracle_step.cpp", "oracle_ic.cpp", "oracle_api.cpp"]
+SOURCES = ["oracle_geom.cpp", "oracle_step.cpp", "oracle_ic.cpp", "oracle_post.cpp", "oracle_api.cpp"]
 FLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-std=c++17",
          "-Wall", "-Wno-unused-variable"]
 

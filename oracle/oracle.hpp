@@ -30,7 +30,7 @@ typedef struct {
   int imax, jmax, kmax;       // grid incl. ghosts (pram.f90:11)
   int metric;                 // 1 Minkowski, 303 KS, 403 MKS (pram.f90:67)
   int ix1, ix2, ix3;          // grid spacing kinds (pram.f90:59)
-  int irec;                   // 5 PPM, 6 MP5, 7 WENO5 (pram.f90:73)
+  int irec;                   // 1 MC, 2 minmod, 5 PPM, 6 MP5, 7 WENO5, 9 WENO-Z (pram.f90:122-131)
   int model;                  // 2 shock tube, 7 FM torus (pram.f90:66)
   int iter;                   // NR iteration cap (pram.f90:27)
   double xmin, xmax, ymin, ymax, zmin, zmax;   // (pram.f90:52-57)
@@ -129,6 +129,7 @@ void calcha(State& s);
 void hlle(State& s);
 void fluxct(State& s);
 void calsf_all(State& s, bool every_cell = false);
+void derived(State& s, const std::vector<double>& uri, int jslice, double* out);
 void rkstage(State& s, int stage);
 void recov1a(State& s, std::vector<double>& uu);
 void bnd4(State& s);

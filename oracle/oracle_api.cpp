@@ -1,6 +1,7 @@
 // oracle_api.cpp -- C entry points of the CPU oracle (test infrastructure only;
 // see oracle.hpp).  Arrays crossing this boundary use the reference layout
 // a(nv,i,j,k): variable fastest, then i, j, k.
+#include <algorithm>
 #include <cstring>
 #include <string>
 
@@ -15,8 +16,9 @@ void* orc_create(const orc_params* p) {
   s->p = *p;
   s->imax = p->imax; s->jmax = p->jmax; s->kmax = p->kmax;
   s->ncell = (size_t)p->imax * p->jmax * p->kmax;
-  // ghost widths (main.f90:176-196): MP5/WENO5 nm0 = 3, PPM nm0 = 4; flux-CT nm1 = nm0+1
-  s->nm0 = (p->irec == 5) ? 4 : 3;
+  // ghost widths (main.f90:176-196): MC/minmod nm0 = 2, MP5/WENO5/WENO-Z nm0 = 3,
+  // PPM nm0 = 4; flux-CT nm1 = nm0+1
+  s->nm0 = (p->irec == 1 || p->irec == 2) ? 2 : (p->irec == 5 ? 4 : 3);
   s->nm1 = s->nm0 + 1;
   orc::grid(*s);
   orc::coord1(*s);
@@ -108,6 +110,17 @@ void orc_fluxes(void* h, const double* uri, double* ww) {
   std::memcpy(ww, s->ww.data(), s->ww.size() * sizeof(double));
 }
 
+// rec2 alone on the given primitives: the six face-state arrays uriil,
+// uriir, urijl, urijr, urikl, urikr (each 9 per cell, reference layout) out
+void orc_rec2(void* h, const double* uri, double* faces) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  std::vector<double>* f[6] = {&s->uriil, &s->uriir, &s->urijl, &s->urijr, &s->urikl, &s->urikr};
+  for (auto* v : f) std::fill(v->begin(), v->end(), 0.0);
+  orc::rec2(*s);
+  for (int m = 0; m < 6; ++m) std::memcpy(faces + m * s->uri.size(), f[m]->data(), s->uri.size() * sizeof(double));
+}
+
 // recov1a over the interior: uu (in/out, uu(6) rewritten), uri (in: guess, out)
 void orc_recov(void* h, double* uu, double* uri) {
   State* s = static_cast<State*>(h);
@@ -145,6 +158,14 @@ void orc_rkt(void* h, int stage, double dt, const double* ww, const double* uo, 
   std::memcpy(unew, out.data(), n * sizeof(double));
 }
 
+// the output converter's derived quantities (7 per point) of the given
+// primitives: every cell (jslice = 0) or the phi plane jslice
+void orc_derived(void* h, const double* uri, int jslice, double* out) {
+  State* s = static_cast<State*>(h);
+  std::vector<double> u(uri, uri + s->uri.size());
+  orc::derived(*s, u, jslice, out);
+}
+
 // cdtcfl4 on the given primitives
 double orc_cdtcfl(void* h, const double* uri) {
   State* s = static_cast<State*>(h);
@@ -178,6 +199,11 @@ long long orc_get_array(void* h, const char* name, double* out, long long cap) {
   if (n == "x1") return vec1(s->x1, s->imax);
   if (n == "x1a") return vec1(s->x1a, s->imax);
   if (n == "x1b") return vec1(s->x1b, s->imax);
+  if (n == "x1ab") return vec1(s->x1ab, s->imax);
+  if (n == "x2a") return vec1(s->x2a, s->jmax);
+  if (n == "x2b") return vec1(s->x2b, s->jmax);
+  if (n == "x2ab") return vec1(s->x2ab, s->jmax);
+  if (n == "x3ab") return vec1(s->x3ab, s->kmax);
   if (n == "dx1b") return vec1(s->dx1b, s->imax);
   if (n == "x2") return vec1(s->x2, s->jmax);
   if (n == "dx2b") return vec1(s->dx2b, s->jmax);

@@ -243,6 +243,94 @@ static void weno5(State& s) {
           }
 }
 
+// rec.f90:208-367 (mclim, MC limiter; mc) and rec.f90:568-739 (minlim,
+// minmod) on i,j,k = 2..n-1.  The slopes divide by (x_p - x_c + small) in the
+// MKS coordinates x?b, x?ab for metric 403, else in x?, x?a; MAX/MIN take the
+// first argument as the seed (Fortran's order).
+static void mclim(State& s, bool mc) {
+  const double small = 1.0e-12;
+  const bool mks = (s.p.metric == 403);
+  const std::vector<double>* X[3] = {mks ? &s.x1b : &s.x1, mks ? &s.x2b : &s.x2, mks ? &s.x3b : &s.x3};
+  const std::vector<double>* XA[3] = {mks ? &s.x1ab : &s.x1a, mks ? &s.x2ab : &s.x2a, mks ? &s.x3ab : &s.x3a};
+  std::vector<double>* L[3] = {&s.uriil, &s.urijl, &s.urikl};
+  std::vector<double>* R[3] = {&s.uriir, &s.urijr, &s.urikr};
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= s.kmax - 1; ++k)
+    for (int j = 2; j <= s.jmax - 1; ++j)
+      for (int i = 2; i <= s.imax - 1; ++i)
+        for (int n = 1; n <= NV; ++n)
+          for (int d = 0; d < 3; ++d) {
+            const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+            const int m = (d == 0) ? i : (d == 1 ? j : k);
+            const std::vector<double>& x = *X[d];
+            const std::vector<double>& xa = *XA[d];
+            const double xp = x[m + 1], xc = x[m], xm = x[m - 1], xap = xa[m], xam = xa[m - 1];
+            const double um = s.uri[s.a(n, i - di, j - dj, k - dk)], u0 = s.uri[s.a(n, i, j, k)],
+                         up = s.uri[s.a(n, i + di, j + dj, k + dk)];
+            const double sp = (up - u0) * (1. / (xp - xc + small));
+            const double sm = (u0 - um) * (1. / (xc - xm + small));
+            const double tmp = (sp < 0.0) ? -1.0 : 1.0;
+            double lim;
+            if (mc) {
+              lim = fmin3(2.0 * std::fabs(sp), tmp * 2.0 * sm, tmp * 0.5 * (sp + sm));
+            } else {
+              lim = std::fabs(sp);
+              if (tmp * sm < lim) lim = tmp * sm;
+            }
+            double mx = 0.0;
+            if (lim > mx) mx = lim;
+            const double dkm = tmp * mx;
+            (*L[d])[s.a(n, i, j, k)] = u0 + dkm * (xap - xc);
+            (*R[d])[s.a(n, i - di, j - dj, k - dk)] = u0 - dkm * (xc - xam);
+          }
+}
+
+// rec.f90:3161-3436 (WENO-Z, Borges et al. 2008) on i,j,k = 3..n-2: WENO5's
+// stencils and coefficients with the weights cd (1 + tau/(beta + eps)),
+// tau = |beta0 - beta2|; (13./12.) is a single-precision literal, and
+// (beta + eps)**p0 with p0 = 1.d0 is the plain sum.
+static void weno5z(State& s) {
+  const double cd0 = 1.0 / 10.0, cd1 = 6.0 / 10.0, cd2 = 3.0 / 10.0;
+  const double c00 = 2.0 / 6.0, c01 = -7.0 / 6.0, c02 = 11.0 / 6.0;
+  const double c10 = -1.0 / 6.0, c11 = 5.0 / 6.0, c12 = 2.0 / 6.0;
+  const double c20 = 2.0 / 6.0, c21 = 5.0 / 6.0, c22 = -1.0 / 6.0;
+  const double epsi = 1.0e-6;
+  const double c1312 = sp(13.0f / 12.0f), c14 = 0.25;
+  std::vector<double>* L[3] = {&s.uriil, &s.urijl, &s.urikl};
+  std::vector<double>* R[3] = {&s.uriir, &s.urijr, &s.urikr};
+  auto sq = [](double x) { return x * x; };
+  auto state = [&](double b0, double b1, double b2, double q0, double q1, double q2) {
+    const double tau = std::fabs(b0 - b2);
+    const double w0 = cd0 * (1.0 + (tau / (b0 + epsi)));
+    const double w1 = cd1 * (1.0 + (tau / (b1 + epsi)));
+    const double w2 = cd2 * (1.0 + (tau / (b2 + epsi)));
+    const double wt = w0 + w1 + w2;
+    const double o0 = w0 / wt, o1 = w1 / wt, o2 = w2 / wt;
+    return o0 * q0 + o1 * q1 + o2 * q2;
+  };
+#pragma omp parallel for schedule(static)
+  for (int k = 3; k <= s.kmax - 2; ++k)
+    for (int j = 3; j <= s.jmax - 2; ++j)
+      for (int i = 3; i <= s.imax - 2; ++i)
+        for (int n = 1; n <= NV; ++n)
+          for (int d = 0; d < 3; ++d) {
+            const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+            auto U = [&](int o) { return s.uri[s.a(n, i + o * di, j + o * dj, k + o * dk)]; };
+            const double um2 = U(-2), um1 = U(-1), u0 = U(0), up1 = U(1), up2 = U(2);
+            const double bl0 = c1312 * sq(um2 - 2. * um1 + u0) + c14 * sq(um2 - 4. * um1 + 3. * u0);
+            const double bl1 = c1312 * sq(um1 - 2. * u0 + up1) + c14 * sq(um1 - up1);
+            const double bl2 = c1312 * sq(u0 - 2. * up1 + up2) + c14 * sq(3. * u0 - 4. * up1 + up2);
+            const double br0 = c1312 * sq(up2 - 2. * up1 + u0) + c14 * sq(up2 - 4. * up1 + 3. * u0);
+            const double br1 = c1312 * sq(up1 - 2. * u0 + um1) + c14 * sq(up1 - um1);
+            const double br2 = c1312 * sq(u0 - 2. * um1 + um2) + c14 * sq(3. * u0 - 4. * um1 + um2);
+            (*L[d])[s.a(n, i, j, k)] = state(bl0, bl1, bl2, c00 * um2 + c01 * um1 + c02 * u0,
+                                             c10 * um1 + c11 * u0 + c12 * up1, c20 * u0 + c21 * up1 + c22 * up2);
+            (*R[d])[s.a(n, i - di, j - dj, k - dk)] =
+                state(br0, br1, br2, c00 * up2 + c01 * up1 + c02 * u0, c10 * up1 + c11 * u0 + c12 * um1,
+                      c20 * u0 + c21 * um1 + c22 * um2);
+          }
+}
+
 // rec.f90:1261-2058 (PPM: interp -> detect -> flaten -> monoto).
 // rec2 declares dx1b(2:imax-1) while main passes dx1b(1:imax-1) (rec.f90:58,
 // main.f90:120), so dummy dx1b(i) is actual dx1b(i-1).  Dummy dx1b(1), read
@@ -499,8 +587,11 @@ static void face_guard(State& s) {
 }
 
 void rec2(State& s) {
-  if (s.p.irec == 6) mp5(s);
+  if (s.p.irec == 1) mclim(s, true);
+  else if (s.p.irec == 2) mclim(s, false);
+  else if (s.p.irec == 6) mp5(s);
   else if (s.p.irec == 7) weno5(s);
+  else if (s.p.irec == 9) weno5z(s);
   else ppm(s);
   if (s.p.guard & 1) face_guard(s);
   const double gam = s.p.gam;

@@ -71,6 +71,8 @@ def _lib():
         lib.orc_cdtcfl.restype = C.c_double
         lib.orc_bnd_floor.argtypes = [P, D, D]
         lib.orc_calsf.argtypes = [P, D, D]
+        lib.orc_rec2.argtypes = [P, D, D]
+        lib.orc_derived.argtypes = [P, D, C.c_int, D]
         lib.orc_rkt.argtypes = [P, C.c_int, C.c_double, D, D, D, D, D]
         lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
         lib.orc_get_array.restype = C.c_longlong
@@ -178,6 +180,25 @@ class Oracle:
         uri = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
         self.lib.orc_recov(self.h, _ptr(uu), _ptr(uri))
         return uu, uri
+
+    def rec2(self, uri) -> np.ndarray:
+        """Face states of rec2: shape (6,) + prims shape, in the order uriil,
+        uriir, urijl, urijr, urikl, urikr (unset entries are 0)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = np.zeros((6,) + self.shape, dtype=np.float64)
+        self.lib.orc_rec2(self.h, _ptr(uri), _ptr(out))
+        return out
+
+    def derived(self, uri, jslice: int = 0) -> np.ndarray:
+        """The output converter's derived quantities (gfa, gfb, b^2, -h u_t,
+        v_r, v_phi, v_theta): shape (kmax, jmax, imax, 7), or (kmax, imax, 7)
+        for the phi plane jslice."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        p = self.params
+        shape = (p["kmax"], p["imax"], 7) if jslice else (p["kmax"], p["jmax"], p["imax"], 7)
+        out = np.zeros(shape, dtype=np.float64)
+        self.lib.orc_derived(self.h, _ptr(uri), jslice, _ptr(out))
+        return out
 
     def calsf(self, uri) -> np.ndarray:
         """sf(2:5,i,j,k) of every cell, shape (kmax, jmax, imax, 4)."""

@@ -28,7 +28,7 @@ STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA"
 EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
-           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -116,6 +116,7 @@ def load(path: str = LIB_PATH):
     lib.rg_bnd_floor.argtypes = [P, I, D, D]
     lib.rg_calsf.argtypes = [P, I, D, D]
     lib.rg_rkt.argtypes = [P, I, I, C.c_double, D, D, D, D, D]
+    lib.rg_run_derived.argtypes = [P, I, I, D]
     lib.rg_calflx_static.argtypes = [P, I, P, P]
     lib.rg_run_horizon_flux.argtypes = [P, I, D, D]
     lib.rg_run_store.argtypes = [P, I, C.c_char_p, I, I, I, C.c_void_p]
@@ -341,6 +342,16 @@ class Run:
         uu = np.ascontiguousarray(uu, dtype=np.float64).reshape(self.shape)
         out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
         _check(self.lib, self.lib.rg_recov(self.ctx.h, self.id, _dptr(uu), _dptr(out)))
+        return out
+
+    def derived(self, jslice: int = 0) -> np.ndarray:
+        """Derived quantities of the output converter (rg_run_derived):
+        (gfa, gfb, b^2, -h u_t, v_r, v_phi, v_theta) per point, shape
+        (kmax, jmax, imax, 7), or (kmax, imax, 7) for the plane jslice."""
+        p = self.params
+        shape = (p["kmax"], p["imax"], 7) if jslice else (p["kmax"], p["jmax"], p["imax"], 7)
+        out = np.zeros(shape, dtype=np.float64)
+        _check(self.lib, self.lib.rg_run_derived(self.ctx.h, self.id, jslice, _dptr(out)))
         return out
 
     def calsf(self, uri) -> np.ndarray:

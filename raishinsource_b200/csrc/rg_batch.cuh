@@ -381,9 +381,14 @@ cudaError_t go_flux(const BatchPlan* B, const BLaunch& L, cudaStream_t s) {
 
 template <int D, typename T, typename S>
 cudaError_t go_flux_irec(const BatchPlan* B, const BLaunch& L, cudaStream_t s) {
-  if (B->irec == 5) return go_flux<D, 5, T, S>(B, L, s);
-  if (B->irec == 6) return go_flux<D, 6, T, S>(B, L, s);
-  return go_flux<D, 7, T, S>(B, L, s);
+  switch (B->irec) {
+    case 1: return go_flux<D, 1, T, S>(B, L, s);
+    case 2: return go_flux<D, 2, T, S>(B, L, s);
+    case 5: return go_flux<D, 5, T, S>(B, L, s);
+    case 6: return go_flux<D, 6, T, S>(B, L, s);
+    case 7: return go_flux<D, 7, T, S>(B, L, s);
+    default: return go_flux<D, 9, T, S>(B, L, s);
+  }
 }
 
 template <typename T, typename S>

@@ -43,6 +43,10 @@ struct Run {
   bool fb_ready = false;
   double* aos = nullptr;   // 9*Nfull staging buffer in the reference layout (allocated on first use)
   double* unew = nullptr;  // 9*Nfull output of rg_rkt (allocated on first use)
+  // scalar block and counters of the per-routine entry points, so that those
+  // calls never touch the run's own time state, buffer rotation or statistics
+  Scal* fscal = nullptr;
+  unsigned long long* fcnt = nullptr;
   int* bad = nullptr;      // device flag: uploaded data not uniform along a slab direction
   size_t nfull = 0;        // imax*jmax*kmax
   int cur = 0;             // index of P^n in b.P
@@ -110,17 +114,24 @@ void free_run(Run* R) {
   delete R;
 }
 
+// Ghost widths of the reconstruction (main.f90:179-190): nm0 = 2 for the
+// second-order limiters, 3 for the five-point schemes, 4 for PPM; flux-CT
+// (ict = 1) adds one layer, nm1 = nm0 + 1.
+int nm0_of(int irec) { return (irec == 1 || irec == 2) ? 2 : (irec == 5 ? 4 : 3); }
+int nm1_of(int irec) { return nm0_of(irec) + 1; }
+
 int check_params(const rg_run_params* p) {
   if (!p) return fail(RG_EINVAL_CONFIG, "null parameters");
-  if (p->irec != 5 && p->irec != 6 && p->irec != 7)
-    return fail(RG_EINVAL_CONFIG, "irec must be 5 (PPM), 6 (MP5) or 7 (WENO5)");
+  if (p->irec != 1 && p->irec != 2 && p->irec != 5 && p->irec != 6 && p->irec != 7 && p->irec != 9)
+    return fail(RG_EINVAL_CONFIG,
+                "irec must be 1 (MC), 2 (minmod), 5 (PPM), 6 (MP5), 7 (WENO5) or 9 (WENO-Z)");
   if (p->metric != 1 && p->metric != 303 && p->metric != 403)
     return fail(RG_EINVAL_CONFIG, "metric must be 1, 303 or 403");
   if (p->ix1 != 1 && p->ix1 != 2) return fail(RG_EINVAL_CONFIG, "ix1 must be 1 or 2");
   if (p->ix2 != 1) return fail(RG_EINVAL_CONFIG, "ix2 must be 1");
   if (p->ix3 != 1 && p->ix3 != 2) return fail(RG_EINVAL_CONFIG, "ix3 must be 1 or 2");
   if (p->precision != RG_FP64 && p->precision != RG_MIXED) return fail(RG_EINVAL_CONFIG, "unknown precision mode");
-  const int nm1 = (p->irec == 5) ? 5 : 4;
+  const int nm1 = nm1_of(p->irec);
   if (p->imax <= 2 * nm1 || p->jmax <= 2 * nm1 || p->kmax <= 2 * nm1)
     return fail(RG_EINVAL_CONFIG, "every extent must exceed 2*nm1 (main.f90:247-254)");
   const double n = (double)p->imax * p->jmax * p->kmax;
@@ -169,7 +180,7 @@ bool slab_direction(const rg_run_params* p, int dir, int nm1) {
 int straggler_cap(size_t N) { return (int)std::max<size_t>(1024, std::min<size_t>(N / 64, (size_t)1 << 20)); }
 
 size_t stored_cells(const rg_run_params* p) {
-  const int nm1 = (p->irec == 5) ? 5 : 4;
+  const int nm1 = nm1_of(p->irec);
   const bool full = (p->flags & RG_FLAG_FULL) != 0;
   const size_t jpl = (!full && slab_direction(p, 2, nm1)) ? 1 : (size_t)p->jmax;
   const size_t kpl = (!full && slab_direction(p, 3, nm1)) ? 1 : (size_t)p->kmax;
@@ -180,7 +191,7 @@ size_t stored_cells(const rg_run_params* p) {
 // per-routine entry points' full-layout buffers are allocated on first use).
 size_t footprint_bytes(const rg_run_params* p) {
   const size_t N = stored_cells(p);
-  const int nm1 = (p->irec == 5) ? 5 : 4;
+  const int nm1 = nm1_of(p->irec);
   const bool kslab = !(p->flags & RG_FLAG_FULL) && slab_direction(p, 3, nm1);
   const size_t nik = (size_t)p->imax * (kslab ? 1 : p->kmax);
   const size_t state = (3 * 9 + 3 * 9 + 6 + 9) * N * sizeof(double);
@@ -211,6 +222,25 @@ std::vector<double> zero_based(const std::vector<double>& v, int n) {
   return std::vector<double>(v.begin() + 1, v.begin() + 1 + n);
 }
 
+// Coefficients of the MC / minmod slopes along one axis (rec.f90:251-278):
+// four planes of n values at index m-1 for the cells m = 2..n-1 (zero at the
+// ends, which the limiters never reconstruct), computed in FP64 exactly as
+// the reference writes them, from the MKS coordinates x?b, x?ab for metric
+// 403 and from x?, x?a otherwise.
+std::vector<double> limiter_coefs(const Axis& a, int n, bool mks) {
+  const double small = 1.0e-12;
+  const std::vector<double>& x = mks ? a.xb : a.x;
+  const std::vector<double>& xa = mks ? a.xab : a.xa;
+  std::vector<double> o(4 * (size_t)n, 0.0);
+  for (int m = 2; m <= n - 1; ++m) {
+    o[m - 1] = 1. / (x[m + 1] - x[m] + small);
+    o[n + m - 1] = 1. / (x[m] - x[m - 1] + small);
+    o[2 * n + m - 1] = xa[m] - x[m];
+    o[3 * n + m - 1] = x[m] - xa[m - 1];
+  }
+  return o;
+}
+
 // rec2's dummy dx?b(2:n-1) receives actual dx?b(1:n-1) (rec.f90:58, main.f90:120):
 // dummy index m holds actual m-1; dummy 1 (outside the actual array) is taken as actual 1.
 std::vector<double> shifted(const std::vector<double>& v, int n) {
@@ -233,7 +263,19 @@ DevRun full_view(const Run* R) {
   d.sk = (size_t)d.imax * d.jmax;
   d.N = R->nfull;
   d.Un = nullptr;
+  d.scal = R->fscal;
+  d.cnt = R->fcnt;
   return d;
+}
+
+// A fresh scalar block for one per-routine call: active, empty queues and the
+// given initial CFL bound (cdtcfl4 starts from dtcfl = 1, cdtcfl.f90:30).
+int reset_fscal(rg_ctx* ctx, Run* R, double dtcfl0 = 0.0) {
+  Scal sc{};
+  sc.active = 1;
+  std::memcpy(&sc.dtcfl_bits, &dtcfl0, sizeof(double));
+  RG_CUDA(cudaMemcpyAsync(R->fscal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
+  return RG_OK;
 }
 
 // Full-layout work buffers of the per-routine entry points, allocated on first use.
@@ -658,7 +700,7 @@ int rg_prep_create(const rg_run_params* p, rg_prep** out) {
   if (rc) return rc;
   rg_prep* P = new rg_prep();
   P->p = *p;
-  const int nm1 = (p->irec == 5) ? 5 : 4;
+  const int nm1 = nm1_of(p->irec);
   const bool full = (p->flags & RG_FLAG_FULL) != 0;
   P->krow = (!full && slab_direction(p, 3, nm1)) ? nm1 + 1 : 0;  // theta slab: one metric row
   P->plane = !full && slab_direction(p, 2, nm1);                   // phi slab: one initial-data plane
@@ -707,7 +749,7 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   R->geom = prep->geom;
   DevRun& d = R->d;
   d.imax = p->imax; d.jmax = p->jmax; d.kmax = p->kmax;
-  d.nm0 = (p->irec == 5) ? 4 : 3;
+  d.nm0 = nm0_of(p->irec);
   d.nm1 = d.nm0 + 1;
   d.irec = p->irec; d.model = p->model; d.guard = p->guard; d.iter = p->iter;
   d.mixed = (p->precision == RG_MIXED);
@@ -769,6 +811,11 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   d.fl_pr = d.fl_de + p->imax;
   if ((rc = dalloc(R, &ptr, sizeof(Scal)))) return bail(rc);
   d.scal = static_cast<Scal*>(ptr);
+  if ((rc = dalloc(R, &ptr, sizeof(Scal)))) return bail(rc);
+  R->fscal = static_cast<Scal*>(ptr);
+  if ((rc = dalloc(R, &ptr, C_NCOUNTERS * sizeof(unsigned long long)))) return bail(rc);
+  R->fcnt = static_cast<unsigned long long*>(ptr);
+  if (cudaMemsetAsync(R->fcnt, 0, C_NCOUNTERS * sizeof(unsigned long long), s) != cudaSuccess) return bail(RG_ECUDA);
   if ((rc = dalloc(R, &ptr, C_NCOUNTERS * sizeof(unsigned long long)))) return bail(rc);
   d.cnt = static_cast<unsigned long long*>(ptr);
   if ((rc = dalloc(R, &ptr, kCarryCap * sizeof(int)))) return bail(rc);
@@ -799,6 +846,9 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   if ((rc = upload(shifted(G.ax[0].dxb, p->imax), &d.dx1s, R, s))) return bail(rc);
   if ((rc = upload(shifted(G.ax[1].dxb, p->jmax), &d.dx2s, R, s))) return bail(rc);
   if ((rc = upload(shifted(G.ax[2].dxb, p->kmax), &d.dx3s, R, s))) return bail(rc);
+  const int ext[3] = {p->imax, p->jmax, p->kmax};
+  for (int a = 0; a < 3; ++a)
+    if ((rc = upload(limiter_coefs(G.ax[a], ext[a], p->metric == 403), &d.lim[a], R, s))) return bail(rc);
   // the caches and floor tables are this run's own allocations: fill their derived parts
   if (launch_geom_derive(d, const_cast<double*>(d.mc), const_cast<double*>(d.mi), const_cast<double*>(d.mk),
                          const_cast<double*>(d.fl_de), const_cast<double*>(d.fl_pr), s) != cudaSuccess)
@@ -1083,10 +1133,7 @@ int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
   const size_t N = d.N;
   DevBufs* B = nullptr;
   int rc = full_bufs(R, ctx->stream, &B);
-  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
-  Scal sc{};
-  sc.active = 1;
-  RG_CUDA(cudaMemcpyAsync(d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
   for (int dir = 1; dir <= 3; ++dir) RG_CUDA(launch_flux(d, dir, B->stage, B->F[dir - 1], ctx->stream));
   RG_CUDA(launch_ct(d, B->F[0], B->F[1], B->F[2], B->CT, ctx->stream));
   std::vector<double> F(27 * N), CT(6 * N);
@@ -1172,6 +1219,60 @@ int rg_rkt(rg_ctx* ctx, int run, int stage, double dt, const double* ww, const d
   return from_soa(ctx, R, R->unew, unew, d);
 }
 
+int rg_run_derived(rg_ctx* ctx, int run, int jslice, double* out) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!out) return fail(RG_EINVAL_CONFIG, "null array");
+  const rg_run_params& p = R->p;
+  if (p.metric != 303 && p.metric != 403)
+    return fail(RG_EINVAL_CONFIG, "derived quantities are defined for the Kerr metrics 303 and 403");
+  if (jslice < 0 || jslice > p.jmax) return fail(RG_EINVAL_CONFIG, "jslice must be 0 or a phi index 1..jmax");
+  // the converter's coordinates (convert_vtk2dn1.f90:138-161) and the
+  // MKS -> KS factors of transmks2ks1 (convert_vtk2dn1.f90:1524-1554)
+  const Axis& a1 = R->geom.ax[0];
+  const Axis& a3 = R->geom.ax[2];
+  std::vector<double> gi(2 * (size_t)p.imax), gk(3 * (size_t)p.kmax);
+  for (int i = 1; i <= p.imax; ++i) {
+    double rr = a1.x[i], rfac = 1.0;
+    if (p.metric == 403) {
+      const double x1t = a1.xb[i];
+      rr = (p.ix1 == 2) ? p.R0 + std::exp(x1t) : x1t;
+      if (p.ix1 == 2) rfac = std::exp(x1t);
+    }
+    gi[2 * (i - 1)] = rr;
+    gi[2 * (i - 1) + 1] = rfac;
+  }
+  for (int k = 1; k <= p.kmax; ++k) {
+    double th = a3.x[k], hfac = 1.0;
+    if (p.metric == 403) {
+      const double x3t = a3.xb[k];
+      th = (p.ix3 == 2) ? x3t + 0.5 * (1. - p.hslope) * std::sin(2. * x3t) : x3t;
+      if (p.ix3 == 2) hfac = 1. + (1. - p.hslope) * std::cos(2. * x3t);
+    }
+    gk[3 * (k - 1)] = std::sin(th);
+    gk[3 * (k - 1) + 1] = std::cos(th);
+    gk[3 * (k - 1) + 2] = hfac;
+  }
+  const size_t npt = (size_t)p.imax * (size_t)p.kmax * (jslice ? 1 : (size_t)p.jmax);
+  double* buf = nullptr;
+  const size_t nbuf = gi.size() + gk.size() + 7 * npt;
+  RG_CUDA(cudaMalloc(&buf, nbuf * sizeof(double)));
+  double* dgi = buf;
+  double* dgk = buf + gi.size();
+  double* dout = dgk + gk.size();
+  cudaError_t e = cudaMemcpyAsync(dgi, gi.data(), gi.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dgk, gk.data(), gk.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = launch_derived(R->d, R->b.P[R->cur], dgi, dgk, p.akm, jslice, dout, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, dout, 7 * npt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(buf);
+  RG_CUDA(e);
+  return RG_OK;
+}
+
+// ------------------------------------------------------------ restart files
 // ------------------------------------------------------------ restart files
 // store1 / restar2 (restar.f90:5-88, 273-346) write and read one rank's state
 // as gfortran sequential unformatted records (a 4-byte length before and
@@ -1252,15 +1353,9 @@ int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot) {
   RG_CUDA(launch_soa_to_aos(R->d, R->b.P[R->cur], B->stage2, ctx->stream));
   int* nobad = nullptr;
   RG_CUDA(launch_aos_to_soa(d, B->stage2, B->stage, nobad, ctx->stream));
-  Scal sc{};
-  sc.active = 1;
-  // fluxes on scratch scalar state: the run's own time state is left alone
-  Scal* tmp = nullptr;
-  RG_CUDA(cudaMalloc(&tmp, sizeof(Scal)));
-  DevRun dv = d;
-  dv.scal = tmp;
-  RG_CUDA(cudaMemcpyAsync(tmp, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
-  RG_CUDA(launch_flux(dv, 1, B->stage, B->F[0], ctx->stream));
+  // fluxes on the per-routine scalar block: the run's own time state is left alone
+  if ((rc = reset_fscal(ctx, R))) return rc;
+  RG_CUDA(launch_flux(d, 1, B->stage, B->F[0], ctx->stream));
   // radial face nm1+1/2 (the inner edge of the interior): F1 of rho u^r and of the energy variable
   const int i = d.nm1;
   std::vector<double> f0((size_t)d.jmax * d.kmax), f4((size_t)d.jmax * d.kmax);
@@ -1271,7 +1366,6 @@ int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot) {
   RG_CUDA(cudaMemcpy2DAsync(f4.data(), sizeof(double), B->F[0] + 4 * d.N + d.cell(i, 1, 1), pitch, sizeof(double),
                             rows, cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
-  cudaFree(tmp);
   const Axis& X2 = R->geom.ax[1];
   const Axis& X3 = R->geom.ax[2];
   double m = 0.0, e = 0.0;
@@ -1295,7 +1389,7 @@ int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri) {
   DevBufs* B = nullptr;
   int rc = full_bufs(R, ctx->stream, &B);
   if (rc || (rc = to_soa(ctx, R, uu, B->stage, d, false))) return rc;
-  if ((rc = to_soa(ctx, R, uri, B->stage2, d, false))) return rc;
+  if ((rc = to_soa(ctx, R, uri, B->stage2, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
   RG_CUDA(launch_recov_only(d, B->stage, B->stage2, B->F[0], ctx->stream));
   return from_soa(ctx, R, B->F[0], uri, d);
 }
@@ -1307,12 +1401,8 @@ int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl) {
   const DevRun d = full_view(R);
   DevBufs* B = nullptr;
   int rc = full_bufs(R, ctx->stream, &B);
-  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false)) || (rc = reset_fscal(ctx, R, 1.0))) return rc;
   Scal sc{};
-  sc.active = 1;
-  const double one = 1.0;
-  std::memcpy(&sc.dtcfl_bits, &one, sizeof(double));
-  RG_CUDA(cudaMemcpyAsync(d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
   RG_CUDA(launch_cfl(d, B->stage, ctx->stream));
   RG_CUDA(cudaMemcpyAsync(&sc, d.scal, sizeof(Scal), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1328,10 +1418,7 @@ int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio) {
   DevBufs* B = nullptr;
   int rc = full_bufs(R, ctx->stream, &B);
   if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
-  if ((rc = to_soa(ctx, R, urio, B->stage2, d, false))) return rc;
-  Scal sc{};
-  sc.active = 1;
-  RG_CUDA(cudaMemcpyAsync(d.scal, &sc, sizeof(Scal), cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = to_soa(ctx, R, urio, B->stage2, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
   RG_CUDA(launch_bc(d, B->stage, B->stage2, ctx->stream));
   RG_CUDA(launch_floor(d, B->stage, ctx->stream));
   return from_soa(ctx, R, B->stage, uri, d);

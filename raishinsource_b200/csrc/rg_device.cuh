@@ -201,13 +201,15 @@ struct PST {
 };
 using PS = PST<double>;
 
+// The state of q with a given Lorentz factor gfl (pstate below computes it
+// with calgfl; the output converter uses its own clamps).
 template <typename T>
-__device__ __forceinline__ void pstate(const T q[9], const MetT<T>& m, T gam, PST<T>& s) {
+__device__ __forceinline__ void pstate_gfl(const T q[9], const MetT<T>& m, T gam, T gfl, PST<T>& s) {
   s.de = q[0];
   s.pr = q[4];
   s.b1 = q[6]; s.b2 = q[7]; s.b3 = q[8];
   s.roh = s.de + (gam / (gam - T(1))) * s.pr;
-  s.gfl = calgfl(q[1], q[2], q[3], m);
+  s.gfl = gfl;
   calucon(q[1], q[2], q[3], s.gfl, m, s.ucon);
   lower_g(s.ucon, s.ucov, m);
   // physfunc.f90:81-100
@@ -217,6 +219,10 @@ __device__ __forceinline__ void pstate(const T q[9], const MetT<T>& m, T gam, PS
   s.bbcon[3] = (s.b3 + s.bbcon[0] * s.ucon[3]) * mrcp(s.ucon[0]);
   lower_g(s.bbcon, s.bbcov, m);
   s.bbsq = s.bbcon[0] * s.bbcov[0] + s.bbcon[1] * s.bbcov[1] + s.bbcon[2] * s.bbcov[2] + s.bbcon[3] * s.bbcov[3];
+}
+template <typename T>
+__device__ __forceinline__ void pstate(const T q[9], const MetT<T>& m, T gam, PST<T>& s) {
+  pstate_gfl(q, m, gam, calgfl(q[1], q[2], q[3], m), s);
 }
 
 // p / rho^Gamma of a state (caluu.f90:303, calflx.f90:474), computed once per state.

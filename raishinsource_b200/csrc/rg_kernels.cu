@@ -747,6 +747,22 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     for (int o = -1; o <= 1; ++o) xx[o + 4] = T(__ldg(xs + f - 1 + o));
     if (side == 0) ppm_cell<D>(P + c, N, st, dx, xx, T(r.gam), other, q);  // uriil(f)
     else ppm_cell<D>(P + c + st, N, st, dx, xx, T(r.gam), q, other);       // uriir(f)
+  } else if (IREC == 1 || IREC == 2) {
+    // owner cell f of this lane's state; left state u + dk (xa(f) - x(f)),
+    // right state u - dk (x(f) - xa(f-1)) (rec.f90:277-278)
+    const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;
+    const int n = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
+    const double* lc = r.lim[D - 1];
+    const T hp = T(__ldg(lc + f - 1)), hm = T(__ldg(lc + n + f - 1));
+    const T w = T(__ldg(lc + (side ? 3 : 2) * n + f - 1));
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
+      const S* p = P + (size_t)v * N + c + side * st;
+      const T u0 = T(p[0]);
+      const T dk = limited_slope<IREC == 1>(T(p[-st]), u0, T(p[st]), hp, hm);
+      q[v] = side ? u0 - dk * w : u0 + dk * w;
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
@@ -756,6 +772,7 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
       const S* p = P + (size_t)v * N + c + side * st;
       const T a2 = T(p[-2 * sd]), a1 = T(p[-sd]), u0 = T(p[0]), b1 = T(p[sd]), b2 = T(p[2 * sd]);
       if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? T(-1) : T(1));
+      else if (IREC == 9) q[v] = weno5z_state(a2, a1, u0, b1, b2);
       else q[v] = weno5_state(a2, a1, u0, b1, b2);
     }
   }
@@ -1220,6 +1237,106 @@ __global__ void __launch_bounds__(128) k_calsf(DevRun r, const double* __restric
   for (int n = 0; n < 4; ++n) SF[(size_t)n * N + c] = sf[n];
 }
 
+// calgfl of the output converter (convert_vtk2dn1.f90:1158-1197): the same
+// quadratic form as physfunc's, clamped at |u~^2| > 1e10 to 1e9.
+__device__ __forceinline__ double calgfl_conv(double u1, double u2, double u3, const Met& m) {
+  double utsq = qform3(m, u1, u2, u3);
+  if (utsq < 0.0) utsq = (fabs(utsq) <= 1.0e-10) ? fabs(utsq) : 1.e-10;
+  if (fabs(utsq) > 1.0e10) utsq = 1.0e9;
+  return sqrt(1. + utsq);
+}
+
+// Derived quantities of one cell as convert_vtk2dn1.f90:254-371 computes them
+// for its output: out = (gfa, gfb, b^2, -h u_t, v1, v2, v3), the Lorentz
+// factors of the Boyer-Lindquist ZAMO and of the static observer at infinity,
+// the field strength, the Bernoulli parameter and the BL velocity
+// u^i + gfa beta^i / alpha; inside r_H = 1 + sqrt(1 - a^2) gfa = gfb = 1 and
+// v = 0.  The run's metric comes from the cell-centre cache (the converter
+// re-evaluates the same coord.f90 formulas); transmks2ks1 and transks2bl1
+// (convert_vtk2dn1.f90:1399-1554) use the Kerr-Schild formulas at
+// (rr, th) with rfac = dr/dx1, hfac = dtheta/dx3 and sin/cos of th given.
+__device__ void derived_cell(const DevRun& r, double akm, const double qin[9], const Met& m, double rr, double rfac,
+                             double sth, double cth, double hfac, double out[7]) {
+  double q[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) q[v] = qin[v];
+  // minimum magnetic field (bmin1 = 1e-20)
+  for (int v = 6; v < 9; ++v)
+    if (fabs(q[v]) < 1.e-20) q[v] = 0.0;
+  PS s;
+  pstate_gfl(q, m, r.gam, calgfl_conv(q[1], q[2], q[3], m), s);
+  out[2] = s.bbsq;
+  out[3] = -(s.roh / s.de) * s.ucov[0];
+  const double rbh1 = 1. + sqrt(1. - akm * akm);
+  if (!(rr > rbh1)) {
+    out[0] = 1.0; out[1] = 1.0; out[4] = 0.0; out[5] = 0.0; out[6] = 0.0;
+    return;
+  }
+  // MKS -> KS 3-velocity, then the KS 4-velocity (Kerr-Schild metric at (rr, th))
+  const double ut1 = rfac * q[1], ut2 = q[2], ut3 = hfac * q[3];
+  const double del = rr * rr - (2. * rr) + akm * akm;
+  const double sig = rr * rr + akm * cth * akm * cth;
+  const double aa = ((rr * rr + akm * akm) * (rr * rr + akm * akm)) - akm * akm * del * sth * sth;
+  Met ks{};
+  ks.g11 = 1. + 2. * rr / sig;
+  ks.g12 = -1. * akm * sth * sth * (1. + 2. * rr / sig);
+  ks.g22 = aa * sth * sth / sig;
+  ks.g33 = sig;
+  const double gfl = calgfl_conv(ut1, ut2, ut3, ks);
+  const double gc00 = -1. - 2. * rr / sig, gc01 = 2. * rr / sig;
+  const double alpha1 = 1. / sqrt(-gc00);
+  const double beta1 = alpha1 * alpha1 * gc01;
+  const double u0 = gfl * (1. / alpha1);
+  const double u1 = ut1 - gfl * beta1 * (1. / alpha1);
+  const double u2 = ut2 - gfl * (alpha1 * alpha1 * 0.0) * (1. / alpha1);
+  const double u3 = ut3 - gfl * (alpha1 * alpha1 * 0.0) * (1. / alpha1);
+  // KS -> BL (transks2bl1): t and phi pick up -2r/Delta u^r and -a/Delta u^r
+  const double tmp2 = rr * rr - (2. * rr) + akm * akm;
+  double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  if (tmp2 > 0.0) {
+    b0 = u0 + (-2. * rr * (1. / tmp2)) * u1;
+    b1 = u1;
+    b2 = (-akm * (1. / tmp2)) * u1 + u2;
+    b3 = u3;
+  }
+  // Boyer-Lindquist lapse and shift at (rr, th)
+  const double gcon1a00 = -aa / (sig * del);
+  const double gcon1a02 = -(2. * akm * rr) / (sig * del);
+  const double gcov1a00 = -(sig - 2. * rr) / sig;
+  const double al = 1. / sqrt(-gcon1a00);
+  const double bt2 = al * al * gcon1a02;
+  out[0] = al * b0;
+  out[1] = b0 * sqrt(-gcov1a00);
+  out[4] = b1 + out[0] * (al * al * 0.0) * (1. / al);
+  out[5] = b2 + out[0] * bt2 * (1. / al);
+  out[6] = b3 + out[0] * (al * al * 0.0) * (1. / al);
+}
+
+// Derived quantities of every cell (jslice = 0, out[7*c_full + f]) or of the
+// phi plane jslice (out[7*((i-1) + imax*(k-1)) + f]); geo_i holds (rr, rfac)
+// per radial index, geo_k (sin th, cos th, hfac) per theta index.
+__global__ void __launch_bounds__(128) k_derived(DevRun r, const double* __restrict__ P,
+                                                 const double* __restrict__ geo_i,
+                                                 const double* __restrict__ geo_k, double akm, int jslice,
+                                                 double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int jj = (int)(blockIdx.y * blockDim.y + threadIdx.y) + 1;
+  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z) + 1;
+  const int j = jslice ? jslice : jj;
+  if (i > r.imax || jj > (jslice ? 1 : r.jmax) || k > r.kmax) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  double q[9], o[7];
+  load9(P, N, c, q);
+  Met m;
+  load_met(r.mc, r.nik, r.ik(i, k), m);
+  derived_cell(r, akm, q, m, geo_i[2 * (i - 1)], geo_i[2 * (i - 1) + 1], geo_k[3 * (k - 1)], geo_k[3 * (k - 1) + 1],
+               geo_k[3 * (k - 1) + 2], o);
+  const size_t pt = jslice ? (size_t)(i - 1) + (size_t)r.imax * (size_t)(k - 1)
+                           : (size_t)(i - 1) + (size_t)r.imax * ((size_t)(j - 1) + (size_t)r.jmax * (size_t)(k - 1));
+#pragma unroll
+  for (int f = 0; f < 7; ++f) out[7 * pt + f] = o[f];
+}
+
 // One RK stage of rkt.f90 (rk2fst, rk3snd or rk3trd, then the matching
 // rk*ads*) on the interior: W[d] holds ww(d, m) of cell c at m*N + c (flux-CT
 // already applied), Uo = uo (stages 2 and 3), Uc = the stage input (uu, uh or
@@ -1348,6 +1465,14 @@ cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <int IREC, typename T, typename S>
+static void flux_dir(const DevRun& r, int dir, dim3 g, dim3 b, const S* P, S* F, float* Fcopy, int icopy, int ilo,
+                     int ihi, cudaStream_t s) {
+  if (dir == 1) k_flux<1, IREC, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+  else if (dir == 2) k_flux<2, IREC, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+  else k_flux<3, IREC, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+}
+
 template <typename T, typename S>
 static void launch_flux_t(const DevRun& r, int dir, const S* P, S* F, float* Fcopy, int icopy, int ilo, int ihi,
                           cudaStream_t s) {
@@ -1355,18 +1480,13 @@ static void launch_flux_t(const DevRun& r, int dir, const S* P, S* F, float* Fco
   const int n = ihi - ilo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b = sblock(r, dim3(64, 2, 1));
   const dim3 g = sgrid(r, 2 * n, m, l, b);  // two lanes per face
-  if (r.irec == 5) {
-    if (dir == 1) k_flux<1, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-    else if (dir == 2) k_flux<2, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-    else k_flux<3, 5, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-  } else if (r.irec == 6) {
-    if (dir == 1) k_flux<1, 6, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-    else if (dir == 2) k_flux<2, 6, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-    else k_flux<3, 6, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-  } else {
-    if (dir == 1) k_flux<1, 7, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-    else if (dir == 2) k_flux<2, 7, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
-    else k_flux<3, 7, T, S><<<g, b, 0, s>>>(r, P, F, Fcopy, icopy, ilo, ihi);
+  switch (r.irec) {
+    case 1: flux_dir<1, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 2: flux_dir<2, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 5: flux_dir<5, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 6: flux_dir<6, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 7: flux_dir<7, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    default: flux_dir<9, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
   }
 }
 
@@ -1543,6 +1663,14 @@ cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t
 cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStream_t s) {
   const dim3 b = sblock(r, dim3(64, 2, 1));
   k_calsf<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P, SF);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_derived(const DevRun& r, const double* P, const double* geo_i, const double* geo_k, double akm,
+                           int jslice, double* out, cudaStream_t s) {
+  const dim3 b(64, 1, 2);
+  const dim3 g = grid3(r.imax, jslice ? 1 : r.jmax, r.kmax, b);
+  k_derived<<<g, b, 0, s>>>(r, P, geo_i, geo_k, akm, jslice, out);
   return cudaGetLastError();
 }
 

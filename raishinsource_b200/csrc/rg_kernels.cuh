@@ -32,6 +32,8 @@ cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s);
 cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s);
 cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s);
 cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStream_t s);
+cudaError_t launch_derived(const DevRun& r, const double* P, const double* geo_i, const double* geo_k, double akm,
+                           int jslice, double* out, cudaStream_t s);
 cudaError_t launch_rkt(const DevRun& r, int stage, const double* W1, const double* W2, const double* W3,
                        const double* Uo, const double* Uc, const double* SF, double* Unew, double dt, cudaStream_t s);
 // reference layout a(nv,i,j,k) of the full array <-> the run's stored SoA

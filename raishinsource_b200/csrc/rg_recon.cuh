@@ -87,6 +87,48 @@ __device__ __forceinline__ T weno5_state(T a2, T a1, T u0, T b1, T b2) {
   return o0 * q0 + o1 * q1 + o2 * q2;
 }
 
+// rec.f90:3161-3436 (WENO-Z, Borges et al. 2008): WENO5 with the weights
+// cd_m (1 + tau / (beta_m + eps)), tau = |beta_0 - beta_2|, the smoothness
+// indicators without eps; p0 = 1 makes (beta + eps)**p0 the plain sum.
+template <typename T>
+__device__ __forceinline__ T weno5z_state(T a2, T a1, T u0, T b1, T b2) {
+  const T cd0 = T(1.0 / 10.0), cd1 = T(6.0 / 10.0), cd2 = T(3.0 / 10.0);
+  const T c00 = T(2.0 / 6.0), c01 = T(-7.0 / 6.0), c02 = T(11.0 / 6.0);
+  const T c10 = T(-1.0 / 6.0), c11 = T(5.0 / 6.0), c12 = T(2.0 / 6.0);
+  const T c20 = T(2.0 / 6.0), c21 = T(5.0 / 6.0), c22 = T(-1.0 / 6.0);
+  const T epsi = T(1.0e-6), c1312 = T((double)(13.0f / 12.0f)), c14 = T(0.25);
+  const T s0 = a2 - T(2.) * a1 + u0, t0 = a2 - T(4.) * a1 + T(3.) * u0;
+  const T s1 = a1 - T(2.) * u0 + b1, t1 = a1 - b1;
+  const T s2 = u0 - T(2.) * b1 + b2, t2 = T(3.) * u0 - T(4.) * b1 + b2;
+  const T be0 = c1312 * (s0 * s0) + c14 * (t0 * t0);
+  const T be1 = c1312 * (s1 * s1) + c14 * (t1 * t1);
+  const T be2 = c1312 * (s2 * s2) + c14 * (t2 * t2);
+  const T tau = mabs(be0 - be2);
+  const T w0 = cd0 * (T(1.0) + tau / (be0 + epsi));
+  const T w1 = cd1 * (T(1.0) + tau / (be1 + epsi));
+  const T w2 = cd2 * (T(1.0) + tau / (be2 + epsi));
+  const T wt = w0 + w1 + w2;
+  const T o0 = w0 / wt, o1 = w1 / wt, o2 = w2 / wt;
+  const T q0 = c00 * a2 + c01 * a1 + c02 * u0;
+  const T q1 = c10 * a1 + c11 * u0 + c12 * b1;
+  const T q2 = c20 * u0 + c21 * b1 + c22 * b2;
+  return o0 * q0 + o1 * q1 + o2 * q2;
+}
+
+// rec.f90:208-367 (mclim, MC limiter) and rec.f90:568-739 (minlim, minmod):
+// the limited slope of a cell from its neighbours um, up with
+// hp = 1/(x_p - x_c + small), hm = 1/(x_c - x_m + small) (small = 1e-12) in
+// the coordinates the reference uses (MKS x?b for metric 403, else x?).
+// MAX/MIN follow Fortran's order: the first argument seeds the result.
+template <bool MC, typename T>
+__device__ __forceinline__ T limited_slope(T um, T u0, T up, T hp, T hm) {
+  const T sp = (up - u0) * hp, sm = (u0 - um) * hm;
+  const T tmp = (sp < T(0)) ? T(-1) : T(1);
+  const T lim = MC ? fmin3(T(2) * mabs(sp), tmp * T(2) * sm, tmp * T(0.5) * (sp + sm))
+                   : dmin2(mabs(sp), tmp * sm);
+  return tmp * dmax2(T(0), lim);
+}
+
 // ------------------------------------------------------------------- PPM
 // rPPM of Marti & Muller (1996) as restated by rec.f90:1261-2058.  The four
 // passes (interp, detect, flaten, monoto) touch only the two face states of

@@ -73,7 +73,8 @@ def test_caluu1(torus2d):
     assert err.max() < TOL, err
 
 
-@pytest.mark.parametrize("irec", [config.IREC_MP5, config.IREC_WENO5, config.IREC_PPM])
+@pytest.mark.parametrize("irec", [config.IREC_MP5, config.IREC_WENO5, config.IREC_PPM, config.IREC_MC,
+                                  config.IREC_MINMOD, config.IREC_WENOZ])
 def test_calflx_guarded(gpu_ctx, irec):
     p = config.torus(nr=48, nth=40, nph=12, irec=irec)
     p["guard"] = 1
@@ -155,6 +156,30 @@ def test_rkt(torus3d, stage):
     assert np.array_equal(got[outside], unew[outside])
 
 
+def _derived_err(got, want):
+    assert np.array_equal(np.isfinite(got), np.isfinite(want))
+    fin = np.isfinite(want)
+    scale = np.abs(np.where(fin, want, 0)).reshape(-1, 7).max(axis=0)
+    diff = np.abs(np.where(fin, got - want, 0)).reshape(-1, 7).max(axis=0)
+    return diff / np.maximum(scale, 1e-300)
+
+
+@pytest.mark.parametrize("case", ["torus3d", "torus2d"])
+def test_derived_matches_oracle(case, request):
+    """The converter's derived quantities on the device (every cell and the
+    meridional cut) against the oracle; NaN (static observer inside the
+    ergosphere) at the same cells.  The 2D run stores its phi slab as one
+    plane and answers for every phi index."""
+    p, o, r = request.getfixturevalue(case)
+    u = o.prims()
+    r.upload_prims(u)
+    got, want = r.derived(), o.derived(u)
+    err = _derived_err(got, want)
+    assert err.max() < TOL, err
+    j = p["jmax"] // 2 + 1
+    assert np.array_equal(r.derived(jslice=j), got[:, j - 1], equal_nan=True)
+
+
 def test_cdtcfl(torus3d):
     _, o, r = torus3d
     u = o.prims()
@@ -203,6 +228,39 @@ def test_step_3d_weno5(gpu_ctx):
     p = dict(config.torus(nr=40, nth=24, nph=16, irec=config.IREC_WENO5), guard=1)
     errs, _ = _step_err(gpu_ctx, p, 2, seed=78)
     assert errs.max() < TOL, errs
+
+
+def _vector_scaled_err(a, b):
+    """Per-variable max |a-b| relative to the largest value of its quantity:
+    the three velocity components share one scale, as do the three field
+    components (a small component such as u^theta carries round-off of the
+    size of the momentum fluxes that produce it)."""
+    a = a.reshape(-1, 9)
+    b = b.reshape(-1, 9)
+    mx = np.abs(b).max(axis=0)
+    scale = mx.copy()
+    scale[1:4] = mx[1:4].max()
+    scale[6:9] = mx[6:9].max()
+    return np.abs(a - b).max(axis=0) / np.maximum(scale, 1e-300)
+
+
+@pytest.mark.parametrize("irec", [config.IREC_MC, config.IREC_MINMOD, config.IREC_WENOZ])
+def test_step_3d_limiters_and_wenoz(gpu_ctx, irec):
+    """MC, minmod (rec.f90:208-739) and WENO-Z (rec.f90:3161-3436): one full
+    step per comparison, 3D torus, 1e-12 of each quantity's scale."""
+    p = dict(config.torus(nr=40, nth=24, nph=16, irec=irec), guard=1)
+    o = Oracle(p)
+    o.ic_torus(seed=80 + irec)
+    r = gpu_ctx.admit(p)
+    r.upload_prims(o.prims())
+    o.init_cons()
+    for _ in range(2):
+        o.step(1)
+        r.step(1)
+        err = _vector_scaled_err(r.prims(), o.prims())
+        assert err.max() < TOL, err
+        r.upload_prims(o.prims(), t0=o.time)
+    r.release()
 
 
 def test_multistep_drift(gpu_ctx):
@@ -295,10 +353,10 @@ def test_slab_rejects_nonuniform_upload(gpu_ctx):
     assert e.value.code == 1
 
 
-@pytest.mark.parametrize("irec", [config.IREC_PPM, config.IREC_WENO5])
-def test_step_2d_slab_ppm_weno5(gpu_ctx, irec):
-    """2D phi slab (stored as one plane; PPM needs nm1 = 5, jmax = 11) against
-    the oracle, which computes every phi cell."""
+@pytest.mark.parametrize("irec", [config.IREC_PPM, config.IREC_WENO5, config.IREC_MC, config.IREC_WENOZ])
+def test_step_2d_slab_schemes(gpu_ctx, irec):
+    """2D phi slab (stored as one plane; jmax = 2*nm1+1: 11 for PPM, 7 for MC)
+    against the oracle, which computes every phi cell."""
     p = dict(config.torus(nr=56, nth=48, irec=irec), guard=1)
     errs, _ = _step_err(gpu_ctx, p, 2, seed=21)
     assert errs.max() < TOL, errs
@@ -333,3 +391,31 @@ def test_thousand_steps_l1_ppm(gpu_ctx):
     assert st["steps"] == 1000
     l1 = _l1(got, want, o.nm1)
     assert l1[[0, 4, 6, 7, 8]].max() < 1e-10, l1
+
+
+def test_per_routine_calls_leave_the_run_alone(gpu_ctx):
+    """The reference-interface entry points compute on their own scratch
+    state: calling them between steps of a run changes neither its result,
+    its time, nor its statistics."""
+    p = dict(config.torus(nr=40, nth=24, nph=16), guard=1)
+    o = Oracle(p)
+    o.ic_torus(seed=31)
+    u = o.prims()
+    a, b = gpu_ctx.admit(p), gpu_ctx.admit(p)
+    a.upload_prims(u)
+    b.upload_prims(u)
+    a.step(1)
+    b.step(1)
+    cur = b.prims()
+    b.calflx(cur)
+    b.cdtcfl(cur)
+    b.recov(b.caluu1(cur), cur)
+    b.bnd_floor(cur, cur)
+    b.calsf(cur)
+    b.horizon_flux()
+    b.derived()
+    sa, sb = a.step(2, stats=True), b.step(2, stats=True)
+    assert sa == sb
+    assert np.array_equal(a.prims(), b.prims())
+    a.release()
+    b.release()

@@ -212,3 +212,94 @@ def test_calsf_covers_every_cell(torus_small):
     ghosts = np.ones(sf.shape[:3], dtype=bool)
     ghosts[n:-n, n:-n, n:-n] = False
     assert (np.abs(sf[ghosts]).max(axis=1) > 0).mean() > 0.5
+
+
+def _face_check(o, u, faces, expect, lo):
+    """Compare the six face-state arrays of rec2 with expect(d, m) (the exact
+    face value of direction d at stored index m, broadcast over the grid):
+    left states at m in lo+1..n-lo, right states at m in lo..n-lo-1 (1-based),
+    over the cells the reconstruction loop covers in the other directions."""
+    worst = 0.0
+    for d in range(3):
+        ax = 2 - d  # numpy axis of direction d in (k, j, i, v)
+        for side, shift in ((0, 1), (1, 0)):
+            got = np.moveaxis(faces[2 * d + side], ax, 0)
+            want = np.moveaxis(expect(d), ax, 0)
+            sl = [slice(lo, -lo)] * 3
+            sl[0] = slice(lo - 1 + shift, got.shape[0] - lo - 1 + shift)
+            g, w = got[tuple(sl)], want[tuple(sl)]
+            worst = max(worst, float(np.abs(g - w).max() / np.abs(w).max()))
+    return worst
+
+
+@pytest.mark.parametrize("irec", [config.IREC_MC, config.IREC_MINMOD])
+def test_slope_limiters_reproduce_linear_data(irec):
+    """MC and minmod (rec.f90:208-739) return the face value of data linear in
+    the reconstruction coordinate (MKS x?b, faces at x?ab) up to the 1e-12
+    regulariser of the spacing."""
+    p = config.torus(nr=24, nth=20, nph=14, irec=irec)
+    o = Oracle(p)
+    xb = [o.array("x1b"), o.array("x2b"), o.array("x3b")]
+    xab = [o.array("x1ab"), o.array("x2ab"), o.array("x3ab")]
+    coef = [0.5, 0.25, 0.125]
+
+    def field(xs):
+        k, j, i = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+        return 1.0 + coef[0] * i + coef[1] * j + coef[2] * k
+
+    u = np.repeat(field(xb)[..., None], 9, axis=3) * (1.0 + 0.1 * np.arange(9))
+    faces = o.rec2(u)
+
+    def expect(d):
+        xs = list(xb)
+        xs[d] = xab[d]
+        return np.repeat(field(xs)[..., None], 9, axis=3) * (1.0 + 0.1 * np.arange(9))
+
+    assert _face_check(o, u, faces, expect, lo=1) < 1e-9
+
+
+@pytest.mark.parametrize("irec", [config.IREC_WENO5, config.IREC_WENOZ])
+def test_weno_reproduces_linear_data(irec):
+    """WENO5 and WENO-Z are exact for data linear in the cell index (every
+    candidate stencil is, and the weights sum to one)."""
+    p = config.torus(nr=24, nth=20, nph=14, irec=irec)
+    o = Oracle(p)
+    shape = o.prims().shape
+    k, j, i = np.meshgrid(*(np.arange(1, n + 1, dtype=float) for n in shape[:3]), indexing="ij")
+    lin = 1.0 + 0.01 * i + 0.02 * j + 0.03 * k
+    u = np.repeat(lin[..., None], 9, axis=3)
+    faces = o.rec2(u)
+    step = [0.01, 0.02, 0.03]
+
+    def expect(d):
+        return np.repeat((lin + 0.5 * step[d])[..., None], 9, axis=3)
+
+    assert _face_check(o, u, faces, expect, lo=2) < 1e-13
+
+
+def test_derived_quantities_sane_and_slice_consistent(torus_small):
+    """The converter's derived quantities: the ZAMO Lorentz factor >= 1 and
+    b^2 >= 0 everywhere; the static-observer factor u^t sqrt(-g_tt) is NaN
+    exactly where no static observer exists (inside the ergosphere, g_tt > 0
+    in Boyer-Lindquist coordinates), as in the converter; the phi-plane cut
+    equals that plane of the full array."""
+    p, o = torus_small
+    u = o.prims()
+    full = o.derived(u)
+    fields = [0, 2, 3, 4, 5, 6]
+    assert np.isfinite(full[..., fields]).all()
+    assert (full[..., 0] >= 1.0 - 1e-12).all()
+    assert (full[..., 2] >= 0.0).all()
+    r = o.array("x1b")
+    th = o.array("x3b")
+    th = th + 0.5 * (1.0 - p["hslope"]) * np.sin(2.0 * th)
+    rr = p["R0"] + np.exp(r)
+    a = p["akm"]
+    sig = rr[None, :] ** 2 + (a * np.cos(th)[:, None]) ** 2
+    ergo = (sig - 2.0 * rr[None, :]) < 0  # (k, i): g_tt > 0
+    rh = 1.0 + np.sqrt(1.0 - a * a)
+    ergo &= rr[None, :] > rh
+    nan = ~np.isfinite(full[..., 1])
+    assert np.array_equal(nan, np.broadcast_to(ergo[:, None, :], nan.shape))
+    j = p["jmax"] // 2 + 1
+    np.testing.assert_array_equal(o.derived(u, jslice=j), full[:, j - 1])
