@@ -16,9 +16,10 @@ void* orc_create(const orc_params* p) {
   s->p = *p;
   s->imax = p->imax; s->jmax = p->jmax; s->kmax = p->kmax;
   s->ncell = (size_t)p->imax * p->jmax * p->kmax;
-  // ghost widths (main.f90:176-196): MC/minmod nm0 = 2, MP5/WENO5/WENO-Z nm0 = 3,
+  // ghost widths (main.f90:176-196): second-order limiters and MUSCL nm0 = 2, MP5/WENO5/WENO-Z nm0 = 3,
   // PPM nm0 = 4; flux-CT nm1 = nm0+1
-  s->nm0 = (p->irec == 1 || p->irec == 2) ? 2 : (p->irec == 5 ? 4 : 3);
+  const int r = p->irec;
+  s->nm0 = (r == 1 || r == 2 || r == 3 || r == 11 || r == 12 || r == 13) ? 2 : (r == 5 ? 4 : 3);
   s->nm1 = s->nm0 + 1;
   orc::grid(*s);
   orc::coord1(*s);

@@ -243,22 +243,27 @@ static void weno5(State& s) {
           }
 }
 
-// rec.f90:208-367 (mclim, MC limiter; mc) and rec.f90:568-739 (minlim,
-// minmod) on i,j,k = 2..n-1.  The slopes divide by (x_p - x_c + small) in the
-// MKS coordinates x?b, x?ab for metric 403, else in x?, x?a; MAX/MIN take the
-// first argument as the seed (Fortran's order).
-static void mclim(State& s, bool mc) {
+// The second-order limiters on i,j,k = 2..n-1: mclim (irec 1,
+// rec.f90:208-367), minlim (2, 568-739), lim03a (11, 4037-4267), mvllim (12,
+// 4269-4477) and koren (13, 4480-4697).  Slopes in the MKS coordinates x?b,
+// x?ab for metric 403, else in x?, x?a; MAX/MIN take the first argument as
+// the seed (Fortran's order).  koren's j sweep takes tmp2i, the sign of the
+// same cell's i-direction slope, in its backward state (rec.f90:4628).
+static void limiters(State& s, int irec) {
   const double small = 1.0e-12;
   const bool mks = (s.p.metric == 403);
   const std::vector<double>* X[3] = {mks ? &s.x1b : &s.x1, mks ? &s.x2b : &s.x2, mks ? &s.x3b : &s.x3};
   const std::vector<double>* XA[3] = {mks ? &s.x1ab : &s.x1a, mks ? &s.x2ab : &s.x2a, mks ? &s.x3ab : &s.x3a};
   std::vector<double>* L[3] = {&s.uriil, &s.urijl, &s.urikl};
   std::vector<double>* R[3] = {&s.uriir, &s.urijr, &s.urikr};
+  auto mx = [](double a, double b) { return (b > a) ? b : a; };  // Fortran MAX(a, b)
+  auto mn = [](double a, double b) { return (b < a) ? b : a; };  // Fortran MIN(a, b)
 #pragma omp parallel for schedule(static)
   for (int k = 2; k <= s.kmax - 1; ++k)
     for (int j = 2; j <= s.jmax - 1; ++j)
       for (int i = 2; i <= s.imax - 1; ++i)
-        for (int n = 1; n <= NV; ++n)
+        for (int n = 1; n <= NV; ++n) {
+          double tmp2i = 1.0;
           for (int d = 0; d < 3; ++d) {
             const int di = (d == 0), dj = (d == 1), dk = (d == 2);
             const int m = (d == 0) ? i : (d == 1 ? j : k);
@@ -267,21 +272,76 @@ static void mclim(State& s, bool mc) {
             const double xp = x[m + 1], xc = x[m], xm = x[m - 1], xap = xa[m], xam = xa[m - 1];
             const double um = s.uri[s.a(n, i - di, j - dj, k - dk)], u0 = s.uri[s.a(n, i, j, k)],
                          up = s.uri[s.a(n, i + di, j + dj, k + dk)];
-            const double sp = (up - u0) * (1. / (xp - xc + small));
-            const double sm = (u0 - um) * (1. / (xc - xm + small));
-            const double tmp = (sp < 0.0) ? -1.0 : 1.0;
-            double lim;
-            if (mc) {
-              lim = fmin3(2.0 * std::fabs(sp), tmp * 2.0 * sm, tmp * 0.5 * (sp + sm));
-            } else {
-              lim = std::fabs(sp);
-              if (tmp * sm < lim) lim = tmp * sm;
+            double left, right;
+            if (irec == 12) {  // mvllim
+              const double ta = xp - xc + small, tb = xc - xm + small;
+              const double sp = (up - u0) / ta, sm = (u0 - um) / tb;
+              const double spm = sp * sm;
+              const double tc = xap - xc + small, td = xc - xam + small;
+              const double cf = ta / tc, cb = tb / td;
+              double dkm;
+              if (spm <= 0.0) {
+                dkm = 0.0;
+              } else {
+                const double t = sm * sm + (cf + cb - 2.0) * sm * sp + sp * sp;
+                dkm = (sm * sp * (cf * sm + cb * sp)) / (t + small);
+              }
+              left = u0 + dkm * tc;
+              right = u0 - dkm * td;
+            } else if (irec == 11 || irec == 13) {  // lim03a, koren
+              const double ta = xp - xc + small, tb = xc - xm + small;
+              const double tc = xap - xc + small, td = xc - xam + small;
+              const double sp = (up - u0) * (1.0 / ta), sm = (u0 - um) * (1.0 / tb);
+              const double cf = ta * (1.0 / tc), cb = tb * (1.0 / td);
+              const double tmp = (sp < 0.0) ? -1.0 : 1.0;
+              if (d == 0) tmp2i = tmp;
+              double dkf, dkb;
+              if (irec == 11) {
+                const double al = 0.5, be = 2.0, ga = 1.6;
+                const double eb = (2.0 * std::fabs(sp) + tmp * sm) * (1.0 / 3.0);
+                const double ef = (std::fabs(sp) + tmp * 2.0 * sm) * (1.0 / 3.0);
+                dkb = mx(0.0, mn(eb, mx(-al * sm * tmp, fmin3(be * sm * tmp, eb, ga * std::fabs(sp)))));
+                dkf = mx(0.0, mn(ef, mx(-al * std::fabs(sp), fmin3(be * std::fabs(sp), ef, ga * tmp * sm))));
+              } else {
+                const double tb_sign = (d == 1) ? tmp2i : tmp;
+                dkf = tmp * mx(0.0, fmin3(std::fabs(cf * sp), tmp * cb * sm, (2.0 * std::fabs(sp) + tmp * sm) * (1.0 / 3.0)));
+                dkb = tmp * mx(0.0, fmin3(std::fabs(cf * sp), tmp * cb * sm,
+                                          (std::fabs(sp) + 2.0 * tb_sign * sm) * (1.0 / 3.0)));
+              }
+              left = u0 + dkf * (xap - xc);
+              right = u0 - dkb * (xc - xam);
+            } else {  // mclim, minlim
+              const double sp = (up - u0) * (1. / (xp - xc + small));
+              const double sm = (u0 - um) * (1. / (xc - xm + small));
+              const double tmp = (sp < 0.0) ? -1.0 : 1.0;
+              const double lim = (irec == 1) ? fmin3(2.0 * std::fabs(sp), tmp * 2.0 * sm, tmp * 0.5 * (sp + sm))
+                                             : mn(std::fabs(sp), tmp * sm);
+              const double dkm = tmp * mx(0.0, lim);
+              left = u0 + dkm * (xap - xc);
+              right = u0 - dkm * (xc - xam);
             }
-            double mx = 0.0;
-            if (lim > mx) mx = lim;
-            const double dkm = tmp * mx;
-            (*L[d])[s.a(n, i, j, k)] = u0 + dkm * (xap - xc);
-            (*R[d])[s.a(n, i - di, j - dj, k - dk)] = u0 - dkm * (xc - xam);
+            (*L[d])[s.a(n, i, j, k)] = left;
+            (*R[d])[s.a(n, i - di, j - dj, k - dk)] = right;
+          }
+        }
+}
+
+// rec.f90:145-205 (muscl, beta = 1/3) on i,j,k = 2..n-2: uriil and uriir of
+// the face i+1/2 from cells i and i+1.
+static void muscl(State& s) {
+  const double beta = 1.0 / 3.0;
+  std::vector<double>* L[3] = {&s.uriil, &s.urijl, &s.urikl};
+  std::vector<double>* R[3] = {&s.uriir, &s.urijr, &s.urikr};
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= s.kmax - 2; ++k)
+    for (int j = 2; j <= s.jmax - 2; ++j)
+      for (int i = 2; i <= s.imax - 2; ++i)
+        for (int n = 1; n <= NV; ++n)
+          for (int d = 0; d < 3; ++d) {
+            const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+            auto U = [&](int o) { return s.uri[s.a(n, i + o * di, j + o * dj, k + o * dk)]; };
+            (*L[d])[s.a(n, i, j, k)] = U(0) + 0.25 * ((1.0 + beta) * (U(1) - U(0)) + (1.0 - beta) * (U(0) - U(-1)));
+            (*R[d])[s.a(n, i, j, k)] = U(1) - 0.25 * ((1.0 + beta) * (U(1) - U(0)) + (1.0 - beta) * (U(2) - U(1)));
           }
 }
 
@@ -327,6 +387,53 @@ static void weno5z(State& s) {
                                              c10 * um1 + c11 * u0 + c12 * up1, c20 * u0 + c21 * up1 + c22 * up2);
             (*R[d])[s.a(n, i - di, j - dj, k - dk)] =
                 state(br0, br1, br2, c00 * up2 + c01 * up1 + c02 * u0, c10 * up1 + c11 * u0 + c12 * um1,
+                      c20 * u0 + c21 * um1 + c22 * um2);
+          }
+}
+
+// rec.f90:3439-3793 (mapped WENO5, Henrick et al. 2005) on i,j,k = 3..n-2:
+// JS weights cd/(beta + eps)**2 with eps = 1e-40, normalised, mapped by
+// w (cd + cd**2 - 3 cd w + w**2) / (cd**2 + w (1 - 2 cd)), normalised again.
+static void weno5m(State& s) {
+  const double cd[3] = {1.0 / 10.0, 6.0 / 10.0, 3.0 / 10.0};
+  const double c00 = 2.0 / 6.0, c01 = -7.0 / 6.0, c02 = 11.0 / 6.0;
+  const double c10 = -1.0 / 6.0, c11 = 5.0 / 6.0, c12 = 2.0 / 6.0;
+  const double c20 = 2.0 / 6.0, c21 = 5.0 / 6.0, c22 = -1.0 / 6.0;
+  const double epsi = 1.0e-40;
+  const double c1312 = sp(13.0f / 12.0f), c14 = 0.25;
+  std::vector<double>* L[3] = {&s.uriil, &s.urijl, &s.urikl};
+  std::vector<double>* R[3] = {&s.uriir, &s.urijr, &s.urikr};
+  auto sq = [](double x) { return x * x; };
+  auto state = [&](const double be[3], double q0, double q1, double q2) {
+    double wa[3], g[3];
+    for (int m = 0; m < 3; ++m) wa[m] = cd[m] / sq(be[m] + epsi);
+    const double wat = wa[0] + wa[1] + wa[2];
+    for (int m = 0; m < 3; ++m) {
+      const double w = wa[m] / wat;
+      g[m] = w * (cd[m] + sq(cd[m]) - 3. * cd[m] * w + sq(w)) / (sq(cd[m]) + w * (1. - 2. * cd[m]));
+    }
+    const double gt = g[0] + g[1] + g[2];
+    return (g[0] / gt) * q0 + (g[1] / gt) * q1 + (g[2] / gt) * q2;
+  };
+#pragma omp parallel for schedule(static)
+  for (int k = 3; k <= s.kmax - 2; ++k)
+    for (int j = 3; j <= s.jmax - 2; ++j)
+      for (int i = 3; i <= s.imax - 2; ++i)
+        for (int n = 1; n <= NV; ++n)
+          for (int d = 0; d < 3; ++d) {
+            const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+            auto U = [&](int o) { return s.uri[s.a(n, i + o * di, j + o * dj, k + o * dk)]; };
+            const double um2 = U(-2), um1 = U(-1), u0 = U(0), up1 = U(1), up2 = U(2);
+            const double bl[3] = {c1312 * sq(um2 - 2. * um1 + u0) + c14 * sq(um2 - 4. * um1 + 3. * u0),
+                                  c1312 * sq(um1 - 2. * u0 + up1) + c14 * sq(um1 - up1),
+                                  c1312 * sq(u0 - 2. * up1 + up2) + c14 * sq(3. * u0 - 4. * up1 + up2)};
+            const double br[3] = {c1312 * sq(up2 - 2. * up1 + u0) + c14 * sq(up2 - 4. * up1 + 3. * u0),
+                                  c1312 * sq(up1 - 2. * u0 + um1) + c14 * sq(up1 - um1),
+                                  c1312 * sq(u0 - 2. * um1 + um2) + c14 * sq(3. * u0 - 4. * um1 + um2)};
+            (*L[d])[s.a(n, i, j, k)] = state(bl, c00 * um2 + c01 * um1 + c02 * u0, c10 * um1 + c11 * u0 + c12 * up1,
+                                             c20 * u0 + c21 * up1 + c22 * up2);
+            (*R[d])[s.a(n, i - di, j - dj, k - dk)] =
+                state(br, c00 * up2 + c01 * up1 + c02 * u0, c10 * up1 + c11 * u0 + c12 * um1,
                       c20 * u0 + c21 * um1 + c22 * um2);
           }
 }
@@ -587,11 +694,12 @@ static void face_guard(State& s) {
 }
 
 void rec2(State& s) {
-  if (s.p.irec == 1) mclim(s, true);
-  else if (s.p.irec == 2) mclim(s, false);
+  if (s.p.irec == 1 || s.p.irec == 2 || s.p.irec == 11 || s.p.irec == 12 || s.p.irec == 13) limiters(s, s.p.irec);
+  else if (s.p.irec == 3) muscl(s);
   else if (s.p.irec == 6) mp5(s);
   else if (s.p.irec == 7) weno5(s);
   else if (s.p.irec == 9) weno5z(s);
+  else if (s.p.irec == 10) weno5m(s);
   else ppm(s);
   if (s.p.guard & 1) face_guard(s);
   const double gam = s.p.gam;

@@ -17,7 +17,9 @@ import math
 PI = 3.14159265358979323  # pram.f90:30
 
 # reconstruction selectors (pram.f90:122-131 / rec.f90:61-112)
-IREC_MC, IREC_MINMOD, IREC_PPM, IREC_MP5, IREC_WENO5, IREC_WENOZ = 1, 2, 5, 6, 7, 9
+IREC_MC, IREC_MINMOD, IREC_MUSCL, IREC_PPM, IREC_MP5, IREC_WENO5, IREC_WENOZ = 1, 2, 3, 5, 6, 7, 9
+IREC_WENOM, IREC_LIMO3, IREC_MVL, IREC_KOREN = 10, 11, 12, 13
+SECOND_ORDER = (IREC_MC, IREC_MINMOD, IREC_MUSCL, IREC_LIMO3, IREC_MVL, IREC_KOREN)
 
 # rg_run_params.flags: compute every cell of a slab direction instead of one plane
 FLAG_FULL = 1
@@ -28,7 +30,7 @@ BC_PERIODIC, BC_COPY, BC_ANTISYM, BC_SYM, BC_OUTFLOW18 = 1, 5, 12, 14, 18
 
 def ghost_widths(irec: int) -> tuple[int, int]:
     """(nm0, nm1) of main.f90:176-196 for flux-CT (ict = 1)."""
-    nm0 = 2 if irec in (IREC_MC, IREC_MINMOD) else (4 if irec == IREC_PPM else 3)
+    nm0 = 2 if irec in SECOND_ORDER else (4 if irec == IREC_PPM else 3)
     return nm0, nm0 + 1
 
 

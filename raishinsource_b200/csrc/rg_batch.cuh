@@ -384,6 +384,11 @@ cudaError_t go_flux_irec(const BatchPlan* B, const BLaunch& L, cudaStream_t s) {
   switch (B->irec) {
     case 1: return go_flux<D, 1, T, S>(B, L, s);
     case 2: return go_flux<D, 2, T, S>(B, L, s);
+    case 3: return go_flux<D, 3, T, S>(B, L, s);
+    case 10: return go_flux<D, 10, T, S>(B, L, s);
+    case 11: return go_flux<D, 11, T, S>(B, L, s);
+    case 12: return go_flux<D, 12, T, S>(B, L, s);
+    case 13: return go_flux<D, 13, T, S>(B, L, s);
     case 5: return go_flux<D, 5, T, S>(B, L, s);
     case 6: return go_flux<D, 6, T, S>(B, L, s);
     case 7: return go_flux<D, 7, T, S>(B, L, s);

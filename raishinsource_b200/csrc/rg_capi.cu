@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <iterator>
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
@@ -117,14 +118,18 @@ void free_run(Run* R) {
 // Ghost widths of the reconstruction (main.f90:179-190): nm0 = 2 for the
 // second-order limiters, 3 for the five-point schemes, 4 for PPM; flux-CT
 // (ict = 1) adds one layer, nm1 = nm0 + 1.
-int nm0_of(int irec) { return (irec == 1 || irec == 2) ? 2 : (irec == 5 ? 4 : 3); }
+int nm0_of(int irec) {
+  return (irec == 1 || irec == 2 || irec == 3 || irec == 11 || irec == 12 || irec == 13) ? 2 : (irec == 5 ? 4 : 3);
+}
 int nm1_of(int irec) { return nm0_of(irec) + 1; }
 
 int check_params(const rg_run_params* p) {
   if (!p) return fail(RG_EINVAL_CONFIG, "null parameters");
-  if (p->irec != 1 && p->irec != 2 && p->irec != 5 && p->irec != 6 && p->irec != 7 && p->irec != 9)
+  static const int built[] = {1, 2, 3, 5, 6, 7, 9, 10, 11, 12, 13};
+  if (std::find(std::begin(built), std::end(built), p->irec) == std::end(built))
     return fail(RG_EINVAL_CONFIG,
-                "irec must be 1 (MC), 2 (minmod), 5 (PPM), 6 (MP5), 7 (WENO5) or 9 (WENO-Z)");
+                "irec must be 1 (MC), 2 (minmod), 3 (MUSCL), 5 (PPM), 6 (MP5), 7 (WENO5), 9 (WENO-Z), "
+                "10 (WENO-M), 11 (LimO3), 12 (MVL) or 13 (Koren)");
   if (p->metric != 1 && p->metric != 303 && p->metric != 403)
     return fail(RG_EINVAL_CONFIG, "metric must be 1, 303 or 403");
   if (p->ix1 != 1 && p->ix1 != 2) return fail(RG_EINVAL_CONFIG, "ix1 must be 1 or 2");
@@ -222,21 +227,32 @@ std::vector<double> zero_based(const std::vector<double>& v, int n) {
   return std::vector<double>(v.begin() + 1, v.begin() + 1 + n);
 }
 
-// Coefficients of the MC / minmod slopes along one axis (rec.f90:251-278):
-// four planes of n values at index m-1 for the cells m = 2..n-1 (zero at the
-// ends, which the limiters never reconstruct), computed in FP64 exactly as
-// the reference writes them, from the MKS coordinates x?b, x?ab for metric
-// 403 and from x?, x?a otherwise.
-std::vector<double> limiter_coefs(const Axis& a, int n, bool mks) {
+// Per-index coefficients of the second-order limiters along one axis, six
+// planes of n values at index m-1 for the cells m = 2..n-1 (zero at the ends,
+// which the limiters never reconstruct), computed in FP64 as the reference
+// writes them, from the MKS coordinates x?b, x?ab for metric 403 and from x?,
+// x?a otherwise.  With small = 1e-12, a = x(m+1) - x(m) + small,
+// b = x(m) - x(m-1) + small, c = xa(m) - x(m) + small, d = x(m) - xa(m-1) + small:
+//   mclim, minlim, lim03a (rec.f90:267-285, 629-646, 4108-4145): 1/a, 1/b, 0, 0, xa(m) - x(m), x(m) - xa(m-1)
+//   koren (rec.f90:4543-4579):  1/a, 1/b, a (1/c), b (1/d), xa(m) - x(m), x(m) - xa(m-1)
+//   mvllim (rec.f90:4334-4365): a, b, a/c, b/d, c, d
+std::vector<double> limiter_coefs(const Axis& ax, int n, bool mks, int irec) {
   const double small = 1.0e-12;
-  const std::vector<double>& x = mks ? a.xb : a.x;
-  const std::vector<double>& xa = mks ? a.xab : a.xa;
-  std::vector<double> o(4 * (size_t)n, 0.0);
+  const std::vector<double>& x = mks ? ax.xb : ax.x;
+  const std::vector<double>& xa = mks ? ax.xab : ax.xa;
+  std::vector<double> o(6 * (size_t)n, 0.0);
   for (int m = 2; m <= n - 1; ++m) {
-    o[m - 1] = 1. / (x[m + 1] - x[m] + small);
-    o[n + m - 1] = 1. / (x[m] - x[m - 1] + small);
-    o[2 * n + m - 1] = xa[m] - x[m];
-    o[3 * n + m - 1] = x[m] - xa[m - 1];
+    const double a = x[m + 1] - x[m] + small, b = x[m] - x[m - 1] + small;
+    const double c = xa[m] - x[m] + small, d = x[m] - xa[m - 1] + small;
+    double* q = o.data() + m - 1;
+    if (irec == 12) {
+      q[0] = a; q[n] = b; q[2 * n] = a / c; q[3 * n] = b / d; q[4 * n] = c; q[5 * n] = d;
+    } else {
+      q[0] = 1.0 / a; q[n] = 1.0 / b;
+      if (irec == 13) { q[2 * n] = a * (1.0 / c); q[3 * n] = b * (1.0 / d); }
+      q[4 * n] = xa[m] - x[m];
+      q[5 * n] = x[m] - xa[m - 1];
+    }
   }
   return o;
 }
@@ -848,7 +864,7 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   if ((rc = upload(shifted(G.ax[2].dxb, p->kmax), &d.dx3s, R, s))) return bail(rc);
   const int ext[3] = {p->imax, p->jmax, p->kmax};
   for (int a = 0; a < 3; ++a)
-    if ((rc = upload(limiter_coefs(G.ax[a], ext[a], p->metric == 403), &d.lim[a], R, s))) return bail(rc);
+    if ((rc = upload(limiter_coefs(G.ax[a], ext[a], p->metric == 403, p->irec), &d.lim[a], R, s))) return bail(rc);
   // the caches and floor tables are this run's own allocations: fill their derived parts
   if (launch_geom_derive(d, const_cast<double*>(d.mc), const_cast<double*>(d.mi), const_cast<double*>(d.mk),
                          const_cast<double*>(d.fl_de), const_cast<double*>(d.fl_pr), s) != cudaSuccess)

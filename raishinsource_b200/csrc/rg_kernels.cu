@@ -747,21 +747,33 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     for (int o = -1; o <= 1; ++o) xx[o + 4] = T(__ldg(xs + f - 1 + o));
     if (side == 0) ppm_cell<D>(P + c, N, st, dx, xx, T(r.gam), other, q);  // uriil(f)
     else ppm_cell<D>(P + c + st, N, st, dx, xx, T(r.gam), q, other);       // uriir(f)
-  } else if (IREC == 1 || IREC == 2) {
-    // owner cell f of this lane's state; left state u + dk (xa(f) - x(f)),
-    // right state u - dk (x(f) - xa(f-1)) (rec.f90:277-278)
+  } else if (IREC == 1 || IREC == 2 || IREC == 11 || IREC == 12 || IREC == 13) {
+    // owner cell f of this lane's state and its coordinate's coefficients
     const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;
     const int n = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
     const double* lc = r.lim[D - 1];
-    const T hp = T(__ldg(lc + f - 1)), hm = T(__ldg(lc + n + f - 1));
-    const T w = T(__ldg(lc + (side ? 3 : 2) * n + f - 1));
+    T co[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) co[a] = T(__ldg(lc + a * n + f - 1));
+    // koren's j sweep takes the i-direction slope sign in its backward state
+    const bool cross = (IREC == 13 && D == 2 && side == 1);
+    const T hpi = cross ? T(__ldg(r.lim[0] + i - 1)) : T(0);
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
       if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       const S* p = P + (size_t)v * N + c + side * st;
       const T u0 = T(p[0]);
-      const T dk = limited_slope<IREC == 1>(T(p[-st]), u0, T(p[st]), hp, hm);
-      q[v] = side ? u0 - dk * w : u0 + dk * w;
+      T tmp_b = T(0);
+      if (cross) tmp_b = ((T(p[1]) - u0) * hpi < T(0)) ? T(-1) : T(1);
+      else if (IREC == 13) tmp_b = ((T(p[st]) - u0) * co[0] < T(0)) ? T(-1) : T(1);
+      q[v] = limiter_state<IREC>(T(p[-st]), u0, T(p[st]), co, side, tmp_b);
+    }
+  } else if (IREC == 3) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
+      const S* p = P + (size_t)v * N + c + side * st;
+      q[v] = muscl_state(T(p[-st]), T(p[0]), T(p[st]), side);
     }
   } else {
 #pragma unroll
@@ -773,6 +785,7 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
       const T a2 = T(p[-2 * sd]), a1 = T(p[-sd]), u0 = T(p[0]), b1 = T(p[sd]), b2 = T(p[2 * sd]);
       if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? T(-1) : T(1));
       else if (IREC == 9) q[v] = weno5z_state(a2, a1, u0, b1, b2);
+      else if (IREC == 10) q[v] = weno5m_state(a2, a1, u0, b1, b2);
       else q[v] = weno5_state(a2, a1, u0, b1, b2);
     }
   }
@@ -1483,6 +1496,11 @@ static void launch_flux_t(const DevRun& r, int dir, const S* P, S* F, float* Fco
   switch (r.irec) {
     case 1: flux_dir<1, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 2: flux_dir<2, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 3: flux_dir<3, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 10: flux_dir<10, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 11: flux_dir<11, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 12: flux_dir<12, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 13: flux_dir<13, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 5: flux_dir<5, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 6: flux_dir<6, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 7: flux_dir<7, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;

@@ -115,18 +115,95 @@ __device__ __forceinline__ T weno5z_state(T a2, T a1, T u0, T b1, T b2) {
   return o0 * q0 + o1 * q1 + o2 * q2;
 }
 
-// rec.f90:208-367 (mclim, MC limiter) and rec.f90:568-739 (minlim, minmod):
-// the limited slope of a cell from its neighbours um, up with
-// hp = 1/(x_p - x_c + small), hm = 1/(x_c - x_m + small) (small = 1e-12) in
-// the coordinates the reference uses (MKS x?b for metric 403, else x?).
-// MAX/MIN follow Fortran's order: the first argument seeds the result.
-template <bool MC, typename T>
-__device__ __forceinline__ T limited_slope(T um, T u0, T up, T hp, T hm) {
-  const T sp = (up - u0) * hp, sm = (u0 - um) * hm;
+// rec.f90:3439-3793 (mapped WENO5, Henrick et al. 2005): the JS weights
+// cd_m / (beta_m + eps)^2 with eps = 1e-40, normalised, mapped by
+// g_m(w) = w (cd_m + cd_m^2 - 3 cd_m w + w^2) / (cd_m^2 + w (1 - 2 cd_m)) and
+// normalised again.
+template <typename T>
+__device__ __forceinline__ T weno5m_state(T a2, T a1, T u0, T b1, T b2) {
+  const T cd[3] = {T(1.0 / 10.0), T(6.0 / 10.0), T(3.0 / 10.0)};
+  const T c00 = T(2.0 / 6.0), c01 = T(-7.0 / 6.0), c02 = T(11.0 / 6.0);
+  const T c10 = T(-1.0 / 6.0), c11 = T(5.0 / 6.0), c12 = T(2.0 / 6.0);
+  const T c20 = T(2.0 / 6.0), c21 = T(5.0 / 6.0), c22 = T(-1.0 / 6.0);
+  const T epsi = T(1.0e-40), c1312 = T((double)(13.0f / 12.0f)), c14 = T(0.25);
+  const T s0 = a2 - T(2.) * a1 + u0, t0 = a2 - T(4.) * a1 + T(3.) * u0;
+  const T s1 = a1 - T(2.) * u0 + b1, t1 = a1 - b1;
+  const T s2 = u0 - T(2.) * b1 + b2, t2 = T(3.) * u0 - T(4.) * b1 + b2;
+  const T be[3] = {c1312 * (s0 * s0) + c14 * (t0 * t0), c1312 * (s1 * s1) + c14 * (t1 * t1),
+                   c1312 * (s2 * s2) + c14 * (t2 * t2)};
+  T wa[3], g[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) wa[m] = cd[m] / ((be[m] + epsi) * (be[m] + epsi));
+  const T wat = wa[0] + wa[1] + wa[2];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const T w = wa[m] / wat;
+    g[m] = w * (cd[m] + cd[m] * cd[m] - T(3.) * cd[m] * w + w * w) / (cd[m] * cd[m] + w * (T(1.) - T(2.) * cd[m]));
+  }
+  const T gt = g[0] + g[1] + g[2];
+  const T o0 = g[0] / gt, o1 = g[1] / gt, o2 = g[2] / gt;
+  const T q0 = c00 * a2 + c01 * a1 + c02 * u0;
+  const T q1 = c10 * a1 + c11 * u0 + c12 * b1;
+  const T q2 = c20 * u0 + c21 * b1 + c22 * b2;
+  return o0 * q0 + o1 * q1 + o2 * q2;
+}
+
+// The second-order limiters of rec.f90 on nonuniform coordinates: mclim
+// (irec 1, rec.f90:208-367), minlim (2, 568-739), lim03a (11, 4037-4267),
+// mvllim (12, 4269-4477) and koren (13, 4480-4697).  One cell's state on the
+// side `side` (0: left state at its +1/2 face, 1: right state at its -1/2
+// face) from its neighbours um, up and the per-index coefficients co[6] of
+// its coordinate (small = 1e-12, a = x_p - x_c + small, b = x_c - x_m + small,
+// c = xa_p - x_c + small, d = x_c - xa_m + small):
+//   irec 1, 2, 11: (1/a, 1/b, -, -, xa_p - x_c, x_c - xa_m)
+//   irec 13:       (1/a, 1/b, a (1/c), b (1/d), xa_p - x_c, x_c - xa_m)
+//   irec 12:       (a, b, a/c, b/d, c, d)
+// MAX/MIN follow Fortran's order (the first argument seeds the result).
+// tmp_b is the sign used in koren's backward slope: the reference takes the
+// i-direction sign there in its j sweep (rec.f90:4628), else the cell's own.
+template <int IREC, typename T>
+__device__ __forceinline__ T limiter_state(T um, T u0, T up, const T co[6], int side, T tmp_b) {
+  const T s3 = T(1.0 / 3.0);
+  if (IREC == 12) {
+    const T sp = (up - u0) / co[0], sm = (u0 - um) / co[1];
+    T dk = T(0);
+    if (!(sp * sm <= T(0))) {
+      const T t = sm * sm + (co[2] + co[3] - T(2)) * sm * sp + sp * sp;
+      dk = (sm * sp * (co[2] * sm + co[3] * sp)) / (t + T(1.0e-12));
+    }
+    return side ? u0 - dk * co[5] : u0 + dk * co[4];
+  }
+  const T sp = (up - u0) * co[0], sm = (u0 - um) * co[1];
   const T tmp = (sp < T(0)) ? T(-1) : T(1);
-  const T lim = MC ? fmin3(T(2) * mabs(sp), tmp * T(2) * sm, tmp * T(0.5) * (sp + sm))
-                   : dmin2(mabs(sp), tmp * sm);
-  return tmp * dmax2(T(0), lim);
+  T dk;
+  if (IREC == 1) {
+    dk = tmp * dmax2(T(0), fmin3(T(2) * mabs(sp), tmp * T(2) * sm, tmp * T(0.5) * (sp + sm)));
+  } else if (IREC == 2) {
+    dk = tmp * dmax2(T(0), dmin2(mabs(sp), tmp * sm));
+  } else if (IREC == 11) {
+    const T al = T(0.5), be = T(2), ga = T(1.6);
+    if (side) {
+      const T e = (T(2) * mabs(sp) + tmp * sm) * s3;
+      dk = dmax2(T(0), dmin2(e, dmax2(-al * sm * tmp, fmin3(be * sm * tmp, e, ga * mabs(sp)))));
+    } else {
+      const T e = (mabs(sp) + tmp * T(2) * sm) * s3;
+      dk = dmax2(T(0), dmin2(e, dmax2(-al * mabs(sp), fmin3(be * mabs(sp), e, ga * tmp * sm))));
+    }
+  } else {  // 13
+    const T e = side ? (mabs(sp) + T(2) * tmp_b * sm) * s3 : (T(2) * mabs(sp) + tmp * sm) * s3;
+    dk = tmp * dmax2(T(0), fmin3(mabs(co[2] * sp), tmp * co[3] * sm, e));
+  }
+  return side ? u0 - dk * co[5] : u0 + dk * co[4];
+}
+
+// rec.f90:145-205 (muscl, irec 3, beta = 1/3, no limiter): the left state of
+// a cell at its +1/2 face (side 0) and its right state at its -1/2 face
+// (side 1; the reference stores it as uriir of the face's left cell).
+template <typename T>
+__device__ __forceinline__ T muscl_state(T um, T u0, T up, int side) {
+  const T beta = T(1.0 / 3.0);
+  if (side) return u0 - T(0.25) * ((T(1.0) + beta) * (u0 - um) + (T(1.0) - beta) * (up - u0));
+  return u0 + T(0.25) * ((T(1.0) + beta) * (up - u0) + (T(1.0) - beta) * (u0 - um));
 }
 
 // ------------------------------------------------------------------- PPM

@@ -88,9 +88,9 @@ struct DevRun {
   const double* dx1s;    // rec2's shifted dx1b: dummy dx1b(i) = actual dx1b(i-1), index i-1
   const double* dx2s;
   const double* dx3s;
-  // Slope-limiter coefficients (MC / minmod) per direction d, four planes of
-  // n_d values at index m-1: 1/(x(m+1)-x(m)+small), 1/(x(m)-x(m-1)+small),
-  // xa(m)-x(m), x(m)-xa(m-1) (rec.f90:251-278; MKS coordinates for metric 403).
+  // Second-order limiter coefficients per direction d (MC, minmod, LimO3,
+  // MVL, Koren): six planes of n_d values at index m-1 of the cell's
+  // coordinate spacings, as limiter_state in rg_recon.cuh reads them.
   const double* lim[3];
   int ibc[6][9];
   double* P[3];          // the run's rotating primitive buffers (P^n = P[scal->cur])

@@ -37,15 +37,16 @@ def test_footprint_and_param_checks_run_on_cpu():
     p = config.torus(nr=256, nth=128, nph=128)
     b = footprint(p)
     assert 2e9 < b < 6e9
-    for irec in (config.IREC_MC, config.IREC_MINMOD, config.IREC_WENOZ):
+    for irec in (config.IREC_MC, config.IREC_MINMOD, config.IREC_MUSCL, config.IREC_WENOZ, config.IREC_LIMO3,
+                 config.IREC_MVL, config.IREC_KOREN):
         assert footprint(dict(p, irec=irec)) > 0
-    bad = dict(p, irec=3)  # MUSCL: not built
+    bad = dict(p, irec=4)  # CENO: not built
     try:
         footprint(bad)
     except RgError as e:
         assert e.code == 1
     else:
-        raise AssertionError("irec=3 must be rejected")
+        raise AssertionError("irec=4 must be rejected")
 
 
 def test_library_load_error_path_without_gpu():

@@ -74,7 +74,8 @@ def test_caluu1(torus2d):
 
 
 @pytest.mark.parametrize("irec", [config.IREC_MP5, config.IREC_WENO5, config.IREC_PPM, config.IREC_MC,
-                                  config.IREC_MINMOD, config.IREC_WENOZ])
+                                  config.IREC_MINMOD, config.IREC_WENOZ, config.IREC_MUSCL, config.IREC_LIMO3,
+                                  config.IREC_MVL, config.IREC_KOREN, config.IREC_WENOM])
 def test_calflx_guarded(gpu_ctx, irec):
     p = config.torus(nr=48, nth=40, nph=12, irec=irec)
     p["guard"] = 1
@@ -244,10 +245,12 @@ def _vector_scaled_err(a, b):
     return np.abs(a - b).max(axis=0) / np.maximum(scale, 1e-300)
 
 
-@pytest.mark.parametrize("irec", [config.IREC_MC, config.IREC_MINMOD, config.IREC_WENOZ])
+@pytest.mark.parametrize("irec", [config.IREC_MC, config.IREC_MINMOD, config.IREC_WENOZ, config.IREC_MUSCL,
+                                  config.IREC_LIMO3, config.IREC_MVL, config.IREC_KOREN, config.IREC_WENOM])
 def test_step_3d_limiters_and_wenoz(gpu_ctx, irec):
-    """MC, minmod (rec.f90:208-739) and WENO-Z (rec.f90:3161-3436): one full
-    step per comparison, 3D torus, 1e-12 of each quantity's scale."""
+    """MC, minmod, MUSCL, LimO3, MVL, Koren (rec.f90:145-739, 4037-4697),
+    WENO-Z (rec.f90:3161-3436) and WENO-M (rec.f90:3439-3793): one full step
+    per comparison, 3D torus, 1e-12 of each quantity's scale."""
     p = dict(config.torus(nr=40, nth=24, nph=16, irec=irec), guard=1)
     o = Oracle(p)
     o.ic_torus(seed=80 + irec)
@@ -353,7 +356,8 @@ def test_slab_rejects_nonuniform_upload(gpu_ctx):
     assert e.value.code == 1
 
 
-@pytest.mark.parametrize("irec", [config.IREC_PPM, config.IREC_WENO5, config.IREC_MC, config.IREC_WENOZ])
+@pytest.mark.parametrize("irec", [config.IREC_PPM, config.IREC_WENO5, config.IREC_MC, config.IREC_WENOZ,
+                                  config.IREC_KOREN])
 def test_step_2d_slab_schemes(gpu_ctx, irec):
     """2D phi slab (stored as one plane; jmax = 2*nm1+1: 11 for PPM, 7 for MC)
     against the oracle, which computes every phi cell."""

@@ -232,11 +232,12 @@ def _face_check(o, u, faces, expect, lo):
     return worst
 
 
-@pytest.mark.parametrize("irec", [config.IREC_MC, config.IREC_MINMOD])
+@pytest.mark.parametrize("irec", [config.IREC_MC, config.IREC_MINMOD, config.IREC_LIMO3, config.IREC_MVL,
+                                  config.IREC_KOREN])
 def test_slope_limiters_reproduce_linear_data(irec):
-    """MC and minmod (rec.f90:208-739) return the face value of data linear in
-    the reconstruction coordinate (MKS x?b, faces at x?ab) up to the 1e-12
-    regulariser of the spacing."""
+    """The second-order limiters (rec.f90:208-739, 4037-4697) return the face
+    value of increasing data linear in the reconstruction coordinate (MKS x?b,
+    faces at x?ab) up to the 1e-12 regulariser of the spacing."""
     p = config.torus(nr=24, nth=20, nph=14, irec=irec)
     o = Oracle(p)
     xb = [o.array("x1b"), o.array("x2b"), o.array("x3b")]
@@ -258,10 +259,10 @@ def test_slope_limiters_reproduce_linear_data(irec):
     assert _face_check(o, u, faces, expect, lo=1) < 1e-9
 
 
-@pytest.mark.parametrize("irec", [config.IREC_WENO5, config.IREC_WENOZ])
+@pytest.mark.parametrize("irec", [config.IREC_WENO5, config.IREC_WENOZ, config.IREC_WENOM])
 def test_weno_reproduces_linear_data(irec):
-    """WENO5 and WENO-Z are exact for data linear in the cell index (every
-    candidate stencil is, and the weights sum to one)."""
+    """WENO5, WENO-Z and WENO-M are exact for data linear in the cell index
+    (every candidate stencil is, and the weights sum to one)."""
     p = config.torus(nr=24, nth=20, nph=14, irec=irec)
     o = Oracle(p)
     shape = o.prims().shape
@@ -303,3 +304,38 @@ def test_derived_quantities_sane_and_slice_consistent(torus_small):
     assert np.array_equal(nan, np.broadcast_to(ergo[:, None, :], nan.shape))
     j = p["jmax"] // 2 + 1
     np.testing.assert_array_equal(o.derived(u, jslice=j), full[:, j - 1])
+
+
+def test_limo3_drops_the_slope_sign():
+    """lim03a's dk2fi/dk2bi are max(0, ...) without the sign factor tmp2i that
+    every other limiter applies (rec.f90:4122-4134), so a decreasing linear
+    profile gets its left face value on the increasing side: u + |s| h."""
+    p = config.torus(nr=24, nth=20, nph=14, irec=config.IREC_LIMO3)
+    o = Oracle(p)
+    shape = o.prims().shape
+    x1b, x1ab = o.array("x1b"), o.array("x1ab")
+    u = np.repeat((5.0 - 0.5 * x1b)[None, None, :, None], 9, axis=3) * np.ones(shape)
+    uil = o.rec2(u)[0]
+    i = np.arange(2, shape[2] - 1)  # 1-based cells 3..n-1 -> zero-based 2..n-2
+    got = uil[5, 5, i, 0]
+    slope = 0.5 * (x1b[i + 1] - x1b[i]) / (x1b[i + 1] - x1b[i] + 1e-12)
+    want = u[5, 5, i, 0] + slope * (x1ab[i] - x1b[i])
+    np.testing.assert_allclose(got, want, rtol=1e-12)
+
+
+def test_muscl_reproduces_linear_data():
+    """MUSCL (rec.f90:145-205) is exact for data linear in the cell index; both
+    face states are stored at the face's left cell m = 2..n-2."""
+    p = config.torus(nr=24, nth=20, nph=14, irec=config.IREC_MUSCL)
+    o = Oracle(p)
+    shape = o.prims().shape
+    k, j, i = np.meshgrid(*(np.arange(1, n + 1, dtype=float) for n in shape[:3]), indexing="ij")
+    step = [0.01, 0.02, 0.03]
+    lin = 1.0 + step[0] * i + step[1] * j + step[2] * k
+    faces = o.rec2(np.repeat(lin[..., None], 9, axis=3))
+    reg = (slice(1, -2),) * 3
+    for d in range(3):
+        want = (lin + 0.5 * step[d])[reg]
+        for side in range(2):
+            got = faces[2 * d + side][reg][..., 0]
+            assert np.abs(got - want).max() < 1e-14 * np.abs(want).max()
