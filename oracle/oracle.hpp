@@ -30,8 +30,8 @@ typedef struct {
   int imax, jmax, kmax;       // grid incl. ghosts (pram.f90:11)
   int metric;                 // 1 Minkowski, 303 KS, 403 MKS (pram.f90:67)
   int ix1, ix2, ix3;          // grid spacing kinds (pram.f90:59)
-  int irec;                   // 1 MC, 2 minmod, 3 MUSCL, 5 PPM, 6 MP5, 7 WENO5, 9 WENO-Z,
-                              // 10 WENO-M, 11 LimO3, 12 MVL, 13 Koren (pram.f90:122-131)
+  int irec;                   // 1 MC, 2 minmod, 3 MUSCL, 4 CENO, 5 PPM, 6 MP5, 7 WENO5, 8 MP-WENO,
+                              // 9 WENO-Z, 10 WENO-M, 11 LimO3, 12 MVL, 13 Koren (pram.f90:122-131)
   int model;                  // 2 shock tube, 7 FM torus (pram.f90:66)
   int iter;                   // NR iteration cap (pram.f90:27)
   double xmin, xmax, ymin, ymax, zmin, zmax;   // (pram.f90:52-57)

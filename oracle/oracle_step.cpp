@@ -326,6 +326,86 @@ static void limiters(State& s, int irec) {
         }
 }
 
+// rec.f90:742-1258 (ceno, convex ENO) in its three passes: the minmod state
+// on i,j,k = 2..n-1 from the physical cell centres x?, the three quadratic
+// candidates and their weighted deviations (alp = 1, 0.7, 1) on 3..n-2, and
+// the selection on 3..n-2.  In the theta sweep's negative branch the
+// reference compares |dklp| with itself (rec.f90:1211), so the third
+// candidate is never taken there.
+static void ceno(State& s) {
+  const double alp1 = 1.0, alp2 = 0.7, alp3 = 1.0;
+  const std::vector<double>* X[3] = {&s.x1, &s.x2, &s.x3};
+  std::vector<double>* L[3] = {&s.uriil, &s.urijl, &s.urikl};
+  std::vector<double>* R[3] = {&s.uriir, &s.urijr, &s.urikr};
+  const size_t nn = s.uri.size();
+  std::vector<double> l1[3], r1[3];
+  for (int d = 0; d < 3; ++d) { l1[d].assign(nn, 0.0); r1[d].assign(nn, 0.0); }
+#pragma omp parallel for schedule(static)
+  for (int k = 2; k <= s.kmax - 1; ++k)
+    for (int j = 2; j <= s.jmax - 1; ++j)
+      for (int i = 2; i <= s.imax - 1; ++i)
+        for (int n = 1; n <= NV; ++n)
+          for (int d = 0; d < 3; ++d) {
+            const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+            const int m = (d == 0) ? i : (d == 1 ? j : k);
+            const std::vector<double>& x = *X[d];
+            const double um = s.uri[s.a(n, i - di, j - dj, k - dk)], u0 = s.uri[s.a(n, i, j, k)],
+                         up = s.uri[s.a(n, i + di, j + dj, k + dk)];
+            const double sp = (up - u0) / (x[m + 1] - x[m]), sm = (u0 - um) / (x[m] - x[m - 1]);
+            double dkm = 0.0;
+            if (!(sp * sm <= 0.0)) {
+              const double tmp = (sp < 0.0) ? -1.0 : 1.0;
+              dkm = tmp * std::min(std::fabs(sp), std::fabs(sm));
+            }
+            l1[d][s.a(n, i, j, k)] = u0 + dkm * (0.5 * (x[m + 1] - x[m]));
+            r1[d][s.a(n, i - di, j - dj, k - dk)] = u0 - dkm * (0.5 * (x[m] - x[m - 1]));
+          }
+  auto pick = [](double u1, double cm, double c0, double cp, double dm, double d0, double dp, bool quirk) {
+    double out = u1;
+    if (dp > 0.0 && d0 > 0.0 && dm > 0.0) {
+      out = cm;
+      if (std::fabs(d0) < std::fabs(dm) && std::fabs(d0) < std::fabs(dp)) out = c0;
+      if (std::fabs(dp) < std::fabs(dm) && std::fabs(dp) < std::fabs(d0)) out = cp;
+    }
+    if (dm < 0.0 && d0 < 0.0 && dp < 0.0) {
+      out = cm;
+      if (std::fabs(d0) < std::fabs(dm) && std::fabs(d0) < std::fabs(dp)) out = c0;
+      if (std::fabs(dp) < std::fabs(dm) && std::fabs(dp) < (quirk ? std::fabs(dp) : std::fabs(d0))) out = cp;
+    }
+    return out;
+  };
+#pragma omp parallel for schedule(static)
+  for (int k = 3; k <= s.kmax - 2; ++k)
+    for (int j = 3; j <= s.jmax - 2; ++j)
+      for (int i = 3; i <= s.imax - 2; ++i)
+        for (int n = 1; n <= NV; ++n)
+          for (int d = 0; d < 3; ++d) {
+            const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+            const int m = (d == 0) ? i : (d == 1 ? j : k);
+            const std::vector<double>& x = *X[d];
+            auto U = [&](int o) { return s.uri[s.a(n, i + o * di, j + o * dj, k + o * dk)]; };
+            const double d2m = 0.5 * (U(0) - U(-2)), d20 = 0.5 * (U(1) - U(-1)), d2p = 0.5 * (U(2) - U(0));
+            const double d3m = U(0) - 2.0 * U(-1) + U(-2), d30 = U(1) - 2.0 * U(0) + U(-1),
+                         d3p = U(2) - 2.0 * U(1) + U(0);
+            const double t2m = (0.5 * (x[m + 1] + x[m]) - x[m - 1]) / (x[m + 1] - x[m]);
+            const double t20 = (0.5 * (x[m + 1] + x[m]) - x[m]) / (x[m + 1] - x[m]);
+            const double t2p = (0.5 * (x[m + 1] + x[m]) - x[m + 1]) / (x[m + 1] - x[m]);
+            const double t3m = (0.5 * (x[m] + x[m - 1]) - x[m - 1]) / (x[m] - x[m - 1]);
+            const double t30 = (0.5 * (x[m] + x[m - 1]) - x[m]) / (x[m] - x[m - 1]);
+            const double t3p = (0.5 * (x[m] + x[m - 1]) - x[m + 1]) / (x[m] - x[m - 1]);
+            const size_t ol = s.a(n, i, j, k), orr = s.a(n, i - di, j - dj, k - dk);
+            const double lm = U(0) + d2m * t2m + 0.5 * d3m * (t2m * t2m);
+            const double l0 = U(0) + d20 * t20 + 0.5 * d30 * (t20 * t20);
+            const double lp = U(0) + d2p * t2p + 0.5 * d3p * (t2p * t2p);
+            const double rm = U(0) + d2m * t3m + 0.5 * d3m * (t3m * t3m);
+            const double r0 = U(0) + d20 * t30 + 0.5 * d30 * (t30 * t30);
+            const double rp = U(0) + d2p * t3p + 0.5 * d3p * (t3p * t3p);
+            const double ul1 = l1[d][ol], ur1 = r1[d][orr];
+            (*L[d])[ol] = pick(ul1, lm, l0, lp, alp1 * (lm - ul1), alp2 * (l0 - ul1), alp3 * (lp - ul1), d == 2);
+            (*R[d])[orr] = pick(ur1, rm, r0, rp, alp1 * (rm - ur1), alp2 * (r0 - ur1), alp3 * (rp - ur1), false);
+          }
+}
+
 // rec.f90:145-205 (muscl, beta = 1/3) on i,j,k = 2..n-2: uriil and uriir of
 // the face i+1/2 from cells i and i+1.
 static void muscl(State& s) {
@@ -388,6 +468,81 @@ static void weno5z(State& s) {
             (*R[d])[s.a(n, i - di, j - dj, k - dk)] =
                 state(br0, br1, br2, c00 * up2 + c01 * up1 + c02 * u0, c10 * up1 + c11 * u0 + c12 * um1,
                       c20 * u0 + c21 * um1 + c22 * um2);
+          }
+}
+
+// rec.f90:2645-3158 (mpweno5) on i,j,k = 3..n-2: the WENO5-JS face value
+// (beta with +epsi, weights cd/beta**2) limited by MP5's bounds, with MP5's
+// right-state sign convention.  The radial right state's beta_1 reads
+// uri(n,i-11,j,k) where uri(n,i-1,j,k) is meant (rec.f90:2757); gfortran
+// addresses it in the column-major array, which below i = 1 is the element
+// (n, imax + i - 11, j - 1, k).
+static void mpweno5(State& s) {
+  const double cd0 = 1.0 / 10.0, cd1 = 6.0 / 10.0, cd2 = 3.0 / 10.0;
+  const double c00 = 2.0 / 6.0, c01 = -7.0 / 6.0, c02 = 11.0 / 6.0;
+  const double c10 = -1.0 / 6.0, c11 = 5.0 / 6.0, c12 = 2.0 / 6.0;
+  const double c20 = 2.0 / 6.0, c21 = 5.0 / 6.0, c22 = -1.0 / 6.0;
+  const double tmp2 = 4.0 / 3.0, alpha = 4.0, eps1 = 1.0e-10, epsi = 1.0e-6;
+  const double c1312 = sp(13.0f / 12.0f), c14 = 0.25;
+  std::vector<double>* L[3] = {&s.uriil, &s.urijl, &s.urikl};
+  std::vector<double>* R[3] = {&s.uriir, &s.urijr, &s.urikr};
+  auto sq = [](double x) { return x * x; };
+#pragma omp parallel for schedule(static)
+  for (int k = 3; k <= s.kmax - 2; ++k)
+    for (int j = 3; j <= s.jmax - 2; ++j)
+      for (int i = 3; i <= s.imax - 2; ++i)
+        for (int n = 1; n <= NV; ++n)
+          for (int d = 0; d < 3; ++d) {
+            const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+            auto U = [&](int o) { return s.uri[s.a(n, i + o * di, j + o * dj, k + o * dk)]; };
+            const double um2 = U(-2), um1 = U(-1), u0 = U(0), up1 = U(1), up2 = U(2);
+            double typo = um1;
+            if (d == 0) typo = (i - 11 >= 1) ? s.uri[s.a(n, i - 11, j, k)] : s.uri[s.a(n, s.imax + i - 11, j - 1, k)];
+            const double bl0 = c1312 * sq(um2 - 2. * um1 + u0) + c14 * sq(um2 - 4. * um1 + 3. * u0) + epsi;
+            const double bl1 = c1312 * sq(um1 - 2. * u0 + up1) + c14 * sq(um1 - up1) + epsi;
+            const double bl2 = c1312 * sq(u0 - 2. * up1 + up2) + c14 * sq(3. * u0 - 4. * up1 + up2) + epsi;
+            const double br0 = c1312 * sq(up2 - 2. * up1 + u0) + c14 * sq(up2 - 4. * up1 + 3. * u0) + epsi;
+            const double br1 = c1312 * sq(up1 - 2. * u0 + typo) + c14 * sq(up1 - um1) + epsi;
+            const double br2 = c1312 * sq(u0 - 2. * um1 + um2) + c14 * sq(3. * u0 - 4. * um1 + um2) + epsi;
+            const double wl0 = cd0 / sq(bl0), wl1 = cd1 / sq(bl1), wl2 = cd2 / sq(bl2), wlt = wl0 + wl1 + wl2;
+            const double wr0 = cd0 / sq(br0), wr1 = cd1 / sq(br1), wr2 = cd2 / sq(br2), wrt = wr0 + wr1 + wr2;
+            const double ul1 = (wl0 / wlt) * (c00 * um2 + c01 * um1 + c02 * u0) +
+                               (wl1 / wlt) * (c10 * um1 + c11 * u0 + c12 * up1) +
+                               (wl2 / wlt) * (c20 * u0 + c21 * up1 + c22 * up2);
+            const double ur1 = (wr0 / wrt) * (c00 * up2 + c01 * up1 + c02 * u0) +
+                               (wr1 / wrt) * (c10 * up1 + c11 * u0 + c12 * um1) +
+                               (wr2 / wrt) * (c20 * u0 + c21 * um1 + c22 * um2);
+            const double dim1 = um2 - 2. * um1 + u0, di1 = um1 - 2. * u0 + up1, dip1 = u0 - 2. * up1 + up2;
+            // left state (as mp5)
+            {
+              const double ulmp = u0 + dmm(up1 - u0, alpha * (u0 - um1));
+              double out = ul1;
+              if (!((ul1 - u0) * (ul1 - ulmp) <= eps1)) {
+                const double dm4iph = dm4(4. * di1 - dip1, 4. * dip1 - di1, di1, dip1);
+                const double dm4imh = dm4(4. * di1 - dim1, 4. * dim1 - di1, di1, dim1);
+                const double ul = u0 + alpha * (u0 - um1), av = 0.5 * (u0 + up1);
+                const double md = av - 0.5 * dm4iph, lc = u0 + 0.5 * (u0 - um1) + tmp2 * dm4imh;
+                const double umax = std::max(fmin3(u0, up1, md), fmin3(u0, ul, lc));
+                const double umin = std::min(fmax3(u0, up1, md), fmax3(u0, ul, lc));
+                out = ul1 + dmm(umin - ul1, umax - ul1);
+              }
+              (*L[d])[s.a(n, i, j, k)] = out;
+            }
+            // right state (as mp5: md = av + 0.5 dm4imh, lc = ... - tmp2 dm4iph)
+            {
+              const double urmp = u0 + dmm(um1 - u0, alpha * (u0 - up1));
+              double out = ur1;
+              if (!((ur1 - u0) * (ur1 - urmp) <= eps1)) {
+                const double dm4iph = dm4(4. * di1 - dip1, 4. * dip1 - di1, di1, dip1);
+                const double dm4imh = dm4(4. * di1 - dim1, 4. * dim1 - di1, di1, dim1);
+                const double ul = u0 + alpha * (u0 - up1), av = 0.5 * (u0 + um1);
+                const double md = av + 0.5 * dm4imh, lc = u0 + 0.5 * (u0 - up1) - tmp2 * dm4iph;
+                const double umax = std::max(fmin3(u0, um1, md), fmin3(u0, ul, lc));
+                const double umin = std::min(fmax3(u0, um1, md), fmax3(u0, ul, lc));
+                out = ur1 + dmm(umin - ur1, umax - ur1);
+              }
+              (*R[d])[s.a(n, i - di, j - dj, k - dk)] = out;
+            }
           }
 }
 
@@ -696,8 +851,10 @@ static void face_guard(State& s) {
 void rec2(State& s) {
   if (s.p.irec == 1 || s.p.irec == 2 || s.p.irec == 11 || s.p.irec == 12 || s.p.irec == 13) limiters(s, s.p.irec);
   else if (s.p.irec == 3) muscl(s);
+  else if (s.p.irec == 4) ceno(s);
   else if (s.p.irec == 6) mp5(s);
   else if (s.p.irec == 7) weno5(s);
+  else if (s.p.irec == 8) mpweno5(s);
   else if (s.p.irec == 9) weno5z(s);
   else if (s.p.irec == 10) weno5m(s);
   else ppm(s);

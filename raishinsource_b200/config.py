@@ -18,7 +18,7 @@ PI = 3.14159265358979323  # pram.f90:30
 
 # reconstruction selectors (pram.f90:122-131 / rec.f90:61-112)
 IREC_MC, IREC_MINMOD, IREC_MUSCL, IREC_PPM, IREC_MP5, IREC_WENO5, IREC_WENOZ = 1, 2, 3, 5, 6, 7, 9
-IREC_WENOM, IREC_LIMO3, IREC_MVL, IREC_KOREN = 10, 11, 12, 13
+IREC_CENO, IREC_MPWENO, IREC_WENOM, IREC_LIMO3, IREC_MVL, IREC_KOREN = 4, 8, 10, 11, 12, 13
 SECOND_ORDER = (IREC_MC, IREC_MINMOD, IREC_MUSCL, IREC_LIMO3, IREC_MVL, IREC_KOREN)
 
 # rg_run_params.flags: compute every cell of a slab direction instead of one plane

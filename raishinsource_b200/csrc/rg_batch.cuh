@@ -385,6 +385,8 @@ cudaError_t go_flux_irec(const BatchPlan* B, const BLaunch& L, cudaStream_t s) {
     case 1: return go_flux<D, 1, T, S>(B, L, s);
     case 2: return go_flux<D, 2, T, S>(B, L, s);
     case 3: return go_flux<D, 3, T, S>(B, L, s);
+    case 4: return go_flux<D, 4, T, S>(B, L, s);
+    case 8: return go_flux<D, 8, T, S>(B, L, s);
     case 10: return go_flux<D, 10, T, S>(B, L, s);
     case 11: return go_flux<D, 11, T, S>(B, L, s);
     case 12: return go_flux<D, 12, T, S>(B, L, s);

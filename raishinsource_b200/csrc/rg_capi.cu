@@ -125,10 +125,10 @@ int nm1_of(int irec) { return nm0_of(irec) + 1; }
 
 int check_params(const rg_run_params* p) {
   if (!p) return fail(RG_EINVAL_CONFIG, "null parameters");
-  static const int built[] = {1, 2, 3, 5, 6, 7, 9, 10, 11, 12, 13};
+  static const int built[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13};
   if (std::find(std::begin(built), std::end(built), p->irec) == std::end(built))
     return fail(RG_EINVAL_CONFIG,
-                "irec must be 1 (MC), 2 (minmod), 3 (MUSCL), 5 (PPM), 6 (MP5), 7 (WENO5), 9 (WENO-Z), "
+                "irec must be 1 (MC), 2 (minmod), 3 (MUSCL), 4 (CENO), 5 (PPM), 6 (MP5), 7 (WENO5), 8 (MP-WENO), 9 (WENO-Z), "
                 "10 (WENO-M), 11 (LimO3), 12 (MVL) or 13 (Koren)");
   if (p->metric != 1 && p->metric != 303 && p->metric != 403)
     return fail(RG_EINVAL_CONFIG, "metric must be 1, 303 or 403");
@@ -227,8 +227,8 @@ std::vector<double> zero_based(const std::vector<double>& v, int n) {
   return std::vector<double>(v.begin() + 1, v.begin() + 1 + n);
 }
 
-// Per-index coefficients of the second-order limiters along one axis, six
-// planes of n values at index m-1 for the cells m = 2..n-1 (zero at the ends,
+// Per-index coefficients of the second-order limiters and of CENO along one
+// axis, up to ten planes of n values at index m-1 for the cells m = 2..n-1 (zero at the ends,
 // which the limiters never reconstruct), computed in FP64 as the reference
 // writes them, from the MKS coordinates x?b, x?ab for metric 403 and from x?,
 // x?a otherwise.  With small = 1e-12, a = x(m+1) - x(m) + small,
@@ -236,11 +236,27 @@ std::vector<double> zero_based(const std::vector<double>& v, int n) {
 //   mclim, minlim, lim03a (rec.f90:267-285, 629-646, 4108-4145): 1/a, 1/b, 0, 0, xa(m) - x(m), x(m) - xa(m-1)
 //   koren (rec.f90:4543-4579):  1/a, 1/b, a (1/c), b (1/d), xa(m) - x(m), x(m) - xa(m-1)
 //   mvllim (rec.f90:4334-4365): a, b, a/c, b/d, c, d
+//   ceno (rec.f90:861-881, 945-951, physical x in every metric): x(m+1) - x(m),
+//     x(m) - x(m-1), half of each, and the quadratic candidates' offsets
+//     (xf - x(m-1), xf - x(m), xf - x(m+1)) / (x(m+1) - x(m)) with
+//     xf = (x(m+1) + x(m))/2, and the same about (x(m) + x(m-1))/2 over x(m) - x(m-1)
 std::vector<double> limiter_coefs(const Axis& ax, int n, bool mks, int irec) {
   const double small = 1.0e-12;
+  std::vector<double> o(10 * (size_t)n, 0.0);
+  if (irec == 4) {
+    const std::vector<double>& x = ax.x;
+    for (int m = 2; m <= n - 1; ++m) {
+      double* q = o.data() + m - 1;
+      const double dp = x[m + 1] - x[m], dm = x[m] - x[m - 1];
+      const double fp = 0.5 * (x[m + 1] + x[m]), fm = 0.5 * (x[m] + x[m - 1]);
+      q[0] = dp; q[n] = dm; q[2 * n] = 0.5 * dp; q[3 * n] = 0.5 * dm;
+      q[4 * n] = (fp - x[m - 1]) / dp; q[5 * n] = (fp - x[m]) / dp; q[6 * n] = (fp - x[m + 1]) / dp;
+      q[7 * n] = (fm - x[m - 1]) / dm; q[8 * n] = (fm - x[m]) / dm; q[9 * n] = (fm - x[m + 1]) / dm;
+    }
+    return o;
+  }
   const std::vector<double>& x = mks ? ax.xb : ax.x;
   const std::vector<double>& xa = mks ? ax.xab : ax.xa;
-  std::vector<double> o(6 * (size_t)n, 0.0);
   for (int m = 2; m <= n - 1; ++m) {
     const double a = x[m + 1] - x[m] + small, b = x[m] - x[m - 1] + small;
     const double c = xa[m] - x[m] + small, d = x[m] - xa[m - 1] + small;

@@ -768,6 +768,19 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
       else if (IREC == 13) tmp_b = ((T(p[st]) - u0) * co[0] < T(0)) ? T(-1) : T(1);
       q[v] = limiter_state<IREC>(T(p[-st]), u0, T(p[st]), co, side, tmp_b);
     }
+  } else if (IREC == 4) {
+    const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;
+    const int n = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
+    const double* lc = r.lim[D - 1];
+    T co[10];
+#pragma unroll
+    for (int a = 0; a < 10; ++a) co[a] = T(__ldg(lc + a * n + f - 1));
+#pragma unroll
+    for (int v = 0; v < 9; ++v) {
+      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
+      const S* p = P + (size_t)v * N + c + side * st;
+      q[v] = ceno_state(T(p[-2 * st]), T(p[-st]), T(p[0]), T(p[st]), T(p[2 * st]), co, side, D == 3 && side == 0);
+    }
   } else if (IREC == 3) {
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
@@ -784,7 +797,19 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
       const S* p = P + (size_t)v * N + c + side * st;
       const T a2 = T(p[-2 * sd]), a1 = T(p[-sd]), u0 = T(p[0]), b1 = T(p[sd]), b2 = T(p[2 * sd]);
       if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? T(-1) : T(1));
-      else if (IREC == 9) q[v] = weno5z_state(a2, a1, u0, b1, b2);
+      else if (IREC == 8) {
+        // mpweno5: WENO5-JS limited by MP5's bounds (rec.f90:2645-3158).  Its
+        // radial right state reads uri(n,i-11,j,k) for uri(n,i-1,j,k) in beta_1
+        // (rec.f90:2757); Fortran addresses it in the column-major array, so
+        // below i = 1 it is cell (imax + i - 11, j - 1, k).
+        T b1s = b1;
+        if (D == 1 && side == 1) {
+          const int f = i + 1;
+          const size_t ct = (f - 11 >= 1) ? r.cell(f - 11, j, k) : r.cell(r.imax + f - 11, j - 1, k);
+          b1s = T(P[(size_t)v * N + ct]);
+        }
+        q[v] = mp_limit(weno5_js(a2, a1, u0, b1, b2, b1s), a2, a1, u0, b1, b2, side ? T(-1) : T(1));
+      } else if (IREC == 9) q[v] = weno5z_state(a2, a1, u0, b1, b2);
       else if (IREC == 10) q[v] = weno5m_state(a2, a1, u0, b1, b2);
       else q[v] = weno5_state(a2, a1, u0, b1, b2);
     }
@@ -1497,6 +1522,8 @@ static void launch_flux_t(const DevRun& r, int dir, const S* P, S* F, float* Fco
     case 1: flux_dir<1, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 2: flux_dir<2, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 3: flux_dir<3, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 4: flux_dir<4, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
+    case 8: flux_dir<8, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 10: flux_dir<10, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 11: flux_dir<11, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;
     case 12: flux_dir<12, T, S>(r, dir, g, b, P, F, Fcopy, icopy, ilo, ihi, s); break;

@@ -41,9 +41,8 @@ __device__ __forceinline__ T dm4(T ww, T xx, T yy, T zz) {
 // (rec.f90:2172-2176).  Negation is exact, so both equal the reference's
 // separate formulas bit for bit, and the two lanes of a face run one code path.
 template <typename T>
-__device__ __forceinline__ T mp5_state(T a2, T a1, T u0, T b1, T b2, T sg) {
-  const T tmp1 = T(1.0) / T(60.0), tmp2 = T(4.0) / T(3.0), alpha = T(4.0), eps1 = T(1.0e-10);
-  const T ul1 = tmp1 * (T(2.) * a2 - T(13.) * a1 + T(47.) * u0 + T(27.) * b1 - T(3.) * b2);
+__device__ __forceinline__ T mp_limit(T ul1, T a2, T a1, T u0, T b1, T b2, T sg) {
+  const T tmp2 = T(4.0) / T(3.0), alpha = T(4.0), eps1 = T(1.0e-10);
   const T ulmp = u0 + dmm(b1 - u0, alpha * (u0 - a1));
   const T t = (ul1 - u0) * (ul1 - ulmp);
   if (t <= eps1) return ul1;
@@ -61,19 +60,27 @@ __device__ __forceinline__ T mp5_state(T a2, T a1, T u0, T b1, T b2, T sg) {
   const T umax = dmax2(m1, m2), umin = dmin2(m3, m4);
   return ul1 + dmm(umin - ul1, umax - ul1);
 }
+template <typename T>
+__device__ __forceinline__ T mp5_state(T a2, T a1, T u0, T b1, T b2, T sg) {
+  const T tmp1 = T(1.0) / T(60.0);
+  const T ul1 = tmp1 * (T(2.) * a2 - T(13.) * a1 + T(47.) * u0 + T(27.) * b1 - T(3.) * b2);
+  return mp_limit(ul1, a2, a1, u0, b1, b2, sg);
+}
 
 // rec.f90:2373-2643 (WENO5-JS); the left state at +1/2 takes
 // (u-2, u-1, u0, u+1, u+2), the right state at -1/2 the mirrored stencil.
 // (13./12.) is a single-precision literal in the reference.
+// b1s is the value the smoothness indicator beta_1 reads in place of b1: b1
+// itself, except in mpweno5's radial right state (rec.f90:2757, see face_lane).
 template <typename T>
-__device__ __forceinline__ T weno5_state(T a2, T a1, T u0, T b1, T b2) {
+__device__ __forceinline__ T weno5_js(T a2, T a1, T u0, T b1, T b2, T b1s) {
   const T cd0 = T(1.0 / 10.0), cd1 = T(6.0 / 10.0), cd2 = T(3.0 / 10.0);
   const T c00 = T(2.0 / 6.0), c01 = T(-7.0 / 6.0), c02 = T(11.0 / 6.0);
   const T c10 = T(-1.0 / 6.0), c11 = T(5.0 / 6.0), c12 = T(2.0 / 6.0);
   const T c20 = T(2.0 / 6.0), c21 = T(5.0 / 6.0), c22 = T(-1.0 / 6.0);
   const T epsi = T(1.0e-6), c1312 = T((double)(13.0f / 12.0f)), c14 = T(0.25);
   const T s0 = a2 - T(2.) * a1 + u0, t0 = a2 - T(4.) * a1 + T(3.) * u0;
-  const T s1 = a1 - T(2.) * u0 + b1, t1 = a1 - b1;
+  const T s1 = a1 - T(2.) * u0 + b1s, t1 = a1 - b1;
   const T s2 = u0 - T(2.) * b1 + b2, t2 = T(3.) * u0 - T(4.) * b1 + b2;
   const T be0 = c1312 * (s0 * s0) + c14 * (t0 * t0) + epsi;
   const T be1 = c1312 * (s1 * s1) + c14 * (t1 * t1) + epsi;
@@ -85,6 +92,10 @@ __device__ __forceinline__ T weno5_state(T a2, T a1, T u0, T b1, T b2) {
   const T q1 = c10 * a1 + c11 * u0 + c12 * b1;
   const T q2 = c20 * u0 + c21 * b1 + c22 * b2;
   return o0 * q0 + o1 * q1 + o2 * q2;
+}
+template <typename T>
+__device__ __forceinline__ T weno5_state(T a2, T a1, T u0, T b1, T b2) {
+  return weno5_js(a2, a1, u0, b1, b2, b1);
 }
 
 // rec.f90:3161-3436 (WENO-Z, Borges et al. 2008): WENO5 with the weights
@@ -194,6 +205,44 @@ __device__ __forceinline__ T limiter_state(T um, T u0, T up, const T co[6], int 
     dk = tmp * dmax2(T(0), fmin3(mabs(co[2] * sp), tmp * co[3] * sm, e));
   }
   return side ? u0 - dk * co[5] : u0 + dk * co[4];
+}
+
+// rec.f90:742-1258 (ceno, irec 4, convex ENO): one cell's state on side
+// `side` from u(-2..+2) along the direction and the per-index coefficients
+// co[10] of its physical coordinate x (rg_capi.cu, ceno_coefs): the minmod
+// state u1, three quadratic candidates (centred at the cell before, at and
+// after it), their deviations from u1 weighted by (1, 0.7, 1), and the
+// candidate of smallest deviation when all three deviate the same way.
+// kquirk drops the third candidate from the negative branch, as the
+// reference's theta sweep compares |dklp| with itself there (rec.f90:1211).
+template <typename T>
+__device__ __forceinline__ T ceno_state(T um2, T um, T u0, T up, T up2, const T co[10], int side, bool kquirk) {
+  const T sp = (up - u0) / co[0], sm = (u0 - um) / co[1];
+  T dk = T(0);
+  if (!(sp * sm <= T(0))) {
+    const T tmp = (sp < T(0)) ? T(-1) : T(1);
+    dk = tmp * dmin2(mabs(sp), mabs(sm));
+  }
+  const T u1 = side ? u0 - dk * co[3] : u0 + dk * co[2];
+  const T d2m = T(0.5) * (u0 - um2), d20 = T(0.5) * (up - um), d2p = T(0.5) * (up2 - u0);
+  const T d3m = u0 - T(2.0) * um + um2, d30 = up - T(2.0) * u0 + um, d3p = up2 - T(2.0) * up + u0;
+  const T tm = side ? co[7] : co[4], t0 = side ? co[8] : co[5], tp = side ? co[9] : co[6];
+  const T cm = u0 + d2m * tm + T(0.5) * d3m * (tm * tm);
+  const T c0 = u0 + d20 * t0 + T(0.5) * d30 * (t0 * t0);
+  const T cp = u0 + d2p * tp + T(0.5) * d3p * (tp * tp);
+  const T dm = T(1.0) * (cm - u1), d0 = T(0.7) * (c0 - u1), dp = T(1.0) * (cp - u1);
+  T out = u1;
+  if (dp > T(0) && d0 > T(0) && dm > T(0)) {
+    out = cm;
+    if (mabs(d0) < mabs(dm) && mabs(d0) < mabs(dp)) out = c0;
+    if (mabs(dp) < mabs(dm) && mabs(dp) < mabs(d0)) out = cp;
+  }
+  if (dm < T(0) && d0 < T(0) && dp < T(0)) {
+    out = cm;
+    if (mabs(d0) < mabs(dm) && mabs(d0) < mabs(dp)) out = c0;
+    if (!kquirk && mabs(dp) < mabs(dm) && mabs(dp) < mabs(d0)) out = cp;
+  }
+  return out;
 }
 
 // rec.f90:145-205 (muscl, irec 3, beta = 1/3, no limiter): the left state of

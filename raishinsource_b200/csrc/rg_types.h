@@ -88,9 +88,9 @@ struct DevRun {
   const double* dx1s;    // rec2's shifted dx1b: dummy dx1b(i) = actual dx1b(i-1), index i-1
   const double* dx2s;
   const double* dx3s;
-  // Second-order limiter coefficients per direction d (MC, minmod, LimO3,
-  // MVL, Koren): six planes of n_d values at index m-1 of the cell's
-  // coordinate spacings, as limiter_state in rg_recon.cuh reads them.
+  // Limiter coefficients per direction d (MC, minmod, LimO3, MVL, Koren,
+  // CENO): ten planes of n_d values at index m-1 of the cell's coordinate
+  // spacings, as limiter_state and ceno_state in rg_recon.cuh read them.
   const double* lim[3];
   int ibc[6][9];
   double* P[3];          // the run's rotating primitive buffers (P^n = P[scal->cur])

@@ -40,13 +40,15 @@ def test_footprint_and_param_checks_run_on_cpu():
     for irec in (config.IREC_MC, config.IREC_MINMOD, config.IREC_MUSCL, config.IREC_WENOZ, config.IREC_LIMO3,
                  config.IREC_MVL, config.IREC_KOREN):
         assert footprint(dict(p, irec=irec)) > 0
-    bad = dict(p, irec=4)  # CENO: not built
+    for irec in (config.IREC_CENO, config.IREC_MPWENO, config.IREC_WENOM):
+        assert footprint(dict(p, irec=irec)) > 0
+    bad = dict(p, irec=14)  # no such scheme
     try:
         footprint(bad)
     except RgError as e:
         assert e.code == 1
     else:
-        raise AssertionError("irec=4 must be rejected")
+        raise AssertionError("irec=14 must be rejected")
 
 
 def test_library_load_error_path_without_gpu():

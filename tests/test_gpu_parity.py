@@ -75,7 +75,8 @@ def test_caluu1(torus2d):
 
 @pytest.mark.parametrize("irec", [config.IREC_MP5, config.IREC_WENO5, config.IREC_PPM, config.IREC_MC,
                                   config.IREC_MINMOD, config.IREC_WENOZ, config.IREC_MUSCL, config.IREC_LIMO3,
-                                  config.IREC_MVL, config.IREC_KOREN, config.IREC_WENOM])
+                                  config.IREC_MVL, config.IREC_KOREN, config.IREC_WENOM, config.IREC_MPWENO,
+                                  config.IREC_CENO])
 def test_calflx_guarded(gpu_ctx, irec):
     p = config.torus(nr=48, nth=40, nph=12, irec=irec)
     p["guard"] = 1
@@ -246,7 +247,8 @@ def _vector_scaled_err(a, b):
 
 
 @pytest.mark.parametrize("irec", [config.IREC_MC, config.IREC_MINMOD, config.IREC_WENOZ, config.IREC_MUSCL,
-                                  config.IREC_LIMO3, config.IREC_MVL, config.IREC_KOREN, config.IREC_WENOM])
+                                  config.IREC_LIMO3, config.IREC_MVL, config.IREC_KOREN, config.IREC_WENOM,
+                                  config.IREC_MPWENO, config.IREC_CENO])
 def test_step_3d_limiters_and_wenoz(gpu_ctx, irec):
     """MC, minmod, MUSCL, LimO3, MVL, Koren (rec.f90:145-739, 4037-4697),
     WENO-Z (rec.f90:3161-3436) and WENO-M (rec.f90:3439-3793): one full step
@@ -357,7 +359,7 @@ def test_slab_rejects_nonuniform_upload(gpu_ctx):
 
 
 @pytest.mark.parametrize("irec", [config.IREC_PPM, config.IREC_WENO5, config.IREC_MC, config.IREC_WENOZ,
-                                  config.IREC_KOREN])
+                                  config.IREC_KOREN, config.IREC_MPWENO])
 def test_step_2d_slab_schemes(gpu_ctx, irec):
     """2D phi slab (stored as one plane; jmax = 2*nm1+1: 11 for PPM, 7 for MC)
     against the oracle, which computes every phi cell."""

@@ -259,10 +259,11 @@ def test_slope_limiters_reproduce_linear_data(irec):
     assert _face_check(o, u, faces, expect, lo=1) < 1e-9
 
 
-@pytest.mark.parametrize("irec", [config.IREC_WENO5, config.IREC_WENOZ, config.IREC_WENOM])
+@pytest.mark.parametrize("irec", [config.IREC_WENO5, config.IREC_WENOZ, config.IREC_WENOM, config.IREC_MPWENO])
 def test_weno_reproduces_linear_data(irec):
-    """WENO5, WENO-Z and WENO-M are exact for data linear in the cell index
-    (every candidate stencil is, and the weights sum to one)."""
+    """WENO5, WENO-Z, WENO-M and MP-WENO are exact for data linear in the cell
+    index (every candidate stencil is, the weights sum to one, and MP5's bounds
+    hold the linear value)."""
     p = config.torus(nr=24, nth=20, nph=14, irec=irec)
     o = Oracle(p)
     shape = o.prims().shape
@@ -339,3 +340,25 @@ def test_muscl_reproduces_linear_data():
         for side in range(2):
             got = faces[2 * d + side][reg][..., 0]
             assert np.abs(got - want).max() < 1e-14 * np.abs(want).max()
+
+
+def test_mpweno_radial_right_state_reads_i_minus_11():
+    """mpweno5's radial right state takes beta_1 from uri(n,i-11,j,k)
+    (rec.f90:2757): changing only that far cell (and nothing within the
+    5-point stencil) changes the right states that read it, and no others."""
+    p = config.torus(nr=32, nth=20, nph=14, irec=config.IREC_MPWENO)
+    o = Oracle(p)
+    shape = o.prims().shape
+    k, j, i = np.meshgrid(*(np.arange(1, n + 1, dtype=float) for n in shape[:3]), indexing="ij")
+    smooth = 1.0 + 0.1 * np.sin(0.4 * i) + 0.05 * np.cos(0.3 * j) + 0.02 * np.sin(0.2 * k)
+    u = np.repeat(smooth[..., None], 9, axis=3)  # smooth: MP5's bounds leave the WENO value
+    base = o.rec2(u)
+    v = u.copy()
+    v[6, 6, 4, 0] += 0.5          # cell (i=5, j=7, k=7), 1-based
+    changed = np.argwhere(o.rec2(v)[1][..., 0] != base[1][..., 0])
+    # uriir(i-1) of cells i = 16 (5 + 11) in the same row: stored at i = 15,
+    # plus the ordinary stencil neighbours of cell 5 (stored at i = 2..6)
+    rows = {tuple(c[:2]) for c in changed}
+    assert rows == {(6, 6)}, rows
+    assert 14 in set(changed[:, 2])  # zero-based i of stored index 15
+
