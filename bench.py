@@ -335,7 +335,7 @@ def section_mixed(ctx, args) -> dict:
                      "recov_nr2": st["recov_nr2"], "recov_fail": st["recov_fail"]}
         r.release()
     (a, (ma, ea), _), (b, (mb, eb), _) = states["mixed"], states["fp64"]
-    l1, linf = _rel_errs(a, b, config.ghost_widths(p["irec"])[1])
+    l1, linf = _rel_errs(a, b, config.ghost_widths(p["irec"], p.get("ict", 1))[1])
     out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     out["l1_rel_mixed_vs_fp64"] = l1
     out["linf_rel_mixed_vs_fp64"] = linf

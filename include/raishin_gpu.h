@@ -59,6 +59,9 @@ typedef struct rg_run_params {
                     which the reference's LLF term breaks (hll.f90:109).  Not in the reference. */
   int precision; /* rg_precision */
   int flags;     /* RG_FLAG_* bits */
+  int ict;       /* constrained transport as pram.f90's ict (pram.f90:148-151, ct.f90:4-27):
+                    0 none, 1 flux-CT (Toth 2000; the reference's setting), 2 modified flux-CT
+                    (Gardiner & Stone 2005, mflct).  Ghost width nm1 = nm0 + ict (main.f90:192-199). */
 } rg_run_params;
 
 /* rg_run_params.flags.  A direction of extent 2*nm1+1 (one interior cell)

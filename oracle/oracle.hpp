@@ -42,6 +42,8 @@ typedef struct {
                               // reconstructed face state with rho <= 0 or p <= 0; bit 2: zero
                               // flux of the normal B component before flux-CT.  Neither is in
                               // the reference (see face_guard and fluxct in oracle_step.cpp).
+  int ict;                    // constrained transport (pram.f90:148-151): 0 none, 1 fluxct,
+                              // 2 mflct
 } orc_params;
 
 typedef struct {
@@ -128,7 +130,7 @@ void caluu1(State& s, const std::vector<double>& uri, std::vector<double>& uu);
 void rec2(State& s);
 void calcha(State& s);
 void hlle(State& s);
-void fluxct(State& s);
+void ct(State& s);
 void calsf_all(State& s, bool every_cell = false);
 void derived(State& s, const std::vector<double>& uri, int jslice, double* out);
 void rkstage(State& s, int stage);

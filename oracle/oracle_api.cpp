@@ -16,11 +16,11 @@ void* orc_create(const orc_params* p) {
   s->p = *p;
   s->imax = p->imax; s->jmax = p->jmax; s->kmax = p->kmax;
   s->ncell = (size_t)p->imax * p->jmax * p->kmax;
-  // ghost widths (main.f90:176-196): second-order limiters and MUSCL nm0 = 2, MP5/WENO5/WENO-Z nm0 = 3,
-  // PPM nm0 = 4; flux-CT nm1 = nm0+1
+  // ghost widths (main.f90:176-199): second-order schemes nm0 = 2, five-point schemes nm0 = 3,
+  // PPM nm0 = 4; constrained transport nm1 = nm0 + ict
   const int r = p->irec;
   s->nm0 = (r == 1 || r == 2 || r == 3 || r == 11 || r == 12 || r == 13) ? 2 : (r == 5 ? 4 : 3);
-  s->nm1 = s->nm0 + 1;
+  s->nm1 = s->nm0 + p->ict;
   orc::grid(*s);
   orc::coord1(*s);
   orc::calchrist(*s);
@@ -107,7 +107,7 @@ void orc_fluxes(void* h, const double* uri, double* ww) {
   orc::rec2(*s);
   orc::calcha(*s);
   orc::hlle(*s);
-  orc::fluxct(*s);
+  orc::ct(*s);
   std::memcpy(ww, s->ww.data(), s->ww.size() * sizeof(double));
 }
 

@@ -943,21 +943,11 @@ void hlle(State& s) {
           }
 }
 
+namespace {
 // ct.f90:30-118 (Toth flux-CT)
 void fluxct(State& s) {
   const int nm0 = s.nm0, nm1 = s.nm1;
   const size_t N = s.ncell;
-  // guard bit 2 (not in the reference): Toth's flux-CT takes the flux of the
-  // normal field component as zero.  The reference keeps the LLF diffusion
-  // -0.5 c (B^d_R - B^d_L) in ww(1,7), ww(2,8), ww(3,9) (hll.f90:109-111),
-  // which CT does not replace, so its corner divergence of B is not conserved.
-  if (s.p.guard & 2) {
-#pragma omp parallel for schedule(static)
-    for (int k = nm0; k <= s.kmax - nm0; ++k)
-      for (int j = nm0; j <= s.jmax - nm0; ++j)
-        for (int i = nm0; i <= s.imax - nm0; ++i)
-          for (int d = 1; d <= 3; ++d) s.ww[s.w(d, 6 + d, i, j, k)] = 0.0;
-  }
   std::vector<double> fyx(N), fzx(N), fxy(N), fzy(N), fxz(N), fyz(N);
 #pragma omp parallel for schedule(static)
   for (int k = nm0; k <= s.kmax - nm0; ++k)
@@ -990,6 +980,92 @@ void fluxct(State& s) {
         s.ww[s.w(2, 9, i, j, k)] = e * (2.0 * fyz[C(i, j, k)] + fyz[C(i, j, k + 1)] + fyz[C(i, j, k - 1)] -
                                         fzy[C(i, j, k)] - fzy[C(i, j + 1, k)] - fzy[C(i, j, k - 1)] - fzy[C(i, j + 1, k - 1)]);
       }
+}
+
+// ct.f90:121-233 (mflct, Gardiner & Stone 2005): cell-centred EMFs from the
+// face fluxes on nm0+1..n-nm0, then the flux-CT brackets weighted 1/4 plus
+// averaged EMFs on nm1..n-nm1.
+void mflct(State& s) {
+  const int nm0 = s.nm0, nm1 = s.nm1;
+  const size_t N = s.ncell;
+  std::vector<double> fyx(N), fzx(N), fxy(N), fzy(N), fxz(N), fyz(N), exc(N), eyc(N), ezc(N);
+  auto C = [&](int i, int j, int k) { return s.cell(i, j, k); };
+#pragma omp parallel for schedule(static)
+  for (int k = nm0; k <= s.kmax - nm0; ++k)
+    for (int j = nm0; j <= s.jmax - nm0; ++j)
+      for (int i = nm0; i <= s.imax - nm0; ++i) {
+        const size_t c = C(i, j, k);
+        fyx[c] = s.ww[s.w(2, 7, i, j, k)];
+        fzx[c] = s.ww[s.w(3, 7, i, j, k)];
+        fxy[c] = s.ww[s.w(1, 8, i, j, k)];
+        fzy[c] = s.ww[s.w(3, 8, i, j, k)];
+        fxz[c] = s.ww[s.w(1, 9, i, j, k)];
+        fyz[c] = s.ww[s.w(2, 9, i, j, k)];
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = nm0 + 1; k <= s.kmax - nm0; ++k)
+    for (int j = nm0 + 1; j <= s.jmax - nm0; ++j)
+      for (int i = nm0 + 1; i <= s.imax - nm0; ++i) {
+        const size_t c = C(i, j, k);
+        ezc[c] = 0.25 * (-fxy[C(i - 1, j, k)] - fxy[c] + fyx[C(i, j - 1, k)] + fyx[c]);
+        exc[c] = 0.25 * (-fyz[C(i, j - 1, k)] - fyz[c] + fzy[C(i, j, k - 1)] + fzy[c]);
+        eyc[c] = 0.25 * (-fzx[C(i, j, k - 1)] - fzx[c] + fxz[C(i - 1, j, k)] + fxz[c]);
+      }
+  const double q = 1.0 / 4.0, h = 1.0 / 8.0;
+#pragma omp parallel for schedule(static)
+  for (int k = nm1; k <= s.kmax - nm1; ++k)
+    for (int j = nm1; j <= s.jmax - nm1; ++j)
+      for (int i = nm1; i <= s.imax - nm1; ++i) {
+        const double fbyx = q * (2.0 * fyx[C(i, j, k)] + fyx[C(i + 1, j, k)] + fyx[C(i - 1, j, k)] - fxy[C(i, j, k)] -
+                                 fxy[C(i, j + 1, k)] - fxy[C(i - 1, j, k)] - fxy[C(i - 1, j + 1, k)]);
+        const double fbzx = q * (2.0 * fzx[C(i, j, k)] + fzx[C(i + 1, j, k)] + fzx[C(i - 1, j, k)] - fxz[C(i, j, k)] -
+                                 fxz[C(i, j, k + 1)] - fxz[C(i - 1, j, k)] - fxz[C(i - 1, j, k + 1)]);
+        const double fbxy = q * (2.0 * fxy[C(i, j, k)] + fxy[C(i, j + 1, k)] + fxy[C(i, j - 1, k)] - fyx[C(i, j, k)] -
+                                 fyx[C(i + 1, j, k)] - fyx[C(i, j - 1, k)] - fyx[C(i + 1, j - 1, k)]);
+        const double fbzy = q * (2.0 * fzy[C(i, j, k)] + fzy[C(i, j + 1, k)] + fzy[C(i, j - 1, k)] - fyz[C(i, j, k)] -
+                                 fyz[C(i, j, k + 1)] - fyz[C(i, j - 1, k)] - fyz[C(i, j - 1, k + 1)]);
+        const double fbxz = q * (2.0 * fxz[C(i, j, k)] + fxz[C(i, j, k + 1)] + fxz[C(i, j, k - 1)] - fzx[C(i, j, k)] -
+                                 fzx[C(i + 1, j, k)] - fzx[C(i, j, k - 1)] - fzx[C(i + 1, j, k - 1)]);
+        const double fbyz = q * (2.0 * fyz[C(i, j, k)] + fyz[C(i, j, k + 1)] + fyz[C(i, j, k - 1)] - fzy[C(i, j, k)] -
+                                 fzy[C(i, j + 1, k)] - fzy[C(i, j, k - 1)] - fzy[C(i, j + 1, k - 1)]);
+        const double fhyx = -h * (2. * ezc[C(i, j, k)] + 2. * ezc[C(i, j + 1, k)] + ezc[C(i + 1, j, k)] +
+                                  ezc[C(i + 1, j + 1, k)] + ezc[C(i - 1, j, k)] + ezc[C(i - 1, j + 1, k)]);
+        const double fhzx = h * (2. * eyc[C(i, j, k)] + 2. * eyc[C(i, j, k + 1)] + eyc[C(i + 1, j, k)] +
+                                 eyc[C(i + 1, j, k + 1)] + eyc[C(i - 1, j, k)] + eyc[C(i - 1, j, k + 1)]);
+        const double fhxy = h * (2. * ezc[C(i, j, k)] + 2. * ezc[C(i + 1, j, k)] + ezc[C(i, j + 1, k)] +
+                                 ezc[C(i + 1, j + 1, k)] + ezc[C(i, j - 1, k)] + ezc[C(i + 1, j - 1, k)]);
+        const double fhzy = -h * (2. * exc[C(i, j, k)] + 2. * exc[C(i, j, k + 1)] + exc[C(i, j + 1, k)] +
+                                  exc[C(i, j + 1, k + 1)] + exc[C(i, j - 1, k)] + exc[C(i, j - 1, k + 1)]);
+        const double fhxz = -h * (2. * eyc[C(i, j, k)] + 2. * eyc[C(i + 1, j, k)] + eyc[C(i, j, k + 1)] +
+                                  eyc[C(i + 1, j, k + 1)] + eyc[C(i, j, k - 1)] + eyc[C(i + 1, j, k - 1)]);
+        const double fhyz = h * (2. * exc[C(i, j, k)] + 2. * exc[C(i, j + 1, k)] + exc[C(i, j, k + 1)] +
+                                 exc[C(i, j + 1, k + 1)] + exc[C(i, j, k - 1)] + exc[C(i, j + 1, k - 1)]);
+        s.ww[s.w(2, 7, i, j, k)] = fbyx + fhyx;
+        s.ww[s.w(3, 7, i, j, k)] = fbzx + fhzx;
+        s.ww[s.w(1, 8, i, j, k)] = fbxy + fhxy;
+        s.ww[s.w(3, 8, i, j, k)] = fbzy + fhzy;
+        s.ww[s.w(1, 9, i, j, k)] = fbxz + fhxz;
+        s.ww[s.w(2, 9, i, j, k)] = fbyz + fhyz;
+      }
+}
+}  // namespace
+
+// ct.f90:4-27: the constrained-transport scheme ict.  guard bit 2 (not in
+// the reference) first zeroes the flux of each face's normal field
+// component: the reference keeps the LLF diffusion -0.5 c (B^d_R - B^d_L) in
+// ww(1,7), ww(2,8), ww(3,9) (hll.f90:109-111), which CT does not replace, so
+// its corner divergence of B is not conserved.
+void ct(State& s) {
+  const int nm0 = s.nm0;
+  if (s.p.guard & 2) {
+#pragma omp parallel for schedule(static)
+    for (int k = nm0; k <= s.kmax - nm0; ++k)
+      for (int j = nm0; j <= s.jmax - nm0; ++j)
+        for (int i = nm0; i <= s.imax - nm0; ++i)
+          for (int d = 1; d <= 3; ++d) s.ww[s.w(d, 6 + d, i, j, k)] = 0.0;
+  }
+  if (s.p.ict == 1) fluxct(s);
+  else if (s.p.ict == 2) mflct(s);
 }
 
 // calsf.f90:6-151 (T^m_n at the cell and S_nu = sqrt(-g) T^m_n Gamma^n_{nu m}).
@@ -1644,7 +1720,7 @@ void step(State& s) {
     rec2(s);
     calcha(s);
     hlle(s);
-    fluxct(s);
+    ct(s);
     calsf_all(s);
     rkstage(s, stage);
     std::vector<double>& un = (stage == 1) ? s.uh : (stage == 2 ? s.us : s.un);

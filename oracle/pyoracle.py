@@ -27,6 +27,7 @@ class OrcParams(C.Structure):
         ("tmax", C.c_double), ("dtmin", C.c_double),
         ("ibc", (C.c_int * 9) * 6),
         ("guard", C.c_int),
+        ("ict", C.c_int),
     ]
 
 
@@ -93,7 +94,8 @@ def make_params(p: dict) -> OrcParams:
                 for m in range(9):
                     o.ibc[s][m] = int(p["ibc"][s][m])
         else:
-            setattr(o, name, p.get(name, 0) if name == "guard" else p[name])
+            default = {"guard": 0, "ict": 1}
+            setattr(o, name, p.get(name, default[name]) if name in default else p[name])
     return o
 
 

@@ -51,6 +51,7 @@ class RunParams(C.Structure):
         ("guard", C.c_int),
         ("precision", C.c_int),
         ("flags", C.c_int),
+        ("ict", C.c_int),
     ]
 
 
@@ -142,6 +143,8 @@ def make_params(p: dict) -> RunParams:
             o.guard = int(p.get("guard", 0))
         elif name == "flags":
             o.flags = int(p.get("flags", 0))
+        elif name == "ict":
+            o.ict = int(p.get("ict", 1))
         elif name == "precision":
             o.precision = {"fp64": 0, "mixed": 1}[p.get("precision", "fp64")]
         else:
@@ -270,7 +273,7 @@ class Run:
             _check(self.lib, self.lib.rg_run_admit_prep(ctx.h, prep.h, C.byref(rid)))
         self.id = rid.value
         self.shape = (params["kmax"], params["jmax"], params["imax"], 9)
-        self.nm0, self.nm1 = ghost_widths(params["irec"])
+        self.nm0, self.nm1 = ghost_widths(params["irec"], params.get("ict", 1))
 
     def release(self):
         if self.id:

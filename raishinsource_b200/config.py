@@ -28,10 +28,10 @@ FLAG_FULL = 1
 BC_PERIODIC, BC_COPY, BC_ANTISYM, BC_SYM, BC_OUTFLOW18 = 1, 5, 12, 14, 18
 
 
-def ghost_widths(irec: int) -> tuple[int, int]:
-    """(nm0, nm1) of main.f90:176-196 for flux-CT (ict = 1)."""
+def ghost_widths(irec: int, ict: int = 1) -> tuple[int, int]:
+    """(nm0, nm1) of main.f90:176-199: nm1 = nm0 + ict (ict = 1: flux-CT)."""
     nm0 = 2 if irec in SECOND_ORDER else (4 if irec == IREC_PPM else 3)
-    return nm0, nm0 + 1
+    return nm0, nm0 + ict
 
 
 def torus_bcs() -> list[list[int]]:
@@ -49,15 +49,16 @@ def torus_bcs() -> list[list[int]]:
 
 def torus(nr: int = 256, nth: int = 256, nph: int | None = None, irec: int = IREC_MP5,
           akm: float = 0.9375, rmin: float = 1.9, rmax: float = 50.0, cfl: float = 0.4,
-          precision: str = "fp64") -> dict:
+          precision: str = "fp64", ict: int = 1) -> dict:
     """Fishbone-Moncrief torus in modified Kerr-Schild coordinates.
 
     ``nr`` x ``nth`` x ``nph`` are imax x kmax x jmax including ghosts.  With
     ``nph=None`` the run is the 2D axisymmetric case: a periodic phi slab of
     jmax = 2*nm1+1 cells (one interior cell).  phi spans 2*pi over the
-    interior: dphi = 2*pi/(jmax-2*nm1), x2(j) = (j-nm1-1/2)*dphi.
+    interior: dphi = 2*pi/(jmax-2*nm1), x2(j) = (j-nm1-1/2)*dphi.  ``ict``
+    selects the constrained transport (1 flux-CT, 2 modified flux-CT, 0 none).
     """
-    _, nm1 = ghost_widths(irec)
+    _, nm1 = ghost_widths(irec, ict)
     jmax = 2 * nm1 + 1 if nph is None else int(nph)
     dphi = 2.0 * math.pi / (jmax - 2 * nm1)
     ymin = (0.5 - nm1) * dphi
@@ -66,19 +67,19 @@ def torus(nr: int = 256, nth: int = 256, nph: int | None = None, irec: int = IRE
         imax=int(nr), jmax=jmax, kmax=int(nth), metric=403, ix1=2, ix2=1, ix3=2, irec=irec, model=7,
         iter=5000, xmin=rmin, xmax=rmax, ymin=ymin, ymax=ymax, zmin=0.02, zmax=PI - 0.02,
         R0=0.0, hslope=0.5, akm=akm, gam=4.0 / 3.0, cfl=cfl, dmin=1.0e-4, pmin=1.0e-6, pmax=1.0e6,
-        tmax=1.0e30, dtmin=1.0e-9, ibc=torus_bcs(), precision=precision,
+        tmax=1.0e30, dtmin=1.0e-9, ibc=torus_bcs(), precision=precision, ict=ict,
     )
 
 
 def tube(n: int = 400, irec: int = IREC_MP5, cfl: float = 0.4, tmax: float = 0.4,
-         precision: str = "fp64") -> dict:
+         precision: str = "fp64", ict: int = 1) -> dict:
     """1D RMHD shock tube in Minkowski space (metric 1, model 2): x in [1, 2]
     (cell centres, ghosts included; x > 0 because the floors use x**-1.5),
     Gamma = 5/3, copy boundaries in x and a 2*nm1+1 slab with copy
     boundaries in y and z.  (With periodic y and z the reference's
     single-rank periodic fill never refreshes the cells that are ghosts in
     both, bnd.f90:50-70/160-180/272-292, and flux-CT reads them.)"""
-    _, nm1 = ghost_widths(irec)
+    _, nm1 = ghost_widths(irec, ict)
     imax = int(n) + 2 * nm1
     w = 2 * nm1 + 1
     dx = 1.0 / (imax - 1)
@@ -87,11 +88,11 @@ def tube(n: int = 400, irec: int = IREC_MP5, cfl: float = 0.4, tmax: float = 0.4
         xmin=1.0, xmax=2.0, ymin=0.0, ymax=(w - 1) * dx, zmin=0.0, zmax=(w - 1) * dx,
         R0=0.0, hslope=0.5, akm=0.0, gam=5.0 / 3.0, cfl=cfl, dmin=1.0e-4, pmin=1.0e-6, pmax=1.0e6,
         tmax=tmax, dtmin=1.0e-9,
-        ibc=[[5] * 9] * 6, precision=precision,
+        ibc=[[5] * 9] * 6, precision=precision, ict=ict,
     )
 
 
 def interior_cells(p: dict) -> int:
     """Zone count of one full step: interior cells (main.f90 loops nm1+1..n-nm1)."""
-    _, nm1 = ghost_widths(p["irec"])
+    _, nm1 = ghost_widths(p["irec"], p.get("ict", 1))
     return (p["imax"] - 2 * nm1) * (p["jmax"] - 2 * nm1) * (p["kmax"] - 2 * nm1)

@@ -116,12 +116,12 @@ void free_run(Run* R) {
 }
 
 // Ghost widths of the reconstruction (main.f90:179-190): nm0 = 2 for the
-// second-order limiters, 3 for the five-point schemes, 4 for PPM; flux-CT
-// (ict = 1) adds one layer, nm1 = nm0 + 1.
+// second-order schemes, 3 for the five-point schemes, 4 for PPM; constrained
+// transport adds ict layers, nm1 = nm0 + ict (main.f90:192-199).
 int nm0_of(int irec) {
   return (irec == 1 || irec == 2 || irec == 3 || irec == 11 || irec == 12 || irec == 13) ? 2 : (irec == 5 ? 4 : 3);
 }
-int nm1_of(int irec) { return nm0_of(irec) + 1; }
+int nm1_of(const rg_run_params* p) { return nm0_of(p->irec) + p->ict; }
 
 int check_params(const rg_run_params* p) {
   if (!p) return fail(RG_EINVAL_CONFIG, "null parameters");
@@ -130,13 +130,15 @@ int check_params(const rg_run_params* p) {
     return fail(RG_EINVAL_CONFIG,
                 "irec must be 1 (MC), 2 (minmod), 3 (MUSCL), 4 (CENO), 5 (PPM), 6 (MP5), 7 (WENO5), 8 (MP-WENO), 9 (WENO-Z), "
                 "10 (WENO-M), 11 (LimO3), 12 (MVL) or 13 (Koren)");
+  if (p->ict < 0 || p->ict > 2)
+    return fail(RG_EINVAL_CONFIG, "ict must be 0 (none), 1 (flux-CT) or 2 (modified flux-CT)");
   if (p->metric != 1 && p->metric != 303 && p->metric != 403)
     return fail(RG_EINVAL_CONFIG, "metric must be 1, 303 or 403");
   if (p->ix1 != 1 && p->ix1 != 2) return fail(RG_EINVAL_CONFIG, "ix1 must be 1 or 2");
   if (p->ix2 != 1) return fail(RG_EINVAL_CONFIG, "ix2 must be 1");
   if (p->ix3 != 1 && p->ix3 != 2) return fail(RG_EINVAL_CONFIG, "ix3 must be 1 or 2");
   if (p->precision != RG_FP64 && p->precision != RG_MIXED) return fail(RG_EINVAL_CONFIG, "unknown precision mode");
-  const int nm1 = nm1_of(p->irec);
+  const int nm1 = nm1_of(p);
   if (p->imax <= 2 * nm1 || p->jmax <= 2 * nm1 || p->kmax <= 2 * nm1)
     return fail(RG_EINVAL_CONFIG, "every extent must exceed 2*nm1 (main.f90:247-254)");
   const double n = (double)p->imax * p->jmax * p->kmax;
@@ -185,7 +187,7 @@ bool slab_direction(const rg_run_params* p, int dir, int nm1) {
 int straggler_cap(size_t N) { return (int)std::max<size_t>(1024, std::min<size_t>(N / 64, (size_t)1 << 20)); }
 
 size_t stored_cells(const rg_run_params* p) {
-  const int nm1 = nm1_of(p->irec);
+  const int nm1 = nm1_of(p);
   const bool full = (p->flags & RG_FLAG_FULL) != 0;
   const size_t jpl = (!full && slab_direction(p, 2, nm1)) ? 1 : (size_t)p->jmax;
   const size_t kpl = (!full && slab_direction(p, 3, nm1)) ? 1 : (size_t)p->kmax;
@@ -196,7 +198,7 @@ size_t stored_cells(const rg_run_params* p) {
 // per-routine entry points' full-layout buffers are allocated on first use).
 size_t footprint_bytes(const rg_run_params* p) {
   const size_t N = stored_cells(p);
-  const int nm1 = nm1_of(p->irec);
+  const int nm1 = nm1_of(p);
   const bool kslab = !(p->flags & RG_FLAG_FULL) && slab_direction(p, 3, nm1);
   const size_t nik = (size_t)p->imax * (kslab ? 1 : p->kmax);
   const size_t state = (3 * 9 + 3 * 9 + 6 + 9) * N * sizeof(double);
@@ -500,7 +502,7 @@ void drop_batches(rg_ctx* ctx, int run) {
 // Runs of one batch class share reconstruction, precision and slab class.
 long long batch_class(const Run* R) {
   const DevRun& d = R->d;
-  return (long long)d.irec * 1000 + d.mixed * 100 + (d.jfix ? 10 : 0) + (d.kfix ? 1 : 0);
+  return (long long)d.ict * 100000 + (long long)d.irec * 1000 + d.mixed * 100 + (d.jfix ? 10 : 0) + (d.kfix ? 1 : 0);
 }
 
 int kind_of(const BatchPlan* B, int idx) {
@@ -732,7 +734,7 @@ int rg_prep_create(const rg_run_params* p, rg_prep** out) {
   if (rc) return rc;
   rg_prep* P = new rg_prep();
   P->p = *p;
-  const int nm1 = nm1_of(p->irec);
+  const int nm1 = nm1_of(p);
   const bool full = (p->flags & RG_FLAG_FULL) != 0;
   P->krow = (!full && slab_direction(p, 3, nm1)) ? nm1 + 1 : 0;  // theta slab: one metric row
   P->plane = !full && slab_direction(p, 2, nm1);                   // phi slab: one initial-data plane
@@ -782,7 +784,8 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   DevRun& d = R->d;
   d.imax = p->imax; d.jmax = p->jmax; d.kmax = p->kmax;
   d.nm0 = nm0_of(p->irec);
-  d.nm1 = d.nm0 + 1;
+  d.nm1 = d.nm0 + p->ict;
+  d.ict = p->ict;
   d.irec = p->irec; d.model = p->model; d.guard = p->guard; d.iter = p->iter;
   d.mixed = (p->precision == RG_MIXED);
 #ifdef RG_EXACT_ARITH

@@ -886,7 +886,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_fl
                                               float* __restrict__ Fcopy, int icopy, int ilo, int ihi) { flux_body<D, IREC, T, S>(r, P, F, Fcopy, icopy, ilo, ihi, blockIdx); }
 
 // ---------------------------------------------------------------- flux-CT
-// ct.f90:30-118 on nm1..n-nm1 in every dimension (edges with i in [ilo, ihi]),
+// ct.f90:30-118 (flux-CT, ict 1), ct.f90:121-233 (mflct, ict 2) or none
+// (ict 0) on nm1..n-nm1 in every dimension (edges with i in [ilo, ihi]),
 // in arithmetic type T on flux storage S.  CTcopy, if given, receives an FP32
 // copy (the FP64 edges next to the FP32 region of the mixed path).
 template <typename T, typename S>
@@ -910,6 +911,37 @@ __device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F
   auto L = [](const S* a, size_t x) { return T(a[x]); };
   const T e = T(1.0) / T(8.0), two = T(2.0);
   T o[6];
+  if (r.ict == 0) {  // no constrained transport: the induction fluxes stay as hll left them
+    o[0] = L(fyx, c); o[1] = L(fzx, c); o[2] = L(fxy, c); o[3] = L(fzy, c); o[4] = L(fxz, c); o[5] = L(fyz, c);
+  } else if (r.ict == 2) {
+    // mflct (ct.f90:121-233): the cell-centred EMFs of its second pass
+    // (ct.f90:174-176), evaluated where the corner formulas need them, and
+    // the flux-CT brackets with weight 1/4 plus the averaged EMFs (ct.f90:191-224)
+    const T q = T(0.25), h = T(1.0) / T(8.0);
+    auto ez = [&](size_t x) { return q * (-L(fxy, x - di) - L(fxy, x) + L(fyx, x - dj) + L(fyx, x)); };
+    auto ex = [&](size_t x) { return q * (-L(fyz, x - dj) - L(fyz, x) + L(fzy, x - dk) + L(fzy, x)); };
+    auto ey = [&](size_t x) { return q * (-L(fzx, x - dk) - L(fzx, x) + L(fxz, x - di) + L(fxz, x)); };
+    const T fbyx = q * (two * L(fyx, c) + L(fyx, c + di) + L(fyx, c - di) - L(fxy, c) - L(fxy, c + dj) -
+                        L(fxy, c - di) - L(fxy, c - di + dj));
+    const T fbzx = q * (two * L(fzx, c) + L(fzx, c + di) + L(fzx, c - di) - L(fxz, c) - L(fxz, c + dk) -
+                        L(fxz, c - di) - L(fxz, c - di + dk));
+    const T fbxy = q * (two * L(fxy, c) + L(fxy, c + dj) + L(fxy, c - dj) - L(fyx, c) - L(fyx, c + di) -
+                        L(fyx, c - dj) - L(fyx, c + di - dj));
+    const T fbzy = q * (two * L(fzy, c) + L(fzy, c + dj) + L(fzy, c - dj) - L(fyz, c) - L(fyz, c + dk) -
+                        L(fyz, c - dj) - L(fyz, c - dj + dk));
+    const T fbxz = q * (two * L(fxz, c) + L(fxz, c + dk) + L(fxz, c - dk) - L(fzx, c) - L(fzx, c + di) -
+                        L(fzx, c - dk) - L(fzx, c + di - dk));
+    const T fbyz = q * (two * L(fyz, c) + L(fyz, c + dk) + L(fyz, c - dk) - L(fzy, c) - L(fzy, c + dj) -
+                        L(fzy, c - dk) - L(fzy, c + dj - dk));
+    const T fhyx = -(h * (two * ez(c) + two * ez(c + dj) + ez(c + di) + ez(c + di + dj) + ez(c - di) + ez(c - di + dj)));
+    const T fhzx = h * (two * ey(c) + two * ey(c + dk) + ey(c + di) + ey(c + di + dk) + ey(c - di) + ey(c - di + dk));
+    const T fhxy = h * (two * ez(c) + two * ez(c + di) + ez(c + dj) + ez(c + di + dj) + ez(c - dj) + ez(c + di - dj));
+    const T fhzy = -(h * (two * ex(c) + two * ex(c + dk) + ex(c + dj) + ex(c + dj + dk) + ex(c - dj) + ex(c - dj + dk)));
+    const T fhxz = -(h * (two * ey(c) + two * ey(c + di) + ey(c + dk) + ey(c + di + dk) + ey(c - dk) + ey(c + di - dk)));
+    const T fhyz = h * (two * ex(c) + two * ex(c + dj) + ex(c + dk) + ex(c + dj + dk) + ex(c - dk) + ex(c + dj - dk));
+    o[0] = fbyx + fhyx; o[1] = fbzx + fhzx; o[2] = fbxy + fhxy;
+    o[3] = fbzy + fhzy; o[4] = fbxz + fhxz; o[5] = fbyz + fhyz;
+  } else {
   o[0] = e * (two * L(fyx, c) + L(fyx, c + di) + L(fyx, c - di) - L(fxy, c) - L(fxy, c + dj) - L(fxy, c - di) -
               L(fxy, c - di + dj));
   o[1] = e * (two * L(fzx, c) + L(fzx, c + di) + L(fzx, c - di) - L(fxz, c) - L(fxz, c + dk) - L(fxz, c - di) -
@@ -922,6 +954,7 @@ __device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F
               L(fzx, c + di - dk));
   o[5] = e * (two * L(fyz, c) + L(fyz, c + dk) + L(fyz, c - dk) - L(fzy, c) - L(fzy, c + dj) - L(fzy, c - dk) -
               L(fzy, c + dj - dk));
+  }
 #pragma unroll
   for (int a = 0; a < 6; ++a) {
     CT[(size_t)a * N + c] = S(o[a]);

@@ -42,6 +42,14 @@ def test_footprint_and_param_checks_run_on_cpu():
         assert footprint(dict(p, irec=irec)) > 0
     for irec in (config.IREC_CENO, config.IREC_MPWENO, config.IREC_WENOM):
         assert footprint(dict(p, irec=irec)) > 0
+    for ict in (0, 2):
+        assert footprint(dict(p, ict=ict)) > 0
+    try:
+        footprint(dict(p, ict=3))  # upflct: not built
+    except RgError as e:
+        assert e.code == 1
+    else:
+        raise AssertionError("ict=3 must be rejected")
     bad = dict(p, irec=14)  # no such scheme
     try:
         footprint(bad)

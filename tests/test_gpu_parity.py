@@ -4,7 +4,7 @@ Tolerance: the FP64 kernels keep the reference's evaluation order; the
 product build contracts multiply-adds into FMA and evaluates x**(4/3) and
 x**(5/3) through cbrt, so results differ from the oracle in the last bits.
 Per-routine results must agree to 1e-12 of each field's maximum (relative
-L-infinity per variable); one full RK3 step likewise (the north-star bound of
+L-infinity per variable); one full RK3 step likewise (the parity bound of
 1e-12 per step).
 """
 import numpy as np
@@ -425,3 +425,34 @@ def test_per_routine_calls_leave_the_run_alone(gpu_ctx):
     assert np.array_equal(a.prims(), b.prims())
     a.release()
     b.release()
+
+
+@pytest.mark.parametrize("ict", [0, 2])
+def test_constrained_transport_variants(gpu_ctx, ict):
+    """ict = 0 (no CT) and ict = 2 (mflct, ct.f90:121-233): fluxes through
+    the C ABI and one full step per comparison against the oracle, 3D torus;
+    ghost width nm1 = nm0 + ict."""
+    p = dict(config.torus(nr=40, nth=28, nph=20, ict=ict), guard=1)
+    o, r = _pair(gpu_ctx, p, seed=40 + ict)
+    assert o.nm1 == 3 + ict
+    u = o.prims()
+    wg, wo = r.calflx(u), o.fluxes(u)
+    n = o.nm1 - 1
+    reg = (slice(n, -n), slice(n, -n), slice(n, -n))
+    assert flux_err(wg[reg], wo[reg]).max() < TOL
+    o.init_cons()
+    for _ in range(2):
+        o.step(1)
+        r.step(1)
+        err = _vector_scaled_err(r.prims(), o.prims())
+        assert err.max() < TOL, err
+        r.upload_prims(o.prims(), t0=o.time)
+    r.release()
+
+
+def test_mflct_2d_slab(gpu_ctx):
+    """mflct on a 2D phi slab (stored as one plane, batched path) against the
+    oracle computing every phi cell."""
+    p = dict(config.torus(nr=48, nth=40, ict=2), guard=1)
+    errs, _ = _step_err(gpu_ctx, p, 2, seed=23)
+    assert errs.max() < TOL, errs

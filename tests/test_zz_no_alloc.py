@@ -26,7 +26,7 @@ def test_calflx_static_matches_calflx_two_calls():
 
     p = dict(config.torus(nr=48, nth=40, nph=12), guard=1)
     N = p["imax"] * p["jmax"] * p["kmax"]
-    nm0, _ = config.ghost_widths(p["irec"])
+    nm0, _ = config.ghost_widths(p["irec"], p.get("ict", 1))
     reg = (slice(nm0, -nm0),) * 3  # inside the hll range (1-based nm0..n-nm0)
     states = []
     for seed in (21, 22):
