@@ -61,14 +61,15 @@ struct FluxB {
   }
 };
 
-template <typename T, typename S>
+template <int ICT, typename T, typename S>
 struct CtB {
   __device__ void operator()(const DevRun& r, const Tile& t) const {
     if constexpr (sizeof(S) == 8)
-      ct_body<T, S>(r, r.F[0], r.F[1], r.F[2], r.CT, r.mixed ? r.CT32 : nullptr, t.ilo, t.ihi,
-                    make_uint3(t.bx, t.by, t.bz));
+      ct_body<ICT, T, S>(r, r.F[0], r.F[1], r.F[2], r.CT, r.mixed ? r.CT32 : nullptr, t.ilo, t.ihi,
+                         make_uint3(t.bx, t.by, t.bz));
     else
-      ct_body<T, S>(r, r.F32[0], r.F32[1], r.F32[2], r.CT32, nullptr, t.ilo, t.ihi, make_uint3(t.bx, t.by, t.bz));
+      ct_body<ICT, T, S>(r, r.F32[0], r.F32[1], r.F32[2], r.CT32, nullptr, t.ilo, t.ihi,
+                         make_uint3(t.bx, t.by, t.bz));
   }
 };
 
@@ -158,6 +159,7 @@ struct BLaunch {
 struct BatchPlan {
   int nruns = 0;
   int irec = 6;
+  int ict = 1;
   int width = 128;            // threads per block of the cell kernels
   DevRun* d_runs = nullptr;
   Tile* d_tiles = nullptr;
@@ -198,6 +200,7 @@ int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
   BatchPlan* B = new BatchPlan();
   B->nruns = (int)runs.size();
   B->irec = runs.empty() ? 6 : runs[0].irec;
+  B->ict = runs.empty() ? 1 : runs[0].ict;
   B->width = width;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -434,7 +437,11 @@ cudaError_t batch_issue(const BatchPlan* B, int idx, cudaStream_t s) {
     case BK_FLUX:
       return L.fp32 ? go_flux_dir<float, float>(B, L, s) : go_flux_dir<double, double>(B, L, s);
     case BK_CT:
-      return L.fp32 ? go_cell(B, L, CtB<float, float>{}, s) : go_cell(B, L, CtB<double, double>{}, s);
+      if (B->ict == 0)
+        return L.fp32 ? go_cell(B, L, CtB<0, float, float>{}, s) : go_cell(B, L, CtB<0, double, double>{}, s);
+      if (B->ict == 2)
+        return L.fp32 ? go_cell(B, L, CtB<2, float, float>{}, s) : go_cell(B, L, CtB<2, double, double>{}, s);
+      return L.fp32 ? go_cell(B, L, CtB<1, float, float>{}, s) : go_cell(B, L, CtB<1, double, double>{}, s);
     case BK_UPDATE:
       if (L.stage == 1) return L.fp32 ? go_update<1, true>(B, L, s) : go_update<1, false>(B, L, s);
       if (L.stage == 2) return L.fp32 ? go_update<2, true>(B, L, s) : go_update<2, false>(B, L, s);

@@ -890,7 +890,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_fl
 // (ict 0) on nm1..n-nm1 in every dimension (edges with i in [ilo, ihi]),
 // in arithmetic type T on flux storage S.  CTcopy, if given, receives an FP32
 // copy (the FP64 edges next to the FP32 region of the mixed path).
-template <typename T, typename S>
+template <int ICT, typename T, typename S>
 __device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F1, const S* __restrict__ F2,
                                             const S* __restrict__ F3, S* __restrict__ CT,
                                             float* __restrict__ CTcopy, int ilo, int ihi, const uint3 bid) {
@@ -911,9 +911,9 @@ __device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F
   auto L = [](const S* a, size_t x) { return T(a[x]); };
   const T e = T(1.0) / T(8.0), two = T(2.0);
   T o[6];
-  if (r.ict == 0) {  // no constrained transport: the induction fluxes stay as hll left them
+  if (ICT == 0) {  // no constrained transport: the induction fluxes stay as hll left them
     o[0] = L(fyx, c); o[1] = L(fzx, c); o[2] = L(fxy, c); o[3] = L(fzy, c); o[4] = L(fxz, c); o[5] = L(fyz, c);
-  } else if (r.ict == 2) {
+  } else if (ICT == 2) {
     // mflct (ct.f90:121-233): the cell-centred EMFs of its second pass
     // (ct.f90:174-176), evaluated where the corner formulas need them, and
     // the flux-CT brackets with weight 1/4 plus the averaged EMFs (ct.f90:191-224)
@@ -961,10 +961,10 @@ __device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F
     if (CTcopy) CTcopy[(size_t)a * N + c] = float(o[a]);
   }
 }
-template <typename T, typename S>
+template <int ICT, typename T, typename S>
 __global__ void __launch_bounds__(256) k_ct(DevRun r, const S* __restrict__ F1, const S* __restrict__ F2,
                                             const S* __restrict__ F3, S* __restrict__ CT,
-                                            float* __restrict__ CTcopy, int ilo, int ihi) { ct_body<T, S>(r, F1, F2, F3, CT, CTcopy, ilo, ihi, blockIdx); }
+                                            float* __restrict__ CTcopy, int ilo, int ihi) { ct_body<ICT, T, S>(r, F1, F2, F3, CT, CTcopy, ilo, ihi, blockIdx); }
 
 // ------------------------------------------------------------ boundaries
 // Transverse indices of a column of direction D: (j,k) for D = 1, (i,k) for
@@ -1588,20 +1588,29 @@ cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cu
   return cudaGetLastError();
 }
 
-cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
-                      cudaStream_t s) {
+template <int ICT>
+static void launch_ct_t(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
+                        cudaStream_t s) {
   const int lo = r.nm1, hi = r.imax - r.nm1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
   const dim3 b = sblock(r, dim3(64, 4, 1));
   if (!r.mixed) {
-    k_ct<double, double><<<sgrid(r, hi - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, nullptr, lo, hi);
+    k_ct<ICT, double, double><<<sgrid(r, hi - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, nullptr, lo, hi);
   } else {
     const int split = fp64_split(r, lo, hi);
     if (split >= lo)
-      k_ct<double, double><<<sgrid(r, split - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, r.CT32, lo, split);
+      k_ct<ICT, double, double><<<sgrid(r, split - lo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, r.CT32, lo,
+                                                                                  split);
     if (split < hi)
-      k_ct<float, float><<<sgrid(r, hi - split, m, l, b), b, 0, s>>>(r, r.F32[0], r.F32[1], r.F32[2], r.CT32,
-                                                                         nullptr, split + 1, hi);
+      k_ct<ICT, float, float><<<sgrid(r, hi - split, m, l, b), b, 0, s>>>(r, r.F32[0], r.F32[1], r.F32[2],
+                                                                              r.CT32, nullptr, split + 1, hi);
   }
+}
+
+cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
+                      cudaStream_t s) {
+  if (r.ict == 0) launch_ct_t<0>(r, F1, F2, F3, CT, s);
+  else if (r.ict == 2) launch_ct_t<2>(r, F1, F2, F3, CT, s);
+  else launch_ct_t<1>(r, F1, F2, F3, CT, s);
   return cudaGetLastError();
 }
 
