@@ -299,20 +299,35 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
 // S_nu = sqrt(-g) sum_{n,m} T^m_n Gamma^n_{nu m} of one cell from its
 // 4-vectors and the Christoffel cache at metric point q, summed in the
 // reference's (n, m) order; sf[0..3] = sf(2:5) (nu = 1, 2, 3, 0).
+// The cache holds Gamma^l_{mn} at l + 4m + 16n, symmetric in (m, n) bit for
+// bit (the geometry builds it from a symmetric metric), so the 40 distinct
+// values of a point are loaded and the 64-term sum reads them in the
+// reference's order.
+template <typename T>
+__device__ __forceinline__ void load_christ_row(const T* __restrict__ chr, size_t nik, size_t q, int n, T g[4][4]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = a; b < 4; ++b) g[a][b] = g[b][a] = __ldg(chr + (size_t)(n + 4 * a + 16 * b) * nik + q);
+}
+
 __device__ __forceinline__ void geom_source(const DevRun& r, const PS& s, size_t q, double detg, double sf[4]) {
   const double a = s.roh + s.bbsq, b = s.pr + 0.5 * s.bbsq;
   double ta = 0.0, tb = 0.0, tc = 0.0, td = 0.0;
   const size_t nik = r.nik;
 #pragma unroll
-  for (int n = 0; n < 4; ++n)
+  for (int n = 0; n < 4; ++n) {
+    double g[4][4];  // g[nu][m] = Gamma^n_{nu m}
+    load_christ_row(r.chr, nik, q, n, g);
 #pragma unroll
     for (int mm = 0; mm < 4; ++mm) {
       const double t = a * s.ucon[mm] * s.ucov[n] + b * (mm == n ? 1.0 : 0.0) - s.bbcon[mm] * s.bbcov[n];
-      ta = ta + t * __ldg(r.chr + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
-      tb = tb + t * __ldg(r.chr + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
-      tc = tc + t * __ldg(r.chr + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
-      td = td + t * __ldg(r.chr + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
+      ta = ta + t * g[1][mm];
+      tb = tb + t * g[2][mm];
+      tc = tc + t * g[3][mm];
+      td = td + t * g[0][mm];
     }
+  }
   sf[0] = detg * ta; sf[1] = detg * tb; sf[2] = detg * tc; sf[3] = detg * td;
 }
 
@@ -438,15 +453,18 @@ __device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met&
     }
     float ta = 0.f, tb = 0.f, tc = 0.f, td = 0.f;
 #pragma unroll
-    for (int n = 0; n < 4; ++n)
+    for (int n = 0; n < 4; ++n) {
+      float g[4][4];
+      load_christ_row(r.chr32, nik, q, n, g);
 #pragma unroll
       for (int mm = 0; mm < 4; ++mm) {
         const float t = a * uc[mm] * ul[n] + (mm == n ? b : 0.f) - bc[mm] * bl[n];
-        ta = ta + t * __ldg(r.chr32 + (size_t)(n + 4 * 1 + 16 * mm) * nik + q);
-        tb = tb + t * __ldg(r.chr32 + (size_t)(n + 4 * 2 + 16 * mm) * nik + q);
-        tc = tc + t * __ldg(r.chr32 + (size_t)(n + 4 * 3 + 16 * mm) * nik + q);
-        td = td + t * __ldg(r.chr32 + (size_t)(n + 4 * 0 + 16 * mm) * nik + q);
+        ta = ta + t * g[1][mm];
+        tb = tb + t * g[2][mm];
+        tc = tc + t * g[3][mm];
+        td = td + t * g[0][mm];
       }
+    }
     const float dg = (float)m.detg;
     sf[0] = dg * ta; sf[1] = dg * tb; sf[2] = dg * tc; sf[3] = dg * td;
   }
@@ -1614,12 +1632,17 @@ cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const
   return cudaGetLastError();
 }
 
+#ifndef RG_UPD_BX
+#define RG_UPD_BX 64
+#define RG_UPD_BY 2
+#define RG_UPD_BZ 1
+#endif
 template <bool MIX>
 static void launch_update_t(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                             const double* F1, const double* F2, const double* F3, const double* CT, int ilo,
                             int ihi, cudaStream_t s) {
   if (ihi < ilo) return;
-  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 b = sblock(r, dim3(RG_UPD_BX, RG_UPD_BY, RG_UPD_BZ));
   const dim3 g = sgrid(r, ihi - ilo + 1, r.jmax, r.kmax, b);
   if (stage == 1) k_update<1, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
   else if (stage == 2) k_update<2, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);

@@ -362,3 +362,12 @@ def test_mpweno_radial_right_state_reads_i_minus_11():
     assert rows == {(6, 6)}, rows
     assert 14 in set(changed[:, 2])  # zero-based i of stored index 15
 
+
+
+def test_christoffel_table_is_symmetric_in_its_lower_indices(torus_small):
+    """Gamma^l_{mn} is stored at l + 4m + 16n; the geometry builds it from a
+    symmetric metric, so the table is symmetric in (m, n) bit for bit, which
+    the device's source term relies on to load each pair once."""
+    _, o = torus_small
+    c = o.array("christ").reshape(-1, 4, 4, 4)  # [point][n][m][l]
+    assert np.array_equal(c, np.swapaxes(c, 1, 2))
