@@ -1632,17 +1632,12 @@ cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const
   return cudaGetLastError();
 }
 
-#ifndef RG_UPD_BX
-#define RG_UPD_BX 64
-#define RG_UPD_BY 2
-#define RG_UPD_BZ 1
-#endif
 template <bool MIX>
 static void launch_update_t(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                             const double* F1, const double* F2, const double* F3, const double* CT, int ilo,
                             int ihi, cudaStream_t s) {
   if (ihi < ilo) return;
-  const dim3 b = sblock(r, dim3(RG_UPD_BX, RG_UPD_BY, RG_UPD_BZ));
+  const dim3 b = sblock(r, dim3(64, 2, 1));
   const dim3 g = sgrid(r, ihi - ilo + 1, r.jmax, r.kmax, b);
   if (stage == 1) k_update<1, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
   else if (stage == 2) k_update<2, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
