@@ -93,6 +93,14 @@ const char* rg_last_error(void);
 int rg_ctx_create(int device, rg_ctx** out);
 int rg_ctx_destroy(rg_ctx* ctx);
 int rg_sync(rg_ctx* ctx);
+/* Marks on the context stream, for a host that keeps work queued while it
+ * prepares more: rg_ctx_mark records a point in the stream in slot
+ * 0..RG_MAX_MARKS-1 (re-marking a slot moves it); rg_ctx_wait_mark blocks
+ * until the work before the mark has completed (block != 0) or only reports
+ * it in *done (block = 0).  No counterpart in the reference. */
+#define RG_MAX_MARKS 8
+int rg_ctx_mark(rg_ctx* ctx, int slot);
+int rg_ctx_wait_mark(rg_ctx* ctx, int slot, int block, int* done);
 /* Run all later work of ctx on a caller-owned cudaStream_t (passed as void*) of
  * the same device, e.g. the stream of an enclosing framework; the context
  * then no longer owns or destroys a stream. */

@@ -25,7 +25,8 @@ STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA"
           5: "RG_ENAN", 6: "RG_ENOTFOUND", 7: "RG_EOVERFLOW"}
 
 #: every entry point include/raishin_gpu.h declares
-EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
+EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_mark", "rg_ctx_wait_mark",
+           "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
            "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
@@ -88,6 +89,8 @@ def load(path: str = LIB_PATH):
     lib.rg_ctx_create.argtypes = [I, C.POINTER(C.c_void_p)]
     lib.rg_ctx_destroy.argtypes = [P]
     lib.rg_sync.argtypes = [P]
+    lib.rg_ctx_mark.argtypes = [P, I]
+    lib.rg_ctx_wait_mark.argtypes = [P, I, I, C.POINTER(C.c_int)]
     lib.rg_ctx_set_stream.argtypes = [P, P]
     lib.rg_run_admit.argtypes = [P, C.POINTER(RunParams), C.POINTER(C.c_int)]
     lib.rg_run_release.argtypes = [P, I]
@@ -180,6 +183,16 @@ class Context:
 
     def sync(self):
         _check(self.lib, self.lib.rg_sync(self.h))
+
+    def mark(self, slot: int):
+        """Record a point of the context stream in slot 0..7 (rg_ctx_mark)."""
+        _check(self.lib, self.lib.rg_ctx_mark(self.h, slot))
+
+    def wait_mark(self, slot: int, block: bool = True) -> bool:
+        """True once the work before the mark has completed (blocking by default)."""
+        done = C.c_int(0)
+        _check(self.lib, self.lib.rg_ctx_wait_mark(self.h, slot, int(block), C.byref(done)))
+        return bool(done.value)
 
     def set_stream(self, stream_handle: int):
         """Issue all later work on a caller-owned cudaStream_t (e.g. torch's current stream)."""

@@ -94,6 +94,7 @@ struct rg_ctx {
   std::vector<cudaEvent_t> pool;
   double ms[K_NKINDS] = {};
   bool own_stream = true;              // false after rg_ctx_set_stream
+  cudaEvent_t marks[RG_MAX_MARKS] = {};  // rg_ctx_mark / rg_ctx_wait_mark
 };
 
 namespace {
@@ -701,6 +702,8 @@ int rg_ctx_destroy(rg_ctx* ctx) {
   for (auto& kv : ctx->runs) free_run(kv.second);
   for (auto& pe : ctx->pending) ctx->pool.push_back(pe.second.first), ctx->pool.push_back(pe.second.second);
   for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->marks)
+    if (e) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return RG_OK;
@@ -718,6 +721,37 @@ int rg_ctx_set_stream(rg_ctx* ctx, void* stream) {
 int rg_sync(rg_ctx* ctx) {
   if (!ctx) return fail(RG_EINVAL_CONFIG, "null context");
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+int rg_ctx_mark(rg_ctx* ctx, int slot) {
+  if (!ctx) return fail(RG_EINVAL_CONFIG, "null context");
+  if (slot < 0 || slot >= RG_MAX_MARKS) return fail(RG_EINVAL_CONFIG, "mark slot out of range");
+  if (!ctx->marks[slot]) RG_CUDA(cudaEventCreateWithFlags(&ctx->marks[slot], cudaEventDisableTiming));
+  RG_CUDA(cudaEventRecord(ctx->marks[slot], ctx->stream));
+  return RG_OK;
+}
+
+int rg_ctx_wait_mark(rg_ctx* ctx, int slot, int block, int* done) {
+  if (!ctx) return fail(RG_EINVAL_CONFIG, "null context");
+  if (slot < 0 || slot >= RG_MAX_MARKS) return fail(RG_EINVAL_CONFIG, "mark slot out of range");
+  if (!ctx->marks[slot]) {  // never marked: nothing to wait for
+    if (done) *done = 1;
+    return RG_OK;
+  }
+  if (block) {
+    RG_CUDA(cudaEventSynchronize(ctx->marks[slot]));
+    if (done) *done = 1;
+    return RG_OK;
+  }
+  const cudaError_t e = cudaEventQuery(ctx->marks[slot]);
+  if (e == cudaErrorNotReady) {
+    (void)cudaGetLastError();
+    if (done) *done = 0;
+    return RG_OK;
+  }
+  RG_CUDA(e);
+  if (done) *done = 1;
   return RG_OK;
 }
 

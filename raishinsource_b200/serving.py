@@ -15,14 +15,17 @@ one context:
 * stepping: all resident runs advance together in ticks of ``tick_steps``
   steps through ``rg_step_batch`` (one launch per kernel kind and batch class,
   replayed from a CUDA graph), so a request that arrives while others are on
-  the GPU joins the next tick and its work overlaps theirs;
-* completion: a run that has taken its steps is read back, released, and its
-  memory and slot go to the waiting requests.
+  the GPU joins the next tick and its work overlaps theirs.  Two ticks are
+  kept queued on the stream (``rg_ctx_mark`` / ``rg_ctx_wait_mark``), so the
+  GPU keeps stepping while the host admits and retires runs;
+* completion: a run leaves the batch with the tick that takes its last steps;
+  once that tick has completed it is read back, released, and its memory and
+  slot go to the waiting requests.
 
 Each run's result is the same alone and in the mix (the batched kernels run
 every run's cells through the single-run code); ``tests/test_gpu_serving.py``
-checks this.  Latency is measured from arrival to the end of the tick in which
-the run finished, on the host clock after a device synchronisation.
+checks this.  Latency is measured from arrival to the moment the host has
+seen the completion of the tick in which the run finished.
 """
 from __future__ import annotations
 
@@ -106,10 +109,23 @@ class Server:
         nxt = 0                                  # next request to arrive
         waiting: list[tuple[Request, cf.Future, int]] = []
         active = []                              # [req, run, steps_done, admitted_at, bytes]
+        finishing: dict[int, list] = {}          # tick -> runs that took their last steps in it
         used = 0
         done: list[Done] = []
         ticks = 0
-        busy = 0.0
+        depth = 2                                # ticks in flight on the stream
+
+        def retire(tick: int):
+            # the tick has completed on the device: its finished runs are read back and released
+            nonlocal used
+            fin = clock() - t0
+            for r, run, steps, admitted, nbytes in finishing.pop(tick, []):
+                prims = run.prims() if self.keep_prims else None
+                done.append(Done(r.rid, r.arrival, admitted, fin, config.interior_cells(r.params), steps,
+                                 r.params.get("precision", "fp64"), prims))
+                run.release()
+                used -= nbytes
+
         while len(done) < len(reqs):
             now = clock() - t0
             if now > max_wall_s:
@@ -133,29 +149,30 @@ class Server:
                 used += nbytes
                 waiting.remove(item)
             if not active:
+                if finishing:                    # drain: the last ticks complete
+                    for t in sorted(finishing):
+                        self.ctx.wait_mark(t % depth)
+                        retire(t)
+                    continue
                 # idle: wait for the next arrival or a preparation
                 if waiting:
                     cf.wait([f for _, f, _ in waiting], timeout=0.01, return_when=cf.FIRST_COMPLETED)
                 elif nxt < len(reqs):
                     time.sleep(max(0.0, min(0.01, reqs[nxt].arrival - (clock() - t0))))
                 continue
+            # at most `depth` ticks in flight: the tick that last used this mark slot completes first
+            if ticks >= depth:
+                self.ctx.wait_mark(ticks % depth)
+                retire(ticks - depth)
             n = min(self.tick_steps, min(a[0].steps - a[2] for a in active))
-            ts = clock()
             self.ctx.step_batch([a[1] for a in active], n)
-            self.ctx.sync()
-            busy += clock() - ts
-            ticks += 1
-            fin = clock() - t0
+            self.ctx.mark(ticks % depth)
             for a in list(active):
                 a[2] += n
                 if a[2] >= a[0].steps:
-                    r, run = a[0], a[1]
-                    prims = run.prims() if self.keep_prims else None
-                    done.append(Done(r.rid, r.arrival, a[3], fin, config.interior_cells(r.params), a[2],
-                                     r.params.get("precision", "fp64"), prims))
-                    run.release()
-                    used -= a[4]
+                    finishing.setdefault(ticks, []).append(tuple(a))
                     active.remove(a)
+            ticks += 1
         wall = clock() - t0
         lat = np.array([d.latency for d in done])
         zones = sum(d.zones * d.steps for d in done)
@@ -167,8 +184,8 @@ class Server:
             "wall_s": wall,
             "zone_updates": zones,
             "zone_updates_per_s": zones / wall,
-            "zone_updates_per_gpu_busy_s": zones / busy if busy > 0 else math.nan,
             "ticks": ticks,
+            "ticks_in_flight": depth,
             "done": done,
         }
 

@@ -51,3 +51,20 @@ def test_admission_respects_budget(gpu_ctx):
     for a, b in zip(done, done[1:]):
         assert b.admitted >= a.finished
     assert out["ticks"] == len(reqs)
+
+
+def test_stream_marks(gpu_ctx):
+    """rg_ctx_mark / rg_ctx_wait_mark: a mark after queued steps completes,
+    an unused slot reports completion, an out-of-range slot is refused."""
+    from raishinsource_b200.capi import RgError
+    p = config.torus(nr=64, nth=64)
+    r = gpu_ctx.admit(p)
+    r.ic_torus(seed=5)
+    gpu_ctx.step_batch([r], 20)
+    gpu_ctx.mark(3)
+    assert gpu_ctx.wait_mark(3) is True
+    assert gpu_ctx.wait_mark(3, block=False) is True
+    assert gpu_ctx.wait_mark(5, block=False) is True
+    with pytest.raises(RgError):
+        gpu_ctx.mark(8)
+    r.release()
