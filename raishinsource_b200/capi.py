@@ -330,9 +330,13 @@ class Run:
         _check(self.lib, self.lib.rg_run_download_prims(self.ctx.h, self.id, C.c_void_p(host_ptr)))
 
     # time stepping
-    def step(self, n: int = 1, stats: bool = False):
+    def step(self, n: int = 1, stats: bool = False, strict: bool = True):
+        """Advance the run n steps (rg_step).  With strict=False a capped
+        rescale loop (RG_ENR_CAP, counted in the stats) does not raise."""
         st = StepStats()
-        _check(self.lib, self.lib.rg_step(self.ctx.h, self.id, int(n), C.byref(st) if stats else None))
+        rc = self.lib.rg_step(self.ctx.h, self.id, int(n), C.byref(st) if stats else None)
+        if not (rc == 4 and not strict):
+            _check(self.lib, rc)
         return st.as_dict() if stats else None
 
     def stats(self) -> dict:

@@ -456,3 +456,30 @@ def test_mflct_2d_slab(gpu_ctx):
     p = dict(config.torus(nr=48, nth=40, ict=2), guard=1)
     errs, _ = _step_err(gpu_ctx, p, 2, seed=23)
     assert errs.max() < TOL, errs
+
+
+def test_kerr_schild_metric(gpu_ctx):
+    """Metric 303 (Kerr-Schild on uniform r and theta grids): initial data,
+    two steps against the oracle (including the cells whose W rescale loop
+    hits its cap, counted alike in the first step) and the converter's derived
+    quantities."""
+    p = dict(config.torus(nr=48, nth=40, nph=12), metric=303, ix1=1, ix3=1, guard=1, xmax=30.0)
+    o = Oracle(p)
+    o.ic_torus(seed=3)
+    r = gpu_ctx.admit(p)
+    r.ic_torus(seed=3)
+    assert field_err(r.prims(), o.prims()).max() < 1e-13
+    o.init_cons()
+    for n in range(2):
+        o.step(1)
+        st = r.step(1, stats=True, strict=False)
+        if n == 0:
+            ost = o.stats()
+            assert (st["recov_cap"], st["recov_nr2"]) == (ost["recov_cap"], ost["recov_nr2"])
+        err = _vector_scaled_err(r.prims(), o.prims())
+        assert err.max() < TOL, err
+        r.upload_prims(o.prims(), t0=o.time)
+    u = o.prims()
+    err = _derived_err(r.derived(), o.derived(u))
+    assert err.max() < TOL, err
+    r.release()
