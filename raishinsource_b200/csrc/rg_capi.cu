@@ -119,10 +119,8 @@ void free_run(Run* R) {
 // Ghost widths of the reconstruction (main.f90:179-190): nm0 = 2 for the
 // second-order schemes, 3 for the five-point schemes, 4 for PPM; constrained
 // transport adds ict layers, nm1 = nm0 + ict (main.f90:192-199).
-int nm0_of(int irec) {
-  return (irec == 1 || irec == 2 || irec == 3 || irec == 11 || irec == 12 || irec == 13) ? 2 : (irec == 5 ? 4 : 3);
-}
-int nm1_of(const rg_run_params* p) { return nm0_of(p->irec) + p->ict; }
+int nm0_of(int irec) { return ghost_nm0(irec); }
+int nm1_of(const rg_run_params* p) { return ghost_nm1(*p); }
 
 int check_params(const rg_run_params* p) {
   if (!p) return fail(RG_EINVAL_CONFIG, "null parameters");

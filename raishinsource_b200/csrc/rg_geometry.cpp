@@ -503,7 +503,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
   // Every phi plane of the torus is the same except for the perturbation,
   // which a 2D phi slab keys by its interior plane: a run that stores the slab
   // as one plane needs only that plane (the others stay zero).
-  const int nm1_pl = (p.irec == 5) ? 5 : 4;
+  const int nm1_pl = ghost_nm1(p);
   const int jlo = plane_only ? nm1_pl + 1 : 1, jhi = plane_only ? nm1_pl + 1 : jmax;
   const size_t N = (size_t)imax * jmax * kmax, nik = G.nik;
   const double gam = p.gam, a = p.akm;
@@ -585,7 +585,7 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
   // normalise rho_max to 1, perturb p (mdgrmhd.f90:1198-1320).  In a 2D phi
   // slab (jmax = 2*nm1+1) the draw is keyed by the (r, theta) cell of the
   // interior phi index, so that the slab holds one axisymmetric state.
-  const int nm1_ic = (p.irec == 5) ? 5 : 4;
+  const int nm1_ic = ghost_nm1(p);
   const bool phi_slab = (jmax == 2 * nm1_ic + 1);
   for (int k = 1; k <= kmax; ++k)
     for (int j = jlo; j <= jhi; ++j)

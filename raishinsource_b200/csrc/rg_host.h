@@ -24,6 +24,14 @@ struct HostGeom {
 };
 
 // krow > 0 computes the single theta row krow (theta slab in Minkowski space).
+// Ghost widths (main.f90:179-199): nm0 = 2 for the second-order schemes
+// (irec 1-3, 11-13), 3 for the five-point schemes, 4 for PPM; constrained
+// transport adds ict layers.
+inline int ghost_nm0(int irec) {
+  return (irec == 1 || irec == 2 || irec == 3 || irec == 11 || irec == 12 || irec == 13) ? 2 : (irec == 5 ? 4 : 3);
+}
+inline int ghost_nm1(const rg_run_params& p) { return ghost_nm0(p.irec) + p.ict; }
+
 void build_geometry(const rg_run_params& p, HostGeom& g, int krow = 0);
 
 // mdtorus1 (mdgrmhd.f90:879-1654) into SoA primitives prim[v*N + c].

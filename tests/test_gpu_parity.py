@@ -66,6 +66,21 @@ def test_ic_torus_matches_oracle(gpu_ctx):
     assert err.max() < 1e-13, err
 
 
+@pytest.mark.parametrize("irec,ict,nph", [(config.IREC_MC, 1, None), (config.IREC_PPM, 1, None),
+                                          (config.IREC_MP5, 2, None), (config.IREC_MC, 0, 12)])
+def test_ic_torus_ghost_widths(gpu_ctx, irec, ict, nph):
+    """Device-side torus initial data for every ghost width nm1 = nm0 + ict: 2D
+    phi slabs (stored as one plane, jmax = 2*nm1+1) and a 3D run."""
+    p = config.torus(nr=48, nth=40, nph=nph, irec=irec, ict=ict)
+    o = Oracle(p)
+    o.ic_torus(seed=61)
+    r = gpu_ctx.admit(p)
+    r.ic_torus(seed=61)
+    err = field_err(r.prims(), o.prims())
+    r.release()
+    assert err.max() < 1e-13, err
+
+
 def test_caluu1(torus2d):
     _, o, r = torus2d
     u = o.prims()
