@@ -61,7 +61,35 @@ BYTES_PER_UNIT = {"flux_r": 136, "flux_phi": 136, "flux_theta": 136, "update": 4
                   "floors": 120, "cfl": 72}
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one launch divided by
 # its units) on the 192x96x96 torus, whose state already exceeds the L2
-DRAM_BYTES_PER_UNIT = {"update": 471.0, "flux_r": 113.0, "flux_phi": 120.0, "flux_theta": 122.0}
+DRAM_BYTES_PER_UNIT = {"update": 469.0, "flux_r": 113.0, "flux_phi": 120.0, "flux_theta": 122.0}
+# Executed FP64 operations per zone-update of one full RK3 step (MP5, FP64): ncu
+# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over every launch of one step
+# of the 192x96x96 torus, dadd + dmul + 2 dfma, divided by its interior cells (1,424,896).  It
+# includes the Newton iterations of the FP64 divisions and square roots.
+FP64_FLOPS_PER_ZONE = 15271.0
+
+
+def fp64_peak_tflops(device) -> float:
+    """FP64 throughput of a plain library DGEMM (torch.matmul, float64,
+    8192^3, best of 5 after 2 warm-up): the FP64 roof the step is compared
+    with (B200 runs FP64 vector and tensor work at the same rate)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = _events()
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -182,7 +210,13 @@ def run_gpu(args) -> dict | None:
     ctx = Context(dev)
     ctx.set_stream(stream.cuda_stream)
     run = ctx.admit(p)
+    # initial data: the host construction, timed, then the device one, which the run keeps
+    t = time.perf_counter()
     run.ic_torus(seed=2012 + rank)
+    ic_host_s = time.perf_counter() - t
+    t = time.perf_counter()
+    run.ic_torus_device(seed=2012 + rank)
+    ic_device_s = time.perf_counter() - t
 
     def barrier():
         if ws > 1:
@@ -258,6 +292,7 @@ def run_gpu(args) -> dict | None:
                     "bytes_per_unit": BYTES_PER_UNIT[top], "units_per_launch": u, "ms_per_launch": per_launch_ms,
                     "note": "FP64-pipe bound path: HBM fraction of algorithmic bytes, see profiles/"}
     run.release()
+    fp64_peak = fp64_peak_tflops(dev) if (rank == 0 and args.prof_steps > 0) else None
     extra = {}
     if ws == 1:
         sections = (("mixed", args.mixed_steps, section_mixed), ("torus2d", args.torus2d_steps, section_torus2d),
@@ -275,6 +310,13 @@ def run_gpu(args) -> dict | None:
     if rank != 0:
         return None
     value = zones * ws * args.steps / (ms * 1e-3)
+    fp64 = None
+    if fp64_peak is not None:
+        achieved = zones * args.steps / (ms * 1e-3) * FP64_FLOPS_PER_ZONE / 1e12  # per GPU
+        fp64 = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "flops_per_unit": FP64_FLOPS_PER_ZONE,
+                "peak_source": "measured: torch.matmul float64 8192^3 (cuBLAS DGEMM), best of 5",
+                "flops_source": "ncu dadd + dmul + 2 dfma executed per zone-update, 192x96x96 torus"}
     line = {
         "metric": "zone-updates/s (FP64, one full RK3 step per update)", "value": value, "unit": "zone-updates/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -283,7 +325,11 @@ def run_gpu(args) -> dict | None:
         "config": dict(config_block(args, p), parallelism=f"replicas x{ws}"),
         "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         "roofline": roofline,
+        "fp64_roofline": fp64,
         "kernel_share": shares,
+        "initial_data": {"host_s": ic_host_s, "device_s": ic_device_s,
+                         "note": "torus initial data of the headline grid: rg_run_ic_torus (host construction "
+                                 "and upload) vs rg_run_ic_torus_device; wall clock of the call"},
         "recov": {k: st[k] for k in ("recov_nr2", "recov_fail", "recov_carry", "recov_cap")},
     }
     line.update(extra)
@@ -319,7 +365,7 @@ def section_mixed(ctx, args) -> dict:
     states = {}
     for prec in ("fp64", "mixed"):
         r = ctx.admit(dict(p, precision=prec))
-        r.ic_torus(seed=2012)
+        r.ic_torus_device(seed=2012)
         r.step(3)  # first use of every kernel; counted in the comparison below
         torch.cuda.synchronize()
         e0, e1 = _events()

@@ -132,6 +132,13 @@ int rg_run_footprint(const rg_run_params* p, size_t* bytes);
  * uniform keyed by (seed, cell).  Also sets time = 0 (main.f90:530-548). */
 int rg_run_ic_torus(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin, double rmax,
                     double beta, double kappa);
+/* The same initial data computed on the device (the step's stream; the call
+ * returns when it is in place): only per-index tables cross to the device,
+ * so large 3D runs start without the host pass over every cell.  Agrees with
+ * rg_run_ic_torus to a few units in the last place (CUDA's exp/log/pow in
+ * the per-cell terms).  Not for theta slabs (RG_EINVAL_CONFIG). */
+int rg_run_ic_torus_device(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin, double rmax,
+                           double beta, double kappa);
 /* Initial data: seeded 1D RMHD Riemann problem number `tube` in the pattern
  * of mdshoctub (mdgrmhd.f90:56-118): a left state for i <= imax/2 and a right
  * state beyond, drawn from a counter-based uniform keyed by (seed, tube):

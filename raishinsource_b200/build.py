@@ -28,7 +28,7 @@ VARIANTS = {
     "fast": (LIB, ["--fmad=true"]),
     "exact": (EXACT_LIB, ["--fmad=false", "-DRG_EXACT_ARITH"]),
 }
-SOURCES = ["rg_kernels.cu", "rg_capi.cu", "rg_geometry.cpp"]
+SOURCES = ["rg_kernels.cu", "rg_ic.cu", "rg_capi.cu", "rg_geometry.cpp"]
 HEADERS = ["rg_device.cuh", "rg_recon.cuh", "rg_kernels.cuh", "rg_batch.cuh", "rg_types.h", "rg_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

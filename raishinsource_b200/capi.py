@@ -28,7 +28,7 @@ STATUS = {0: "RG_OK", 1: "RG_EINVAL_CONFIG", 2: "RG_ENOMEM_ADMIT", 3: "RG_ECUDA"
 EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ctx_mark", "rg_ctx_wait_mark",
            "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
-           "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
+           "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_torus_device", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
            "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
 
 
@@ -100,6 +100,8 @@ def load(path: str = LIB_PATH):
     lib.rg_prep_destroy.argtypes = [P]
     lib.rg_run_footprint.argtypes = [C.POINTER(RunParams), C.POINTER(C.c_size_t)]
     lib.rg_run_ic_torus.argtypes = [P, I, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double,
+                                    C.c_double]
+    lib.rg_run_ic_torus_device.argtypes = [P, I, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double]
     lib.rg_run_ic_tube.argtypes = [P, I, C.c_uint64, C.c_uint64]
     lib.rg_run_upload_prims.argtypes = [P, I, C.c_void_p, C.c_double]
@@ -299,6 +301,10 @@ class Run:
     # initial data / state transfer
     def ic_torus(self, seed=2012, amp=0.04, rin=6.0, rmax=12.0, beta=100.0, kappa=1e-3):
         _check(self.lib, self.lib.rg_run_ic_torus(self.ctx.h, self.id, seed, amp, rin, rmax, beta, kappa))
+
+    def ic_torus_device(self, seed=2012, amp=0.04, rin=6.0, rmax=12.0, beta=100.0, kappa=1e-3):
+        """The torus initial data of ic_torus computed on the device (rg_run_ic_torus_device)."""
+        _check(self.lib, self.lib.rg_run_ic_torus_device(self.ctx.h, self.id, seed, amp, rin, rmax, beta, kappa))
 
     def ic_tube(self, seed=2012, tube=0):
         """Seeded 1D Riemann problem (left state for i <= imax/2, pattern of mdshoctub)."""

@@ -990,6 +990,37 @@ int rg_run_ic_torus(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin,
   return RG_OK;
 }
 
+int rg_run_ic_torus_device(rg_ctx* ctx, int run, uint64_t seed, double amp, double rin, double rmax, double beta,
+                           double kappa) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  const DevRun& d = R->d;
+  if (d.kmet || d.kfix) return fail(RG_EINVAL_CONFIG, "torus initial data needs a Kerr metric on a full theta range");
+  if (d.imax < 3 || d.kmax < 3) return fail(RG_EINVAL_CONFIG, "torus initial data needs imax, kmax >= 3");
+  TorusTables T;
+  torus_tables(R->p, R->geom, rin, rmax, T);
+  void* buf = nullptr;
+  const size_t tab_bytes = T.tab.size() * sizeof(double);
+  RG_CUDA(cudaMalloc(&buf, tab_bytes + 2 * sizeof(unsigned long long)));
+  IcTorusArgs a{};
+  a.tab = static_cast<const double*>(buf);
+  a.red = reinterpret_cast<unsigned long long*>(static_cast<char*>(buf) + tab_bytes);
+  a.seed = seed; a.amp = amp; a.rin = rin; a.kappa = kappa; a.beta = beta; a.akm = R->p.akm;
+  a.ell = T.ell; a.h_in = T.h_in; a.edge0 = T.edge0; a.edge1 = T.edge1;
+  a.metric = R->p.metric; a.ix1 = R->p.ix1; a.ix3 = R->p.ix3;
+  const int nm1 = nm1_of(&R->p);
+  a.phi_slab = (d.jmax == 2 * nm1 + 1);
+  a.slab_j = nm1 + 1;
+  cudaError_t e = cudaMemcpyAsync(buf, T.tab.data(), tab_bytes, cudaMemcpyHostToDevice, ctx->stream);
+  R->cur = 0;
+  if (e == cudaSuccess) e = launch_ic_torus(d, a, R->b.P[0], ctx->stream);
+  if (e == cudaSuccess && d.P32) e = launch_to_f32(R->b.P[0], d.P32, 9 * d.N, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(RG_ECUDA, cudaGetErrorString(e));
+  return set_time(ctx, R, 0.0);
+}
+
 int rg_run_ic_tube(rg_ctx* ctx, int run, uint64_t seed, uint64_t tube) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");

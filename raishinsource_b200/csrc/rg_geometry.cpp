@@ -680,4 +680,50 @@ void torus_ic(const rg_run_params& p, const HostGeom& G, uint64_t seed, double a
     for (int v = 6; v <= 8; ++v) P[(size_t)v * N + c] = P[(size_t)v * N + c] * bnorm;
 }
 
+void torus_tables(const rg_run_params& p, const HostGeom& G, double rin, double rmax, TorusTables& T) {
+  const int imax = p.imax, kmax = p.kmax;
+  const double gam = p.gam, a = p.akm;
+  const Axis& X1 = G.ax[0];
+  const Axis& X3 = G.ax[2];
+  const bool mks = (p.metric == 403);
+  T.tab.assign((size_t)kIcTabI * imax + (size_t)kIcTabK * kmax, 0.0);
+  auto ti = [&](int f, int i) -> double& { return T.tab[(size_t)f * imax + (i - 1)]; };
+  auto tk = [&](int f, int k) -> double& { return T.tab[(size_t)kIcTabI * imax + (size_t)f * kmax + (k - 1)]; };
+  for (int i = 1; i <= imax; ++i) {
+    const double r = X1.x[i];
+    ti(IC_R, i) = r;
+    ti(IC_DE, i) = p.dmin * std::pow(r, -1.5);
+    ti(IC_PR, i) = p.pmin * (gam - 1.) * std::pow(r, -2.5);
+    if (i >= 2 && i <= imax - 1)
+      ti(IC_H1, i) = mks ? 0.5 * (X1.xb[i + 1] + X1.xb[i]) - 0.5 * (X1.xb[i] + X1.xb[i - 1])
+                         : 0.5 * (X1.x[i + 1] + X1.x[i]) - 0.5 * (X1.x[i] + X1.x[i - 1]);
+  }
+  for (int k = 1; k <= kmax; ++k) {
+    const double th = X3.x[k];
+    double sth = std::sin(th);
+    if (std::fabs(sth) < 1.e-12) sth = (sth >= 0.0) ? 1.e-12 : -1.e-12;
+    tk(IC_TH, k) = th;
+    tk(IC_STH, k) = sth;
+    tk(IC_CTH, k) = std::cos(th);
+    const double thb = (th > kPi) ? 2. * kPi - th : th;  // bl_cov's theta
+    tk(IC_SBL, k) = clamp_small(std::sin(thb));
+    tk(IC_CBL, k) = clamp_small(std::cos(thb));
+    tk(IC_HDEN, k) = 1. + (1. - p.hslope) * std::cos(2. * X3.xb[k]);
+    if (k >= 2 && k <= kmax - 1)
+      tk(IC_H3, k) = mks ? 0.5 * (X3.xb[k + 1] + X3.xb[k]) - 0.5 * (X3.xb[k] + X3.xb[k - 1])
+                         : 0.5 * (X3.x[k + 1] + X3.x[k]) - 0.5 * (X3.x[k] + X3.x[k - 1]);
+  }
+  T.edge0 = (double)0.02f * kPi;
+  T.edge1 = (double)0.98f * kPi;
+  T.ell = fm_ell(a, rmax);
+  const double ell = T.ell;
+  const double dl = rin * rin - 2.0 * rin + a * a;
+  const double al = (rin * rin + a * a) * (rin * rin + a * a) - dl * a * a;
+  const double sl = rin * rin;
+  const double e2a = 4.0 * (ell * ell * sl * sl) * dl * (1.0 / (al * al));
+  const double e2c = sl * dl * (1.0 / al);
+  T.h_in = 0.5 * std::log((1.0 + std::sqrt(1. + e2a)) * (1.0 / e2c)) - 0.5 * std::sqrt(1.0 + e2a) -
+           2.0 * a * rin * ell * (1.0 / al);
+}
+
 }  // namespace rg

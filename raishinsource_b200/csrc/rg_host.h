@@ -38,6 +38,18 @@ void build_geometry(const rg_run_params& p, HostGeom& g, int krow = 0);
 void torus_ic(const rg_run_params& p, const HostGeom& g, uint64_t seed, double amp, double rin, double rmax,
               double beta, double kappa, std::vector<double>& prim, bool plane_only = false);
 
+// Inputs of the device torus construction (rg_ic.cu), evaluated on the host
+// with the libm calls torus_ic makes: per radial index r, the floors
+// dmin r^-1.5 and pmin (gam-1) r^-2.5 and the corner spacing h1; per theta
+// index theta, its clamped sine and cosine, bl_cov's clamped sine and cosine,
+// the MKS factor 1 + (1-hslope) cos(2 theta_MKS) and the spacing h3; and the
+// run's scalars (angular momentum, ln h at the inner edge, polar edges).
+struct TorusTables {
+  std::vector<double> tab;  // kIcTabI planes of imax, then kIcTabK planes of kmax (rg_types.h)
+  double ell = 0, h_in = 0, edge0 = 0, edge1 = 0;
+};
+void torus_tables(const rg_run_params& p, const HostGeom& g, double rin, double rmax, TorusTables& out);
+
 // Left/right primitive states of the seeded Riemann tube `tube` (mdshoctub pattern).
 void tube_states(uint64_t seed, uint64_t tube, double gam, double state[2][9]);
 

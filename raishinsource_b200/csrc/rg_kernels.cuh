@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <vector>
 
 #include "rg_types.h"
@@ -49,6 +50,17 @@ cudaError_t launch_to_f32(const double* a, float* b, size_t n, cudaStream_t s);
 // derived metric fields of the three caches and the radial floor profiles (run setup)
 cudaError_t launch_geom_derive(const DevRun& r, double* mc, double* mi, double* mk, double* fl_de, double* fl_pr,
                                cudaStream_t s);
+
+// Fishbone-Moncrief torus initial data on the device (rg_ic.cu).
+struct IcTorusArgs {
+  const double* tab;        // TorusTables::tab on the device
+  unsigned long long* red;  // two reduction words: rho_max bits, ordered key of beta_min
+  uint64_t seed;
+  double amp, rin, kappa, beta, akm, ell, h_in, edge0, edge1;
+  int metric, ix1, ix3;
+  int phi_slab, slab_j;     // jmax == 2*nm1+1: the draw is keyed by the plane slab_j = nm1+1
+};
+cudaError_t launch_ic_torus(const DevRun& r, const IcTorusArgs& a, double* P, cudaStream_t s);
 
 // Batched steps of runs of one class (rg_batch.cuh).
 struct BatchPlan;

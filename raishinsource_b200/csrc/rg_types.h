@@ -21,6 +21,11 @@ constexpr int NV = 9;
 constexpr int kMetBase = 18;
 constexpr int kMetComps = 26;
 
+// Planes of the torus initial-data table (TorusTables): per radial index,
+// then per theta index.
+enum IcTabI { IC_R = 0, IC_DE, IC_PR, IC_H1, kIcTabI };
+enum IcTabK { IC_TH = 0, IC_STH, IC_CTH, IC_SBL, IC_CBL, IC_HDEN, IC_H3, kIcTabK };
+
 // Device scalars of a run (one small block of device memory).
 struct Scal {
   unsigned long long dtcfl_bits;  // min-reduced CFL time step (bits of a positive double)

@@ -81,6 +81,41 @@ def test_ic_torus_ghost_widths(gpu_ctx, irec, ict, nph):
     assert err.max() < 1e-13, err
 
 
+@pytest.mark.parametrize("case", ["mks3d", "slab_mc_ict0", "slab_ppm", "ks303", "mixed3d", "full_slab"])
+def test_ic_torus_device(gpu_ctx, case):
+    """Torus initial data computed on the device (rg_run_ic_torus_device)
+    against the oracle's construction and the host one: the same torus cells,
+    every primitive within a few units in the last place (CUDA's exp, log and
+    pow in the per-cell terms), on MKS and Kerr-Schild grids, phi slabs
+    stored as one plane or in full, every ghost width and the FP32-mixed
+    layout."""
+    p = {
+        "mks3d": lambda: config.torus(nr=64, nth=48, nph=12),
+        "slab_mc_ict0": lambda: config.torus(nr=48, nth=40, irec=config.IREC_MC, ict=0),
+        "slab_ppm": lambda: config.torus(nr=64, nth=64, irec=config.IREC_PPM),
+        "ks303": lambda: dict(config.torus(nr=48, nth=40, nph=12), metric=303, ix1=1, ix3=1, xmax=30.0),
+        "mixed3d": lambda: config.torus(nr=48, nth=32, nph=12, precision="mixed"),
+        "full_slab": lambda: dict(config.torus(nr=48, nth=40), flags=config.FLAG_FULL),
+    }[case]()
+    o = Oracle(p)
+    o.ic_torus(seed=17, amp=0.04, beta=50.0)
+    rh = gpu_ctx.admit(p)
+    rd = gpu_ctx.admit(p)
+    try:
+        rh.ic_torus(seed=17, amp=0.04, beta=50.0)
+        rd.ic_torus_device(seed=17, amp=0.04, beta=50.0)
+        ref, host, dev = o.prims(), rh.prims(), rd.prims()
+    finally:
+        rh.release()
+        rd.release()
+    assert field_err(host, ref).max() < 1e-13
+    torus = ref[..., 1:4].any(axis=-1)
+    assert torus.sum() > 100
+    assert np.array_equal(dev[..., 1:4].any(axis=-1), torus)
+    err = field_err(dev, ref)
+    assert err.max() < 1e-12, err
+
+
 def test_caluu1(torus2d):
     _, o, r = torus2d
     u = o.prims()
