@@ -61,7 +61,9 @@ typedef struct rg_run_params {
   int flags;     /* RG_FLAG_* bits */
   int ict;       /* constrained transport as pram.f90's ict (pram.f90:148-151, ct.f90:4-27):
                     0 none, 1 flux-CT (Toth 2000; the reference's setting), 2 modified flux-CT
-                    (Gardiner & Stone 2005, mflct).  Ghost width nm1 = nm0 + ict (main.f90:192-199). */
+                    (Gardiner & Stone 2005, mflct), 3 upwind flux-CT (upflct; FP64 precision
+                    only, stepped by rg_step alone: rg_step_batch and rg_calflx_static refuse it).
+                    Ghost width nm1 = nm0 + ict (main.f90:192-199). */
 } rg_run_params;
 
 /* rg_run_params.flags.  A direction of extent 2*nm1+1 (one interior cell)

@@ -111,6 +111,15 @@ void orc_fluxes(void* h, const double* uri, double* ww) {
   std::memcpy(ww, s->ww.data(), s->ww.size() * sizeof(double));
 }
 
+// ct alone (ct.f90:4-27, the run's ict) on given primitives and fluxes ww(3,nv,i,j,k), in place
+void orc_ct(void* h, const double* uri, double* ww) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  std::memcpy(s->ww.data(), ww, s->ww.size() * sizeof(double));
+  orc::ct(*s);
+  std::memcpy(ww, s->ww.data(), s->ww.size() * sizeof(double));
+}
+
 // rec2 alone on the given primitives: the six face-state arrays uriil,
 // uriir, urijl, urijr, urikl, urikr (each 9 per cell, reference layout) out
 void orc_rec2(void* h, const double* uri, double* faces) {

@@ -1048,6 +1048,109 @@ void mflct(State& s) {
         s.ww[s.w(2, 9, i, j, k)] = fbyz + fhyz;
       }
 }
+
+// ct.f90:236-445 (upflct, ict 3): upwinded corner EMFs.  Level 1 (on
+// nm0+1..n-nm0-1): cell-centred EMFs e?c, face-pair EMFs e?b and 1/8 flux-CT
+// brackets fb??; level 2 (on nm0+1..n-nm0-2): differences d?e? upwinded by
+// the sign of the velocity uri(2..4) at the cell; level 3 (on nm1..n-nm1):
+// corner EMFs averaged into the six induction fluxes.  Every index is the
+// reference's as written: eyb reads fzx at j+1; each fb?? takes the 2-1-1
+// average of its own flux along the direction that is neither its face
+// normal nor its field component (fluxct takes it along the face normal);
+// every elseif after dyez's tests uri(2); dzey's negative-velocity branch
+// subtracts eyc(i), not eyc(i+1).
+void upflct(State& s) {
+  const int nm0 = s.nm0, nm1 = s.nm1, nm2 = nm0 + 1, nm3 = nm0 + 2;
+  const size_t N = s.ncell;
+  std::vector<double> fyx(N), fzx(N), fxy(N), fzy(N), fxz(N), fyz(N);
+  std::vector<double> exc(N), eyc(N), ezc(N), exb(N), eyb(N), ezb(N);
+  std::vector<double> fbyx(N), fbzx(N), fbxy(N), fbzy(N), fbxz(N), fbyz(N);
+  std::vector<double> dyez(N), dxez(N), dyex(N), dzex(N), dxey(N), dzey(N);
+  auto C = [&](int i, int j, int k) { return s.cell(i, j, k); };
+#pragma omp parallel for schedule(static)
+  for (int k = nm0; k <= s.kmax - nm0; ++k)
+    for (int j = nm0; j <= s.jmax - nm0; ++j)
+      for (int i = nm0; i <= s.imax - nm0; ++i) {
+        const size_t c = C(i, j, k);
+        fyx[c] = s.ww[s.w(2, 7, i, j, k)];
+        fzx[c] = s.ww[s.w(3, 7, i, j, k)];
+        fxy[c] = s.ww[s.w(1, 8, i, j, k)];
+        fzy[c] = s.ww[s.w(3, 8, i, j, k)];
+        fxz[c] = s.ww[s.w(1, 9, i, j, k)];
+        fyz[c] = s.ww[s.w(2, 9, i, j, k)];
+      }
+  const double q = 0.25, e = 1.0 / 8.0, h = 0.5;
+#pragma omp parallel for schedule(static)
+  for (int k = nm2; k <= s.kmax - nm2; ++k)
+    for (int j = nm2; j <= s.jmax - nm2; ++j)
+      for (int i = nm2; i <= s.imax - nm2; ++i) {
+        const size_t c = C(i, j, k);
+        ezc[c] = q * (-fxy[C(i - 1, j, k)] - fxy[c] + fyx[C(i, j - 1, k)] + fyx[c]);
+        exc[c] = q * (-fyz[C(i, j - 1, k)] - fyz[c] + fzy[C(i, j, k - 1)] + fzy[c]);
+        eyc[c] = q * (-fzx[C(i, j, k - 1)] - fzx[c] + fxz[C(i - 1, j, k)] + fxz[c]);
+        ezb[c] = q * (fyx[c] + fyx[C(i + 1, j, k)] - fxy[c] - fxy[C(i, j + 1, k)]);
+        exb[c] = q * (fzy[c] + fzy[C(i, j + 1, k)] - fyz[c] - fyz[C(i, j, k + 1)]);
+        eyb[c] = q * (fxz[c] + fxz[C(i + 1, j, k)] - fzx[c] - fzx[C(i, j + 1, k)]);
+        fbyx[c] = e * (2.0 * fyx[c] + fyx[C(i, j, k + 1)] + fyx[C(i, j, k - 1)] - fxy[c] - fxy[C(i, j + 1, k)] -
+                       fxy[C(i - 1, j, k)] - fxy[C(i - 1, j + 1, k)]);
+        fbzx[c] = e * (2.0 * fzx[c] + fzx[C(i, j + 1, k)] + fzx[C(i, j - 1, k)] - fxz[c] - fxz[C(i, j, k + 1)] -
+                       fxz[C(i - 1, j, k)] - fxz[C(i - 1, j, k + 1)]);
+        fbxy[c] = e * (2.0 * fxy[c] + fxy[C(i, j, k + 1)] + fxy[C(i, j, k - 1)] - fyx[c] - fyx[C(i + 1, j, k)] -
+                       fyx[C(i, j - 1, k)] - fyx[C(i + 1, j - 1, k)]);
+        fbzy[c] = e * (2.0 * fzy[c] + fzy[C(i + 1, j, k)] + fzy[C(i - 1, j, k)] - fyz[c] - fyz[C(i, j, k + 1)] -
+                       fyz[C(i, j - 1, k)] - fyz[C(i, j - 1, k + 1)]);
+        fbxz[c] = e * (2.0 * fxz[c] + fxz[C(i, j + 1, k)] + fxz[C(i, j - 1, k)] - fzx[c] - fzx[C(i + 1, j, k)] -
+                       fzx[C(i, j, k - 1)] - fzx[C(i + 1, j, k - 1)]);
+        fbyz[c] = e * (2.0 * fyz[c] + fyz[C(i + 1, j, k)] + fyz[C(i - 1, j, k)] - fzy[c] - fzy[C(i, j + 1, k)] -
+                       fzy[C(i, j, k - 1)] - fzy[C(i, j + 1, k - 1)]);
+      }
+  // upwinded differences: a(c) - b(c) when u > 0, a(n) - b(n) when u < 0
+  // (n the neighbour up the direction), the mean of both otherwise
+  auto up = [&](double u, double ul, const std::vector<double>& a, const std::vector<double>& b, size_t c, size_t n,
+                size_t bneg) {
+    if (u > 0.0) return a[c] - b[c];
+    if (ul < 0.0) return a[n] - b[bneg];
+    return h * (a[c] + a[n] - b[c] - b[n]);
+  };
+#pragma omp parallel for schedule(static)
+  for (int k = nm2; k <= s.kmax - nm3; ++k)
+    for (int j = nm2; j <= s.jmax - nm3; ++j)
+      for (int i = nm2; i <= s.imax - nm3; ++i) {
+        const size_t c = C(i, j, k), ci = C(i + 1, j, k), cj = C(i, j + 1, k), ck = C(i, j, k + 1);
+        const double u1 = s.uri[s.a(2, i, j, k)], u2 = s.uri[s.a(3, i, j, k)], u3 = s.uri[s.a(4, i, j, k)];
+        dyez[c] = up(u1, u1, fbyx, ezc, c, ci, ci);
+        dxez[c] = up(u2, u1, fbxy, ezc, c, cj, cj);
+        dyex[c] = up(u3, u1, fbyz, exc, c, ck, ck);
+        dzex[c] = up(u2, u1, fbzy, exc, c, cj, cj);
+        dxey[c] = up(u3, u1, fbxz, eyc, c, ck, ck);
+        dzey[c] = up(u1, u1, fbzx, eyc, c, ci, c);
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = nm1; k <= s.kmax - nm1; ++k)
+    for (int j = nm1; j <= s.jmax - nm1; ++j)
+      for (int i = nm1; i <= s.imax - nm1; ++i) {
+        const size_t c = C(i, j, k);
+        const size_t im = C(i - 1, j, k), jm = C(i, j - 1, k), km = C(i, j, k - 1);
+        const size_t ip = C(i + 1, j, k), jp = C(i, j + 1, k), kp = C(i, j, k + 1);
+        const size_t imjp = C(i - 1, j + 1, k), ipjm = C(i + 1, j - 1, k), jmkp = C(i, j - 1, k + 1);
+        const size_t jpkm = C(i, j + 1, k - 1), imkp = C(i - 1, j, k + 1), ipkm = C(i + 1, j, k - 1);
+        const double ezh = ezb[c] + q * (dyez[c] - dyez[jp]) + q * (dxez[c] - dxez[ip]);
+        const double ezhmi = ezb[im] + q * (dyez[im] - dyez[imjp]) + q * (dxez[im] - dxez[c]);
+        const double ezhmj = ezb[jm] + q * (dyez[jm] - dyez[c]) + q * (dxez[jm] - dxez[ipjm]);
+        const double exh = exb[c] + q * (dyex[c] - dyex[jp]) + q * (dzex[c] - dzex[kp]);
+        const double exhmj = exb[jm] + q * (dyex[jm] - dyex[c]) + q * (dzex[jm] - dzex[jmkp]);
+        const double exhmk = exb[km] + q * (dyex[km] - dyex[jpkm]) + q * (dzex[km] - dzex[c]);
+        const double eyh = eyb[c] + q * (dxey[c] - dxey[ip]) + q * (dzey[c] - dzey[kp]);
+        const double eyhmi = eyb[im] + q * (dxey[im] - dxey[c]) + q * (dzey[im] - dzey[imkp]);
+        const double eyhmk = eyb[km] + q * (dxey[km] - dxey[ipkm]) + q * (dzey[km] - dzey[c]);
+        s.ww[s.w(2, 7, i, j, k)] = h * (ezh + ezhmi);
+        s.ww[s.w(3, 7, i, j, k)] = h * (-eyh - eyhmi);
+        s.ww[s.w(1, 8, i, j, k)] = h * (-ezh - ezhmj);
+        s.ww[s.w(3, 8, i, j, k)] = h * (exh + exhmj);
+        s.ww[s.w(1, 9, i, j, k)] = h * (eyh + eyhmk);
+        s.ww[s.w(2, 9, i, j, k)] = h * (-exh - exhmk);
+      }
+}
 }  // namespace
 
 // ct.f90:4-27: the constrained-transport scheme ict.  guard bit 2 (not in
@@ -1066,6 +1169,7 @@ void ct(State& s) {
   }
   if (s.p.ict == 1) fluxct(s);
   else if (s.p.ict == 2) mflct(s);
+  else if (s.p.ict == 3) upflct(s);
 }
 
 // calsf.f90:6-151 (T^m_n at the cell and S_nu = sqrt(-g) T^m_n Gamma^n_{nu m}).

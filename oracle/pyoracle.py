@@ -73,6 +73,7 @@ def _lib():
         lib.orc_bnd_floor.argtypes = [P, D, D]
         lib.orc_calsf.argtypes = [P, D, D]
         lib.orc_rec2.argtypes = [P, D, D]
+        lib.orc_ct.argtypes = [P, D, D]
         lib.orc_derived.argtypes = [P, D, C.c_int, D]
         lib.orc_rkt.argtypes = [P, C.c_int, C.c_double, D, D, D, D, D]
         lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
@@ -175,6 +176,13 @@ class Oracle:
         uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
         out = np.zeros(self.shape + (3,), dtype=np.float64)
         self.lib.orc_fluxes(self.h, _ptr(uri), _ptr(out))
+        return out
+
+    def ct(self, uri, ww):
+        """ct (the run's ict) applied to given fluxes ww of shape (kmax, jmax, imax, 9, 3)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = np.array(ww, dtype=np.float64, order="C").reshape(self.shape + (3,))
+        self.lib.orc_ct(self.h, _ptr(uri), _ptr(out))
         return out
 
     def recov(self, uu, uri):

@@ -56,7 +56,8 @@ def torus(nr: int = 256, nth: int = 256, nph: int | None = None, irec: int = IRE
     ``nph=None`` the run is the 2D axisymmetric case: a periodic phi slab of
     jmax = 2*nm1+1 cells (one interior cell).  phi spans 2*pi over the
     interior: dphi = 2*pi/(jmax-2*nm1), x2(j) = (j-nm1-1/2)*dphi.  ``ict``
-    selects the constrained transport (1 flux-CT, 2 modified flux-CT, 0 none).
+    selects the constrained transport (1 flux-CT, 2 modified flux-CT, 3 upwind
+    flux-CT, 0 none).
     """
     _, nm1 = ghost_widths(irec, ict)
     jmax = 2 * nm1 + 1 if nph is None else int(nph)

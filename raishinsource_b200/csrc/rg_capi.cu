@@ -129,8 +129,10 @@ int check_params(const rg_run_params* p) {
     return fail(RG_EINVAL_CONFIG,
                 "irec must be 1 (MC), 2 (minmod), 3 (MUSCL), 4 (CENO), 5 (PPM), 6 (MP5), 7 (WENO5), 8 (MP-WENO), 9 (WENO-Z), "
                 "10 (WENO-M), 11 (LimO3), 12 (MVL) or 13 (Koren)");
-  if (p->ict < 0 || p->ict > 2)
-    return fail(RG_EINVAL_CONFIG, "ict must be 0 (none), 1 (flux-CT) or 2 (modified flux-CT)");
+  if (p->ict < 0 || p->ict > 3)
+    return fail(RG_EINVAL_CONFIG, "ict must be 0 (none), 1 (flux-CT), 2 (modified flux-CT) or 3 (upwind flux-CT)");
+  if (p->ict == 3 && p->precision == RG_MIXED)
+    return fail(RG_EINVAL_CONFIG, "upwind flux-CT (ict 3) runs in FP64 only");
   if (p->metric != 1 && p->metric != 303 && p->metric != 403)
     return fail(RG_EINVAL_CONFIG, "metric must be 1, 303 or 403");
   if (p->ix1 != 1 && p->ix1 != 2) return fail(RG_EINVAL_CONFIG, "ix1 must be 1 or 2");
@@ -205,7 +207,8 @@ size_t footprint_bytes(const rg_run_params* p) {
   size_t mixed = 0;
   if (p->precision == RG_MIXED)  // P32, F32 x3, CT32; FP32 metric caches and Christoffels
     mixed = (9 + 27 + 6) * N * sizeof(float) + (3 * kMetComps + 64) * nik * sizeof(float);
-  return state + geom + mixed + sizeof(Scal) + C_NCOUNTERS * 8 + (kCarryCap + straggler_cap(N)) * sizeof(int);
+  const size_t upct = (p->ict == 3) ? 6 * N * sizeof(double) : 0;  // upflct's EMF differences
+  return state + geom + mixed + upct + sizeof(Scal) + C_NCOUNTERS * 8 + (kCarryCap + straggler_cap(N)) * sizeof(int);
 }
 
 Run* find(rg_ctx* ctx, int id) {
@@ -329,6 +332,10 @@ int full_bufs(Run* R, cudaStream_t s, DevBufs** out) {
     R->fb.stage = static_cast<double*>(p);
     if ((rc = dalloc(R, &p, 9 * N * sizeof(double)))) return rc;
     R->fb.stage2 = static_cast<double*>(p);
+    if (R->d.ict == 3) {
+      if ((rc = dalloc(R, &p, 6 * N * sizeof(double)))) return rc;
+      R->fb.ctd = static_cast<double*>(p);
+    }
     R->fb_ready = true;
   }
   *out = &R->fb;
@@ -449,7 +456,7 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
   RG_CUDA(issue(ctx, K_FLUX1, nf, [&] { return launch_flux(d, 1, Pc, R->b.F[0], s); }));
   RG_CUDA(issue(ctx, K_FLUX2, nf, [&] { return launch_flux(d, 2, Pc, R->b.F[1], s); }));
   RG_CUDA(issue(ctx, K_FLUX3, nf, [&] { return launch_flux(d, 3, Pc, R->b.F[2], s); }));
-  RG_CUDA(issue(ctx, K_CT, n_ct_launches(d), [&] { return launch_ct(d, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s); }));
+  RG_CUDA(issue(ctx, K_CT, n_ct_launches(d), [&] { return launch_ct(d, Pc, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s); }));
   RG_CUDA(issue(ctx, K_UPDATE, n_update_launches(d), [&] {
     return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s);
   }));
@@ -866,6 +873,11 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   R->b.CT = static_cast<double*>(ptr);
   for (int k = 0; k < 3; ++k) d.F[k] = R->b.F[k];
   d.CT = R->b.CT;
+  if (d.ict == 3) {
+    if ((rc = dalloc(R, &ptr, 6 * N * sizeof(double)))) return bail(rc);
+    R->b.ctd = static_cast<double*>(ptr);
+    d.ctd = R->b.ctd;
+  }
   if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
   d.Un = static_cast<double*>(ptr);
   if ((rc = dalloc(R, &ptr, sizeof(int)))) return bail(rc);
@@ -1087,7 +1099,8 @@ int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats) {
   // A run with a slab direction steps as a batch of one: it then runs the same
   // compiled kernels alone as in any batch, so its results do not depend on
   // the company it keeps, and its step is replayed from a CUDA graph.
-  if (R->d.jfix || R->d.kfix) return rg_step_batch(ctx, &run, 1, nsteps, stats);
+  // (upwind flux-CT has no batched kernels: such a run keeps the launches below)
+  if ((R->d.jfix || R->d.kfix) && R->d.ict != 3) return rg_step_batch(ctx, &run, 1, nsteps, stats);
   cudaStream_t s = ctx->stream;
   for (int n = 0; n < nsteps; ++n) {
     double* Pn = R->b.P[R->cur];
@@ -1117,6 +1130,7 @@ int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_s
   for (int a = 0; a < nruns; ++a) {
     Run* R = find(ctx, runs[a]);
     if (!R) return fail(RG_ENOTFOUND, "unknown run in batch");
+    if (R->d.ict == 3) return fail(RG_EINVAL_CONFIG, "upwind flux-CT (ict 3) runs step alone (rg_step)");
     groups[batch_class(R)].push_back(runs[a]);
   }
   std::vector<BatchEntry*> es;
@@ -1227,13 +1241,14 @@ int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!uri || !ww) return fail(RG_EINVAL_CONFIG, "null array");
-  const DevRun d = full_view(R);
+  DevRun d = full_view(R);
   const size_t N = d.N;
   DevBufs* B = nullptr;
   int rc = full_bufs(R, ctx->stream, &B);
   if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
+  d.ctd = B->ctd;
   for (int dir = 1; dir <= 3; ++dir) RG_CUDA(launch_flux(d, dir, B->stage, B->F[dir - 1], ctx->stream));
-  RG_CUDA(launch_ct(d, B->F[0], B->F[1], B->F[2], B->CT, ctx->stream));
+  RG_CUDA(launch_ct(d, B->stage, B->F[0], B->F[1], B->F[2], B->CT, ctx->stream));
   std::vector<double> F(27 * N), CT(6 * N);
   for (int dir = 0; dir < 3; ++dir)
     RG_CUDA(cudaMemcpyAsync(F.data() + (size_t)dir * 9 * N, B->F[dir], 9 * N * sizeof(double),
@@ -1571,6 +1586,8 @@ extern "C" int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, dou
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!d_prims || !d_ww) return fail(RG_EINVAL_CONFIG, "null device buffer");
+  if (R->d.ict == 3)
+    return fail(RG_EINVAL_CONFIG, "rg_calflx_static: upwind flux-CT (ict 3) needs its difference planes (rg_calflx)");
   const size_t N = R->nfull;
   if (N > kStaticMaxCells)
     return fail(RG_EINVAL_CONFIG, "rg_calflx_static: grid of " + std::to_string(N) +
@@ -1597,7 +1614,7 @@ extern "C" int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, dou
   k_static_scal_reset<<<1, 1, 0, s>>>(d.scal);
   RG_CUDA(cudaGetLastError());
   for (int dir = 1; dir <= 3; ++dir) RG_CUDA(launch_flux(d, dir, d_prims, d_ww + (size_t)(dir - 1) * 9 * N, s));
-  RG_CUDA(launch_ct(d, d_ww, d_ww + 9 * N, d_ww + 18 * N, ct, s));
+  RG_CUDA(launch_ct(d, d_prims, d_ww, d_ww + 9 * N, d_ww + 18 * N, ct, s));
   const dim3 b(64, 4, 1);
   const int n = d.imax - 2 * d.nm1 + 1, m = d.jmax - 2 * d.nm1 + 1, l = d.kmax - 2 * d.nm1 + 1;
   k_ct_scatter<<<dim3((n + 63) / 64, (m + 3) / 4, l), b, 0, s>>>(d, ct, d_ww);

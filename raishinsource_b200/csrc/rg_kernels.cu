@@ -904,8 +904,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_fl
                                               float* __restrict__ Fcopy, int icopy, int ilo, int ihi) { flux_body<D, IREC, T, S>(r, P, F, Fcopy, icopy, ilo, ihi, blockIdx); }
 
 // ---------------------------------------------------------------- flux-CT
-// ct.f90:30-118 (flux-CT, ict 1), ct.f90:121-233 (mflct, ict 2) or none
-// (ict 0) on nm1..n-nm1 in every dimension (edges with i in [ilo, ihi]),
+// ct.f90:30-118 (flux-CT, ict 1), ct.f90:121-233 (mflct, ict 2),
+// ct.f90:236-445 (upflct, ict 3: its last level) or none (ict 0) on nm1..n-nm1 in every dimension (edges with i in [ilo, ihi]),
 // in arithmetic type T on flux storage S.  CTcopy, if given, receives an FP32
 // copy (the FP64 edges next to the FP32 region of the mixed path).
 template <int ICT, typename T, typename S>
@@ -929,9 +929,9 @@ __device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F
   auto L = [](const S* a, size_t x) { return T(a[x]); };
   const T e = T(1.0) / T(8.0), two = T(2.0);
   T o[6];
-  if (ICT == 0) {  // no constrained transport: the induction fluxes stay as hll left them
+  if constexpr (ICT == 0) {  // no constrained transport: the induction fluxes stay as hll left them
     o[0] = L(fyx, c); o[1] = L(fzx, c); o[2] = L(fxy, c); o[3] = L(fzy, c); o[4] = L(fxz, c); o[5] = L(fyz, c);
-  } else if (ICT == 2) {
+  } else if constexpr (ICT == 2) {
     // mflct (ct.f90:121-233): the cell-centred EMFs of its second pass
     // (ct.f90:174-176), evaluated where the corner formulas need them, and
     // the flux-CT brackets with weight 1/4 plus the averaged EMFs (ct.f90:191-224)
@@ -959,6 +959,31 @@ __device__ __forceinline__ void ct_body(const DevRun& r, const S* __restrict__ F
     const T fhyz = h * (two * ex(c) + two * ex(c + dj) + ex(c + dk) + ex(c + dj + dk) + ex(c - dk) + ex(c + dj - dk));
     o[0] = fbyx + fhyx; o[1] = fbzx + fhzx; o[2] = fbxy + fhxy;
     o[3] = fbzy + fhzy; o[4] = fbxz + fhxz; o[5] = fbyz + fhyz;
+  } else if constexpr (ICT == 3) {
+    // upflct's corner EMFs (ct.f90:391-433) from the face-pair EMFs e?b,
+    // evaluated here, and the upwinded differences of k_upct_diff
+    const T q = T(0.25), h = T(0.5);
+    const double* D = r.ctd;
+    const double *dyez = D, *dxez = D + N, *dyex = D + 2 * N, *dzex = D + 3 * N, *dxey = D + 4 * N, *dzey = D + 5 * N;
+    auto ezb = [&](size_t x) { return q * (L(fyx, x) + L(fyx, x + di) - L(fxy, x) - L(fxy, x + dj)); };
+    auto exb = [&](size_t x) { return q * (L(fzy, x) + L(fzy, x + dj) - L(fyz, x) - L(fyz, x + dk)); };
+    auto eyb = [&](size_t x) { return q * (L(fxz, x) + L(fxz, x + di) - L(fzx, x) - L(fzx, x + dj)); };
+    const size_t im = c - di, jm = c - dj, km = c - dk, ip = c + di, jp = c + dj, kp = c + dk;
+    const T ezh = ezb(c) + q * (L(dyez, c) - L(dyez, jp)) + q * (L(dxez, c) - L(dxez, ip));
+    const T ezhmi = ezb(im) + q * (L(dyez, im) - L(dyez, im + dj)) + q * (L(dxez, im) - L(dxez, c));
+    const T ezhmj = ezb(jm) + q * (L(dyez, jm) - L(dyez, c)) + q * (L(dxez, jm) - L(dxez, ip - dj));
+    const T exh = exb(c) + q * (L(dyex, c) - L(dyex, jp)) + q * (L(dzex, c) - L(dzex, kp));
+    const T exhmj = exb(jm) + q * (L(dyex, jm) - L(dyex, c)) + q * (L(dzex, jm) - L(dzex, jm + dk));
+    const T exhmk = exb(km) + q * (L(dyex, km) - L(dyex, jp - dk)) + q * (L(dzex, km) - L(dzex, c));
+    const T eyh = eyb(c) + q * (L(dxey, c) - L(dxey, ip)) + q * (L(dzey, c) - L(dzey, kp));
+    const T eyhmi = eyb(im) + q * (L(dxey, im) - L(dxey, c)) + q * (L(dzey, im) - L(dzey, im + dk));
+    const T eyhmk = eyb(km) + q * (L(dxey, km) - L(dxey, ip - dk)) + q * (L(dzey, km) - L(dzey, c));
+    o[0] = h * (ezh + ezhmi);
+    o[1] = h * (-eyh - eyhmi);
+    o[2] = h * (-ezh - ezhmj);
+    o[3] = h * (exh + exhmj);
+    o[4] = h * (eyh + eyhmk);
+    o[5] = h * (-exh - exhmk);
   } else {
   o[0] = e * (two * L(fyx, c) + L(fyx, c + di) + L(fyx, c - di) - L(fxy, c) - L(fxy, c + dj) - L(fxy, c - di) -
               L(fxy, c - di + dj));
@@ -983,6 +1008,77 @@ template <int ICT, typename T, typename S>
 __global__ void __launch_bounds__(256) k_ct(DevRun r, const S* __restrict__ F1, const S* __restrict__ F2,
                                             const S* __restrict__ F3, S* __restrict__ CT,
                                             float* __restrict__ CTcopy, int ilo, int ihi) { ct_body<ICT, T, S>(r, F1, F2, F3, CT, CTcopy, ilo, ihi, blockIdx); }
+
+// upflct's first two levels (ct.f90:300-389, ict 3) on nm0+1..n-nm0-2 in
+// every dimension: the six upwinded EMF differences d?e? of each cell, from
+// the cell-centred EMFs e?c and the 1/8 brackets fb?? at the cell and at its
+// upper neighbour, both evaluated from the face fluxes where needed; the sign
+// tests read the cell's velocity uri(2..4).  Every index is the
+// reference's as written: each fb?? averages its own flux along the direction
+// that is neither its face normal nor its field component, every test after
+// dyez's falls back on uri(2) < 0, and dzey's negative-velocity branch
+// subtracts eyc at the cell itself.  Written to r.ctd (six planes of N).
+__global__ void __launch_bounds__(256) k_upct_diff(DevRun r, const double* __restrict__ P,
+                                                   const double* __restrict__ F1, const double* __restrict__ F2,
+                                                   const double* __restrict__ F3, int hi_i, int hi_j, int hi_k) {
+  if (!r.scal->active) return;
+  const int lo = r.nm0 + 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + lo;
+  const int j = jidx(r, lo, blockIdx);
+  const int k = kidx(r, lo, blockIdx);
+  if (i > hi_i || j > hi_j || k > hi_k) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  const size_t di = 1, dj = r.sj, dk = r.sk;
+  const double* fyx = F2 + 6 * N;
+  const double* fzx = F3 + 6 * N;
+  const double* fxy = F1 + 7 * N;
+  const double* fzy = F3 + 7 * N;
+  const double* fxz = F1 + 8 * N;
+  const double* fyz = F2 + 8 * N;
+  auto L = [](const double* a, size_t x) { return __ldg(a + x); };
+  const double q = 0.25, e = 1.0 / 8.0, two = 2.0, h = 0.5;
+  auto ezc = [&](size_t x) { return q * (-L(fxy, x - di) - L(fxy, x) + L(fyx, x - dj) + L(fyx, x)); };
+  auto exc = [&](size_t x) { return q * (-L(fyz, x - dj) - L(fyz, x) + L(fzy, x - dk) + L(fzy, x)); };
+  auto eyc = [&](size_t x) { return q * (-L(fzx, x - dk) - L(fzx, x) + L(fxz, x - di) + L(fxz, x)); };
+  auto fbyx = [&](size_t x) {
+    return e * (two * L(fyx, x) + L(fyx, x + dk) + L(fyx, x - dk) - L(fxy, x) - L(fxy, x + dj) - L(fxy, x - di) -
+                L(fxy, x - di + dj));
+  };
+  auto fbzx = [&](size_t x) {
+    return e * (two * L(fzx, x) + L(fzx, x + dj) + L(fzx, x - dj) - L(fxz, x) - L(fxz, x + dk) - L(fxz, x - di) -
+                L(fxz, x - di + dk));
+  };
+  auto fbxy = [&](size_t x) {
+    return e * (two * L(fxy, x) + L(fxy, x + dk) + L(fxy, x - dk) - L(fyx, x) - L(fyx, x + di) - L(fyx, x - dj) -
+                L(fyx, x + di - dj));
+  };
+  auto fbzy = [&](size_t x) {
+    return e * (two * L(fzy, x) + L(fzy, x + di) + L(fzy, x - di) - L(fyz, x) - L(fyz, x + dk) - L(fyz, x - dj) -
+                L(fyz, x - dj + dk));
+  };
+  auto fbxz = [&](size_t x) {
+    return e * (two * L(fxz, x) + L(fxz, x + dj) + L(fxz, x - dj) - L(fzx, x) - L(fzx, x + di) - L(fzx, x - dk) -
+                L(fzx, x + di - dk));
+  };
+  auto fbyz = [&](size_t x) {
+    return e * (two * L(fyz, x) + L(fyz, x + di) + L(fyz, x - di) - L(fzy, x) - L(fzy, x + dj) - L(fzy, x - dk) -
+                L(fzy, x + dj - dk));
+  };
+  // a(c) - b(c) for u > 0, a(n) - b(m) for ul < 0, else the mean over c and n
+  auto up = [&](double u, double ul, auto a, auto b, size_t n, size_t m) {
+    if (u > 0.0) return a(c) - b(c);
+    if (ul < 0.0) return a(n) - b(m);
+    return h * (a(c) + a(n) - b(c) - b(n));
+  };
+  const double u1 = P[1 * N + c], u2 = P[2 * N + c], u3 = P[3 * N + c];
+  double* D = r.ctd;
+  D[0 * N + c] = up(u1, u1, fbyx, ezc, c + di, c + di);  // dyez
+  D[1 * N + c] = up(u2, u1, fbxy, ezc, c + dj, c + dj);  // dxez
+  D[2 * N + c] = up(u3, u1, fbyz, exc, c + dk, c + dk);  // dyex
+  D[3 * N + c] = up(u2, u1, fbzy, exc, c + dj, c + dj);  // dzex
+  D[4 * N + c] = up(u3, u1, fbxz, eyc, c + dk, c + dk);  // dxey
+  D[5 * N + c] = up(u1, u1, fbzx, eyc, c + di, c);       // dzey
+}
 
 // ------------------------------------------------------------ boundaries
 // Transverse indices of a column of direction D: (j,k) for D = 1, (i,k) for
@@ -1624,11 +1720,22 @@ static void launch_ct_t(const DevRun& r, const double* F1, const double* F2, con
   }
 }
 
-cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
-                      cudaStream_t s) {
-  if (r.ict == 0) launch_ct_t<0>(r, F1, F2, F3, CT, s);
-  else if (r.ict == 2) launch_ct_t<2>(r, F1, F2, F3, CT, s);
-  else launch_ct_t<1>(r, F1, F2, F3, CT, s);
+cudaError_t launch_ct(const DevRun& r, const double* P, const double* F1, const double* F2, const double* F3,
+                      double* CT, cudaStream_t s) {
+  if (r.ict == 0) {
+    launch_ct_t<0>(r, F1, F2, F3, CT, s);
+  } else if (r.ict == 2) {
+    launch_ct_t<2>(r, F1, F2, F3, CT, s);
+  } else if (r.ict == 3) {  // FP64 only (the run parameters exclude the mixed path)
+    const int lo = r.nm0 + 1, hi_i = r.imax - r.nm0 - 2, hi_j = r.jmax - r.nm0 - 2, hi_k = r.kmax - r.nm0 - 2;
+    const dim3 b = sblock(r, dim3(64, 4, 1));
+    k_upct_diff<<<sgrid(r, hi_i - lo + 1, hi_j - lo + 1, hi_k - lo + 1, b), b, 0, s>>>(r, P, F1, F2, F3, hi_i,
+                                                                                      hi_j, hi_k);
+    const int clo = r.nm1, chi = r.imax - r.nm1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
+    k_ct<3, double, double><<<sgrid(r, chi - clo + 1, m, l, b), b, 0, s>>>(r, F1, F2, F3, CT, nullptr, clo, chi);
+  } else {
+    launch_ct_t<1>(r, F1, F2, F3, CT, s);
+  }
   return cudaGetLastError();
 }
 
@@ -1672,6 +1779,7 @@ int n_flux_launches(const DevRun& r) {
   return (split >= lo) + (split < hi);
 }
 int n_ct_launches(const DevRun& r) {
+  if (r.ict == 3) return 2;
   if (!r.mixed) return 1;
   const int lo = r.nm1, hi = r.imax - r.nm1, split = fp64_split(r, lo, hi);
   return (split >= lo) + (split < hi);

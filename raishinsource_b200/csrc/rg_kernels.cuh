@@ -16,6 +16,7 @@ struct DevBufs {
   double* CT;     // 6*N flux-CT averaged induction fluxes
   double* stage;  // 9*N staging buffer (layout conversion, per-routine entry points)
   double* stage2; // 9*N second staging buffer
+  double* ctd;    // 6*N upwinded EMF differences of upflct (ict 3 only)
 };
 
 cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s);
@@ -23,8 +24,9 @@ cudaError_t launch_step_begin(const DevRun& r, cudaStream_t s);
 cudaError_t launch_dt(const DevRun& r, cudaStream_t s);
 cudaError_t launch_step_end(const DevRun& r, cudaStream_t s);
 cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s);
-cudaError_t launch_ct(const DevRun& r, const double* F1, const double* F2, const double* F3, double* CT,
-                      cudaStream_t s);
+// P: the stage's primitives (upflct's upwinding reads their velocities)
+cudaError_t launch_ct(const DevRun& r, const double* P, const double* F1, const double* F2, const double* F3,
+                      double* CT, cudaStream_t s);
 cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                           const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s);
 cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t s);

@@ -97,7 +97,8 @@ struct DevRun {
   // CENO): ten planes of n_d values at index m-1 of the cell's coordinate
   // spacings, as limiter_state and ceno_state in rg_recon.cuh read them.
   const double* lim[3];
-  int ict;               // constrained transport: 0 none, 1 flux-CT, 2 modified flux-CT
+  int ict;               // constrained transport: 0 none, 1 flux-CT, 2 modified flux-CT, 3 upwind flux-CT
+  double* ctd;           // ict 3: six planes (6*N) of upflct's upwinded EMF differences
   int ibc[6][9];
   double* P[3];          // the run's rotating primitive buffers (P^n = P[scal->cur])
   double* F[3];          // FP64 face fluxes per direction

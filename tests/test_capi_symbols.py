@@ -44,12 +44,16 @@ def test_footprint_and_param_checks_run_on_cpu():
         assert footprint(dict(p, irec=irec)) > 0
     for ict in (0, 2):
         assert footprint(dict(p, ict=ict)) > 0
-    try:
-        footprint(dict(p, ict=3))  # upflct: not built
-    except RgError as e:
-        assert e.code == 1
-    else:
-        raise AssertionError("ict=3 must be rejected")
+    # upflct keeps six planes of EMF differences besides the step state
+    n = config.torus(nr=256, nth=128, nph=128, ict=3)
+    assert footprint(n) > footprint(dict(n, ict=2))
+    for bad_ct in (dict(n, precision="mixed"), dict(p, ict=4)):  # upflct is FP64 only; no ict 4
+        try:
+            footprint(bad_ct)
+        except RgError as e:
+            assert e.code == 1
+        else:
+            raise AssertionError("must be rejected: %s" % bad_ct)
     bad = dict(p, irec=14)  # no such scheme
     try:
         footprint(bad)

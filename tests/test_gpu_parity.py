@@ -477,11 +477,11 @@ def test_per_routine_calls_leave_the_run_alone(gpu_ctx):
     b.release()
 
 
-@pytest.mark.parametrize("ict", [0, 2])
+@pytest.mark.parametrize("ict", [0, 2, 3])
 def test_constrained_transport_variants(gpu_ctx, ict):
-    """ict = 0 (no CT) and ict = 2 (mflct, ct.f90:121-233): fluxes through
-    the C ABI and one full step per comparison against the oracle, 3D torus;
-    ghost width nm1 = nm0 + ict."""
+    """ict = 0 (no CT), ict = 2 (mflct, ct.f90:121-233) and ict = 3 (upflct,
+    ct.f90:236-445): fluxes through the C ABI and one full step per comparison
+    against the oracle, 3D torus; ghost width nm1 = nm0 + ict."""
     p = dict(config.torus(nr=40, nth=28, nph=20, ict=ict), guard=1)
     o, r = _pair(gpu_ctx, p, seed=40 + ict)
     assert o.nm1 == 3 + ict
@@ -500,12 +500,21 @@ def test_constrained_transport_variants(gpu_ctx, ict):
     r.release()
 
 
-def test_mflct_2d_slab(gpu_ctx):
-    """mflct on a 2D phi slab (stored as one plane, batched path) against the
-    oracle computing every phi cell."""
-    p = dict(config.torus(nr=48, nth=40, ict=2), guard=1)
+@pytest.mark.parametrize("ict", [2, 3])
+def test_ct_variants_2d_slab(gpu_ctx, ict):
+    """mflct and upflct on a 2D phi slab stored as one plane (mflct through the
+    batched kernels, upflct through the single-run launches) against the
+    oracle computing every phi cell; a batch refuses an upflct run."""
+    p = dict(config.torus(nr=48, nth=40, ict=ict), guard=1)
     errs, _ = _step_err(gpu_ctx, p, 2, seed=23)
     assert errs.max() < TOL, errs
+    if ict == 3:
+        from raishinsource_b200.capi import RgError
+        r = gpu_ctx.admit(p)
+        r.ic_torus(seed=23)
+        with pytest.raises(RgError):
+            gpu_ctx.step_batch([r])
+        r.release()
 
 
 def test_kerr_schild_metric(gpu_ctx):

@@ -371,3 +371,54 @@ def test_christoffel_table_is_symmetric_in_its_lower_indices(torus_small):
     _, o = torus_small
     c = o.array("christ").reshape(-1, 4, 4, 4)  # [point][n][m][l]
     assert np.array_equal(c, np.swapaxes(c, 1, 2))
+
+
+def _ct_case(ict, seed=5):
+    p = config.torus(nr=24, nth=20, nph=18, ict=ict)
+    o = Oracle(p)
+    rng = np.random.default_rng(seed)
+    return p, o, rng
+
+
+def test_ct_variants_agree_on_uniform_fluxes():
+    """Face fluxes constant in space: flux-CT, mflct and upflct all give
+    ww(2,7) = (fyx - fxy)/2 and its five companions on their ranges (every
+    EMF difference of the upwind scheme vanishes, whatever the velocity)."""
+    out = {}
+    for ict in (1, 2, 3):
+        p, o, rng = _ct_case(ict)
+        f = np.random.default_rng(1).uniform(-1, 1, 6)
+        ww = np.zeros(o.shape + (3,))
+        for (d, n), v in zip([(2, 7), (3, 7), (1, 8), (3, 8), (1, 9), (2, 9)], f):
+            ww[..., n - 1, d - 1] = v
+        uri = rng.uniform(-1, 1, o.shape)  # velocities of both signs
+        w = o.ct(uri, ww)
+        n = o.nm1  # 1-based range nm1..n-nm1
+        reg = w[n - 1:-n, n - 1:-n, n - 1:-n]
+        fyx, fzx, fxy, fzy, fxz, fyz = f
+        want = {(2, 7): (fyx - fxy) / 2, (3, 7): (fzx - fxz) / 2, (1, 8): (fxy - fyx) / 2,
+                (3, 8): (fzy - fyz) / 2, (1, 9): (fxz - fzx) / 2, (2, 9): (fyz - fzy) / 2}
+        for (d, m), v in want.items():
+            assert np.allclose(reg[..., m - 1, d - 1], v, rtol=0, atol=1e-15), (ict, d, m)
+        out[ict] = reg
+    assert out[1].shape != out[3].shape  # nm1 = nm0 + ict
+
+
+def test_upflct_upwinding_falls_back_on_the_radial_velocity():
+    """upflct's else-if branches after the first EMF test uri(2) (ct.f90:357-387):
+    with u^r = 0 a negative u^phi or u^theta selects the same averaged
+    branch as a zero one, while a positive one selects the upwind value."""
+    p, o, rng = _ct_case(3)
+    ww = rng.uniform(-1, 1, o.shape + (3,))
+    base = np.zeros(o.shape)
+    base[..., 0] = 1.0
+    def run(u2, u3):
+        uri = base.copy()
+        uri[..., 2] = u2
+        uri[..., 3] = u3
+        return o.ct(uri, ww.copy())
+    zero, neg, pos = run(0.0, 0.0), run(-1.0, -1.0), run(1.0, 1.0)
+    n = o.nm1
+    reg = (slice(n - 1, -n), slice(n - 1, -n), slice(n - 1, -n))
+    assert np.array_equal(zero[reg], neg[reg])
+    assert not np.allclose(zero[reg], pos[reg])
