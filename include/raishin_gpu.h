@@ -64,6 +64,10 @@ typedef struct rg_run_params {
                     (Gardiner & Stone 2005, mflct), 3 upwind flux-CT (upflct; FP64 precision
                     only, stepped by rg_step alone: rg_step_batch and rg_calflx_static refuse it).
                     Ghost width nm1 = nm0 + ict (main.f90:192-199). */
+  int iwvec;     /* primitive recovery as pram.f90's iwvec (pram.f90:160-161, recov.f90:2-47):
+                    1 (or 0) recov1a, the reference's setting; 2 recov2 (Mignone & McKinney,
+                    one-variable W; FP64 precision only, stepped by rg_step alone:
+                    rg_step_batch refuses it). */
 } rg_run_params;
 
 /* rg_run_params.flags.  A direction of extent 2*nm1+1 (one interior cell)

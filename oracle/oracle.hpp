@@ -43,7 +43,8 @@ typedef struct {
                               // flux of the normal B component before flux-CT.  Neither is in
                               // the reference (see face_guard and fluxct in oracle_step.cpp).
   int ict;                    // constrained transport (pram.f90:148-151): 0 none, 1 fluxct,
-                              // 2 mflct
+                              // 2 mflct, 3 upflct
+  int iwvec;                  // primitive recovery (pram.f90:160-161): 1 recov1a, 2 recov2
 } orc_params;
 
 typedef struct {
@@ -135,6 +136,8 @@ void calsf_all(State& s, bool every_cell = false);
 void derived(State& s, const std::vector<double>& uri, int jslice, double* out);
 void rkstage(State& s, int stage);
 void recov1a(State& s, std::vector<double>& uu);
+void recov2(State& s, std::vector<double>& uu);
+void recov(State& s, std::vector<double>& uu);  // recov.f90:2-47: recov1a or recov2 by iwvec
 void bnd4(State& s);
 void infchk(State& s);
 void atmosphere1a(State& s);

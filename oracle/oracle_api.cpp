@@ -136,7 +136,7 @@ void orc_recov(void* h, double* uu, double* uri) {
   State* s = static_cast<State*>(h);
   std::vector<double> u(uu, uu + s->uu.size());
   std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
-  orc::recov1a(*s, u);
+  orc::recov(*s, u);
   std::memcpy(uu, u.data(), u.size() * sizeof(double));
   std::memcpy(uri, s->uri.data(), s->uri.size() * sizeof(double));
 }

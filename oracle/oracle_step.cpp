@@ -1463,6 +1463,215 @@ bool recov_cell(const State& s, double* u, double* q, const M4& g, const M4& gc,
 
 }  // namespace
 
+namespace {
+// recov.f90:1919-2456 (recov2, Mignone & McKinney 2007: one-variable
+// Newton-Raphson on W' = W - D, gamma-law EoS), one interior cell, with the
+// reference's own choices kept: D = alpha uu(1) / detg (a division where the
+// other terms multiply by 1/detg), u~^2 < 0 beyond the tolerance reset to
+// 1e4, the "make sure v^2 < 1" pressure p = (W gamma - D sqrt(gamma)) (gam-1)/gam,
+// and p/rho^(gam-1) for uri(6).  As in recov1a the first guess of W is the
+// previous cell's final W when the quadratic has no non-negative root (the
+// caller supplies it, or the cell is reported pending), and the unbounded
+// rescale loop (go to 95) is capped, a capped cell keeping its primitives.
+bool recov2_cell(const State& s, const double* u, double* q, const M4& g, const M4& gc, double detg1,
+                 double x1i, const double* wg_carry, RecovResult& res) {
+  const double gam = s.p.gam;
+  const int iter = s.p.iter;
+  const double safty = 1.0e-5, dv = 1.0e-4;
+  const double gam1 = gam / (gam - 1.0), gam2 = 1.0 / gam1;
+  double delta = 1.0;
+  const double deltaend = 1.e-8;
+  int irecov = 0;
+  const double alpha1 = 1. / std::sqrt(-gc.a[0][0]);
+  const double dro = alpha1 * u[0] / detg1;
+  double qcov[4], qcon[4], bcon[4], bcov[4], oncov[4], oncon[4];
+  qcov[0] = alpha1 * (u[4] - u[0]) * (1. / detg1);
+  qcov[1] = alpha1 * u[1] * (1. / detg1);
+  qcov[2] = alpha1 * u[2] * (1. / detg1);
+  qcov[3] = alpha1 * u[3] * (1. / detg1);
+  bcon[0] = 0.0;
+  bcon[1] = alpha1 * u[6] * (1. / detg1);
+  bcon[2] = alpha1 * u[7] * (1. / detg1);
+  bcon[3] = alpha1 * u[8] * (1. / detg1);
+  double ro = q[0], pp = q[4];
+  double util[4] = {0.0, q[1], q[2], q[3]};
+  const double ro1 = q[0], pp1 = q[4];
+  const double util1[4] = {0.0, q[1], q[2], q[3]};
+  lower(bcon, bcov, g);
+  upper(qcov, qcon, gc);
+  const double bsq = bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
+  const double qdotb = qcov[0] * bcon[0] + qcov[1] * bcon[1] + qcov[2] * bcon[2] + qcov[3] * bcon[3];
+  const double qdotbsq = qdotb * qdotb;
+  oncov[0] = -1.0 * alpha1; oncov[1] = 0.0; oncov[2] = 0.0; oncov[3] = 0.0;
+  upper(oncov, oncon, gc);
+  const double qdotn = qcon[0] * oncov[0];
+  const double qsq = qcov[0] * qcon[0] + qcov[1] * qcon[1] + qcov[2] * qcon[2] + qcov[3] * qcon[3];
+  const double qtsq = qsq + (qdotn * qdotn);
+  double utsq = 0.0;
+  for (int m = 1; m <= 3; ++m)
+    for (int n = 1; n <= 3; ++n) utsq = utsq + g.a[m][n] * util[m] * util[n];
+  if (utsq < 0.0 && std::fabs(utsq) <= safty) utsq = std::fabs(utsq);
+  if (utsq < 0.0 || std::fabs(utsq) > 1.e4) utsq = 1.e4;
+  double gfsq = 1. + utsq;
+  double gf = std::sqrt(gfsq);
+  double vsq = (gfsq - 1.) * (1. / gfsq);
+  const double tmp1a = 4. - vsq;
+  const double tmp1b = 4. * (bsq + qdotn);
+  const double tmp1c = qtsq + bsq * bsq + 2. * bsq * qdotn;
+  double tmp1d = (tmp1b * tmp1b) - 4. * tmp1a * tmp1c;
+  if (tmp1d <= 0.0) tmp1d = std::fabs(tmp1d);
+  const double wgp = (-tmp1b + std::sqrt(tmp1d)) * (1. / (2. * tmp1a));
+  const double wgm = (-tmp1b - std::sqrt(tmp1d)) * (1. / (2. * tmp1a));
+  double wg;
+  if (wgp > 0.0) wg = wgp;
+  else if (wgm >= 0.0) wg = wgm;
+  else {
+    if (!wg_carry) return false;
+    wg = *wg_carry;
+  }
+  bool cap = false;
+  for (int cnt = 0;; ++cnt) {  // recov.f90:2147-2169
+    if (cnt >= kRescaleCap) { cap = true; break; }
+    pp = gam2 * (wg * gf - dro * std::sqrt(gf));
+    const double tmp3a = (wg * wg * wg) * (wg + 2. * bsq) - qdotbsq * (2. * wg + bsq);
+    const double tmp3b = (wg * wg) * (qtsq - bsq * bsq);
+    const double tmp3c = (wg * wg * wg) + (wg * wg) * (0.5 * bsq + qdotn - pp) - 0.5 * qdotbsq;
+    if (tmp3a <= tmp3b) { wg = std::fabs(1.5 * wg); continue; }
+    if (tmp3c > 0.0) { wg = std::fabs(sp(0.9f) * wg); continue; }
+    break;
+  }
+  if (cap) irecov = 1;
+  // Newton-Raphson on W' (recov.f90:2174-2306)
+  double wgd = wg - dro;
+  double xxn = wgd;
+  for (int nnn = 1; nnn <= iter; ++nnn) {
+    if (!(std::fabs(delta) >= deltaend && irecov == 0)) continue;
+    if (nnn == iter) { irecov = 1; continue; }
+    wgd = xxn;
+    wg = wgd + dro;
+    const double wsq = wg * wg, w3 = wsq * wg, xsq = (bsq + wg) * (bsq + wg);
+    vsq = std::fabs((wsq * qtsq + qdotbsq * (bsq + 2. * wg)) * (1. / (wsq * xsq)));
+    if (std::fabs(vsq) > 1.0) vsq = 1.0 - dv;
+    if (vsq < 0.0) vsq = std::fabs(vsq);
+    double gtmp = 1. - vsq;
+    if (gtmp < 0.0 || gtmp < safty) { gtmp = safty; vsq = 1. - gtmp; }
+    const double usq = (1. - gtmp) / (gtmp);
+    gf = std::sqrt(1. + usq);
+    gfsq = gf * gf;
+    ro = dro / gf;
+    const double xi = (wg - dro * gf) * (1. / gfsq);
+    pp = gam2 * xi;
+    const double dpdxi = gam2, dpdro = 0.0;
+    const double ta = (bsq + wg);
+    const double tb = (bsq + wg) * (bsq + wg) * (bsq + wg);
+    const double tc = (qtsq == 0.0) ? 0.0 : -2. * qtsq * (1. / tb);
+    const double td = (qdotbsq == 0.0) ? 0.0 : -2. * qdotbsq * (3. * wg * ta + bsq * bsq) * (1. / (tb * w3));
+    const double dvdwd = tc + td;
+    const double dxidwd = (1. / gfsq) - 0.5 * gf * (dro + 2. * gf * xi) * dvdwd;
+    const double drodwd = -0.5 * dro * gf * dvdwd;
+    const double dpdwd = dpdxi * dxidwd + dpdro * drodwd;
+    const double t5a = bsq * qtsq - qdotbsq;
+    const double t5b = bsq + wgd + dro;
+    double t5c = 0.0, t5d = 0.0;
+    if (t5a != 0.0) {
+      t5c = 0.5 * t5a * (1. / (t5b * t5b));
+      t5d = t5a * (1. / (t5b * t5b * t5b));
+    }
+    const double f = -(qdotn + dro) - wgd + pp - 0.5 * bsq - t5c;
+    const double df = -1. + dpdwd + t5d;
+    delta = f / df;
+    xxn = wgd - delta;
+    if (xxn < 0.0) xxn = std::fabs(xxn);
+    if (xxn > 1.e8) xxn = 1.e8;
+  }
+  if (irecov == 0) {  // recov.f90:2310-2377
+    wgd = xxn;
+    wg = wgd + dro;
+    const double wsq = wg * wg, xsq = (bsq + wg) * (bsq + wg);
+    vsq = std::fabs((wsq * qtsq + qdotbsq * (bsq + 2. * wg)) * (1. / (wsq * xsq)));
+    if (vsq < 0.0) vsq = std::fabs(vsq);
+    if (vsq > 1.0) vsq = 1.0 - dv;
+    double gtmp = 1. - vsq;
+    if (gtmp < safty) gtmp = safty;
+    const double usq = (1. - gtmp) / gtmp;
+    gf = std::sqrt(1. + usq);
+    gfsq = gf * gf;
+    ro = dro / gf;
+    const double xi = wg * (1. / gfsq) - ro;
+    pp = gam2 * xi;
+    if (ro < 0.0) ro = s.p.dmin * std::pow(x1i, -3. / 2.);
+    if (pp < 0.0) pp = s.p.pmin * (gam - 1.) * std::pow(x1i, -5. / 2.);
+    for (int a = 1; a <= 3; ++a) {
+      const double qt = qcon[a] + oncon[a] * qdotn;
+      util[a] = (gf * (1. / (wg + bsq))) * (qt + qdotb * bcon[a] * (1. / wg));
+    }
+  }
+  res.nr2 = false;
+  res.cap = cap;
+  res.fail = (irecov != 0);
+  res.wg_final = wg;
+  // recov.f90:2407-2441
+  if (irecov == 0) {
+    q[0] = ro; q[1] = util[1]; q[2] = util[2]; q[3] = util[3]; q[4] = pp;
+    q[5] = pp / std::pow(ro, gam - 1.);
+  } else {
+    q[0] = ro1; q[1] = util1[1]; q[2] = util1[2]; q[3] = util1[3]; q[4] = pp1;
+    q[5] = pp1 / std::pow(ro1, gam - 1.);
+  }
+  q[6] = u[6] * (1. / detg1); q[7] = u[7] * (1. / detg1); q[8] = u[8] * (1. / detg1);
+  return true;
+}
+}  // namespace
+
+// recov.f90:1919-2456 over the interior, with recov1a's treatment of the
+// loop-order W carry (cells without a root redone in loop order).
+void recov2(State& s, std::vector<double>& uu) {
+  const int nm1 = s.nm1;
+  const int i0 = nm1 + 1, i1 = s.imax - nm1, j0 = nm1 + 1, j1 = s.jmax - nm1, k0 = nm1 + 1, k1 = s.kmax - nm1;
+  const int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return;
+  const size_t nint = (size_t)ni * nj * nk;
+  std::vector<double> wgfin(nint, 0.0);
+  std::vector<unsigned char> pending(nint, 0);
+  long long c_fail = 0, c_cap = 0;
+  auto lin = [&](int i, int j, int k) { return (size_t)(i - i0) + (size_t)ni * ((size_t)(j - j0) + (size_t)nj * (k - k0)); };
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : c_fail, c_cap)
+  for (int k = k0; k <= k1; ++k)
+    for (int j = j0; j <= j1; ++j)
+      for (int i = i0; i <= i1; ++i) {
+        const size_t q = s.ik(i, k);
+        RecovResult r{0, false, false, false};
+        if (!recov2_cell(s, &uu[s.a(1, i, j, k)], &s.uri[s.a(1, i, j, k)], s.gcov[q], s.gcon[q], s.detg[q], s.x1[i],
+                         nullptr, r)) {
+          pending[lin(i, j, k)] = 1;
+          continue;
+        }
+        wgfin[lin(i, j, k)] = r.wg_final;
+        c_fail += r.fail; c_cap += r.cap;
+      }
+  long long c_carry = 0;
+  for (size_t l = 0; l < nint; ++l) {
+    if (!pending[l]) continue;
+    const int i = i0 + (int)(l % ni), j = j0 + (int)((l / ni) % nj), k = k0 + (int)(l / ((size_t)ni * nj));
+    const double wprev = (l == 0) ? 0.0 : wgfin[l - 1];
+    const size_t q = s.ik(i, k);
+    RecovResult r{0, false, false, false};
+    recov2_cell(s, &uu[s.a(1, i, j, k)], &s.uri[s.a(1, i, j, k)], s.gcov[q], s.gcon[q], s.detg[q], s.x1[i], &wprev, r);
+    wgfin[l] = r.wg_final;
+    c_fail += r.fail; c_cap += r.cap;
+    ++c_carry;
+  }
+  s.st.recov_calls += (long long)nint;
+  s.st.recov_fail += c_fail;
+  s.st.recov_cap += c_cap;
+  s.st.recov_carry += c_carry;
+}
+
+void recov(State& s, std::vector<double>& uu) {
+  if (s.p.iwvec == 2) recov2(s, uu);
+  else recov1a(s, uu);
+}
+
 // recov.f90:578-1228 over the interior.  The reference carries W from one cell
 // to the next in loop order when the quadratic has no non-negative root; the
 // cells are computed in parallel first and those few cells are then redone
@@ -1828,7 +2037,7 @@ void step(State& s) {
     calsf_all(s);
     rkstage(s, stage);
     std::vector<double>& un = (stage == 1) ? s.uh : (stage == 2 ? s.us : s.un);
-    recov1a(s, un);
+    recov(s, un);
     bnd4(s);
     if (inflow) infchk(s);
     if (torus) atmosphere1a(s);

@@ -28,6 +28,7 @@ class OrcParams(C.Structure):
         ("ibc", (C.c_int * 9) * 6),
         ("guard", C.c_int),
         ("ict", C.c_int),
+        ("iwvec", C.c_int),
     ]
 
 
@@ -95,7 +96,7 @@ def make_params(p: dict) -> OrcParams:
                 for m in range(9):
                     o.ibc[s][m] = int(p["ibc"][s][m])
         else:
-            default = {"guard": 0, "ict": 1}
+            default = {"guard": 0, "ict": 1, "iwvec": 1}
             setattr(o, name, p.get(name, default[name]) if name in default else p[name])
     return o
 

@@ -53,6 +53,7 @@ class RunParams(C.Structure):
         ("precision", C.c_int),
         ("flags", C.c_int),
         ("ict", C.c_int),
+        ("iwvec", C.c_int),
     ]
 
 
@@ -150,6 +151,8 @@ def make_params(p: dict) -> RunParams:
             o.flags = int(p.get("flags", 0))
         elif name == "ict":
             o.ict = int(p.get("ict", 1))
+        elif name == "iwvec":
+            o.iwvec = int(p.get("iwvec", 1))
         elif name == "precision":
             o.precision = {"fp64": 0, "mixed": 1}[p.get("precision", "fp64")]
         else:

@@ -133,6 +133,10 @@ int check_params(const rg_run_params* p) {
     return fail(RG_EINVAL_CONFIG, "ict must be 0 (none), 1 (flux-CT), 2 (modified flux-CT) or 3 (upwind flux-CT)");
   if (p->ict == 3 && p->precision == RG_MIXED)
     return fail(RG_EINVAL_CONFIG, "upwind flux-CT (ict 3) runs in FP64 only");
+  if (p->iwvec < 0 || p->iwvec > 2)
+    return fail(RG_EINVAL_CONFIG, "iwvec must be 1 (recov1a; 0 means 1) or 2 (recov2)");
+  if (p->iwvec == 2 && p->precision == RG_MIXED)
+    return fail(RG_EINVAL_CONFIG, "recov2 (iwvec 2) runs in FP64 only");
   if (p->metric != 1 && p->metric != 303 && p->metric != 403)
     return fail(RG_EINVAL_CONFIG, "metric must be 1, 303 or 403");
   if (p->ix1 != 1 && p->ix1 != 2) return fail(RG_EINVAL_CONFIG, "ix1 must be 1 or 2");
@@ -208,7 +212,8 @@ size_t footprint_bytes(const rg_run_params* p) {
   if (p->precision == RG_MIXED)  // P32, F32 x3, CT32; FP32 metric caches and Christoffels
     mixed = (9 + 27 + 6) * N * sizeof(float) + (3 * kMetComps + 64) * nik * sizeof(float);
   const size_t upct = (p->ict == 3) ? 6 * N * sizeof(double) : 0;  // upflct's EMF differences
-  return state + geom + mixed + upct + sizeof(Scal) + C_NCOUNTERS * 8 + (kCarryCap + straggler_cap(N)) * sizeof(int);
+  const size_t rec2 = (p->iwvec == 2) ? 22 * N * sizeof(double) : 0;  // recov2 stage scratch
+  return state + geom + mixed + upct + rec2 + sizeof(Scal) + C_NCOUNTERS * 8 + (kCarryCap + straggler_cap(N)) * sizeof(int);
 }
 
 Run* find(rg_ctx* ctx, int id) {
@@ -457,9 +462,17 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
   RG_CUDA(issue(ctx, K_FLUX2, nf, [&] { return launch_flux(d, 2, Pc, R->b.F[1], s); }));
   RG_CUDA(issue(ctx, K_FLUX3, nf, [&] { return launch_flux(d, 3, Pc, R->b.F[2], s); }));
   RG_CUDA(issue(ctx, K_CT, n_ct_launches(d), [&] { return launch_ct(d, Pc, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s); }));
-  RG_CUDA(issue(ctx, K_UPDATE, n_update_launches(d), [&] {
-    return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s);
-  }));
+  if (d.iwvec == 2) {
+    const size_t N = d.N;
+    RG_CUDA(issue(ctx, K_UPDATE, 6, [&] {
+      return launch_stage_recov2(d, stage, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, R->b.r2,
+                                 R->b.r2 + 9 * N, R->b.r2 + 13 * N, s);
+    }));
+  } else {
+    RG_CUDA(issue(ctx, K_UPDATE, n_update_launches(d), [&] {
+      return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s);
+    }));
+  }
   RG_CUDA(issue(ctx, K_BC, n_bc_launches(d), [&] { return launch_bc(d, Pw, Pn, s); }));
   RG_CUDA(issue(ctx, K_FLOOR, 1, [&] { return launch_floor(d, Pw, s); }));
   return RG_OK;
@@ -825,6 +838,7 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   d.nm0 = nm0_of(p->irec);
   d.nm1 = d.nm0 + p->ict;
   d.ict = p->ict;
+  d.iwvec = (p->iwvec == 2) ? 2 : 1;
   d.irec = p->irec; d.model = p->model; d.guard = p->guard; d.iter = p->iter;
   d.mixed = (p->precision == RG_MIXED);
 #ifdef RG_EXACT_ARITH
@@ -877,6 +891,10 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
     if ((rc = dalloc(R, &ptr, 6 * N * sizeof(double)))) return bail(rc);
     R->b.ctd = static_cast<double*>(ptr);
     d.ctd = R->b.ctd;
+  }
+  if (d.iwvec == 2) {
+    if ((rc = dalloc(R, &ptr, 22 * N * sizeof(double)))) return bail(rc);
+    R->b.r2 = static_cast<double*>(ptr);
   }
   if ((rc = dalloc(R, &ptr, 9 * N * sizeof(double)))) return bail(rc);
   d.Un = static_cast<double*>(ptr);
@@ -1099,8 +1117,8 @@ int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats) {
   // A run with a slab direction steps as a batch of one: it then runs the same
   // compiled kernels alone as in any batch, so its results do not depend on
   // the company it keeps, and its step is replayed from a CUDA graph.
-  // (upwind flux-CT has no batched kernels: such a run keeps the launches below)
-  if ((R->d.jfix || R->d.kfix) && R->d.ict != 3) return rg_step_batch(ctx, &run, 1, nsteps, stats);
+  // (upwind flux-CT and recov2 have no batched kernels: such a run keeps the launches below)
+  if ((R->d.jfix || R->d.kfix) && R->d.ict != 3 && R->d.iwvec != 2) return rg_step_batch(ctx, &run, 1, nsteps, stats);
   cudaStream_t s = ctx->stream;
   for (int n = 0; n < nsteps; ++n) {
     double* Pn = R->b.P[R->cur];
@@ -1131,6 +1149,7 @@ int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_s
     Run* R = find(ctx, runs[a]);
     if (!R) return fail(RG_ENOTFOUND, "unknown run in batch");
     if (R->d.ict == 3) return fail(RG_EINVAL_CONFIG, "upwind flux-CT (ict 3) runs step alone (rg_step)");
+    if (R->d.iwvec == 2) return fail(RG_EINVAL_CONFIG, "recov2 (iwvec 2) runs step alone (rg_step)");
     groups[batch_class(R)].push_back(runs[a]);
   }
   std::vector<BatchEntry*> es;

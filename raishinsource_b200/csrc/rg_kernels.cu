@@ -294,6 +294,170 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
   return true;
 }
 
+// recov.f90:1919-2456 (recov2, iwvec 2: Mignone & McKinney's one-variable
+// Newton-Raphson on W' = W - D, gamma-law EoS), one interior cell, with the
+// interface of recov_cell: the first W guess of a cell whose quadratic has no
+// non-negative root comes from the previous cell in loop order (wg_carry, or
+// false without one), and the unbounded rescale loop is capped (the capped
+// cell keeps its primitives).  The reference's own choices are kept: D =
+// alpha uu(1)/detg by division, u~^2 < 0 beyond the tolerance reset to 1e4,
+// p = (W gamma - D sqrt(gamma)) (gam-1)/gam in the rescale loop, and
+// p/rho^(gam-1) for uri(6).  No deferral: the iteration is one-dimensional.
+__device__ bool recov2_cell(const double u[9], const double q[9], double out[9], const Met& m, double gam, int gkind,
+                            int iter, double demin_i, double prmin_i, const double* wg_carry, RecovOut& res) {
+  const double safty = 1.0e-5, dv = 1.0e-4;
+  const double gam1 = gam / (gam - 1.0), gam2 = 1.0 / gam1;
+  const double idetg1 = m.idetg;
+  double delta = 1.0;
+  const double deltaend = 1.e-8;
+  int irecov = 0;
+  const double alpha1 = m.al;
+  const double dro = alpha1 * u[0] / m.detg;
+  double qcov[4], qcon[4], bcon[4], bcov[4], oncov[4], oncon[4];
+  qcov[0] = alpha1 * (u[4] - u[0]) * idetg1;
+  qcov[1] = alpha1 * u[1] * idetg1;
+  qcov[2] = alpha1 * u[2] * idetg1;
+  qcov[3] = alpha1 * u[3] * idetg1;
+  bcon[0] = 0.0;
+  bcon[1] = alpha1 * u[6] * idetg1;
+  bcon[2] = alpha1 * u[7] * idetg1;
+  bcon[3] = alpha1 * u[8] * idetg1;
+  double ro = q[0], pp = q[4];
+  double util[4] = {0.0, q[1], q[2], q[3]};
+  lower_g(bcon, bcov, m);
+  upper_gc(qcov, qcon, m);
+  const double bsq = bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
+  const double qdotb = qcov[0] * bcon[0] + qcov[1] * bcon[1] + qcov[2] * bcon[2] + qcov[3] * bcon[3];
+  const double qdotbsq = qdotb * qdotb;
+  oncov[0] = -1.0 * alpha1; oncov[1] = 0.0; oncov[2] = 0.0; oncov[3] = 0.0;
+  upper_gc(oncov, oncon, m);
+  const double qdotn = qcon[0] * oncov[0];
+  const double qsq = qcov[0] * qcon[0] + qcov[1] * qcon[1] + qcov[2] * qcon[2] + qcov[3] * qcon[3];
+  const double qtsq = qsq + (qdotn * qdotn);
+  double utsq = qform3(m, util[1], util[2], util[3]);
+  if (utsq < 0.0 && fabs(utsq) <= safty) utsq = fabs(utsq);
+  if (utsq < 0.0 || fabs(utsq) > 1.e4) utsq = 1.e4;
+  double gfsq = 1. + utsq;
+  double gf = sqrt(gfsq);
+  double vsq = (gfsq - 1.) * (1. / gfsq);
+  const double t1a = 4. - vsq;
+  const double t1b = 4. * (bsq + qdotn);
+  const double t1c = qtsq + bsq * bsq + 2. * bsq * qdotn;
+  double t1d = (t1b * t1b) - 4. * t1a * t1c;
+  if (t1d <= 0.0) t1d = fabs(t1d);
+  const double wgp = (-t1b + sqrt(t1d)) * (1. / (2. * t1a));
+  const double wgm = (-t1b - sqrt(t1d)) * (1. / (2. * t1a));
+  double wg;
+  if (wgp > 0.0) wg = wgp;
+  else if (wgm >= 0.0) wg = wgm;
+  else {
+    if (!wg_carry) return false;
+    wg = *wg_carry;
+  }
+  bool cap = false;
+  for (int cnt = 0;; ++cnt) {  // recov.f90:2147-2169
+    if (cnt >= kRescaleCap) { cap = true; break; }
+    pp = gam2 * (wg * gf - dro * sqrt(gf));
+    const double t3a = (wg * wg * wg) * (wg + 2. * bsq) - qdotbsq * (2. * wg + bsq);
+    const double t3b = (wg * wg) * (qtsq - bsq * bsq);
+    const double t3c = (wg * wg * wg) + (wg * wg) * (0.5 * bsq + qdotn - pp) - 0.5 * qdotbsq;
+    if (t3a <= t3b) { wg = fabs(1.5 * wg); continue; }
+    if (t3c > 0.0) { wg = fabs((double)0.9f * wg); continue; }
+    break;
+  }
+  if (cap) irecov = 1;
+  // Newton-Raphson on W' (recov.f90:2174-2306)
+  double wgd = wg - dro;
+  double xxn = wgd;
+  for (int nnn = 1; nnn <= iter; ++nnn) {
+    if (!(fabs(delta) >= deltaend && irecov == 0)) break;  // nothing changes in the remaining iterations
+    if (nnn == iter) { irecov = 1; break; }
+    wgd = xxn;
+    wg = wgd + dro;
+    const double wsq = wg * wg, w3 = wsq * wg, xsq = (bsq + wg) * (bsq + wg);
+    vsq = fabs((wsq * qtsq + qdotbsq * (bsq + 2. * wg)) * (1. / (wsq * xsq)));
+    if (fabs(vsq) > 1.0) vsq = 1.0 - dv;
+    if (vsq < 0.0) vsq = fabs(vsq);
+    double gtmp = 1. - vsq;
+    if (gtmp < 0.0 || gtmp < safty) { gtmp = safty; vsq = 1. - gtmp; }
+    const double usq = (1. - gtmp) / (gtmp);
+    gf = sqrt(1. + usq);
+    gfsq = gf * gf;
+    ro = dro / gf;
+    const double xi = (wg - dro * gf) * (1. / gfsq);
+    pp = gam2 * xi;
+    const double dpdxi = gam2, dpdro = 0.0;
+    const double ta = (bsq + wg);
+    const double tb = (bsq + wg) * (bsq + wg) * (bsq + wg);
+    const double tc = (qtsq == 0.0) ? 0.0 : -2. * qtsq * (1. / tb);
+    const double td = (qdotbsq == 0.0) ? 0.0 : -2. * qdotbsq * (3. * wg * ta + bsq * bsq) * (1. / (tb * w3));
+    const double dvdwd = tc + td;
+    const double dxidwd = (1. / gfsq) - 0.5 * gf * (dro + 2. * gf * xi) * dvdwd;
+    const double drodwd = -0.5 * dro * gf * dvdwd;
+    const double dpdwd = dpdxi * dxidwd + dpdro * drodwd;
+    const double t5a = bsq * qtsq - qdotbsq;
+    const double t5b = bsq + wgd + dro;
+    double t5c = 0.0, t5d = 0.0;
+    if (t5a != 0.0) {
+      t5c = 0.5 * t5a * (1. / (t5b * t5b));
+      t5d = t5a * (1. / (t5b * t5b * t5b));
+    }
+    const double f = -(qdotn + dro) - wgd + pp - 0.5 * bsq - t5c;
+    const double df = -1. + dpdwd + t5d;
+    delta = f / df;
+    xxn = wgd - delta;
+    if (xxn < 0.0) xxn = fabs(xxn);
+    if (xxn > 1.e8) xxn = 1.e8;
+  }
+  if (irecov == 0) {  // recov.f90:2310-2377
+    wgd = xxn;
+    wg = wgd + dro;
+    const double wsq = wg * wg, xsq = (bsq + wg) * (bsq + wg);
+    vsq = fabs((wsq * qtsq + qdotbsq * (bsq + 2. * wg)) * (1. / (wsq * xsq)));
+    if (vsq < 0.0) vsq = fabs(vsq);
+    if (vsq > 1.0) vsq = 1.0 - dv;
+    double gtmp = 1. - vsq;
+    if (gtmp < safty) gtmp = safty;
+    const double usq = (1. - gtmp) / gtmp;
+    gf = sqrt(1. + usq);
+    gfsq = gf * gf;
+    ro = dro / gf;
+    const double xi = wg * (1. / gfsq) - ro;
+    pp = gam2 * xi;
+    if (ro < 0.0) ro = demin_i;
+    if (pp < 0.0) pp = prmin_i;
+#pragma unroll
+    for (int a = 1; a <= 3; ++a) {
+      const double qt = qcon[a] + oncon[a] * qdotn;
+      util[a] = (gf * (1. / (wg + bsq))) * (qt + qdotb * bcon[a] * (1. / wg));
+    }
+  }
+  res.nr2 = false;
+  res.cap = cap;
+  res.fail = (irecov != 0);
+  res.wg = wg;
+  if (irecov == 0) {  // recov.f90:2407-2441
+    out[0] = ro; out[1] = util[1]; out[2] = util[2]; out[3] = util[3]; out[4] = pp;
+    out[5] = pp / pow_gam1(ro, gam, gkind);
+  } else {
+    out[0] = q[0]; out[1] = q[1]; out[2] = q[2]; out[3] = q[3]; out[4] = q[4];
+    out[5] = q[4] / pow_gam1(q[0], gam, gkind);
+  }
+  out[6] = u[6] * idetg1;
+  out[7] = u[7] * idetg1;
+  out[8] = u[8] * idetg1;
+  return true;
+}
+
+// recov1a (IWVEC 1) or recov2 (IWVEC 2) of one cell.
+template <int IWVEC>
+__device__ __forceinline__ bool recov_any(const double u[9], const double q[9], double out[9], const Met& m, double gam,
+                                          int gkind, int iter, double demin_i, double prmin_i,
+                                          const double* wg_carry, RecovOut& res) {
+  if constexpr (IWVEC == 2) return recov2_cell(u, q, out, m, gam, gkind, iter, demin_i, prmin_i, wg_carry, res);
+  else return recov_cell(u, q, out, m, gam, gkind, iter, demin_i, prmin_i, wg_carry, res);
+}
+
 // ------------------------------------------------------------ stage update
 // calsf.f90:107-151 with caltenr's T^m_n (calsf.f90:6-104): the source
 // S_nu = sqrt(-g) sum_{n,m} T^m_n Gamma^n_{nu m} of one cell from its
@@ -641,7 +805,7 @@ __global__ void __launch_bounds__(128, RG_UPDATE_MINB) k_update(DevRun r, const 
 // (k, j, i over the interior): each takes the final W of its predecessor cell.
 // One thread; runs only when cells were queued, which the reference data
 // rarely produces.  MODE 0: stage update; MODE 1: recov-only entry point.
-template <int MODE, int STAGE>
+template <int MODE, int STAGE, int IWVEC = 1>
 __device__ void carry_fix_body(const DevRun& r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                                double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                                const double* __restrict__ F3, const double* __restrict__ CT,
@@ -676,7 +840,7 @@ __device__ void carry_fix_body(const DevRun& r, const double* __restrict__ Pn, c
     else if (MODE == 0) stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, dt, u);
     else load9(U, r.N, c, u);
     load9(Pc, r.N, c, qo);
-    const bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, r.fl_de[i - 1], r.fl_pr[i - 1], carry, o);
+    const bool ok = recov_any<IWVEC>(u, qo, qn, m, r.gam, r.gkind, r.iter, r.fl_de[i - 1], r.fl_pr[i - 1], carry, o);
     if (ok) {
       wg_out = o.wg;
       if (write)
@@ -711,11 +875,11 @@ __device__ void carry_fix_body(const DevRun& r, const double* __restrict__ Pn, c
   }
   r.scal->carry_count = 0;
 }
-template <int MODE, int STAGE>
+template <int MODE, int STAGE, int IWVEC = 1>
 __global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                             double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                             const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) carry_fix_body<MODE, STAGE>(r, Pn, Pc, Pw, F1, F2, F3, CT, U);
+  if (threadIdx.x == 0 && blockIdx.x == 0) carry_fix_body<MODE, STAGE, IWVEC>(r, Pn, Pc, Pw, F1, F2, F3, CT, U);
 }
 
 // ------------------------------------------------------------- face fluxes
@@ -1356,6 +1520,9 @@ __global__ void k_dt(DevRun r) { dt_body(r); }
 __global__ void k_step_end(DevRun r) { step_end_body(r); }
 
 // ------------------------------------------------- per-routine entry points
+// recov (recov.f90:2-47) of every interior cell; other cells, and every cell
+// of a run that has passed tmax, keep Pc.
+template <int IWVEC>
 __global__ void __launch_bounds__(128) k_recov(DevRun r, const double* __restrict__ U, const double* __restrict__ Pc,
                                                double* __restrict__ Pw) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -1363,7 +1530,7 @@ __global__ void __launch_bounds__(128) k_recov(DevRun r, const double* __restric
   const int k = kidx(r, 1, blockIdx);
   if (i > r.imax || j > r.jmax || k > r.kmax) return;
   const size_t N = r.N, c = r.cell(i, j, k);
-  if (!is_interior(r, i, j, k)) {
+  if (!r.scal->active || !is_interior(r, i, j, k)) {
 #pragma unroll
     for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = Pc[(size_t)v * N + c];
     return;
@@ -1374,7 +1541,8 @@ __global__ void __launch_bounds__(128) k_recov(DevRun r, const double* __restric
   load9(U, N, c, u);
   load9(Pc, N, c, qo);
   RecovOut o{0.0, false, false, false};
-  const bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, __ldg(r.fl_de + i - 1), __ldg(r.fl_pr + i - 1), nullptr, o);
+  const bool ok =
+      recov_any<IWVEC>(u, qo, qn, m, r.gam, r.gkind, r.iter, __ldg(r.fl_de + i - 1), __ldg(r.fl_pr + i - 1), nullptr, o);
   if (!ok) queue_carry(r, i, j, k);
   else
 #pragma unroll
@@ -1530,7 +1698,8 @@ template <int STAGE>
 __global__ void __launch_bounds__(128) k_rkt(DevRun r, const double* __restrict__ W1, const double* __restrict__ W2,
                                              const double* __restrict__ W3, const double* __restrict__ Uo,
                                              const double* __restrict__ Uc, const double* __restrict__ SF,
-                                             double* __restrict__ Unew, double dt) {
+                                             double* __restrict__ Unew, double dt, bool step_dt = false) {
+  if (step_dt) dt = r.scal->dt;  // inside a step: the step's dt (main.f90:763)
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = jidx(r, 1, blockIdx);
   const int k = kidx(r, 1, blockIdx);
@@ -1862,8 +2031,53 @@ cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s) {
 
 cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s) {
   const dim3 b = sblock(r, dim3(64, 2, 1));
-  k_recov<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
-  k_carry_fix<1, 1><<<1, 1, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
+  if (r.iwvec == 2) {
+    k_recov<2><<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
+    k_carry_fix<1, 1, 2><<<1, 1, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
+  } else {
+    k_recov<1><<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
+    k_carry_fix<1, 1><<<1, 1, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
+  }
+  return cudaGetLastError();
+}
+
+// A stage of a recov2 run in the reference's sequence (main.f90:807-899):
+// the CT values written into the face fluxes (ct edits ww in place), the
+// conserved variables of the stage's primitives (caluu1; those of P^n, the
+// step's uo, kept from stage 1), the geometric source, the RK combine with
+// the step's dt, then recov2 with its loop-order carry pass.
+__global__ void k_ct_into_fluxes(DevRun r, const double* __restrict__ CT, double* __restrict__ F1,
+                                 double* __restrict__ F2, double* __restrict__ F3) {
+  const int nm1 = r.nm1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + nm1;
+  const int j = jidx(r, nm1, blockIdx);
+  const int k = kidx(r, nm1, blockIdx);
+  if (i > r.imax - nm1 || j > r.jmax - nm1 || k > r.kmax - nm1) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  // ww(2,7) ww(3,7) ww(1,8) ww(3,8) ww(1,9) ww(2,9)
+  F2[6 * N + c] = CT[0 * N + c];
+  F3[6 * N + c] = CT[1 * N + c];
+  F1[7 * N + c] = CT[2 * N + c];
+  F3[7 * N + c] = CT[3 * N + c];
+  F1[8 * N + c] = CT[4 * N + c];
+  F2[8 * N + c] = CT[5 * N + c];
+}
+
+cudaError_t launch_stage_recov2(const DevRun& r, int stage, const double* Pc, double* Pw, double* F1, double* F2,
+                                double* F3, const double* CT, double* Uc, double* SF, double* Unew, cudaStream_t s) {
+  const dim3 bc = sblock(r, dim3(64, 4, 1));
+  const int n = r.imax - 2 * r.nm1 + 1, m = r.jmax - 2 * r.nm1 + 1, l = r.kmax - 2 * r.nm1 + 1;
+  k_ct_into_fluxes<<<sgrid(r, n, m, l, bc), bc, 0, s>>>(r, CT, F1, F2, F3);
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 g = sgrid(r, r.imax, r.jmax, r.kmax, b);
+  double* Ucur = (stage == 1) ? r.Un : Uc;
+  k_p2c<<<g, b, 0, s>>>(r, Pc, Ucur);
+  k_calsf<<<g, b, 0, s>>>(r, Pc, SF);
+  if (stage == 1) k_rkt<1><<<g, b, 0, s>>>(r, F1, F2, F3, r.Un, Ucur, SF, Unew, 0.0, true);
+  else if (stage == 2) k_rkt<2><<<g, b, 0, s>>>(r, F1, F2, F3, r.Un, Ucur, SF, Unew, 0.0, true);
+  else k_rkt<3><<<g, b, 0, s>>>(r, F1, F2, F3, r.Un, Ucur, SF, Unew, 0.0, true);
+  k_recov<2><<<g, b, 0, s>>>(r, Unew, Pc, Pw);
+  k_carry_fix<1, 1, 2><<<1, 1, 0, s>>>(r, nullptr, Pc, Pw, nullptr, nullptr, nullptr, nullptr, Unew);
   return cudaGetLastError();
 }
 

@@ -17,6 +17,7 @@ struct DevBufs {
   double* stage;  // 9*N staging buffer (layout conversion, per-routine entry points)
   double* stage2; // 9*N second staging buffer
   double* ctd;    // 6*N upwinded EMF differences of upflct (ict 3 only)
+  double* r2;     // recov2 runs: 22*N of stage scratch (Uc 9N, SF 4N, Unew 9N)
 };
 
 cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s);
@@ -33,6 +34,10 @@ cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t
 cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s);
 // per-routine entry points
 cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s);
+// One RK stage of a recov2 run after its fluxes and CT: the CT values are
+// written into F1-F3; Uc, SF, Unew are 9N, 4N and 9N of scratch.
+cudaError_t launch_stage_recov2(const DevRun& r, int stage, const double* Pc, double* Pw, double* F1, double* F2,
+                                double* F3, const double* CT, double* Uc, double* SF, double* Unew, cudaStream_t s);
 cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s);
 cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStream_t s);
 cudaError_t launch_derived(const DevRun& r, const double* P, const double* geo_i, const double* geo_k, double akm,

@@ -99,6 +99,7 @@ struct DevRun {
   const double* lim[3];
   int ict;               // constrained transport: 0 none, 1 flux-CT, 2 modified flux-CT, 3 upwind flux-CT
   double* ctd;           // ict 3: six planes (6*N) of upflct's upwinded EMF differences
+  int iwvec;             // primitive recovery: 1 recov1a, 2 recov2
   int ibc[6][9];
   double* P[3];          // the run's rotating primitive buffers (P^n = P[scal->cur])
   double* F[3];          // FP64 face fluxes per direction

@@ -47,7 +47,10 @@ def test_footprint_and_param_checks_run_on_cpu():
     # upflct keeps six planes of EMF differences besides the step state
     n = config.torus(nr=256, nth=128, nph=128, ict=3)
     assert footprint(n) > footprint(dict(n, ict=2))
-    for bad_ct in (dict(n, precision="mixed"), dict(p, ict=4)):  # upflct is FP64 only; no ict 4
+    # recov2 keeps 22 planes of stage scratch
+    assert footprint(dict(p, iwvec=2)) > footprint(p)
+    for bad_ct in (dict(n, precision="mixed"), dict(p, ict=4),  # upflct is FP64 only; no ict 4
+                   dict(p, iwvec=2, precision="mixed"), dict(p, iwvec=3)):  # recov2 is FP64 only
         try:
             footprint(bad_ct)
         except RgError as e:

@@ -542,3 +542,38 @@ def test_kerr_schild_metric(gpu_ctx):
     err = _derived_err(r.derived(), o.derived(u))
     assert err.max() < TOL, err
     r.release()
+
+
+@pytest.mark.parametrize("nph", [16, None])
+def test_recov2(gpu_ctx, nph):
+    """recov2 (iwvec 2, recov.f90:1919-2456): two full steps (the reference's
+    stage sequence: fluxes with CT, caluu1, calsf, rkt, recov2) per comparison
+    on a 3D torus and on a 2D phi slab stored as one plane, with the oracle's
+    count of cells that keep their primitives; then rg_recov on perturbed
+    conserved variables (after the steps: the oracle's recov leaves its result
+    in the oracle's state).  A batch refuses the run."""
+    p = dict(config.torus(nr=40, nth=28, nph=nph), guard=1, iwvec=2)
+    o, r = _pair(gpu_ctx, p, seed=77)
+    o.init_cons()
+    for _ in range(2):
+        o.step(1)
+        st = r.step(1, stats=True, strict=False)
+        err = _vector_scaled_err(r.prims(), o.prims())
+        assert err.max() < TOL, err
+        r.upload_prims(o.prims(), t0=o.time)
+    assert st["recov_fail"] == o.stats()["recov_fail"]  # both counted over the two steps
+    u = o.prims()
+    n = o.nm1
+    reg = (slice(n, -n), slice(n, -n), slice(n, -n))
+    uu = o.caluu1(u)
+    pert = uu.copy()
+    rng = np.random.default_rng(1)
+    pert[n:-n, n:-n, n:-n, :5] *= 1 + 1e-3 * rng.standard_normal(pert[n:-n, n:-n, n:-n, :5].shape)
+    got = r.recov(pert, u)
+    _, want = o.recov(pert, u)
+    err = field_err(got, want, reg)
+    assert err[[0, 1, 2, 3, 4, 6, 7, 8]].max() < TOL, err
+    from raishinsource_b200.capi import RgError
+    with pytest.raises(RgError):
+        gpu_ctx.step_batch([r])
+    r.release()

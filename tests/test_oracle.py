@@ -422,3 +422,28 @@ def test_upflct_upwinding_falls_back_on_the_radial_velocity():
     reg = (slice(n - 1, -n), slice(n - 1, -n), slice(n - 1, -n))
     assert np.array_equal(zero[reg], neg[reg])
     assert not np.allclose(zero[reg], pos[reg])
+
+
+def test_recov2_recovers_the_primitives_of_their_conserved_variables():
+    """recov2 (iwvec 2, recov.f90:1919-2456) applied to caluu1 of a torus state,
+    starting from perturbed guesses, returns that state wherever its
+    one-variable Newton-Raphson converges (W' to 1e-8), as recov1a does."""
+    p = dict(config.torus(nr=48, nth=40), iwvec=2)
+    o = Oracle(p)
+    o.ic_torus(seed=8)
+    q = o.prims()
+    u = o.caluu1(q)
+    guess = q.copy()
+    rng = np.random.default_rng(3)
+    guess[..., 1:5] *= 1.0 + 0.01 * rng.uniform(-1, 1, guess[..., 1:5].shape)
+    _, got = o.recov(u, guess)
+    n = o.nm1
+    reg = (slice(n, -n), slice(n, -n), slice(n, -n))
+    st = o.stats()
+    assert st["recov_fail"] == 0 and st["recov_cap"] == 0
+    rel = np.abs(got[reg] - q[reg])[..., [0, 4]] / np.abs(q[reg])[..., [0, 4]]
+    assert np.median(rel) < 1e-10 and rel.max() < 1e-5, (np.median(rel), rel.max())
+    o1 = Oracle(dict(p, iwvec=1))
+    _, got1 = o1.recov(u, guess)
+    assert not np.array_equal(got1[reg], got[reg])  # a different inversion ran
+    assert np.abs(got1[reg] - got[reg])[..., [0, 4]].max() / np.abs(q[reg])[..., [0, 4]].min() < 1e-3
