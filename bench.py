@@ -295,7 +295,8 @@ def run_gpu(args) -> dict | None:
     fp64_peak = fp64_peak_tflops(dev) if (rank == 0 and args.prof_steps > 0) else None
     extra = {}
     if ws == 1:
-        sections = (("mixed", args.mixed_steps, section_mixed), ("torus2d", args.torus2d_steps, section_torus2d),
+        sections = (("scheme_variants", args.variant_steps, section_variants),
+                    ("mixed", args.mixed_steps, section_mixed), ("torus2d", args.torus2d_steps, section_torus2d),
                     ("batched_tubes", args.tubes, section_tubes), ("serving", args.serve_requests, section_serving))
         for name, n, fn in sections:
             if n > 0:
@@ -351,6 +352,33 @@ def _rel_errs(got, ref, n):
     linf = d.max(axis=(0, 1, 2)) / np.abs(b).max(axis=(0, 1, 2)).clip(1e-300)
     names = {"rho": 0, "p": 4, "B1": 6, "B2": 7, "B3": 8}
     return ({k: float(l1[v]) for k, v in names.items()}, {k: float(linf[v]) for k, v in names.items()})
+
+
+def section_variants(ctx, args) -> dict:
+    """The headline grid with the other reconstructions of its workload
+    family, PPM and WENO5 (FP64, same initial data and time step rules)."""
+    import torch
+    from raishinsource_b200 import config
+    stream = torch.cuda.current_stream()
+    out = {}
+    for name, irec in (("ppm", config.IREC_PPM), ("weno5", config.IREC_WENO5)):
+        p = dict(config.torus(nr=args.nr, nth=args.nth, nph=args.nph, irec=irec), guard=args.guard)
+        zones = config.interior_cells(p)
+        r = ctx.admit(p)
+        r.ic_torus_device(seed=2012)
+        r.step(3, strict=False)  # first use of every kernel
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record(stream)
+        r.step(args.variant_steps, strict=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"workload": f"fm_torus_3d_{args.nr}x{args.nth}x{args.nph}_{name}_fp64", "interior_cells": zones,
+                     "value": zones * args.variant_steps / (ms * 1e-3), "unit": "zone-updates/s",
+                     "ms_per_step": ms / args.variant_steps, "steps": args.variant_steps, "warmup": 3}
+        r.release()
+    return out
 
 
 def section_mixed(ctx, args) -> dict:
@@ -521,6 +549,8 @@ def main():
     ap.add_argument("--nth", type=int, default=128)
     ap.add_argument("--nph", type=int, default=128)
     ap.add_argument("--irec", type=int, default=6)
+    ap.add_argument("--variant-steps", type=int, default=20,
+                    help="timed steps of the PPM and WENO5 runs of the headline grid (0: skip)")
     ap.add_argument("--guard", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--prof-steps", type=int, default=3)
