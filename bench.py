@@ -181,10 +181,11 @@ def workload(args) -> dict:
 
 def config_block(args, p) -> dict:
     from raishinsource_b200 import config
-    return {"workload": f"fm_torus_3d_{args.nr}x{args.nth}x{args.nph}_{'mp5' if args.irec == 6 else 'weno5'}_fp64",
+    rec = {5: "ppm", 6: "mp5", 7: "weno5"}.get(args.irec, f"irec{args.irec}")
+    return {"workload": f"fm_torus_3d_{args.nr}x{args.nth}x{args.nph}_{rec}_fp64",
             "grid_incl_ghosts": [args.nr, args.nth, args.nph], "interior_cells": config.interior_cells(p),
-            "metric": "MKS a=0.9375", "scheme": "MP5+HLLE(LLF)+fluxCT+RK3" if args.irec == 6 else
-            "WENO5+HLLE(LLF)+fluxCT+RK3", "cfl": p["cfl"], "guard": p["guard"],
+            "metric": "MKS a=0.9375", "scheme": f"{rec.upper()}+HLLE(LLF)+fluxCT+RK3", "cfl": p["cfl"],
+            "guard": p["guard"],
             "l2": "inputs larger than L2: one primitive copy is %.0f MB (126 MB L2); no flush" %
                   (72e-6 * p["imax"] * p["jmax"] * p["kmax"])}
 
