@@ -62,6 +62,13 @@ BYTES_PER_UNIT = {"flux_r": 136, "flux_phi": 136, "flux_theta": 136, "update": 4
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one launch divided by
 # its units) on the 192x96x96 torus, whose state already exceeds the L2
 DRAM_BYTES_PER_UNIT = {"update": 469.0, "flux_r": 113.0, "flux_phi": 120.0, "flux_theta": 122.0}
+BYTES_PER_UNIT["flux"] = 136
+DRAM_BYTES_PER_UNIT["flux"] = (113.0 + 120.0 + 122.0) / 3
+# FP64 pipe utilisation of the face kernels from ncu (sm__inst_executed_pipe_fp64, percent of the peak
+# sustained rate while active), mean over the three directions on the 192x96x96 torus
+FP64_PIPE_FRAC = {"flux": 0.425, "update": 0.24}
+# algorithmic HBM bytes of one zone-update (FP64): only primitives persist between stages
+STEP_BYTES_PER_ZONE = 648
 # Executed FP64 operations per zone-update of one full RK3 step (MP5, FP64): ncu
 # smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over every launch of one step
 # of the 192x96x96 torus, dadd + dmul + 2 dfma, divided by its interior cells (1,424,896).  It
@@ -223,6 +230,7 @@ def run_gpu(args) -> dict | None:
         if ws > 1:
             torch.distributed.barrier()
 
+    divb0 = run.divb()
     # warm-up (also the first use of every kernel)
     run.step(args.warmup)
     torch.cuda.synchronize()
@@ -239,6 +247,13 @@ def run_gpu(args) -> dict | None:
     ms = max_over_ranks(e0.elapsed_time(e1))
     launches = sum(v["launches"] for v in ctx.profile_read().values())
     st = run.stats()
+    divb1 = run.divb()
+    divb = {"guard": p["guard"], "initial": divb0[0] / divb0[1], "after_steps": divb1[0] / divb1[1],
+            "steps": args.warmup + args.steps,
+            "measure": "max over interior corners of |corner-centred div(sqrt(-g) B)| / max |sqrt(-g) B^d| / dx_d "
+                       "(rg_run_divb)",
+            "note": "guard 1 keeps the reference's LLF flux of the normal field (hll.f90:109-111), which flux-CT "
+                    "does not replace, so div B drifts; guard 3 (Toth's zero normal flux) holds it at round-off"}
 
     # end to end through the public API with host buffers (pinned)
     e2e = None
@@ -263,7 +278,8 @@ def run_gpu(args) -> dict | None:
                "ms_per_step": e_ms / args.e2e_steps, "api": "rg_run_upload_prims + rg_step + rg_run_download_prims"}
 
     # per-kernel device times (separate pass: CUDA events around every launch on the library stream)
-    roofline, shares = None, {}
+    roofline, shares, step_roof = None, {}, None
+    peak, peak_kind = measured_peaks()
     if args.prof_steps > 0:
         ctx.profile(True)
         run.step(args.prof_steps)
@@ -271,32 +287,43 @@ def run_gpu(args) -> dict | None:
         ctx.profile(False)
         total = sum(v["ms"] for v in prof.values())
         shares = {k: round(v["ms"] / total, 4) for k, v in prof.items()}
-        top = max((k for k in prof if k in BYTES_PER_UNIT), key=lambda k: prof[k]["ms"])
+        # The face kernels of the three directions are one family (one launch per direction and stage, the
+        # same faces per launch): together they are the largest share of the step.
+        fam = ("flux_r", "flux_phi", "flux_theta")
+        kinds = {"flux": {"ms": sum(prof[k]["ms"] for k in fam), "launches": sum(prof[k]["launches"] for k in fam)}}
+        kinds.update({k: prof[k] for k in prof if k in BYTES_PER_UNIT and k not in fam})
+        top = max(kinds, key=lambda k: kinds[k]["ms"])
         # one update per stage comprises the cell kernel, the straggler pass and the W-carry pass
-        n_launch = 3 * args.prof_steps if top == "update" else prof[top]["launches"]
+        n_launch = 3 * args.prof_steps if top == "update" else kinds[top]["launches"]
         nm0, nm1 = run.nm0, run.nm1
         faces = (p["imax"] - 2 * nm0 + 1) * (p["jmax"] - 2 * nm0 + 1) * (p["kmax"] - 2 * nm0 + 1)
-        units = {"update": zones,
+        units = {"update": zones, "flux": faces,
                  "flux_ct": (p["imax"] - 2 * nm1 + 1) * (p["jmax"] - 2 * nm1 + 1) * (p["kmax"] - 2 * nm1 + 1),
                  "floors": p["imax"] * p["jmax"] * p["kmax"],
                  "cfl": (p["imax"] - 2) * (p["jmax"] - 2) * (p["kmax"] - 2)}
-        u = units.get(top, faces)
-        per_launch_ms = prof[top]["ms"] / max(n_launch, 1)
-        peak, peak_kind = measured_peaks()
+        u = units[top]
+        per_launch_ms = kinds[top]["ms"] / max(n_launch, 1)
         achieved = BYTES_PER_UNIT[top] * u / (per_launch_ms * 1e-3) / 1e9
         traffic = DRAM_BYTES_PER_UNIT.get(top)
-        roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+        roofline = {"bound": "hbm", "kernel": "k_flux (r, phi, theta faces)" if top == "flux" else top,
+                    "achieved": achieved, "peak": peak, "peak_source": peak_kind,
                     "unit": "GB/s", "frac": achieved / peak,
                     "traffic": None if traffic is None else traffic * u,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on the "
                                       "192x96x96 torus, scaled by the units of one launch",
                     "bytes_per_unit": BYTES_PER_UNIT[top], "units_per_launch": u, "ms_per_launch": per_launch_ms,
-                    "note": "FP64-pipe bound path: HBM fraction of algorithmic bytes, see profiles/"}
+                    "share_of_step": round(kinds[top]["ms"] / total, 4),
+                    "fp64_pipe_frac": FP64_PIPE_FRAC.get(top),
+                    "fp64_pipe_source": "ncu sm__inst_executed_pipe_fp64 (pct of peak sustained active), "
+                                        "192x96x96 torus",
+                    "note": "FP64-pipe bound kernel: HBM fraction of algorithmic bytes with the FP64 pipe beside it"}
+    run.release()
     run.release()
     fp64_peak = fp64_peak_tflops(dev) if (rank == 0 and args.prof_steps > 0) else None
     extra = {}
     if ws == 1:
-        sections = (("scheme_variants", args.variant_steps, section_variants),
+        sections = (("exact_build", args.exact_steps, section_exact),
+                    ("scheme_variants", args.variant_steps, section_variants),
                     ("mixed", args.mixed_steps, section_mixed), ("torus2d", args.torus2d_steps, section_torus2d),
                     ("batched_tubes", args.tubes, section_tubes), ("serving", args.serve_requests, section_serving))
         for name, n, fn in sections:
@@ -312,6 +339,11 @@ def run_gpu(args) -> dict | None:
     if rank != 0:
         return None
     value = zones * ws * args.steps / (ms * 1e-3)
+    # the whole step against the algorithmic minimum of 648 B per zone-update (FP64 primitives only:
+    # one CFL pass, then 2 + 3 + 3 reads/writes of the 9 primitives in the three stages)
+    step_gbs = STEP_BYTES_PER_ZONE * zones * args.steps / (ms * 1e-3) / 1e9
+    step_roof = {"bound": "hbm", "bytes_per_zone_update": STEP_BYTES_PER_ZONE, "achieved": step_gbs,
+                 "peak": peak, "unit": "GB/s", "frac": step_gbs / peak}
     fp64 = None
     if fp64_peak is not None:
         achieved = zones * args.steps / (ms * 1e-3) * FP64_FLOPS_PER_ZONE / 1e12  # per GPU
@@ -327,7 +359,9 @@ def run_gpu(args) -> dict | None:
         "config": dict(config_block(args, p), parallelism=f"replicas x{ws}"),
         "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         "roofline": roofline,
+        "step_roofline": step_roof,
         "fp64_roofline": fp64,
+        "divb": divb,
         "kernel_share": shares,
         "initial_data": {"host_s": ic_host_s, "device_s": ic_device_s,
                          "note": "torus initial data of the headline grid: rg_run_ic_torus (host construction "
@@ -357,12 +391,18 @@ def _rel_errs(got, ref, n):
 
 def section_variants(ctx, args) -> dict:
     """The headline grid with the other reconstructions of its workload
-    family, PPM and WENO5 (FP64, same initial data and time step rules)."""
+    family, PPM and WENO5 (FP64, same seed, same time step rules), timed and
+    run for --variant-steps steps, and each compared with MP5 run as long from
+    the same seed.  WENO5 and MP5 share the grid (nm1 = 4), so their fields are
+    compared cell by cell; PPM's wider ghost zones (nm1 = 5) shift the phi
+    grid, so PPM is compared through the phi-averaged fields on the (r, theta)
+    cells both interiors cover."""
+    import numpy as np
     import torch
     from raishinsource_b200 import config
     stream = torch.cuda.current_stream()
-    out = {}
-    for name, irec in (("ppm", config.IREC_PPM), ("weno5", config.IREC_WENO5)):
+    out, finals = {}, {}
+    for name, irec in (("mp5", config.IREC_MP5), ("ppm", config.IREC_PPM), ("weno5", config.IREC_WENO5)):
         p = dict(config.torus(nr=args.nr, nth=args.nth, nph=args.nph, irec=irec), guard=args.guard)
         zones = config.interior_cells(p)
         r = ctx.admit(p)
@@ -371,15 +411,76 @@ def section_variants(ctx, args) -> dict:
         torch.cuda.synchronize()
         e0, e1 = _events()
         e0.record(stream)
-        r.step(args.variant_steps, strict=False)
+        r.step(args.variant_steps - 3, strict=False)
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        st = r.stats()
+        finals[name] = (r.prims(), r.nm1)
         out[name] = {"workload": f"fm_torus_3d_{args.nr}x{args.nth}x{args.nph}_{name}_fp64", "interior_cells": zones,
-                     "value": zones * args.variant_steps / (ms * 1e-3), "unit": "zone-updates/s",
-                     "ms_per_step": ms / args.variant_steps, "steps": args.variant_steps, "warmup": 3}
+                     "value": zones * (args.variant_steps - 3) / (ms * 1e-3), "unit": "zone-updates/s",
+                     "ms_per_step": ms / (args.variant_steps - 3), "steps": args.variant_steps, "time": st["time"],
+                     "finite": bool(np.isfinite(finals[name][0]).all())}
         r.release()
+    ref, n_ref = finals["mp5"]
+    names = {"rho": 0, "p": 4, "B1": 6, "B2": 7, "B3": 8}
+    for name in ("ppm", "weno5"):
+        got, n = finals[name]
+        if n == n_ref:
+            sl = (slice(n, -n),) * 3
+            a, b = got[sl], ref[sl]
+            how = "cell by cell over the common interior"
+        else:
+            m = max(n, n_ref)
+            a = got[m:-m, n:-n, m:-m].mean(axis=1)
+            b = ref[m:-m, n_ref:-n_ref, m:-m].mean(axis=1)
+            how = "phi-averaged fields over the (r, theta) cells of both interiors"
+        l1 = np.abs(a - b).sum(axis=(0, 1)) if a.ndim == 3 else np.abs(a - b).sum(axis=(0, 1, 2))
+        den = np.abs(b).sum(axis=(0, 1)) if b.ndim == 3 else np.abs(b).sum(axis=(0, 1, 2))
+        out[name]["l1_rel_vs_mp5"] = {k: float(l1[v] / max(den[v], 1e-300)) for k, v in names.items()}
+        out[name]["compared"] = how
     return out
+
+
+def section_exact(ctx, args) -> dict:
+    """The uncontracted build (libraishin_gpu_exact.so: no FMA, rg_pow for every
+    power), which agrees with the oracle bit for bit, timed on the headline
+    workload in a child process (the library is process-global)."""
+    env = dict(os.environ, RAISHIN_GPU_LIB="exact")
+    cmd = [sys.executable, os.path.abspath(__file__), "--exact-child", "--steps", str(args.exact_steps),
+           "--nr", str(args.nr), "--nth", str(args.nth), "--nph", str(args.nph), "--irec", str(args.irec),
+           "--guard", str(args.guard)]
+    res = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+    if res.returncode != 0:
+        return {"error": res.stderr[-500:]}
+    return json.loads(res.stdout.strip().splitlines()[-1])
+
+
+def exact_child(args) -> None:
+    import torch
+    from raishinsource_b200 import Context, config
+    p = workload(args)
+    zones = config.interior_cells(p)
+    with Context(0) as ctx:
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        r = ctx.admit(p)
+        r.ic_torus_device(seed=2012)
+        r.step(3)
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        r.step(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        r.release()
+    maps = open("/proc/self/maps").read()
+    lib = sorted({os.path.basename(x.split()[-1]) for x in maps.splitlines() if "libraishin_gpu" in x})
+    print(json.dumps({"workload": config_block(args, p)["workload"], "library": lib, "steps": args.steps, "warmup": 3,
+                      "value": zones * args.steps / (ms * 1e-3), "unit": "zone-updates/s",
+                      "ms_per_step": ms / args.steps,
+                      "note": "no FMA contraction and the library's own pow: bit-identical to the oracle (CPU "
+                              "restatement) step after step"}))
 
 
 def section_mixed(ctx, args) -> dict:
@@ -391,6 +492,11 @@ def section_mixed(ctx, args) -> dict:
     zones = config.interior_cells(p)
     stream = torch.cuda.current_stream()
     out = {"workload": f"fm_torus_3d_{nr}x{nth}x{nph}_mp5", "steps": args.mixed_steps, "interior_cells": zones}
+    # a radial shell inside the FP32 region (r > 2 r_H): the last face below r = 6 M, the torus's inner edge
+    # (cell centres x1(i) = xmin (xmax/xmin)^((i-1)/(imax-1)), grid.f90 for ix1 = 2)
+    x1 = [p["xmin"] * (p["xmax"] / p["xmin"]) ** ((i - 1) / (p["imax"] - 1)) for i in range(1, p["imax"] + 1)]
+    shell = max(i for i in range(1, p["imax"]) if 0.5 * (x1[i - 1] + x1[i]) <= 6.0)
+    r_shell = 0.5 * (x1[shell - 1] + x1[shell])
     states = {}
     for prec in ("fp64", "mixed"):
         r = ctx.admit(dict(p, precision=prec))
@@ -404,19 +510,25 @@ def section_mixed(ctx, args) -> dict:
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         st = r.stats()
-        states[prec] = (r.prims(), r.horizon_flux(), st)
+        states[prec] = (r.prims(), r.horizon_flux(), st, r.radial_flux(shell))
         out[prec] = {"value": zones * (args.mixed_steps - 3) / (ms * 1e-3), "unit": "zone-updates/s",
                      "ms_per_step": ms / (args.mixed_steps - 3), "time": st["time"],
                      "recov_nr2": st["recov_nr2"], "recov_fail": st["recov_fail"]}
         r.release()
-    (a, (ma, ea), _), (b, (mb, eb), _) = states["mixed"], states["fp64"]
+    (a, (ma, ea), _, (sma, sea)), (b, (mb, eb), _, (smb, seb)) = states["mixed"], states["fp64"]
     l1, linf = _rel_errs(a, b, config.ghost_widths(p["irec"], p.get("ict", 1))[1])
     out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     out["l1_rel_mixed_vs_fp64"] = l1
     out["linf_rel_mixed_vs_fp64"] = linf
     out["horizon"] = {"mdot_fp64": mb, "mdot_mixed": ma, "edot_fp64": eb, "edot_mixed": ea,
                       "mdot_rel_err": abs(ma - mb) / max(abs(mb), 1e-300),
-                      "edot_rel_err": abs(ea - eb) / max(abs(eb), 1e-300)}
+                      "edot_rel_err": abs(ea - eb) / max(abs(eb), 1e-300),
+                      "note": "inner edge of the interior (just outside the horizon), inside the FP64 region"}
+    out["shell_flux"] = {"r": r_shell, "face_index": shell, "mdot_fp64": smb, "mdot_mixed": sma, "edot_fp64": seb,
+                         "edot_mixed": sea, "mdot_rel_err": abs(sma - smb) / max(abs(smb), 1e-300),
+                         "edot_rel_err": abs(sea - seb) / max(abs(seb), 1e-300),
+                         "note": "mass and energy flux through the radial shell at the torus inner edge, inside the "
+                                 "FP32 region (r > 2 r_H) of the mixed run (rg_run_radial_flux)"}
     out["precision"] = ("FP32 reconstruction, LLF fluxes, flux-CT and RK combine (compensated accumulation) "
                         "beyond 2 r_H; FP64 recovery, floors, CFL, metric and sources inside 2 r_H")
     return out
@@ -516,6 +628,12 @@ def section_serving(ctx, args) -> dict:
     res = srv.serve(reqs)
     srv.close()
     res.pop("done")
+    peak, peak_kind = measured_peaks()
+    res["hbm"] = {"bytes_per_zone_update": STEP_BYTES_PER_ZONE, "achieved_gbs":
+                  STEP_BYTES_PER_ZONE * res["zone_updates_per_s"] / 1e9, "peak": peak, "peak_source": peak_kind,
+                  "frac": STEP_BYTES_PER_ZONE * res["zone_updates_per_s"] / 1e9 / peak,
+                  "note": "aggregate zone-updates/s times the FP64 algorithmic bytes of one zone-update (648 B; "
+                          "the mixed half moves less), against the measured copy bandwidth"}
     res.update({"arrival_rate_per_s": args.serve_rate, "steps_per_request": args.serve_steps,
                 "mem_budget_gb": budget / 2**30, "unit": "zone-updates/s",
                 "grids": [128, 256, 384, 512], "mix": "half FP64, half FP32-mixed"})
@@ -550,8 +668,11 @@ def main():
     ap.add_argument("--nth", type=int, default=128)
     ap.add_argument("--nph", type=int, default=128)
     ap.add_argument("--irec", type=int, default=6)
-    ap.add_argument("--variant-steps", type=int, default=20,
-                    help="timed steps of the PPM and WENO5 runs of the headline grid (0: skip)")
+    ap.add_argument("--variant-steps", type=int, default=1000,
+                    help="steps of the MP5, PPM and WENO5 runs of the headline grid compared at the end (0: skip)")
+    ap.add_argument("--exact-steps", type=int, default=20,
+                    help="timed steps of the uncontracted (bit-exact) build on the headline grid (0: skip)")
+    ap.add_argument("--exact-child", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--guard", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--prof-steps", type=int, default=3)
@@ -561,7 +682,7 @@ def main():
     ap.add_argument("--torus2d-steps", type=int, default=1000, help="steps of the 2D torus section (0 = skip)")
     ap.add_argument("--tubes", type=int, default=1024, help="Riemann tubes of the batched section (0 = skip)")
     ap.add_argument("--tube-tmax", type=float, default=0.4)
-    ap.add_argument("--tube-steps", type=int, default=96,
+    ap.add_argument("--tube-steps", type=int, default=0,
                     help="batch steps timed in the tube section (0 = run every tube to tmax)")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving section (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate (requests/s)")
@@ -569,15 +690,20 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="device memory budget for admission")
     args = ap.parse_args()
     ws, rank, _ = dist_env()
+    if args.exact_child:
+        exact_child(args)
+        return
     if args.impl == "reference":
         if rank != 0:
             return
-        ref = time_reference(args, max(1, min(args.steps, 2)))
+        nref = max(1, min(args.steps, 2))
+        ref = time_reference(args, nref)
         line = {"impl": "reference", "metric": "zone-updates/s (FP64, one full RK3 step per update)",
-                "value": ref["value"], "unit": "zone-updates/s", "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "value": ref["value"], "unit": "zone-updates/s", "n_gpus": ws, "steps": nref,
+                "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (seeded Fishbone-Moncrief torus initial data)",
-                "config": config_block(args, workload(args)),
+                "config": dict(config_block(args, workload(args)), parallelism=f"replicas x{ws}"),
+                "note": "bounded sample: %d full step(s) of about 2 s each on the host cores, no warm-up" % nref,
                 "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": ref["value"], "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}

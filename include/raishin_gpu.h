@@ -7,7 +7,8 @@
  * uri(nv,is1:ie1,js1:je1,ks1:ke1).  This library replaces those calls with
  * sm_100a kernels on one GPU.  Every entry point is extern "C" with plain
  * pointers and sizes so that the Fortran driver can bind it with
- * ISO_C_BINDING.
+ * ISO_C_BINDING (bind(C) interfaces with value integers and type(c_ptr) or
+ * real(c_double) arrays).
  *
  * Conventions
  *  - Host arrays of primitives/conserved variables use the reference layout
@@ -175,17 +176,21 @@ int rg_run_stats(rg_ctx* ctx, int run, rg_step_stats* stats);
  * whose step is one launch per kernel kind over a per-run tile table
  * (persistent grid), captured once in a CUDA graph and replayed each step.
  * Meant for many small runs (2D slabs, 1D tubes); a large 3D run alone is
- * faster through rg_step.  The first call for a set of
- * runs tunes the tile width and grid size on trial steps from a snapshot of
- * the runs' state, which it restores.  Each run's result equals its result
- * stepped alone.  stats, if given, receives nruns records.  Replaces the
- * reference's one-run-per-job time loop (main.f90:586-1151) for ensembles. */
+ * faster through rg_step.  The launch shape (block width, cells per tile
+ * along i, persistent grid size) is tuned per batch class and context: a new
+ * class starts with a default shape and, at the first segment boundary after
+ * 32 steps of its batch, times every candidate shape on trial steps from a
+ * snapshot of the runs' state (which it restores) and keeps the fastest.
+ * Each run's result equals its result stepped alone.  stats, if given,
+ * receives nruns records.  Replaces the reference's one-run-per-job time loop
+ * (main.f90:586-1151) for ensembles. */
 int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_stats* stats);
-/* The tuned shape of the batch of exactly these runs: block width of the cell
+/* The shape of the batch of exactly these runs: block width of the cell
  * kernels, persistent blocks per SM (0: one block per tile), launches per
- * step and the step time measured by the tuner (ms). */
+ * step, the step time measured by the tuner (ms; 0 while tuning is still
+ * pending) and the cells along i of one tile of the cell kernels. */
 int rg_batch_info(rg_ctx* ctx, const int* runs, int nruns, int* width, int* grid_factor, int* launches,
-                  double* tuned_ms);
+                  double* tuned_ms, int* tile_cells);
 
 /* Kernel timing: rg_profile(ctx, 1) clears the counters and brackets every
  * following launch of rg_step with CUDA events on the context stream;
@@ -242,6 +247,21 @@ int rg_run_restore(rg_ctx* ctx, int run, const char* path, int* it0, int* ih0, i
  * The reference has no such diagnostic; it is how the mixed-precision path's
  * effect on the accretion is measured. */
 int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot);
+/* The same rates through the radial face iface+1/2 (iface in nm0..imax-nm0,
+ * 1-based cell index; rg_run_horizon_flux is iface = nm1): a shell at any
+ * radius, e.g. inside the FP32 region of a mixed run (r > 2 r_H), where the
+ * mixed path's effect on the flow is measured. */
+int rg_run_radial_flux(rg_ctx* ctx, int run, int iface, double* mdot, double* edot);
+
+/* Corner-centred divergence of sqrt(-g) B of the run's current primitives:
+ * at each corner between interior cells, D = sum over d of the four
+ * differences of sqrt(-g) B^d across the corner along d, divided by 4 dx_d.
+ * Toth's flux-CT (ct.f90:30-118) keeps D constant when the flux of the normal
+ * field component is zero (guard bit 2); the reference's LLF term
+ * (hll.f90:109-111) lets it drift.  *divb_max = max |D| (NaN if any D is);
+ * *b_scale = max |sqrt(-g) B^d| / dx_d over the same cells, the natural unit
+ * of D.  No counterpart in the reference. */
+int rg_run_divb(rg_ctx* ctx, int run, double* divb_max, double* b_scale);
 
 /* Derived quantities of the output converter (convert_vtk2dn1.f90:254-371,
  * with transmks2ks1 / transks2bl1, convert_vtk2dn1.f90:1399-1554) from the
@@ -256,22 +276,34 @@ int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot);
  * converter; the VTK writing itself stays with the caller. */
 int rg_run_derived(rg_ctx* ctx, int run, int jslice, double* out);
 
-/* Allocation-free variant of rg_calflx, for callers that cannot call
- * cudaMalloc when they need the fluxes (code running inside a CUDA stream
- * capture, or a host program whose device memory comes only from its own pool).
- * No counterpart in the reference.  The caller passes device buffers:
- * d_prims, the primitives in structure-of-arrays order (variable v of cell c
- * at v*N + c, c = (i-1) + imax*((j-1) + jmax*(k-1))), and d_ww, 27*N doubles
- * receiving ww(d,v) of cell c at ((d-1)*9 + v)*N + c on the hll range, with
- * flux-CT applied on its range.  The flux-CT intermediate lives in a
- * file-scope device array that holds grids of at most 262144 cells (larger
- * grids return RG_EINVAL_CONFIG); every GPU that loads the library keeps that
- * array (about 12.6 MB) until exit.  The run's geometry, allocated by
- * rg_run_admit beforehand, is read; nothing is allocated or freed.  The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress)
- * and should therefore come before any stream capture.  All calls share the
- * array: calls whose work overlaps on the GPU (other contexts or streams) race.
- * The call returns after its work has completed on the context stream. */
+/* The power function of the uncontracted build (rg_pow, include/rg_pow.h),
+ * evaluated on the device: out[i] = x[i]**y[i] for n host values.  A host
+ * program that evaluates rg_pow itself gets the same bits; this entry point
+ * lets it check that.  The reference's x**y is gfortran's call of the C
+ * library's pow (calflx.f90:474, caluu.f90:303, recov.f90:1044-1186). */
+int rg_pow_eval(rg_ctx* ctx, const double* x, const double* y, double* out, size_t n);
+
+/* Allocation-free variant of rg_calflx.  No counterpart in the reference.
+ * For host programs that cannot let the library call cudaMalloc when they need
+ * the fluxes: a framework or driver whose device memory comes only from its
+ * own pool or arena, where an allocation behind its back would synchronise the
+ * device and take memory its pool does not account for.  The caller passes
+ * device buffers: d_prims, the primitives in structure-of-arrays order
+ * (variable v of cell c at v*N + c, c = (i-1) + imax*((j-1) + jmax*(k-1))),
+ * and d_ww, 27*N doubles receiving ww(d,v) of cell c at ((d-1)*9 + v)*N + c on
+ * the hll range, with flux-CT applied on its range.  The flux-CT intermediate
+ * lives in a file-scope device array that holds grids of at most 262144 cells
+ * (larger grids return RG_EINVAL_CONFIG); every GPU that loads the library
+ * keeps that array (about 12.6 MB) until exit.  The run's geometry, allocated
+ * by rg_run_admit beforehand, is read; the call itself allocates and frees
+ * nothing, with one exception: a device's first call looks up the array's
+ * device address (cudaGetSymbolAddress), which with CUDA's lazy module loading
+ * may load the module and so allocate the array.  Make that first call during
+ * set-up, before any stream capture and before the program restricts itself to
+ * its own pool.  All calls share the one array and each starts by clearing
+ * it: calls whose work overlaps on the GPU (other contexts or streams) race,
+ * so callers must serialise them.  The call returns after its work has
+ * completed on the context stream. */
 int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, double* d_ww);
 
 #ifdef __cplusplus

@@ -5,4 +5,4 @@ package, as the checker.  The product (raishinsource_b200) never imports it.
 Parity status: unpinned (the reference ships no golden data and cannot be
 compiled here); see oracle/oracle.hpp.
 """
-from .pyoracle import Oracle, build  # noqa: F401
+from .pyoracle import Oracle, build, pow_eval, set_pow_mode  # noqa: F401

@@ -23,7 +23,7 @@ FLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-sh
 
 def build(force: bool = False) -> str:
     srcs = [os.path.join(HERE, s) for s in SOURCES]
-    deps = srcs + [os.path.join(HERE, "oracle.hpp")]
+    deps = srcs + [os.path.join(HERE, "oracle.hpp"), os.path.join(HERE, "..", "include", "rg_pow.h")]
     if not force and os.path.exists(LIB):
         t = os.path.getmtime(LIB)
         if all(os.path.getmtime(d) <= t for d in deps):

@@ -19,9 +19,12 @@
 // (i,j,k) but which depend only on (r,theta) for every metric this build
 // supports, are stored per (i,k); this changes no arithmetic.
 #pragma once
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <vector>
+
+#include "../include/rg_pow.h"
 
 extern "C" {
 
@@ -65,6 +68,16 @@ constexpr double PI = 3.14159265358979323;   // pram.f90:30
 
 // Fortran single-precision literal as the double gfortran produces from it.
 inline double sp(float f) { return (double)f; }
+
+// x**y in the step.  Mode 0 (the default): the C library's pow, which
+// gfortran calls for the reference's ** with a real exponent.  Mode 1: the
+// library's own power function (include/rg_pow.h), which the uncontracted GPU
+// build evaluates to the same bits on the device; with it, that build and
+// this restatement carry out one and the same sequence of IEEE operations.
+// Both are accurate to about half a unit in the last place and differ in the
+// last bit of a small fraction of results.  Set once before stepping.
+extern int g_pow_mode;
+inline double fpow(double x, double y) { return g_pow_mode ? rgm::pow(x, y) : std::pow(x, y); }
 
 struct M4 { double a[4][4]; };   // a[m][n] == gcov(m,n)
 

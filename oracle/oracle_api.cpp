@@ -9,7 +9,22 @@
 
 using orc::State;
 
+int orc::g_pow_mode = 0;
+
 extern "C" {
+
+// Selects the power function of the step (0: the C library's pow, 1: rg_pow,
+// see orc::fpow); returns the previous mode.  Process-wide.
+int orc_set_pow_mode(int mode) {
+  const int old = orc::g_pow_mode;
+  orc::g_pow_mode = mode ? 1 : 0;
+  return old;
+}
+
+// x[i]**y[i] by either power function, for the accuracy tests of rg_pow.
+void orc_pow_eval(const double* x, const double* y, double* out, long long n, int mode) {
+  for (long long i = 0; i < n; ++i) out[i] = mode ? rgm::pow(x[i], y[i]) : std::pow(x[i], y[i]);
+}
 
 void* orc_create(const orc_params* p) {
   State* s = new State();

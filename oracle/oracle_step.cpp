@@ -67,7 +67,7 @@ inline void p2c(const PS& s, double gam, double detg, double* u) {
   u[0] = s.de * s.ucon[0];
   for (int m = 1; m <= 3; ++m) u[m] = a * s.ucon[0] * s.ucov[m] + b * 0.0 - s.bbcon[0] * s.bbcov[m];
   u[4] = a * s.ucon[0] * s.ucov[0] + b * 1.0 - s.bbcon[0] * s.bbcov[0] + s.de * s.ucon[0];
-  u[5] = s.de * (s.pr / std::pow(s.de, gam)) * s.ucon[0];
+  u[5] = s.de * (s.pr / fpow(s.de, gam)) * s.ucon[0];
   u[6] = s.bcon[1]; u[7] = s.bcon[2]; u[8] = s.bcon[3];
   for (int n = 0; n < 9; ++n) u[n] = detg * u[n];
 }
@@ -79,7 +79,7 @@ inline void flux(const PS& s, int d, double gam, double detg, double* w) {
   w[0] = s.de * ud;
   for (int m = 1; m <= 3; ++m) w[m] = a * ud * s.ucov[m] + b * (d == m ? 1.0 : 0.0) - s.bbcon[d] * s.bbcov[m];
   w[4] = a * ud * s.ucov[0] + b * 0.0 - s.bbcon[d] * s.bbcov[0] + s.de * ud;
-  w[5] = s.de * (s.pr / std::pow(s.de, gam)) * ud;
+  w[5] = s.de * (s.pr / fpow(s.de, gam)) * ud;
   for (int m = 1; m <= 3; ++m) {
     if (m == d) w[5 + m] = 0.0;
     else w[5 + m] = (ud * (1. / s.ucon[0])) * s.bcon[m] - (s.ucon[m] * (1. / s.ucon[0])) * s.bcon[d];
@@ -1400,14 +1400,14 @@ bool recov_cell(const State& s, double* u, double* q, const M4& g, const M4& gc,
         gf = 1. / std::sqrt(gtmp);
         gfsq = gf * gf;
         ro = dro * (1. / gf);
-        pp = (gss / dro) * std::pow(ro, gam);
+        pp = (gss / dro) * fpow(ro, gam);
         const double roh = ro + gam1 * pp;
         wg = std::fabs(gfsq * roh);
         wsq = wg * wg;
         const double w3 = wsq * wg;
-        const double dgfdvsq = 0.5 * std::pow(gtmp, -1.5);
-        const double dwdvsq = dro * dgfdvsq + gam1 * gss * std::pow(dro, gam - 1.) * (2. - gam) *
-                                                  std::pow(gf, 1. - gam) * dgfdvsq;
+        const double dgfdvsq = 0.5 * fpow(gtmp, -1.5);
+        const double dwdvsq = dro * dgfdvsq + gam1 * gss * fpow(dro, gam - 1.) * (2. - gam) *
+                                                  fpow(gf, 1. - gam) * dgfdvsq;
         const double f = qtsq - vsq * (wg + bsq) * (wg + bsq) + (qdotbsq * (bsq + 2. * wg)) / wsq;
         const double ta = -((wg + bsq) * (wg + bsq));
         const double tb = -(2. * vsq * (wg + bsq));
@@ -1426,9 +1426,9 @@ bool recov_cell(const State& s, double* u, double* q, const M4& g, const M4& gc,
         gf = 1. / std::sqrt(gtmp);
         gfsq = gf * gf;
         ro = dro * (1. / gf);
-        pp = (gss * (1. / gf)) * std::pow(ro, gam - 1.);
-        if (ro < 0.0) ro = s.p.dmin * std::pow(x1i, -1.5);
-        if (pp < 0.0) pp = (gam - 1.) * s.p.pmin * std::pow(x1i, -2.5);
+        pp = (gss * (1. / gf)) * fpow(ro, gam - 1.);
+        if (ro < 0.0) ro = s.p.dmin * fpow(x1i, -1.5);
+        if (pp < 0.0) pp = (gam - 1.) * s.p.pmin * fpow(x1i, -2.5);
         const double roh = ro + gam1 * pp;
         wg = std::fabs(gfsq * roh);
         for (int m = 1; m <= 3; ++m) {
@@ -1447,13 +1447,13 @@ bool recov_cell(const State& s, double* u, double* q, const M4& g, const M4& gc,
   double ucon[4];
   if (irecov == 0) {
     q[0] = ro; q[1] = util[1]; q[2] = util[2]; q[3] = util[3]; q[4] = pp;
-    q[5] = ro * pp / std::pow(ro, gam - 1.);
+    q[5] = ro * pp / fpow(ro, gam - 1.);
     q[6] = u[6] * (1. / detg1); q[7] = u[7] * (1. / detg1); q[8] = u[8] * (1. / detg1);
     calucon(util, ucon, gf, gc);
     u[5] = detg1 * q[5] * ucon[0];
   } else {
     q[0] = ro1; q[1] = util1[1]; q[2] = util1[2]; q[3] = util1[3]; q[4] = pp1;
-    q[5] = ro1 * pp1 / std::pow(ro1, gam);
+    q[5] = ro1 * pp1 / fpow(ro1, gam);
     q[6] = u[6] * (1. / detg1); q[7] = u[7] * (1. / detg1); q[8] = u[8] * (1. / detg1);
     calucon(util, ucon, gf, gc);
     u[5] = detg1 * ro1 * q[5] * ucon[0];
@@ -1599,8 +1599,8 @@ bool recov2_cell(const State& s, const double* u, double* q, const M4& g, const 
     ro = dro / gf;
     const double xi = wg * (1. / gfsq) - ro;
     pp = gam2 * xi;
-    if (ro < 0.0) ro = s.p.dmin * std::pow(x1i, -3. / 2.);
-    if (pp < 0.0) pp = s.p.pmin * (gam - 1.) * std::pow(x1i, -5. / 2.);
+    if (ro < 0.0) ro = s.p.dmin * fpow(x1i, -3. / 2.);
+    if (pp < 0.0) pp = s.p.pmin * (gam - 1.) * fpow(x1i, -5. / 2.);
     for (int a = 1; a <= 3; ++a) {
       const double qt = qcon[a] + oncon[a] * qdotn;
       util[a] = (gf * (1. / (wg + bsq))) * (qt + qdotb * bcon[a] * (1. / wg));
@@ -1613,10 +1613,10 @@ bool recov2_cell(const State& s, const double* u, double* q, const M4& g, const 
   // recov.f90:2407-2441
   if (irecov == 0) {
     q[0] = ro; q[1] = util[1]; q[2] = util[2]; q[3] = util[3]; q[4] = pp;
-    q[5] = pp / std::pow(ro, gam - 1.);
+    q[5] = pp / fpow(ro, gam - 1.);
   } else {
     q[0] = ro1; q[1] = util1[1]; q[2] = util1[2]; q[3] = util1[3]; q[4] = pp1;
-    q[5] = pp1 / std::pow(ro1, gam - 1.);
+    q[5] = pp1 / fpow(ro1, gam - 1.);
   }
   q[6] = u[6] * (1. / detg1); q[7] = u[7] * (1. / detg1); q[8] = u[8] * (1. / detg1);
   return true;
@@ -1899,8 +1899,8 @@ void atmosphere1a(State& s) {
         double de = q[0], pr = q[4];
         double util[4] = {0.0, q[1], q[2], q[3]};
         const double b1 = q[6], b2 = q[7], b3 = q[8];
-        const double demin = s.p.dmin * std::pow(rr, -1.5);
-        const double prmin = (gam - 1.) * s.p.pmin * std::pow(rr, -2.5);
+        const double demin = s.p.dmin * fpow(rr, -1.5);
+        const double prmin = (gam - 1.) * s.p.pmin * fpow(rr, -2.5);
         const double dthe = 1.0 * (1. + epsilon) * demin;
         const double dthe1 = 1.0 * (1. + epsilon) * prmin;
         const double bsq = b1 * b1 + b2 * b2 + b3 * b3;
@@ -1970,8 +1970,8 @@ void pminmax2b(State& s) {
         }
         if (de != q[0]) q[0] = de;
         else if (pr != q[4]) q[4] = pr;
-        const double demin = s.p.dmin * std::pow(rr, -1.5);
-        const double prmin = (gam - 1.) * s.p.pmin * std::pow(rr, -2.5);
+        const double demin = s.p.dmin * fpow(rr, -1.5);
+        const double prmin = (gam - 1.) * s.p.pmin * fpow(rr, -2.5);
         const double bbromax = 50.0, bbprmax = 2.e3, prromax = 1.e6;
         if (pr < prmin) q[4] = prmin;
         if (pr > s.p.pmax) q[4] = s.p.pmax;

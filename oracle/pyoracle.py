@@ -79,6 +79,9 @@ def _lib():
         lib.orc_rkt.argtypes = [P, C.c_int, C.c_double, D, D, D, D, D]
         lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
         lib.orc_get_array.restype = C.c_longlong
+        lib.orc_set_pow_mode.argtypes = [C.c_int]
+        lib.orc_set_pow_mode.restype = C.c_int
+        lib.orc_pow_eval.argtypes = [D, D, D, C.c_longlong, C.c_int]
         _LIB = lib
     return _LIB
 
@@ -86,6 +89,24 @@ def _lib():
 def _ptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def set_pow_mode(mode: str) -> str:
+    """Power function of the oracle's step: "libc" (the C library's pow, as
+    the reference's gfortran build calls it; the default) or "rg" (rg_pow of
+    include/rg_pow.h, the uncontracted GPU build's).  Returns the previous
+    mode.  Process-wide."""
+    old = _lib().orc_set_pow_mode({"libc": 0, "rg": 1}[mode])
+    return "rg" if old else "libc"
+
+
+def pow_eval(x: np.ndarray, y: np.ndarray, mode: str) -> np.ndarray:
+    """x**y elementwise by the C library's pow ("libc") or rg_pow ("rg")."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(np.broadcast_to(y, x.shape), dtype=np.float64)
+    out = np.empty_like(x)
+    _lib().orc_pow_eval(_ptr(x), _ptr(y), _ptr(out), x.size, {"libc": 0, "rg": 1}[mode])
+    return out
 
 
 def make_params(p: dict) -> OrcParams:

@@ -7,11 +7,13 @@ entry points (include/raishin_gpu.h).  Two variants of the same sources:
 * libraishin_gpu.so (the product): multiply-adds contracted into FMA, and
   x**gam for gam = 4/3 or 5/3 evaluated through cbrt.  The parity tests hold
   it to 1e-12 of the oracle per step.
-* libraishin_gpu_exact.so: no FMA contraction (--fmad=false) and pow() for
-  every power, so that the operation sequence is the reference's (gfortran
-  -O2 on x86-64 emits no FMA); the remaining differences are last-bit
-  differences between CUDA's and glibc's pow/exp/log/sin/cos.  It exists for long-horizon parity (1000 steps) where MP5's
-  limiter switches amplify last-bit differences.
+* libraishin_gpu_exact.so: no FMA contraction (--fmad=false) and every power
+  of the step through the library's own rg_pow (include/rg_pow.h, IEEE basic
+  operations only), so that the operation sequence is the reference's
+  (gfortran -O2 on x86-64 emits no FMA) and a host restatement that uses
+  rg_pow as well reproduces it bit for bit, step after step.  It exists for
+  long-horizon parity (1000 steps), where MP5's limiter switches amplify any
+  last-bit difference.
 """
 from __future__ import annotations
 
@@ -51,7 +53,8 @@ def _command(variant: str, out: str, verbose: bool) -> list:
 
 def _stale(path: str) -> bool:
     deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [
-        os.path.join(HERE, "..", "include", "raishin_gpu.h"), os.path.abspath(__file__)]
+        os.path.join(HERE, "..", "include", "raishin_gpu.h"), os.path.join(HERE, "..", "include", "rg_pow.h"),
+        os.path.abspath(__file__)]
     if not os.path.exists(path):
         return True
     t = os.path.getmtime(path)

@@ -29,7 +29,7 @@ EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ct
            "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_torus_device", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
-           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_horizon_flux", "rg_run_store", "rg_run_restore", "rg_calflx_static")
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_divb", "rg_run_horizon_flux", "rg_run_radial_flux", "rg_run_store", "rg_run_restore", "rg_pow_eval", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -113,7 +113,7 @@ def load(path: str = LIB_PATH):
     lib.rg_run_stats.argtypes = [P, I, C.POINTER(StepStats)]
     lib.rg_step_batch.argtypes = [P, C.POINTER(C.c_int), I, I, C.POINTER(StepStats)]
     lib.rg_batch_info.argtypes = [P, C.POINTER(C.c_int), I, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                  C.POINTER(C.c_int), C.POINTER(C.c_double)]
+                                  C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]
     lib.rg_profile.argtypes = [P, I]
     lib.rg_profile_read.argtypes = [P, D, C.POINTER(C.c_longlong), I]
     lib.rg_caluu1.argtypes = [P, I, D, D]
@@ -125,7 +125,10 @@ def load(path: str = LIB_PATH):
     lib.rg_rkt.argtypes = [P, I, I, C.c_double, D, D, D, D, D]
     lib.rg_run_derived.argtypes = [P, I, I, D]
     lib.rg_calflx_static.argtypes = [P, I, P, P]
+    lib.rg_pow_eval.argtypes = [P, D, D, D, C.c_size_t]
     lib.rg_run_horizon_flux.argtypes = [P, I, D, D]
+    lib.rg_run_divb.argtypes = [P, I, D, D]
+    lib.rg_run_radial_flux.argtypes = [P, I, I, D, D]
     lib.rg_run_store.argtypes = [P, I, C.c_char_p, I, I, I, C.c_void_p]
     lib.rg_run_restore.argtypes = [P, I, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.c_void_p]
@@ -216,6 +219,15 @@ class Context:
         _check(self.lib, self.lib.rg_profile_read(self.h, ms, cnt, n))
         return {k: {"ms": ms[i], "launches": cnt[i]} for i, k in enumerate(self.KINDS)}
 
+    def pow_eval(self, x, y) -> np.ndarray:
+        """x**y elementwise on the device by the uncontracted build's power
+        function (rg_pow of include/rg_pow.h; rg_pow_eval)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(np.broadcast_to(y, x.shape), dtype=np.float64)
+        out = np.empty_like(x)
+        _check(self.lib, self.lib.rg_pow_eval(self.h, _dptr(x), _dptr(y), _dptr(out), x.size))
+        return out
+
     def admit(self, params: dict) -> "Run":
         return Run(self, params)
 
@@ -237,10 +249,11 @@ class Context:
     def batch_info(self, runs) -> dict:
         """Tuned shape of the batch of exactly these runs."""
         ids = (C.c_int * len(runs))(*[r.id for r in runs])
-        w, f, nl, ms = C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0)
+        w, f, nl, ms, tc = C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0), C.c_int(0)
         _check(self.lib, self.lib.rg_batch_info(self.h, ids, len(runs), C.byref(w), C.byref(f), C.byref(nl),
-                                                C.byref(ms)))
-        return {"width": w.value, "grid_per_sm": f.value, "launches_per_step": nl.value, "tuned_ms_per_step": ms.value}
+                                                C.byref(ms), C.byref(tc)))
+        return {"width": w.value, "tile_cells": tc.value, "grid_per_sm": f.value, "launches_per_step": nl.value,
+                "tuned_ms_per_step": ms.value}
 
     def __enter__(self):
         return self
@@ -436,6 +449,19 @@ class Run:
         m, e = C.c_double(0), C.c_double(0)
         _check(self.lib, self.lib.rg_run_horizon_flux(self.ctx.h, self.id, C.byref(m), C.byref(e)))
         return m.value, e.value
+
+    def radial_flux(self, iface: int) -> tuple[float, float]:
+        """(mdot, edot) through the radial face iface+1/2 (rg_run_radial_flux)."""
+        m, e = C.c_double(0), C.c_double(0)
+        _check(self.lib, self.lib.rg_run_radial_flux(self.ctx.h, self.id, int(iface), C.byref(m), C.byref(e)))
+        return m.value, e.value
+
+    def divb(self) -> tuple[float, float]:
+        """(max |D|, B scale) of the corner-centred div(sqrt(-g) B) of the
+        current state (rg_run_divb)."""
+        m, b = C.c_double(0), C.c_double(0)
+        _check(self.lib, self.lib.rg_run_divb(self.ctx.h, self.id, C.byref(m), C.byref(b)))
+        return m.value, b.value
 
     def bnd_floor(self, uri, urio) -> np.ndarray:
         out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)

@@ -16,9 +16,11 @@
 
 namespace {
 
+// nsub: the tile covers blocks bx .. bx+nsub-1 of the run's grid (the tile
+// shape along i is nsub blocks of the cell kernels' width).
 struct Tile {
   int run, bx, by, bz;
-  int ilo, ihi, aux, pad;
+  int ilo, ihi, aux, nsub;
 };
 
 // P^n, the stage input and the stage output of a run (stage 0: CFL, P^n only).
@@ -42,8 +44,12 @@ __global__ void __launch_bounds__(NT, MINB) kb(const DevRun* __restrict__ runs, 
     unsigned* dst = reinterpret_cast<unsigned*>(&sr);
     for (int w = tid; w < (int)(sizeof(DevRun) / 4); w += nt) dst[w] = src[w];
     __syncthreads();
-    body(sr, tl);
-    __syncthreads();
+    for (int u = 0; u < tl.nsub; ++u) {
+      Tile su = tl;
+      su.bx = tl.bx + u;
+      body(sr, su);
+      __syncthreads();
+    }
   }
 }
 
@@ -161,6 +167,7 @@ struct BatchPlan {
   int irec = 6;
   int ict = 1;
   int width = 128;            // threads per block of the cell kernels
+  int group = 1;              // blocks along i per tile of the cell kernels
   DevRun* d_runs = nullptr;
   Tile* d_tiles = nullptr;
   std::vector<BLaunch> launches;
@@ -169,10 +176,11 @@ struct BatchPlan {
 
 namespace {
 
-inline void add_tiles(std::vector<Tile>& T, int run, dim3 g, int ilo, int ihi, int aux) {
+inline void add_tiles(std::vector<Tile>& T, int run, dim3 g, int ilo, int ihi, int aux, int group = 1) {
   for (unsigned z = 0; z < g.z; ++z)
     for (unsigned y = 0; y < g.y; ++y)
-      for (unsigned x = 0; x < g.x; ++x) T.push_back(Tile{run, (int)x, (int)y, (int)z, ilo, ihi, aux, 0});
+      for (unsigned x = 0; x < g.x; x += (unsigned)group)
+        T.push_back(Tile{run, (int)x, (int)y, (int)z, ilo, ihi, aux, (int)std::min<unsigned>(group, g.x - x)});
 }
 
 // Block shape of a cell kernel in a batch of slab runs: `width` threads along i.
@@ -195,13 +203,18 @@ void plan_append(BatchPlan& B, std::vector<Tile>& T, BLaunch L, const std::vecto
 
 // Tile tables of one batched step for runs of one class (same irec,
 // precision, slab class); `width` is the block width of the cell kernels
-// (128: the batched kernels are compiled for it).
-int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
+// along i (64 or 128: the batched kernels are compiled for at most 128, the
+// CT kernel for 2 * 128) and `group` the blocks along i of one tile, so a
+// tile of a cell kernel covers width * group cells along i.
+int batch_build(const std::vector<DevRun>& runs, int width, int group, BatchPlan** out) {
+  if (width != 64 && width != 128) return 1;
+  if (group < 1) group = 1;
   BatchPlan* B = new BatchPlan();
   B->nruns = (int)runs.size();
   B->irec = runs.empty() ? 6 : runs[0].irec;
   B->ict = runs.empty() ? 1 : runs[0].ict;
   B->width = width;
+  B->group = group;
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&B->sm_count, cudaDevAttrMultiProcessorCount, dev);
@@ -216,7 +229,7 @@ int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
   L.kind = BK_CFL;
   L.block = wblock(r0, dim3(64, 2, 1), width);
   plan_append(*B, T, L, runs, [&](int a, const DevRun& r, std::vector<Tile>& t) {
-    add_tiles(t, a, sgrid(r, r.imax - 2, r.jmax - 2, r.kmax - 2, L.block), 0, 0, 0);
+    add_tiles(t, a, sgrid(r, r.imax - 2, r.jmax - 2, r.kmax - 2, L.block), 0, 0, 0, group);
   });
   L.kind = BK_DT;
   L.block = dim3(32, 1, 1);
@@ -245,7 +258,7 @@ int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
               ilo = split + 1;
             }
           }
-          add_tiles(t, a, sgrid(r, 2 * (ihi - ilo + 1), m, l, L.block), ilo, ihi, aux);
+          add_tiles(t, a, sgrid(r, 2 * (ihi - ilo + 1), m, l, L.block), ilo, ihi, aux, group);
         });
       }
     }
@@ -264,7 +277,7 @@ int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
           if (part == 0) { if (split < lo) return; ihi = split; }
           else { if (split >= hi) return; ilo = split + 1; }
         }
-        add_tiles(t, a, sgrid(r, ihi - ilo + 1, m, l, L.block), ilo, ihi, 0);
+        add_tiles(t, a, sgrid(r, ihi - ilo + 1, m, l, L.block), ilo, ihi, 0, group);
       });
     }
     L.kind = BK_UPDATE;
@@ -280,7 +293,7 @@ int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
           if (part == 0) { if (split < 1) return; ihi = split; }
           else { if (split >= r.imax) return; ilo = split + 1; }
         }
-        add_tiles(t, a, sgrid(r, ihi - ilo + 1, r.jmax, r.kmax, L.block), ilo, ihi, 0);
+        add_tiles(t, a, sgrid(r, ihi - ilo + 1, r.jmax, r.kmax, L.block), ilo, ihi, 0, group);
       });
     }
     L.fp32 = 0;
@@ -320,7 +333,7 @@ int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out) {
     L.dir = 0;
     L.block = wblock(r0, dim3(64, 2, 1), width);
     plan_append(*B, T, L, runs, [&](int a, const DevRun& r, std::vector<Tile>& t) {
-      add_tiles(t, a, sgrid(r, r.imax, r.jmax, r.kmax, L.block), 0, 0, 0);
+      add_tiles(t, a, sgrid(r, r.imax, r.jmax, r.kmax, L.block), 0, 0, 0, group);
     });
   }
   L = BLaunch{};

@@ -9,10 +9,12 @@
 #include <cstring>
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/raishin_gpu.h"
+#include "../../include/rg_pow.h"
 #include "rg_host.h"
 #include "rg_kernels.cuh"
 #include "rg_types.h"
@@ -76,8 +78,10 @@ struct BatchEntry {
   std::vector<int> ids;        // member runs, sorted
   BatchPlan* plan = nullptr;
   cudaGraphExec_t graph = nullptr;
-  int width = 128, grid_factor = 0;
+  int width = 128, group = 1, grid_factor = 0;
   double tuned_ms = 0.0;       // step time of the chosen shape
+  bool tune_pending = false;   // the class has no tuned shape yet: tune once kTuneAfter steps have run
+  long long steps_run = 0;     // batched steps taken by this entry
 };
 
 struct rg_ctx {
@@ -85,7 +89,7 @@ struct rg_ctx {
   cudaStream_t stream = nullptr;
   std::map<int, Run*> runs;
   std::map<std::vector<int>, BatchEntry*> batches;
-  struct Tuned { int width, grid_factor; double ms; };
+  struct Tuned { int width, group, grid_factor; double ms; };
   std::map<long long, Tuned> tuned;  // batch class -> shape chosen by the tuner and its step time
   int next_id = 1;
   long long launches[K_NKINDS] = {};   // kernel launches issued, per kind
@@ -578,37 +582,58 @@ struct Snapshot {
   }
 };
 
-// Build, tune and capture the batched step of runs of one class.  The tuner
-// times candidate persistent grid sizes (one block per tile, or 2, 4 or 8
-// blocks per SM, over tiles of 128 cells along i) on trial steps that start
-// from a snapshot of the runs' state, restores the state and keeps the
-// fastest; the grid size changes which block handles a tile, never a cell's
-// arithmetic.  The chosen size is kept per batch class for later batches of
-// the context, and the one-step launch sequence is captured once in a CUDA
-// graph.
+// Build and capture the batched step of runs of one class.  A class that
+// has been tuned in this context (e.g. a serving batch whose members changed)
+// gets its tuned shape at once; otherwise the batch starts with the default
+// shape (128-thread blocks, one block per tile, one block per tile along i)
+// and is tuned by tune_batch once it has run kTuneAfter steps, so that the
+// trial steps see the evolved state (shocks, deferred Newton-Raphson cells)
+// rather than the initial data.  The one-step launch sequence is captured in
+// a CUDA graph.
 int capture_batch(BatchEntry* E);
+constexpr int kTuneAfter = 32;
 
 int make_batch(rg_ctx* ctx, std::vector<Run*>& rs, const std::vector<int>& ids, BatchEntry** out) {
-  cudaStream_t s = ctx->stream;
   std::vector<DevRun> dr;
   for (Run* R : rs) dr.push_back(R->d);
   const long long cls = batch_class(rs[0]);
   auto tk = ctx->tuned.find(cls);
-  if (tk != ctx->tuned.end()) {  // shape already tuned for this class (e.g. a serving batch that changed members)
-    BatchEntry* E = new BatchEntry();
-    E->ids = ids;
-    if (batch_build(dr, tk->second.width, &E->plan)) {
-      delete E;
-      return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
-    }
+  BatchEntry* E = new BatchEntry();
+  E->ids = ids;
+  if (tk != ctx->tuned.end()) {
     E->width = tk->second.width;
+    E->group = tk->second.group;
     E->grid_factor = tk->second.grid_factor;
     E->tuned_ms = tk->second.ms;
-    batch_set_grid(E->plan, E->grid_factor);
-    const int rc = capture_batch(E);
-    if (rc) return rc;
-    *out = E;
-    return RG_OK;
+  } else {
+    E->tune_pending = true;
+  }
+  if (batch_build(dr, E->width, E->group, &E->plan)) {
+    delete E;
+    return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
+  }
+  batch_set_grid(E->plan, E->grid_factor);
+  const int rc = capture_batch(E);
+  if (rc) return rc;
+  *out = E;
+  return RG_OK;
+}
+
+// The tuner: times every candidate shape -- block width 64 or 128 along i,
+// tiles of 1, 2 or 4 blocks along i, and persistent grids of one block per
+// tile or 2, 4 or 8 blocks per SM -- on trial steps (one warm-up, two timed)
+// that start from a snapshot of the members' current state, restores the
+// state after each, and keeps the fastest.  The shape decides which block
+// computes which cells, never a cell's arithmetic.  The choice is kept per
+// batch class for later batches of the context.
+int tune_batch(rg_ctx* ctx, BatchEntry* E) {
+  cudaStream_t s = ctx->stream;
+  std::vector<Run*> rs;
+  std::vector<DevRun> dr;
+  for (int id : E->ids) {
+    Run* R = find(ctx, id);
+    rs.push_back(R);
+    dr.push_back(R->d);
   }
   Snapshot snap;
   int rc = snap.save(rs, s);
@@ -616,52 +641,59 @@ int make_batch(rg_ctx* ctx, std::vector<Run*>& rs, const std::vector<int>& ids, 
   cudaEvent_t e0, e1;
   RG_CUDA(cudaEventCreate(&e0));
   RG_CUDA(cudaEventCreate(&e1));
-  BatchEntry* E = new BatchEntry();
-  E->ids = ids;
+  struct Shape { int width, group; };
+  const Shape shapes[4] = {{64, 1}, {128, 1}, {128, 2}, {128, 4}};
+  const int factors[4] = {0, 2, 4, 8};
   double best = 1e30;
-  const int widths[1] = {128}, factors[4] = {0, 2, 4, 8};
-  for (int w : widths) {
+  Shape keep{E->width, E->group};
+  int keep_factor = E->grid_factor;
+  for (const Shape& sh : shapes) {
     BatchPlan* P = nullptr;
-    if (batch_build(dr, w, &P)) {
-      delete E;
-      return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
-    }
-    int keep_factor = -1;
+    if (batch_build(dr, sh.width, sh.group, &P)) return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
     for (int f : factors) {
       batch_set_grid(P, f);
       float ms = 0.f;
-      for (int rep = 0; rep < 3; ++rep) {  // one warm-up step, two timed
-        if (rep == 1) RG_CUDA(cudaEventRecord(e0, s));
-        RG_CUDA(batch_step(P, s));
+      cudaError_t e = cudaSuccess;
+      for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {  // one warm-up step, two timed
+        if (rep == 1) e = cudaEventRecord(e0, s);
+        if (e == cudaSuccess) e = batch_step(P, s);
       }
-      RG_CUDA(cudaEventRecord(e1, s));
-      RG_CUDA(cudaEventSynchronize(e1));
-      RG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      if ((rc = snap.restore(rs, s))) return rc;
+      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) {
+        batch_destroy(P);
+        return fail(RG_ECUDA, std::string("batch tuner: ") + cudaGetErrorString(e));
+      }
+      if ((rc = snap.restore(rs, s))) {
+        batch_destroy(P);
+        return rc;
+      }
       if (ms < best) {
         best = ms;
+        keep = sh;
         keep_factor = f;
       }
     }
-    if (keep_factor >= 0) {
-      if (E->plan) batch_destroy(E->plan);
-      E->plan = P;
-      E->width = w;
-      E->grid_factor = keep_factor;
-      E->tuned_ms = best / 2.0;
-      batch_set_grid(P, keep_factor);
-    } else {
-      batch_destroy(P);
-    }
+    batch_destroy(P);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   RG_CUDA(cudaStreamSynchronize(s));
-  ctx->tuned[cls] = {E->width, E->grid_factor, E->tuned_ms};
-  const int crc = capture_batch(E);
-  if (crc) return crc;
-  *out = E;
-  return RG_OK;
+  BatchPlan* P = nullptr;
+  if (batch_build(dr, keep.width, keep.group, &P)) return fail(RG_ENOMEM_ADMIT, "batch tables do not fit");
+  batch_set_grid(P, keep_factor);
+  if (E->graph) cudaGraphExecDestroy(E->graph);
+  E->graph = nullptr;
+  batch_destroy(E->plan);
+  E->plan = P;
+  E->width = keep.width;
+  E->group = keep.group;
+  E->grid_factor = keep_factor;
+  E->tuned_ms = best / 2.0;
+  E->tune_pending = false;
+  ctx->tuned[batch_class(rs[0])] = {E->width, E->group, E->grid_factor, E->tuned_ms};
+  return capture_batch(E);
 }
 
 int capture_batch(BatchEntry* E) {
@@ -1170,19 +1202,34 @@ int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_s
     es.push_back(it->second);
   }
   cudaStream_t s = ctx->stream;
-  for (int n = 0; n < nsteps; ++n)
+  // Steps run in segments whose ends keep the host-side buffer rotation up
+  // to date, so that an entry due for tuning is tuned between segments.
+  for (int done = 0; done < nsteps;) {
+    int seg = nsteps - done;
     for (BatchEntry* E : es) {
-      const int nl = batch_launch_count(E->plan);
-      if (!ctx->prof) {
-        RG_CUDA(cudaGraphLaunch(E->graph, s));
-        for (int a = 0; a < nl; ++a) ctx->launches[kind_of(E->plan, a)] += 1;
-      } else {
-        for (int a = 0; a < nl; ++a) RG_CUDA(issue(ctx, kind_of(E->plan, a), 1, [&] { return batch_issue(E->plan, a, s); }));
+      if (E->tune_pending && E->steps_run >= kTuneAfter) {
+        const int rc = tune_batch(ctx, E);
+        if (rc) return rc;
       }
+      if (E->tune_pending) seg = std::min<long long>(seg, kTuneAfter - E->steps_run);
     }
-  for (int a = 0; a < nruns; ++a) {
-    Run* R = find(ctx, runs[a]);
-    R->cur = (R->cur + nsteps) % 3;
+    for (int n = 0; n < seg; ++n)
+      for (BatchEntry* E : es) {
+        const int nl = batch_launch_count(E->plan);
+        if (!ctx->prof) {
+          RG_CUDA(cudaGraphLaunch(E->graph, s));
+          for (int a = 0; a < nl; ++a) ctx->launches[kind_of(E->plan, a)] += 1;
+        } else {
+          for (int a = 0; a < nl; ++a)
+            RG_CUDA(issue(ctx, kind_of(E->plan, a), 1, [&] { return batch_issue(E->plan, a, s); }));
+        }
+        E->steps_run += 1;
+      }
+    for (int a = 0; a < nruns; ++a) {
+      Run* R = find(ctx, runs[a]);
+      R->cur = (R->cur + seg) % 3;
+    }
+    done += seg;
   }
   if (ctx->prof) {
     int rc = drain_events(ctx);
@@ -1201,7 +1248,7 @@ int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_s
 }
 
 int rg_batch_info(rg_ctx* ctx, const int* runs, int nruns, int* width, int* grid_factor, int* launches,
-                  double* tuned_ms) {
+                  double* tuned_ms, int* tile_cells) {
   if (!ctx || !runs || nruns <= 0) return fail(RG_EINVAL_CONFIG, "empty batch");
   std::vector<int> ids(runs, runs + nruns);
   std::sort(ids.begin(), ids.end());
@@ -1210,7 +1257,8 @@ int rg_batch_info(rg_ctx* ctx, const int* runs, int nruns, int* width, int* grid
   if (width) *width = it->second->width;
   if (grid_factor) *grid_factor = it->second->grid_factor;
   if (launches) *launches = batch_launch_count(it->second->plan);
-  if (tuned_ms) *tuned_ms = it->second->tuned_ms;
+  if (tuned_ms) *tuned_ms = it->second->tune_pending ? 0.0 : it->second->tuned_ms;
+  if (tile_cells) *tile_cells = it->second->width * it->second->group;
   return RG_OK;
 }
 
@@ -1476,7 +1524,15 @@ int rg_run_restore(rg_ctx* ctx, int run, const char* path, int* it0, int* ih0, i
 int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  return rg_run_radial_flux(ctx, run, R->d.nm1, mdot, edot);
+}
+
+int rg_run_radial_flux(rg_ctx* ctx, int run, int iface, double* mdot, double* edot) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!mdot || !edot) return fail(RG_EINVAL_CONFIG, "null output");
+  if (iface < R->d.nm0 || iface > R->d.imax - R->d.nm0)
+    return fail(RG_EINVAL_CONFIG, "radial face index outside the hll range nm0..imax-nm0");
   const DevRun d = full_view(R);
   DevBufs* B = nullptr;
   int rc = full_bufs(R, ctx->stream, &B);
@@ -1488,8 +1544,8 @@ int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot) {
   // fluxes on the per-routine scalar block: the run's own time state is left alone
   if ((rc = reset_fscal(ctx, R))) return rc;
   RG_CUDA(launch_flux(d, 1, B->stage, B->F[0], ctx->stream));
-  // radial face nm1+1/2 (the inner edge of the interior): F1 of rho u^r and of the energy variable
-  const int i = d.nm1;
+  // radial face iface+1/2: F1 of rho u^r and of the energy variable
+  const int i = iface;
   std::vector<double> f0((size_t)d.jmax * d.kmax), f4((size_t)d.jmax * d.kmax);
   // in the full layout the faces (i, j, k) of fixed i lie imax values apart
   const size_t rows = (size_t)d.jmax * d.kmax, pitch = (size_t)d.imax * sizeof(double);
@@ -1510,6 +1566,24 @@ int rg_run_horizon_flux(rg_ctx* ctx, int run, double* mdot, double* edot) {
     }
   *mdot = -m;
   *edot = -e;
+  return RG_OK;
+}
+
+int rg_run_divb(rg_ctx* ctx, int run, double* divb_max, double* b_scale) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!divb_max || !b_scale) return fail(RG_EINVAL_CONFIG, "null output");
+  RG_CUDA(cudaSetDevice(ctx->device));
+  unsigned long long* red = nullptr;
+  RG_CUDA(cudaMalloc(&red, 2 * sizeof(unsigned long long)));
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = launch_divb(R->d, R->b.P[R->cur], red, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, red, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(red);
+  if (e != cudaSuccess) return fail(RG_ECUDA, std::string("rg_run_divb: ") + cudaGetErrorString(e));
+  std::memcpy(divb_max, &h[0], sizeof(double));
+  std::memcpy(b_scale, &h[1], sizeof(double));
   return RG_OK;
 }
 
@@ -1558,15 +1632,49 @@ int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio) {
 
 }  // extern "C"
 
+// ------------------------------------------------------ the step's power function
+namespace {
+__global__ void k_pow_eval(const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ o,
+                           size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) o[i] = rgm::pow(x[i], y[i]);
+}
+}  // namespace
+
+extern "C" int rg_pow_eval(rg_ctx* ctx, const double* x, const double* y, double* out, size_t n) {
+  if (!ctx) return fail(RG_EINVAL_CONFIG, "null context");
+  if (n == 0) return RG_OK;
+  if (!x || !y || !out) return fail(RG_EINVAL_CONFIG, "null array");
+  RG_CUDA(cudaSetDevice(ctx->device));
+  double* d = nullptr;
+  RG_CUDA(cudaMalloc(&d, 3 * n * sizeof(double)));
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(d, x, n * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d + n, y, n * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    k_pow_eval<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d, d + n, d + 2 * n, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(RG_ECUDA, std::string("rg_pow_eval: ") + cudaGetErrorString(e));
+  return RG_OK;
+}
+
 // ------------------------------------------------------ allocation-free fluxes
-// rg_calflx_static serves callers that cannot call cudaMalloc when they need
-// the fluxes: a driver running inside a CUDA stream capture, or a host code
-// whose device memory comes only from its own pool or arena.  The caller owns
-// the input and output device buffers; the flux-CT intermediate (the six
-// averaged induction fluxes) and the kernels' scalar block live in the
-// file-scope device arrays below, sized for grids of at most
+// rg_calflx_static serves callers that cannot let the library call cudaMalloc
+// when they need the fluxes: a host program whose device memory comes only
+// from its own pool or arena (a framework's caching allocator, a driver given
+// a fixed memory budget), where a cudaMalloc behind its back would
+// synchronise the device and take memory the pool does not know about.  The
+// caller owns the input and output device buffers; the flux-CT intermediate
+// (the six averaged induction fluxes) and the kernels' scalar block live in
+// the file-scope device arrays below, sized for grids of at most
 // kStaticMaxCells cells.  Every GPU that loads this library holds these
-// arrays (about 12.6 MB) until the process exits.
+// arrays (about 12.6 MB) until the process exits; with CUDA's lazy module
+// loading the module, and with it the arrays, is typically loaded by a
+// device's first call, which is therefore the one call that may allocate.
 namespace {
 
 constexpr size_t kStaticMaxCells = (size_t)1 << 18;
@@ -1576,6 +1684,7 @@ __device__ __align__(256) Scal g_static_scal;
 constexpr int kMaxDevices = 64;
 double* g_static_ct_addr[kMaxDevices] = {};
 Scal* g_static_scal_addr[kMaxDevices] = {};
+std::mutex g_static_mu;  // guards the per-device address look-up above
 
 // Copy the flux-CT values from the static array into the caller's fluxes over
 // the CT range nm1..n-nm1 (ct.f90:60-109); elsewhere the raw LLF fluxes stay.
@@ -1615,18 +1724,26 @@ extern "C" int rg_calflx_static(rg_ctx* ctx, int run, const double* d_prims, dou
   if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(RG_EINVAL_CONFIG, "device index out of range");
   RG_CUDA(cudaSetDevice(ctx->device));
   // Set-up once per device, with that device current: the host-side names of
-  // the arrays are not device addresses, so their addresses are looked up here.
-  if (!g_static_ct_addr[ctx->device]) {
-    void* a = nullptr;
-    void* b = nullptr;
-    RG_CUDA(cudaGetSymbolAddress(&a, g_static_ct));
-    RG_CUDA(cudaGetSymbolAddress(&b, g_static_scal));
-    g_static_ct_addr[ctx->device] = static_cast<double*>(a);
-    g_static_scal_addr[ctx->device] = static_cast<Scal*>(b);
+  // the arrays are not device addresses, so their addresses are looked up here
+  // (under a lock, so that threads making their first calls on one device at
+  // the same time do not race on the table).
+  double* ct = nullptr;
+  Scal* scal = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ct_addr[ctx->device]) {
+      void* a = nullptr;
+      void* b = nullptr;
+      RG_CUDA(cudaGetSymbolAddress(&a, g_static_ct));
+      RG_CUDA(cudaGetSymbolAddress(&b, g_static_scal));
+      g_static_ct_addr[ctx->device] = static_cast<double*>(a);
+      g_static_scal_addr[ctx->device] = static_cast<Scal*>(b);
+    }
+    ct = g_static_ct_addr[ctx->device];
+    scal = g_static_scal_addr[ctx->device];
   }
-  double* ct = g_static_ct_addr[ctx->device];
   DevRun d = full_view(R);
-  d.scal = g_static_scal_addr[ctx->device];  // the run's own time state is not touched
+  d.scal = scal;  // the run's own time state is not touched
   cudaStream_t s = ctx->stream;
   // The arrays keep the previous call's contents: clear them first.
   RG_CUDA(cudaMemsetAsync(ct, 0, 6 * N * sizeof(double), s));

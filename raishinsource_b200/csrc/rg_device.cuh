@@ -8,9 +8,22 @@
 #pragma once
 #include <cstdint>
 
+#include "../../include/rg_pow.h"
 #include "rg_types.h"
 
 namespace rg {
+
+// A power of the step with a real exponent (the reference's x**y): CUDA's pow
+// in the product build; in the uncontracted build (RG_EXACT_ARITH) the
+// library's own rg_pow, which a host program evaluates to the same bits, so
+// that build repeats a host restatement's arithmetic exactly.
+__device__ __forceinline__ double spow(double x, double y) {
+#ifdef RG_EXACT_ARITH
+  return rgm::pow(x, y);
+#else
+  return pow(x, y);
+#endif
+}
 
 // Type-exact math: no silent promotion of float arguments to double.
 __device__ __forceinline__ double msqrt(double x) { return sqrt(x); }
@@ -118,7 +131,7 @@ __device__ __forceinline__ void met_derive(const double base[kMetBase], double o
 // reconstructed negative density makes the entropy variable NaN.
 // kind: 1 for gam == 4/3, 2 for gam == 5/3 (bitwise), 0 otherwise.
 __device__ __forceinline__ double pow_gam(double x, double gam, int kind) {
-  if (kind == 0 || !(x >= 0.0)) return pow(x, gam);
+  if (kind == 0 || !(x >= 0.0)) return spow(x, gam);
   const double c = cbrt(x);
   return kind == 1 ? x * c : x * c * c;
 }
@@ -129,13 +142,13 @@ __device__ __forceinline__ float pow_gam(float x, float gam, int kind) {
 }
 // x**(1-gam) for x > 0: 1/cbrt(x) for 4/3, 1/cbrt(x)^2 for 5/3.
 __device__ __forceinline__ double pow_1mgam(double x, double gam, int kind) {
-  if (kind == 0 || !(x > 0.0)) return pow(x, 1. - gam);
+  if (kind == 0 || !(x > 0.0)) return spow(x, 1. - gam);
   const double c = rcbrt(x);
   return kind == 1 ? c : c * c;
 }
 // x**(gam-1): cbrt(x) for 4/3, cbrt(x)^2 for 5/3.
 __device__ __forceinline__ double pow_gam1(double x, double gam, int kind) {
-  if (kind == 0 || !(x >= 0.0)) return pow(x, gam - 1.);
+  if (kind == 0 || !(x >= 0.0)) return spow(x, gam - 1.);
   const double c = cbrt(x);
   return kind == 1 ? c : c * c;
 }

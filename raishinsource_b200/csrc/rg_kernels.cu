@@ -213,7 +213,7 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
       long long cyc_s = __double_as_longlong(xxn);
       int cyc_pow2 = 1, cyc_lam2 = 0, cyc_at = 1;
       bool cyc_on = true;
-      const double dro_g1 = pow(dro, gam - 1.);  // loop-invariant factor of dW/dv^2
+      const double dro_g1 = spow(dro, gam - 1.);  // loop-invariant factor of dW/dv^2
       for (int nnn = 1; nnn <= iter; ++nnn) {
         if (!(fabs(delta) >= deltaend && irecov == 0)) break;
         if (nnn == iter) { irecov = 1; break; }
@@ -241,7 +241,11 @@ __device__ bool recov_cell(const double u[9], const double q[9], double out[9], 
         wg = fabs(gfsq * roh);
         wsq = wg * wg;
         const double w3 = wsq * wg;
+#ifdef RG_EXACT_ARITH
+        const double dgfdvsq = 0.5 * spow(gtmp, -1.5);  // as recov.f90 writes it
+#else
         const double dgfdvsq = 0.5 * (gfsq * gf);  // 0.5 gtmp^-1.5 with gf = gtmp^-1/2
+#endif
         const double dwdvsq =
             dro * dgfdvsq + gam1 * gss * dro_g1 * (2. - gam) * pow_1mgam(gf, gam, gkind) * dgfdvsq;
         const double f = qtsq - vsq * (wg + bsq) * (wg + bsq) + (qdotbsq * (bsq + 2. * wg)) / wsq;
@@ -1519,6 +1523,69 @@ __global__ void k_step_begin(DevRun r) { step_begin_body(r); }
 __global__ void k_dt(DevRun r) { dt_body(r); }
 __global__ void k_step_end(DevRun r) { step_end_body(r); }
 
+// ------------------------------------------------------ div B diagnostic
+// Corner-centred divergence of sqrt(-g) B (the quantity Toth's flux-CT,
+// ct.f90:30-118, keeps constant when the normal-field flux is zero): at the
+// corner between cells (i..i+1, j..j+1, k..k+1) of the interior,
+//   D = sum_d (1/(4 dx_d)) sum of the four differences along d
+//       of [sqrt(-g) B^d](cell + e_d) - [sqrt(-g) B^d](cell),
+// with dx_d the spacing of the lower cell.  A slab direction (one interior
+// cell, uniform along it) has one corner plane and no difference along it.
+// red[0] receives max |D|, red[1] max |sqrt(-g) B^d| / dx_d over the same
+// cells, both as bit patterns of non-negative doubles (atomicMax).
+__global__ void __launch_bounds__(256) k_divb(DevRun r, const double* __restrict__ P,
+                                              unsigned long long* __restrict__ red) {
+  const int nm1 = r.nm1;
+  const int i0 = nm1 + 1, j0 = r.jfix ? r.jfix : nm1 + 1, k0 = r.kfix ? r.kfix : nm1 + 1;
+  const int ni = r.imax - 2 * nm1 - 1;
+  const int nj = r.jfix ? 1 : r.jmax - 2 * nm1 - 1;
+  const int nk = r.kfix ? 1 : r.kmax - 2 * nm1 - 1;
+  const long long total = (long long)ni * nj * nk;
+  const size_t N = r.N;
+  double dmax = 0.0, bmax = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = i0 + (int)(t % ni);
+    const int j = j0 + (int)((t / ni) % nj);
+    const int k = k0 + (int)(t / ((long long)ni * nj));
+    double b[2][2][2][3];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+          const size_t cell = r.cell(i + a, j + bb, k + c);
+          const double g = __ldg(r.mc + 17 * r.nik + r.ik(i + a, k + c));
+#pragma unroll
+          for (int d = 0; d < 3; ++d) b[c][bb][a][d] = g * P[(size_t)(6 + d) * N + cell];
+        }
+    const double dx1 = r.dx1b[i - 1], dx2 = r.dx2b[j - 1], dx3 = r.dx3b[k - 1];
+    double d1 = 0.0, d2 = 0.0, d3 = 0.0;
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        d1 += b[u][v][1][0] - b[u][v][0][0];
+        d2 += b[u][1][v][1] - b[u][0][v][1];
+        d3 += b[1][u][v][2] - b[0][u][v][2];
+      }
+    const double D = d1 / (4.0 * dx1) + (r.jfix ? 0.0 : d2 / (4.0 * dx2)) + (r.kfix ? 0.0 : d3 / (4.0 * dx3));
+    dmax = fmax(dmax, fabs(D));
+    if (D != D) dmax = D;
+    bmax = fmax(bmax, fmax(fabs(b[0][0][0][0]) / dx1, fmax(fabs(b[0][0][0][1]) / dx2, fabs(b[0][0][0][2]) / dx3)));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double x = __shfl_xor_sync(0xffffffffu, dmax, o), y = __shfl_xor_sync(0xffffffffu, bmax, o);
+    dmax = (x != x) ? x : fmax(dmax, x);
+    bmax = fmax(bmax, y);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(red, (unsigned long long)__double_as_longlong(fabs(dmax)));
+    atomicMax(red + 1, (unsigned long long)__double_as_longlong(bmax));
+  }
+}
+
 // ------------------------------------------------- per-routine entry points
 // recov (recov.f90:2-47) of every interior cell; other cells, and every cell
 // of a run that has passed tmax, keep Pc.
@@ -1777,8 +1844,8 @@ __global__ void k_geom_derive(DevRun r, double* mc, double* mi, double* mk, doub
   }
   if (q < (size_t)r.imax) {
     const double rr = r.x1[q];
-    fl_de[q] = r.dmin * pow(rr, -1.5);
-    fl_pr[q] = (r.gam - 1.) * r.pmin * pow(rr, -2.5);
+    fl_de[q] = r.dmin * spow(rr, -1.5);
+    fl_pr[q] = (r.gam - 1.) * r.pmin * spow(rr, -2.5);
   }
 }
 
@@ -2087,6 +2154,12 @@ cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t
   return cudaGetLastError();
 }
 
+cudaError_t launch_divb(const DevRun& r, const double* P, unsigned long long* red, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(red, 0, 2 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  k_divb<<<148 * 4, 256, 0, s>>>(r, P, red);
+  return cudaGetLastError();
+}
 cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStream_t s) {
   const dim3 b = sblock(r, dim3(64, 2, 1));
   k_calsf<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P, SF);

@@ -40,6 +40,9 @@ cudaError_t launch_stage_recov2(const DevRun& r, int stage, const double* Pc, do
                                 double* F3, const double* CT, double* Uc, double* SF, double* Unew, cudaStream_t s);
 cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s);
 cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStream_t s);
+// corner-centred div(sqrt(-g) B) of P over the interior: red[0] = max |D|,
+// red[1] = max |sqrt(-g) B^d| / dx_d (bit patterns of doubles)
+cudaError_t launch_divb(const DevRun& r, const double* P, unsigned long long* red, cudaStream_t s);
 cudaError_t launch_derived(const DevRun& r, const double* P, const double* geo_i, const double* geo_k, double akm,
                            int jslice, double* out, cudaStream_t s);
 cudaError_t launch_rkt(const DevRun& r, int stage, const double* W1, const double* W2, const double* W3,
@@ -71,7 +74,7 @@ cudaError_t launch_ic_torus(const DevRun& r, const IcTorusArgs& a, double* P, cu
 
 // Batched steps of runs of one class (rg_batch.cuh).
 struct BatchPlan;
-int batch_build(const std::vector<DevRun>& runs, int width, BatchPlan** out);
+int batch_build(const std::vector<DevRun>& runs, int width, int group, BatchPlan** out);
 void batch_destroy(BatchPlan* B);
 int batch_launch_count(const BatchPlan* B);
 void batch_set_grid(BatchPlan* B, int factor);

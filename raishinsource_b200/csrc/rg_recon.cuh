@@ -40,15 +40,23 @@ __device__ __forceinline__ T dm4(T ww, T xx, T yy, T zz) {
 // reference's right state flips the signs of the dm4 terms of md and lc
 // (rec.f90:2172-2176).  Negation is exact, so both equal the reference's
 // separate formulas bit for bit, and the two lanes of a face run one code path.
+// The second differences are the exception: the reference evaluates them once
+// per cell in stencil order, (u-2 - 2 u-1) + u0, (u-1 - 2 u0) + u+1 and
+// (u0 - 2 u+1) + u+2, for both states, and a sum taken in the mirrored order
+// can round differently; the right state therefore picks its operands so
+// that each difference is summed as the reference sums it.
 template <typename T>
 __device__ __forceinline__ T mp_limit(T ul1, T a2, T a1, T u0, T b1, T b2, T sg) {
   const T tmp2 = T(4.0) / T(3.0), alpha = T(4.0), eps1 = T(1.0e-10);
   const T ulmp = u0 + dmm(b1 - u0, alpha * (u0 - a1));
   const T t = (ul1 - u0) * (ul1 - ulmp);
   if (t <= eps1) return ul1;
-  const T dim1 = a2 - T(2.) * a1 + u0;
-  const T di1 = a1 - T(2.) * u0 + b1;
-  const T dip1 = u0 - T(2.) * b1 + b2;
+  const bool right = sg < T(0);
+  // left: dim1 = (a2 - 2 a1) + u0, di1 = (a1 - 2 u0) + b1, dip1 = (u0 - 2 b1) + b2;
+  // right (a = u+, b = u-): dim1 = (u0 - 2 a1) + a2, di1 = (b1 - 2 u0) + a1, dip1 = (b2 - 2 b1) + u0
+  const T dim1 = (right ? u0 : a2) - T(2.) * a1 + (right ? a2 : u0);
+  const T di1 = (right ? b1 : a1) - T(2.) * u0 + (right ? a1 : b1);
+  const T dip1 = (right ? b2 : u0) - T(2.) * b1 + (right ? u0 : b2);
   const T dm4p = dm4(T(4.) * di1 - dip1, T(4.) * dip1 - di1, di1, dip1);
   const T dm4m = dm4(T(4.) * di1 - dim1, T(4.) * dim1 - di1, di1, dim1);
   const T ul = u0 + alpha * (u0 - a1);

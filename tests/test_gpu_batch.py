@@ -88,14 +88,18 @@ def _alone_vs_batch(gpu_ctx, params, ics, steps):
 
 
 def test_batch_tubes_equal_alone(gpu_ctx):
+    """70 steps in one call: the batch starts with the default shape, is tuned
+    after its 32nd step (block width, cells per tile, persistent grid) and
+    continues with the chosen shape; every tube still equals itself alone."""
     lengths = [400, 517, 1203, 64, 900]
     params = [config.tube(n=n, tmax=0.4) for n in lengths]
     ics = [lambda r, t=t: r.ic_tube(seed=2012, tube=t) for t in range(len(lengths))]
-    out, info = _alone_vs_batch(gpu_ctx, params, ics, 25)
+    out, info = _alone_vs_batch(gpu_ctx, params, ics, 70)
     for a, b, sa, sb in out:
         assert np.array_equal(a, b)
-        assert sa["time"] == sb["time"] and sa["steps"] == sb["steps"] == 25
-    assert info["launches_per_step"] > 0 and info["width"] == 128
+        assert sa["time"] == sb["time"] and sa["steps"] == sb["steps"] == 70
+    assert info["launches_per_step"] > 0 and info["tuned_ms_per_step"] > 0
+    assert info["width"] in (64, 128) and info["tile_cells"] in (64, 128, 256, 512)
 
 
 def test_batch_tori_fp64_and_mixed_equal_alone(gpu_ctx):

@@ -1,8 +1,9 @@
 """The allocation-free flux entry point (rg_calflx_static).
 
-Callers that cannot call cudaMalloc when they need the fluxes — code inside a
-CUDA stream capture, or a host program whose device memory comes only from its
-own pool — pass their own device buffers and get the same fluxes as rg_calflx,
+A host program whose device memory comes only from its own pool or arena
+cannot let the library call cudaMalloc behind its back (the allocation would
+synchronise the device and take memory the pool does not know about).  Such a
+caller passes its own device buffers and gets the same fluxes as rg_calflx,
 with flux-CT's intermediate held in the library's static device array.  This
 file is collected last so that a run stopping at the first failure has already
 run every other test; it also passes alone in a fresh process.
