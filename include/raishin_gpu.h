@@ -239,6 +239,17 @@ int rg_rkt(rg_ctx* ctx, int run, int stage, double dt, const double* ww, const d
 int rg_run_store(rg_ctx* ctx, int run, const char* path, int it0, int ih0, int nd, const double* uri0);
 int rg_run_restore(rg_ctx* ctx, int run, const char* path, int* it0, int* ih0, int* nd, double* uri0);
 
+/* Snapshot file of output1 (restar.f90:91-185) for one rank holding the
+ * whole grid, byte-compatible with structrNNNN-MMMM.outdat (the caller passes
+ * the file name): gfortran sequential unformatted records with 4-byte length
+ * markers, (time, myrank, npe), (is, ie, js, je, ks, ke) = (1, imax, 1,
+ * jmax, 1, kmax), then for i, j, k (k fastest) the 13 doubles x1(i), x2(j),
+ * x3(k), uri(1:9,i,j,k), detg(i,j,k); the coordinates are the MKS x?b for
+ * metric 403 and x? otherwise (main.f90:711-717), time the loop-top time.
+ * The records are formatted on the device and copied chunk by chunk into
+ * pinned host memory, overlapping the file writes. */
+int rg_run_output(rg_ctx* ctx, int run, const char* path, int myrank, int npe);
+
 /* Accretion rates through the inner edge of the interior (the radial face
  * nm1+1/2, just outside the horizon for the torus grids): mdot = -sum of the
  * radial flux of sqrt(-g) rho u^r over the interior (phi, theta) faces times

@@ -2,6 +2,7 @@
 // see oracle.hpp).  Arrays crossing this boundary use the reference layout
 // a(nv,i,j,k): variable fastest, then i, j, k.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <string>
 
@@ -213,6 +214,42 @@ void orc_bnd_floor(void* h, double* uri, const double* urio) {
 // Grid and metric arrays by name.  1D grid arrays: n = extent (1-based values
 // copied to out[0..n-1]).  Metric per (i,k): 16 (gcov*/gcon*) or 1 (detg*)
 // or 64 (christ) values per point, point index i-1 + imax*(k-1).
+// output1 (restar.f90:91-185) for one rank holding the whole grid
+// (is..ie = 1..imax etc.): gfortran sequential unformatted records, each
+// framed by its 4-byte length: (time, myrank, npe), (is, ie, js, je, ks, ke),
+// then for i, j, k (k fastest) x1(i), x2(j), x3(k), uri(1:9,i,j,k), detg.
+// The coordinates are x?b for metric 403 and x? otherwise (main.f90:711-717);
+// time is the loop-top time.  Returns 0 on success.
+int orc_output1(void* h, const char* path, int myrank, int npe) {
+  State* s = static_cast<State*>(h);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return 1;
+  auto rec = [&](const void* d, uint32_t n) {
+    return std::fwrite(&n, 4, 1, f) == 1 && std::fwrite(d, n, 1, f) == 1 && std::fwrite(&n, 4, 1, f) == 1;
+  };
+  unsigned char h1[16];
+  std::memcpy(h1, &s->timeh, 8);
+  std::memcpy(h1 + 8, &myrank, 4);
+  std::memcpy(h1 + 12, &npe, 4);
+  const int32_t h2[6] = {1, s->imax, 1, s->jmax, 1, s->kmax};
+  bool ok = rec(h1, 16) && rec(h2, 24);
+  const bool mks = (s->p.metric == 403);
+  const std::vector<double>& X1 = mks ? s->x1b : s->x1;
+  const std::vector<double>& X2 = mks ? s->x2b : s->x2;
+  const std::vector<double>& X3 = mks ? s->x3b : s->x3;
+  for (int i = 1; ok && i <= s->imax; ++i)
+    for (int j = 1; ok && j <= s->jmax; ++j)
+      for (int k = 1; ok && k <= s->kmax; ++k) {
+        double v[13];
+        v[0] = X1[i]; v[1] = X2[j]; v[2] = X3[k];
+        for (int n = 1; n <= orc::NV; ++n) v[2 + n] = s->uri[s->a(n, i, j, k)];
+        v[12] = s->detg[s->ik(i, k)];
+        ok = rec(v, 104);
+      }
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? 0 : 1;
+}
+
 long long orc_get_array(void* h, const char* name, double* out, long long cap) {
   State* s = static_cast<State*>(h);
   const std::string n(name);

@@ -79,6 +79,8 @@ def _lib():
         lib.orc_rkt.argtypes = [P, C.c_int, C.c_double, D, D, D, D, D]
         lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
         lib.orc_get_array.restype = C.c_longlong
+        lib.orc_output1.argtypes = [P, C.c_char_p, C.c_int, C.c_int]
+        lib.orc_output1.restype = C.c_int
         lib.orc_set_pow_mode.argtypes = [C.c_int]
         lib.orc_set_pow_mode.restype = C.c_int
         lib.orc_pow_eval.argtypes = [D, D, D, C.c_longlong, C.c_int]
@@ -252,6 +254,11 @@ class Oracle:
     def cdtcfl(self, uri) -> float:
         uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
         return self.lib.orc_cdtcfl(self.h, _ptr(uri))
+
+    def output1(self, path: str, myrank: int = 0, npe: int = 1):
+        """Write the current primitives as output1's structr file (restar.f90:91-185)."""
+        if self.lib.orc_output1(self.h, os.fsencode(path), myrank, npe) != 0:
+            raise OSError("orc_output1 failed: " + path)
 
     def bnd_floor(self, uri, urio):
         uri = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)

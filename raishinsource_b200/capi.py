@@ -29,7 +29,7 @@ EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ct
            "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_torus_device", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
-           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_divb", "rg_run_horizon_flux", "rg_run_radial_flux", "rg_run_store", "rg_run_restore", "rg_pow_eval", "rg_calflx_static")
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_divb", "rg_run_horizon_flux", "rg_run_radial_flux", "rg_run_store", "rg_run_restore", "rg_run_output", "rg_pow_eval", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -128,6 +128,7 @@ def load(path: str = LIB_PATH):
     lib.rg_pow_eval.argtypes = [P, D, D, D, C.c_size_t]
     lib.rg_run_horizon_flux.argtypes = [P, I, D, D]
     lib.rg_run_divb.argtypes = [P, I, D, D]
+    lib.rg_run_output.argtypes = [P, I, C.c_char_p, I, I]
     lib.rg_run_radial_flux.argtypes = [P, I, I, D, D]
     lib.rg_run_store.argtypes = [P, I, C.c_char_p, I, I, I, C.c_void_p]
     lib.rg_run_restore.argtypes = [P, I, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -435,6 +436,10 @@ class Run:
             uri0 = np.ascontiguousarray(uri0, dtype=np.float64).reshape(self.shape)
             ptr = uri0.ctypes.data
         _check(self.lib, self.lib.rg_run_store(self.ctx.h, self.id, os.fsencode(path), it0, ih0, nd, ptr))
+
+    def output(self, path: str, myrank: int = 0, npe: int = 1):
+        """Write output1's snapshot file of the current state (rg_run_output)."""
+        _check(self.lib, self.lib.rg_run_output(self.ctx.h, self.id, os.fsencode(path), int(myrank), int(npe)))
 
     def restore(self, path: str) -> dict:
         """Read a restart file of this grid (rg_run_restore); returns it0, ih0, nd and uri0."""

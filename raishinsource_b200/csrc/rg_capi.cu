@@ -1569,6 +1569,94 @@ int rg_run_radial_flux(rg_ctx* ctx, int run, int iface, double* mdot, double* ed
   return RG_OK;
 }
 
+// output1 (restar.f90:91-185): the records are formatted on the device in
+// chunks, each copied by one cudaMemcpyAsync into one of two pinned host
+// buffers, so that the formatting and copy of a chunk overlap the file write
+// of the previous one.
+int rg_run_output(rg_ctx* ctx, int run, const char* path, int myrank, int npe) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!path) return fail(RG_EINVAL_CONFIG, "null path");
+  RG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  Scal sc{};
+  RG_CUDA(cudaMemcpyAsync(&sc, R->d.scal, sizeof(Scal), cudaMemcpyDeviceToHost, s));
+  RG_CUDA(cudaStreamSynchronize(s));
+  const DevRun& d = R->d;
+  // the coordinates output1 carries: x?b for metric 403, x? otherwise (main.f90:711-717)
+  const bool mks = (R->p.metric == 403);
+  std::vector<double> axes;
+  const int ext[3] = {d.imax, d.jmax, d.kmax};
+  for (int a = 0; a < 3; ++a) {
+    const std::vector<double>& x = mks ? R->geom.ax[a].xb : R->geom.ax[a].x;
+    for (int m = 1; m <= ext[a]; ++m) axes.push_back(x[m]);
+  }
+  const size_t nrec = (size_t)d.imax * d.jmax * d.kmax;
+  const size_t chunk = std::min<size_t>(nrec, (size_t)1 << 19);  // records per chunk (56 MB)
+  const size_t cbytes = chunk * 112;
+  double* dax = nullptr;
+  unsigned* dbuf = nullptr;
+  unsigned char* hbuf = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  FILE* f = nullptr;
+  int rc = RG_OK;
+  auto cleanup = [&]() {
+    if (f) std::fclose(f);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+    cudaFree(dax);
+    cudaFree(dbuf);
+    cudaFreeHost(hbuf);
+  };
+  cudaError_t e = cudaMalloc(&dax, axes.size() * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dbuf, 2 * cbytes);
+  if (e == cudaSuccess) e = cudaMallocHost(&hbuf, 2 * cbytes);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dax, axes.data(), axes.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(RG_ECUDA, std::string("rg_run_output: ") + cudaGetErrorString(e));
+  }
+  f = std::fopen(path, "wb");
+  if (!f) {
+    cleanup();
+    return fail(RG_EINVAL_CONFIG, std::string("cannot open ") + path);
+  }
+  unsigned char h1[16];
+  std::memcpy(h1, &sc.timeh, 8);
+  std::memcpy(h1 + 8, &myrank, 4);
+  std::memcpy(h1 + 12, &npe, 4);
+  const int32_t h2[6] = {1, d.imax, 1, d.jmax, 1, d.kmax};
+  bool ok = put_record(f, h1, 16) && put_record(f, h2, 24);
+  const size_t nchunks = (nrec + chunk - 1) / chunk;
+  for (size_t c = 0; ok && c <= nchunks; ++c) {
+    if (c < nchunks) {  // format and copy chunk c
+      const int b = (int)(c % 2);
+      const size_t r0 = c * chunk, n = std::min(chunk, nrec - r0);
+      unsigned* db = dbuf + (size_t)b * (cbytes / 4);
+      e = launch_output1(d, R->b.P[R->cur], dax, dax + d.imax, dax + d.imax + d.jmax, r0, n, db, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(hbuf + (size_t)b * cbytes, db, n * 112, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaEventRecord(ev[b], s);
+      if (e != cudaSuccess) break;
+    }
+    if (c >= 1) {  // write chunk c-1 while chunk c is formatted and copied
+      const int b = (int)((c - 1) % 2);
+      const size_t n = std::min(chunk, nrec - (c - 1) * chunk);
+      e = cudaEventSynchronize(ev[b]);
+      if (e != cudaSuccess) break;
+      ok = std::fwrite(hbuf + (size_t)b * cbytes, n * 112, 1, f) == 1;
+    }
+  }
+  if (e != cudaSuccess) rc = fail(RG_ECUDA, std::string("rg_run_output: ") + cudaGetErrorString(e));
+  else if (!ok) rc = fail(RG_EINVAL_CONFIG, std::string("write failed: ") + path);
+  if (std::fclose(f) != 0 && rc == RG_OK) rc = fail(RG_EINVAL_CONFIG, std::string("write failed: ") + path);
+  f = nullptr;
+  cudaStreamSynchronize(s);
+  cleanup();
+  return rc;
+}
+
 int rg_run_divb(rg_ctx* ctx, int run, double* divb_max, double* b_scale) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");

@@ -1523,6 +1523,41 @@ __global__ void k_step_begin(DevRun r) { step_begin_body(r); }
 __global__ void k_dt(DevRun r) { dt_body(r); }
 __global__ void k_step_end(DevRun r) { step_end_body(r); }
 
+// ------------------------------------------------------ snapshot output
+// The byte image of output1's data records (restar.f90:160-167): record
+// rec0 + t, for (i, j, k) with k fastest, then j, then i, is 13 doubles
+// x1(i), x2(j), x3(k), uri(1:9,i,j,k), detg(i,j,k) framed by the 4-byte
+// record length 104 of gfortran's sequential unformatted files: 28 words of
+// 4 bytes, so that the image is the file's bytes.  cx/cy/cz are the three
+// coordinate axes the file carries (index i-1 etc.).
+__global__ void __launch_bounds__(128) k_output1(DevRun r, const double* __restrict__ P, const double* __restrict__ cx,
+                                                 const double* __restrict__ cy, const double* __restrict__ cz,
+                                                 size_t rec0, size_t nrec, unsigned* __restrict__ out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrec) return;
+  const size_t rr = rec0 + t;
+  const int k = (int)(rr % (size_t)r.kmax) + 1;
+  const int j = (int)((rr / (size_t)r.kmax) % (size_t)r.jmax) + 1;
+  const int i = (int)(rr / ((size_t)r.kmax * (size_t)r.jmax)) + 1;
+  const size_t c = r.cell(i, j, k);
+  double v[13];
+  v[0] = cx[i - 1];
+  v[1] = cy[j - 1];
+  v[2] = cz[k - 1];
+#pragma unroll
+  for (int n = 0; n < 9; ++n) v[3 + n] = P[(size_t)n * r.N + c];
+  v[12] = r.mc[17 * r.nik + r.ik(i, k)];
+  unsigned* o = out + t * 28;
+  o[0] = 104u;
+#pragma unroll
+  for (int m = 0; m < 13; ++m) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v[m]);
+    o[1 + 2 * m] = (unsigned)(b & 0xffffffffull);
+    o[2 + 2 * m] = (unsigned)(b >> 32);
+  }
+  o[27] = 104u;
+}
+
 // ------------------------------------------------------ div B diagnostic
 // Corner-centred divergence of sqrt(-g) B (the quantity Toth's flux-CT,
 // ct.f90:30-118, keeps constant when the normal-field flux is zero): at the
@@ -2154,6 +2189,12 @@ cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t
   return cudaGetLastError();
 }
 
+cudaError_t launch_output1(const DevRun& r, const double* P, const double* cx, const double* cy, const double* cz,
+                           size_t rec0, size_t nrec, unsigned* out, cudaStream_t s) {
+  if (nrec == 0) return cudaSuccess;
+  k_output1<<<(unsigned)((nrec + 127) / 128), 128, 0, s>>>(r, P, cx, cy, cz, rec0, nrec, out);
+  return cudaGetLastError();
+}
 cudaError_t launch_divb(const DevRun& r, const double* P, unsigned long long* red, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(red, 0, 2 * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;

@@ -43,6 +43,9 @@ cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStrea
 // corner-centred div(sqrt(-g) B) of P over the interior: red[0] = max |D|,
 // red[1] = max |sqrt(-g) B^d| / dx_d (bit patterns of doubles)
 cudaError_t launch_divb(const DevRun& r, const double* P, unsigned long long* red, cudaStream_t s);
+// records rec0 .. rec0+nrec-1 of output1's data (restar.f90:160-167) as the file's bytes, 112 per record
+cudaError_t launch_output1(const DevRun& r, const double* P, const double* cx, const double* cy, const double* cz,
+                           size_t rec0, size_t nrec, unsigned* out, cudaStream_t s);
 cudaError_t launch_derived(const DevRun& r, const double* P, const double* geo_i, const double* geo_k, double akm,
                            int jslice, double* out, cudaStream_t s);
 cudaError_t launch_rkt(const DevRun& r, int stage, const double* W1, const double* W2, const double* W3,

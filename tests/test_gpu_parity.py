@@ -449,6 +449,27 @@ def test_thousand_steps_l1_ppm(gpu_ctx):
     assert l1[[0, 4, 6, 7, 8]].max() < 1e-10, l1
 
 
+def test_thousand_steps_l1_mp5_3d(gpu_ctx):
+    """1000 steps of the product (FMA-contracted) build on the 40x24x16 3D
+    torus, MP5 with the positivity fallback (the benchmark's scheme): L1 of
+    rho, the internal energy (p) and B against the oracle stays below 1e-10.
+    (The uncontracted build is bit-identical to the oracle over the same run,
+    tests/test_gpu_exact.py.)"""
+    p = dict(config.torus(nr=40, nth=24, nph=16), guard=1)
+    o = Oracle(p)
+    o.ic_torus(seed=2012)
+    o.init_cons()
+    r = gpu_ctx.admit(p)
+    r.upload_prims(o.prims())
+    o.step(1000)
+    st = r.step(1000, stats=True)
+    got, want = r.prims(), o.prims()
+    r.release()
+    assert st["steps"] == 1000
+    l1 = _l1(got, want, o.nm1)
+    assert l1[[0, 4, 6, 7, 8]].max() < 1e-10, l1
+
+
 def test_per_routine_calls_leave_the_run_alone(gpu_ctx):
     """The reference-interface entry points compute on their own scratch
     state: calling them between steps of a run changes neither its result,

@@ -66,3 +66,23 @@ def test_store_layout_and_restore(gpu_ctx, tmp_path):
     assert np.array_equal(r.prims(), r2.prims())
     r.release()
     r2.release()
+
+
+@pytest.mark.parametrize("nph", [12, None])
+def test_output1_snapshot_equals_oracle_file(gpu_ctx, tmp_path, nph):
+    """rg_run_output formats output1's records on the device and writes them
+    through pinned buffers: the file equals the oracle's restatement of
+    output1 (restar.f90:91-185) byte for byte, for a 3D run and a 2D run whose
+    phi slab is stored as one plane."""
+    p = dict(config.torus(nr=40, nth=32, nph=nph), guard=1)
+    o = Oracle(p)
+    o.ic_torus(seed=23)
+    r = gpu_ctx.admit(p)
+    r.upload_prims(o.prims())
+    a, b = str(tmp_path / "dev.outdat"), str(tmp_path / "orc.outdat")
+    r.output(a, myrank=0, npe=1)
+    r.release()
+    o.output1(b, myrank=0, npe=1)
+    da, db = open(a, "rb").read(), open(b, "rb").read()
+    assert len(da) == len(db) == 56 + p["imax"] * p["jmax"] * p["kmax"] * 112
+    assert da == db

@@ -447,3 +447,45 @@ def test_recov2_recovers_the_primitives_of_their_conserved_variables():
     _, got1 = o1.recov(u, guess)
     assert not np.array_equal(got1[reg], got[reg])  # a different inversion ran
     assert np.abs(got1[reg] - got[reg])[..., [0, 4]].max() / np.abs(q[reg])[..., [0, 4]].min() < 1e-3
+
+
+def _read_records(path):
+    import struct
+    with open(path, "rb") as f:
+        data = f.read()
+    recs, off = [], 0
+    while off < len(data):
+        (n,) = struct.unpack_from("<i", data, off)
+        (m,) = struct.unpack_from("<i", data, off + 4 + n)
+        assert m == n
+        recs.append(data[off + 4: off + 4 + n])
+        off += n + 8
+    return recs
+
+
+def test_output1_layout(tmp_path):
+    """output1's snapshot file (restar.f90:91-185) from the oracle: header
+    records (time, myrank, npe) and (is, ie, js, je, ks, ke), then one record
+    of 13 doubles per cell with k fastest, then j, then i: the MKS coordinates
+    x1b, x2b, x3b (metric 403), the nine primitives and sqrt(-g)."""
+    import struct
+    p = config.torus(nr=20, nth=16, nph=10)
+    o = Oracle(p)
+    o.ic_torus(seed=3)
+    path = str(tmp_path / "structr0000-0001.outdat")
+    o.output1(path, myrank=0, npe=1)
+    recs = _read_records(path)
+    imax, jmax, kmax = p["imax"], p["jmax"], p["kmax"]
+    assert len(recs) == 2 + imax * jmax * kmax
+    t, rank, npe = struct.unpack("<dii", recs[0])
+    assert (t, rank, npe) == (o.time, 0, 1)
+    assert struct.unpack("<6i", recs[1]) == (1, imax, 1, jmax, 1, kmax)
+    body = np.frombuffer(b"".join(recs[2:]), dtype="<f8").reshape(imax, jmax, kmax, 13)
+    u = o.prims()  # (kmax, jmax, imax, 9)
+    assert np.array_equal(body[..., 3:12], np.transpose(u, (2, 1, 0, 3)))
+    assert np.array_equal(body[:, 0, 0, 0], o.array("x1b"))
+    assert np.array_equal(body[0, :, 0, 1], o.array("x2b"))
+    assert np.array_equal(body[0, 0, :, 2], o.array("x3b"))
+    detg = o.array("detg").reshape(kmax, imax)
+    assert np.array_equal(body[:, 3, :, 12], detg.T)
+    assert len(open(path, "rb").read()) == 24 + 32 + imax * jmax * kmax * 112
