@@ -91,7 +91,6 @@ struct UpdateB {
 template <int STAGE>
 struct CarryB {
   __device__ void operator()(const DevRun& r, const Tile&) const {
-    if (threadIdx.x != 0 || threadIdx.y != 0 || threadIdx.z != 0) return;
     double *Pn, *Pc, *Pw;
     stage_ptrs(r, STAGE, Pn, Pc, Pw);
     carry_fix_body<0, STAGE>(r, Pn, Pc, Pw, r.F[0], r.F[1], r.F[2], r.CT, nullptr);
@@ -303,7 +302,7 @@ int batch_build(const std::vector<DevRun>& runs, int width, int group, BatchPlan
       if (r.strag_list) add_tiles(t, a, dim3((unsigned)((r.strag_cap + 127) / 128), 1, 1), 0, 0, 0);
     });
     L.kind = BK_CARRY;
-    L.block = dim3(32, 1, 1);
+    L.block = dim3(128, 1, 1);
     plan_append(*B, T, L, runs, one);
     for (int per = 1; per >= 0; --per)
       for (int dir = 1; dir <= 3; ++dir) {
@@ -464,9 +463,9 @@ cudaError_t batch_issue(const BatchPlan* B, int idx, cudaStream_t s) {
       if (L.stage == 2) return kb_go<StragB<2>, 128, 1>(B, L, StragB<2>{}, s);
       return kb_go<StragB<3>, 128, 1>(B, L, StragB<3>{}, s);
     case BK_CARRY:
-      if (L.stage == 1) return kb_go<CarryB<1>, 32, 1>(B, L, CarryB<1>{}, s);
-      if (L.stage == 2) return kb_go<CarryB<2>, 32, 1>(B, L, CarryB<2>{}, s);
-      return kb_go<CarryB<3>, 32, 1>(B, L, CarryB<3>{}, s);
+      if (L.stage == 1) return kb_go<CarryB<1>, 128, 1>(B, L, CarryB<1>{}, s);
+      if (L.stage == 2) return kb_go<CarryB<2>, 128, 1>(B, L, CarryB<2>{}, s);
+      return kb_go<CarryB<3>, 128, 1>(B, L, CarryB<3>{}, s);
     case BK_BCPER:
     case BK_BCPHYS:
       if (L.dir == 1) return go_bc<1>(B, L, s);

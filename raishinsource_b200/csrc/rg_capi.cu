@@ -1,11 +1,13 @@
 // rg_capi.cu -- the C ABI of include/raishin_gpu.h: contexts, run admission
 // by device footprint, host<->device layout conversion, the device-resident
 // RK3 step driver and the per-routine entry points.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <iterator>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 #include <map>
@@ -56,6 +58,10 @@ struct Run {
   std::vector<void*> allocs;
   size_t bytes = 0;
   HostGeom geom;
+  // TMA tensor maps of the primitive buffers b.P[buffer] for the staged face
+  // kernel, per direction (flux_tma_box); tma is set when all nine exist
+  CUtensorMap tmap[3][3];
+  bool tma = false;
 };
 
 }  // namespace
@@ -99,6 +105,7 @@ struct rg_ctx {
   double ms[K_NKINDS] = {};
   bool own_stream = true;              // false after rg_ctx_set_stream
   cudaEvent_t marks[RG_MAX_MARKS] = {};  // rg_ctx_mark / rg_ctx_wait_mark
+  bool tma = true;                     // staged face kernel where a run allows it (RAISHIN_FLUX_TMA=0: off)
 };
 
 namespace {
@@ -118,6 +125,50 @@ void free_run(Run* R) {
   for (void* p : R->allocs) cudaFree(p);
   R->allocs.clear();
   delete R;
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      (void)cudaGetLastError();
+  });
+  return fn;
+}
+
+// Tensor maps of the three primitive buffers as 4D FP64 arrays (i, j, k, v)
+// with the boxes of the staged face kernel; a run they do not fit keeps the
+// generic face kernel.
+void make_tmaps(Run* R) {
+  R->tma = false;
+  const DevRun& d = R->d;
+  if (!flux_tma_eligible(d)) return;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return;
+  const cuuint64_t dims[4] = {(cuuint64_t)d.imax, (cuuint64_t)d.jmax, (cuuint64_t)d.kmax, 9};
+  const cuuint64_t strides[3] = {(cuuint64_t)d.imax * 8, (cuuint64_t)d.imax * d.jmax * 8, (cuuint64_t)d.N * 8};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  for (int b = 0; b < 3; ++b)
+    for (int dir = 1; dir <= 3; ++dir) {
+      unsigned box[4];
+      flux_tma_box(dir, box);
+      const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+      if (enc(&R->tmap[b][dir - 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, R->b.P[b], dims, strides, bx, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return;
+    }
+  R->tma = true;
 }
 
 // Ghost widths of the reconstruction (main.f90:179-190): nm0 = 2 for the
@@ -217,7 +268,7 @@ size_t footprint_bytes(const rg_run_params* p) {
     mixed = (9 + 27 + 6) * N * sizeof(float) + (3 * kMetComps + 64) * nik * sizeof(float);
   const size_t upct = (p->ict == 3) ? 6 * N * sizeof(double) : 0;  // upflct's EMF differences
   const size_t rec2 = (p->iwvec == 2) ? 22 * N * sizeof(double) : 0;  // recov2 stage scratch
-  return state + geom + mixed + upct + rec2 + sizeof(Scal) + C_NCOUNTERS * 8 + (kCarryCap + straggler_cap(N)) * sizeof(int);
+  return state + geom + mixed + upct + rec2 + sizeof(Scal) + C_NCOUNTERS * 8 + (2 * kCarryCap + straggler_cap(N)) * sizeof(int);
 }
 
 Run* find(rg_ctx* ctx, int id) {
@@ -462,9 +513,16 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
   const DevRun& d = R->d;
   cudaStream_t s = ctx->stream;
   const int nf = n_flux_launches(d);
-  RG_CUDA(issue(ctx, K_FLUX1, nf, [&] { return launch_flux(d, 1, Pc, R->b.F[0], s); }));
-  RG_CUDA(issue(ctx, K_FLUX2, nf, [&] { return launch_flux(d, 2, Pc, R->b.F[1], s); }));
-  RG_CUDA(issue(ctx, K_FLUX3, nf, [&] { return launch_flux(d, 3, Pc, R->b.F[2], s); }));
+  // the faces with the stencil staged by TMA where the run allows it
+  const int bi = (Pc == R->b.P[0]) ? 0 : (Pc == R->b.P[1] ? 1 : 2);
+  const bool tma = R->tma && ctx->tma && Pc == R->b.P[bi];
+  auto faces = [&](int dir) {
+    return tma ? launch_flux_tma(d, dir, &R->tmap[bi][dir - 1], R->b.F[dir - 1], s)
+               : launch_flux(d, dir, Pc, R->b.F[dir - 1], s);
+  };
+  RG_CUDA(issue(ctx, K_FLUX1, nf, [&] { return faces(1); }));
+  RG_CUDA(issue(ctx, K_FLUX2, nf, [&] { return faces(2); }));
+  RG_CUDA(issue(ctx, K_FLUX3, nf, [&] { return faces(3); }));
   RG_CUDA(issue(ctx, K_CT, n_ct_launches(d), [&] { return launch_ct(d, Pc, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s); }));
   if (d.iwvec == 2) {
     const size_t N = d.N;
@@ -499,6 +557,7 @@ int read_stats(rg_ctx* ctx, Run* R, rg_step_stats* st) {
   st->carry_overflow = (long long)c[C_CARRY_OVF];
   st->time = sc.timeh;
   st->dt = sc.dt;
+  if (c[C_TMAWAIT]) return fail(RG_ECUDA, "a TMA wait of the staged face kernel ran out");
   if (c[C_CARRY_OVF]) return fail(RG_EOVERFLOW, "W-carry list overflowed");
   if (c[C_CAP] || c[C_FLOORCAP]) return fail(RG_ENR_CAP, "a capped rescale loop was hit");
   return RG_OK;
@@ -735,6 +794,7 @@ int rg_ctx_create(int device, rg_ctx** out) {
   RG_CUDA(cudaSetDevice(device));
   rg_ctx* c = new rg_ctx();
   c->device = device;
+  if (const char* t = std::getenv("RAISHIN_FLUX_TMA")) c->tma = std::strcmp(t, "0") != 0;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;
@@ -947,8 +1007,9 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
   if (cudaMemsetAsync(R->fcnt, 0, C_NCOUNTERS * sizeof(unsigned long long), s) != cudaSuccess) return bail(RG_ECUDA);
   if ((rc = dalloc(R, &ptr, C_NCOUNTERS * sizeof(unsigned long long)))) return bail(rc);
   d.cnt = static_cast<unsigned long long*>(ptr);
-  if ((rc = dalloc(R, &ptr, kCarryCap * sizeof(int)))) return bail(rc);
+  if ((rc = dalloc(R, &ptr, 2 * (size_t)kCarryCap * sizeof(int)))) return bail(rc);
   d.carry_list = static_cast<int*>(ptr);
+  d.carry_sorted = d.carry_list + kCarryCap;
   d.strag_cap = straggler_cap(N);
   if ((rc = dalloc(R, &ptr, (size_t)d.strag_cap * sizeof(int)))) return bail(rc);
   d.strag_list = static_cast<int*>(ptr);
@@ -1011,6 +1072,7 @@ int rg_run_admit_prep(rg_ctx* ctx, rg_prep* prep, int* run_id) {
     }
   }
   if ((rc = set_time(ctx, R, 0.0))) return bail(rc);
+  make_tmaps(R);
   if (!prep->ic.empty()) {  // initial data computed with the preparation
     const std::vector<double> Ps = stored_from_full(d, prep->ic, R->nfull);
     if (cudaMemcpyAsync(R->b.P[0], Ps.data(), Ps.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)

@@ -9,6 +9,7 @@
 //             k_floor       infchk + atmosphere1a + pminmax2b (pointwise)
 // Per step:   k_step_begin, k_cfl (block min + atomicMin), k_dt, k_step_end.
 // All state is FP64 structure-of-arrays; a step never synchronises the host.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -806,36 +807,45 @@ __global__ void __launch_bounds__(128, RG_UPDATE_MINB) k_update(DevRun r, const 
                                                 const double* __restrict__ CT, int ilo, int ihi) { update_body<STAGE, MIX>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi, blockIdx); }
 
 // Resolve cells queued by k_update / k_recov in the reference's loop order
-// (k, j, i over the interior): each takes the final W of its predecessor cell.
-// One thread; runs only when cells were queued, which the reference data
-// rarely produces.  MODE 0: stage update; MODE 1: recov-only entry point.
+// (k, j, i over the interior): each takes the final W of its predecessor cell
+// (recov.f90:810-815).  Runs only when cells were queued.  The whole block
+// works on the run's list: the queued cells are ranked into loop order
+// (carry_sorted), and every maximal chain of consecutive queued cells is one
+// sequential task, given to one thread: its first cell takes the W of its
+// unqueued predecessor (recomputed, it has a root of its own), every later
+// cell the W its predecessor in the chain ends with.  That is the reference's
+// sequence of W values, so the result equals a serial sweep over the list;
+// chains proceed in parallel.  MODE 0: stage update; MODE 1: recov-only
+// entry point.  Every thread of the block calls it.
 template <int MODE, int STAGE, int IWVEC = 1>
 __device__ void carry_fix_body(const DevRun& r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                                double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                                const double* __restrict__ F3, const double* __restrict__ CT,
                                const double* __restrict__ U) {
-  if (MODE == 0) r.scal->strag_count = 0;  // the straggler pass of this stage has run
-  if (MODE == 0 && !r.scal->active) return;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const bool active = MODE != 0 || r.scal->active;
   int n = r.scal->carry_count;
-  if (n <= 0) return;
-  if (n > r.carry_cap) n = r.carry_cap;
-  int* L = r.carry_list;
-  for (int a = 1; a < n; ++a) {  // insertion sort: the list is short
-    const int x = L[a];
-    int b = a - 1;
-    while (b >= 0 && L[b] > x) { L[b + 1] = L[b]; --b; }
-    L[b + 1] = x;
+  __syncthreads();  // every thread has read the scalars before thread 0 resets them
+  if (MODE == 0 && tid == 0) r.scal->strag_count = 0;  // the straggler pass of this stage has run
+  if (!active || n <= 0) {
+    if (tid == 0 && n > 0) r.scal->carry_count = 0;
+    return;
   }
+  if (n > r.carry_cap) n = r.carry_cap;
+  const int* L = r.carry_list;
+  int* S = r.carry_sorted;
+  for (int a = tid; a < n; a += nt) {  // rank of each queued cell in loop order (indices are distinct)
+    const int x = L[a];
+    int rank = 0;
+    for (int b = 0; b < n; ++b) rank += (L[b] < x);
+    S[rank] = x;
+  }
+  __syncthreads();
   const int ni = r.imax - 2 * r.nm1, nj = r.jmax - 2 * r.nm1;
   const double dt = (MODE == 0) ? r.scal->dt : 0.0;
-  auto coords = [&](int lin, int& i, int& j, int& k) {
-    i = lin % ni + r.nm1 + 1;
-    j = (lin / ni) % nj + r.nm1 + 1;
-    k = lin / (ni * nj) + r.nm1 + 1;
-  };
   auto run_cell = [&](int lin, const double* carry, double& wg_out, bool write, RecovOut& o) -> bool {
-    int i, j, k;
-    coords(lin, i, j, k);
+    const int i = lin % ni + r.nm1 + 1, j = (lin / ni) % nj + r.nm1 + 1, k = lin / (ni * nj) + r.nm1 + 1;
     const size_t c = r.cell(i, j, k);
     Met m;
     load_met(r.mc, r.nik, r.ik(i, k), m);
@@ -852,35 +862,30 @@ __device__ void carry_fix_body(const DevRun& r, const double* __restrict__ Pn, c
     }
     return ok;
   };
-  int prev_lin = -2;
-  double prev_wg = 0.0;
-  for (int a = 0; a < n; ++a) {
-    const int lin = L[a];
+  for (int p = tid; p < n; p += nt) {
+    if (p > 0 && S[p - 1] == S[p] - 1) continue;  // inside a chain: its head's thread takes it
     double wg_in = 0.0;  // the first cell of the sweep starts from W = 0 (recov.f90:642)
-    if (lin > 0) {
-      if (prev_lin == lin - 1) {
-        wg_in = prev_wg;
-      } else {
-        RecovOut po{0.0, false, false, false};
-        double w = 0.0;
-        run_cell(lin - 1, nullptr, w, false, po);  // the predecessor has a root of its own
-        wg_in = w;
-      }
+    if (S[p] > 0) {
+      RecovOut po{0.0, false, false, false};
+      run_cell(S[p] - 1, nullptr, wg_in, false, po);  // the predecessor has a root of its own
     }
-    RecovOut o{0.0, false, false, false};
-    double w = 0.0;
-    run_cell(lin, &wg_in, w, true, o);
-    prev_lin = lin;
-    prev_wg = w;
-    atomicAdd(r.cnt + C_CARRY, 1ull);
-    if (o.nr2) atomicAdd(r.cnt + C_NR2, 1ull);
-    if (o.fail) atomicAdd(r.cnt + C_FAIL, 1ull);
-    if (o.cap) atomicAdd(r.cnt + C_CAP, 1ull);
+    for (int q = p; q < n && (q == p || S[q] == S[q - 1] + 1); ++q) {
+      RecovOut o{0.0, false, false, false};
+      double w = 0.0;
+      run_cell(S[q], &wg_in, w, true, o);
+      wg_in = w;
+      atomicAdd(r.cnt + C_CARRY, 1ull);
+      if (o.nr2) atomicAdd(r.cnt + C_NR2, 1ull);
+      if (o.fail) atomicAdd(r.cnt + C_FAIL, 1ull);
+      if (o.cap) atomicAdd(r.cnt + C_CAP, 1ull);
+    }
   }
-  r.scal->carry_count = 0;
+  __syncthreads();
+  if (tid == 0) r.scal->carry_count = 0;
 }
+constexpr int kCarryThreads = 128;
 template <int MODE, int STAGE, int IWVEC = 1>
-__global__ void k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
+__global__ void __launch_bounds__(kCarryThreads) k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                             double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                             const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
   if (threadIdx.x == 0 && blockIdx.x == 0) carry_fix_body<MODE, STAGE, IWVEC>(r, Pn, Pc, Pw, F1, F2, F3, CT, U);
@@ -914,13 +919,22 @@ __device__ __forceinline__ const float* met_of<2, float>(const DevRun& r) { retu
 template <>
 __device__ __forceinline__ const float* met_of<3, float>(const DevRun& r) { return r.mk32; }
 
-template <int D, int IREC, typename T, typename S>
+//
+// VIEW: the stencil (and the positivity fallback) is read from a staged copy
+// of the primitives instead of P: variable v of the lane's cell at
+// Vp[v * Vn + Vc], neighbours along D Vst apart (the shared-memory box of
+// k_flux_tma).  Stores, metric and coordinates stay global.
+template <int D, int IREC, typename T, typename S, bool VIEW = false>
 __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__ P, S* __restrict__ F,
                                           float* __restrict__ Fcopy, int icopy, int i, int j, int k, int side,
-                                          bool valid) {
+                                          bool valid, const S* Vp = nullptr, size_t Vn = 0, size_t Vc = 0,
+                                          long long Vst = 0) {
   const unsigned mask = __activemask();
   const size_t N = r.N, c = r.cell(i, j, k);
   const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.sj : (long long)r.sk);
+  const S* Pv = VIEW ? Vp : P;
+  const size_t Nv = VIEW ? Vn : N, cv = VIEW ? Vc : c;
+  const long long sv = VIEW ? Vst : st;
   T q[9];
   if (IREC == 5) {
     const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;  // owner cell of this lane's state
@@ -931,8 +945,8 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     for (int o = -2; o <= 2; ++o) dx[o + 4] = T(__ldg(dxs + f - 1 + o));
 #pragma unroll
     for (int o = -1; o <= 1; ++o) xx[o + 4] = T(__ldg(xs + f - 1 + o));
-    if (side == 0) ppm_cell<D>(P + c, N, st, dx, xx, T(r.gam), other, q);  // uriil(f)
-    else ppm_cell<D>(P + c + st, N, st, dx, xx, T(r.gam), q, other);       // uriir(f)
+    if (side == 0) ppm_cell<D>(Pv + cv, Nv, sv, dx, xx, T(r.gam), other, q);  // uriil(f)
+    else ppm_cell<D>(Pv + cv + sv, Nv, sv, dx, xx, T(r.gam), q, other);       // uriir(f)
   } else if (IREC == 1 || IREC == 2 || IREC == 11 || IREC == 12 || IREC == 13) {
     // owner cell f of this lane's state and its coordinate's coefficients
     const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;
@@ -947,12 +961,12 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
       if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
-      const S* p = P + (size_t)v * N + c + side * st;
+      const S* p = Pv + (size_t)v * Nv + cv + side * sv;
       const T u0 = T(p[0]);
       T tmp_b = T(0);
       if (cross) tmp_b = ((T(p[1]) - u0) * hpi < T(0)) ? T(-1) : T(1);
-      else if (IREC == 13) tmp_b = ((T(p[st]) - u0) * co[0] < T(0)) ? T(-1) : T(1);
-      q[v] = limiter_state<IREC>(T(p[-st]), u0, T(p[st]), co, side, tmp_b);
+      else if (IREC == 13) tmp_b = ((T(p[sv]) - u0) * co[0] < T(0)) ? T(-1) : T(1);
+      q[v] = limiter_state<IREC>(T(p[-sv]), u0, T(p[sv]), co, side, tmp_b);
     }
   } else if (IREC == 4) {
     const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;
@@ -964,23 +978,23 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
       if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
-      const S* p = P + (size_t)v * N + c + side * st;
-      q[v] = ceno_state(T(p[-2 * st]), T(p[-st]), T(p[0]), T(p[st]), T(p[2 * st]), co, side, D == 3 && side == 0);
+      const S* p = Pv + (size_t)v * Nv + cv + side * sv;
+      q[v] = ceno_state(T(p[-2 * sv]), T(p[-sv]), T(p[0]), T(p[sv]), T(p[2 * sv]), co, side, D == 3 && side == 0);
     }
   } else if (IREC == 3) {
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
       if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
-      const S* p = P + (size_t)v * N + c + side * st;
-      q[v] = muscl_state(T(p[-st]), T(p[0]), T(p[st]), side);
+      const S* p = Pv + (size_t)v * Nv + cv + side * sv;
+      q[v] = muscl_state(T(p[-sv]), T(p[0]), T(p[sv]), side);
     }
   } else {
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
       if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       // owner cell f + side; the right state reads its stencil mirrored
-      const long long sd = side ? -st : st;
-      const S* p = P + (size_t)v * N + c + side * st;
+      const long long sd = side ? -sv : sv;
+      const S* p = Pv + (size_t)v * Nv + cv + side * sv;
       const T a2 = T(p[-2 * sd]), a1 = T(p[-sd]), u0 = T(p[0]), b1 = T(p[sd]), b2 = T(p[2 * sd]);
       if (IREC == 6) q[v] = mp5_state(a2, a1, u0, b1, b2, side ? T(-1) : T(1));
       else if (IREC == 8) {
@@ -1002,7 +1016,7 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
   }
   if ((r.guard & 1) && !(q[0] > T(0) && q[4] > T(0))) {
 #pragma unroll
-    for (int v = 0; v < 9; ++v) q[v] = T(P[(size_t)v * N + c + side * st]);
+    for (int v = 0; v < 9; ++v) q[v] = T(Pv[(size_t)v * Nv + cv + side * sv]);
   }
   MetT<T> m;
   load_met(met_of<D, S>(r), r.nik, r.ik(i, k), m);
@@ -1070,6 +1084,78 @@ __device__ __forceinline__ void flux_body(const DevRun& r, const S* __restrict__
 template <int D, int IREC, typename T, typename S>
 __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_flux(DevRun r, const S* __restrict__ P, S* __restrict__ F,
                                               float* __restrict__ Fcopy, int icopy, int ilo, int ihi) { flux_body<D, IREC, T, S>(r, P, F, Fcopy, icopy, ilo, ihi, blockIdx); }
+
+// The FP64 MP5 face kernel with its stencil staged in shared memory by one
+// TMA tile load per block (cp.async.bulk.tensor, this GPU's own buffer, no
+// multicast).  A block takes the same 32 x 2 faces as k_flux (32 along i, two
+// rows along j, one k); the tensor map views the primitives as the 4D array
+// (i, j, k, v) and the box covers the block's stencil for all nine variables:
+// 40 x 2 x 1 cells for r faces (i-2 .. i+3 of 32 faces), 34 x 7 x 1 for phi
+// faces (two rows, j-2 .. j+3 each), 34 x 2 x 6 for theta faces.  Cells past
+// the array read as zeros (the TMA's out-of-bounds fill); only lanes working
+// on a clamped face could reach them, and those store nothing.  The wait on
+// the transaction barrier is bounded: if the copy has not landed after
+// kTmaWaitCap polls the block counts C_TMAWAIT, waits once more (bounded) for
+// the copy and returns without computing; the host reports RG_ECUDA.
+constexpr int kTmaWaitCap = 1 << 22;
+template <int D>
+struct TmaBox {
+  static constexpr int X = (D == 1) ? 40 : 34, Y = (D == 2) ? 7 : 2, Z = (D == 3) ? 6 : 1;
+  static constexpr int PLANE = X * Y * Z;                      // cells per variable
+  static constexpr unsigned BYTES = (unsigned)PLANE * 9u * 8u;  // whole box
+};
+
+__device__ __forceinline__ bool tma_wait(unsigned bar) {
+  unsigned done = 0;
+  for (int it = 0; it < kTmaWaitCap && !done; ++it)
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(0)
+        : "memory");
+  return done != 0;
+}
+
+template <int D>
+__global__ void __launch_bounds__(128, RG_FLUX_MINB64)
+    k_flux_tma(const __grid_constant__ CUtensorMap tm, DevRun r, double* __restrict__ F, int ilo, int ihi) {
+  extern __shared__ __align__(128) double box[];
+  __shared__ __align__(8) unsigned long long bar;
+  if (!r.scal->active) return;
+  using B = TmaBox<D>;
+  const int nm0 = r.nm0;
+  const int fi0 = ilo + (int)blockIdx.x * 32, fj0 = nm0 + 2 * (int)blockIdx.y, fk0 = nm0 + (int)blockIdx.z;
+  // 0-based origin of the box: the first stencil cell along D, the block's first face elsewhere
+  const int x0 = (D == 1) ? fi0 - 3 : fi0 - 1;
+  const int y0 = (D == 2) ? fj0 - 3 : fj0 - 1;
+  const int z0 = (D == 3) ? fk0 - 3 : fk0 - 1;
+  const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
+  const unsigned box_a = (unsigned)__cvta_generic_to_shared(box);
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(B::BYTES) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(box_a),
+        "l"(reinterpret_cast<unsigned long long>(&tm)), "r"(x0), "r"(y0), "r"(z0), "r"(0), "r"(bar_a)
+        : "memory");
+  }
+  __syncthreads();
+  if (!tma_wait(bar_a)) {
+    if (tid == 0) atomicAdd(r.cnt + C_TMAWAIT, 1ull);
+    tma_wait(bar_a);  // the copy in flight writes this block's shared memory: give it one more bounded wait
+    return;
+  }
+  const int side = threadIdx.x & 1;
+  const int i0 = fi0 + (int)(threadIdx.x >> 1), j0 = fj0 + (int)threadIdx.y;
+  const bool valid = i0 <= ihi && j0 <= r.jmax - nm0 && fk0 <= r.kmax - nm0;
+  const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(fk0, r.kmax - nm0);
+  const size_t vc = (size_t)((i - 1 - x0) + B::X * ((j - 1 - y0) + B::Y * (k - 1 - z0)));
+  const long long vst = (D == 1) ? 1 : (D == 2 ? B::X : B::X * B::Y);
+  face_lane<D, 6, double, double, true>(r, nullptr, F, nullptr, 0, i, j, k, side, valid, box, B::PLANE, vc, vst);
+}
 
 // ---------------------------------------------------------------- flux-CT
 // ct.f90:30-118 (flux-CT, ict 1), ct.f90:121-233 (mflct, ict 2),
@@ -1958,6 +2044,30 @@ static int fp64_split(const DevRun& r, int lo, int hi) {
   return r.i_fp64 < lo ? lo - 1 : (r.i_fp64 > hi ? hi : r.i_fp64);
 }
 
+bool flux_tma_eligible(const DevRun& r) {
+  return !r.mixed && r.irec == 6 && r.nm0 == 3 && !r.jfix && !r.kfix && !r.kmet && (r.imax % 2) == 0 &&
+         r.N == (size_t)r.imax * r.jmax * r.kmax;
+}
+
+cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap, double* F, cudaStream_t s) {
+  const int lo = r.nm0, hi = r.imax - r.nm0;
+  const int n = hi - lo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
+  const dim3 b(64, 2, 1);
+  const dim3 g((unsigned)((n + 31) / 32), (unsigned)((m + 1) / 2), (unsigned)l);
+  const CUtensorMap& tm = *static_cast<const CUtensorMap*>(tmap);
+  if (dir == 1) k_flux_tma<1><<<g, b, TmaBox<1>::BYTES, s>>>(tm, r, F, lo, hi);
+  else if (dir == 2) k_flux_tma<2><<<g, b, TmaBox<2>::BYTES, s>>>(tm, r, F, lo, hi);
+  else k_flux_tma<3><<<g, b, TmaBox<3>::BYTES, s>>>(tm, r, F, lo, hi);
+  return cudaGetLastError();
+}
+
+void flux_tma_box(int dir, unsigned box[4]) {
+  box[0] = dir == 1 ? TmaBox<1>::X : (dir == 2 ? TmaBox<2>::X : TmaBox<3>::X);
+  box[1] = dir == 1 ? TmaBox<1>::Y : (dir == 2 ? TmaBox<2>::Y : TmaBox<3>::Y);
+  box[2] = dir == 1 ? TmaBox<1>::Z : (dir == 2 ? TmaBox<2>::Z : TmaBox<3>::Z);
+  box[3] = 9;
+}
+
 cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s) {
   const int lo = r.nm0, hi = r.imax - r.nm0;
   if (!r.mixed) {
@@ -2037,9 +2147,9 @@ cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const do
     else if (stage == 2) k_straggler<2><<<gs, 128, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
     else k_straggler<3><<<gs, 128, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT);
   }
-  if (stage == 1) k_carry_fix<0, 1><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  else if (stage == 2) k_carry_fix<0, 2><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
-  else k_carry_fix<0, 3><<<1, 1, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  if (stage == 1) k_carry_fix<0, 1><<<1, kCarryThreads, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  else if (stage == 2) k_carry_fix<0, 2><<<1, kCarryThreads, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
+  else k_carry_fix<0, 3><<<1, kCarryThreads, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, nullptr);
   return cudaGetLastError();
 }
 
@@ -2135,10 +2245,10 @@ cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Po
   const dim3 b = sblock(r, dim3(64, 2, 1));
   if (r.iwvec == 2) {
     k_recov<2><<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
-    k_carry_fix<1, 1, 2><<<1, 1, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
+    k_carry_fix<1, 1, 2><<<1, kCarryThreads, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
   } else {
     k_recov<1><<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, U, Pold, Pw);
-    k_carry_fix<1, 1><<<1, 1, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
+    k_carry_fix<1, 1><<<1, kCarryThreads, 0, s>>>(r, nullptr, Pold, Pw, nullptr, nullptr, nullptr, nullptr, U);
   }
   return cudaGetLastError();
 }
@@ -2179,7 +2289,7 @@ cudaError_t launch_stage_recov2(const DevRun& r, int stage, const double* Pc, do
   else if (stage == 2) k_rkt<2><<<g, b, 0, s>>>(r, F1, F2, F3, r.Un, Ucur, SF, Unew, 0.0, true);
   else k_rkt<3><<<g, b, 0, s>>>(r, F1, F2, F3, r.Un, Ucur, SF, Unew, 0.0, true);
   k_recov<2><<<g, b, 0, s>>>(r, Unew, Pc, Pw);
-  k_carry_fix<1, 1, 2><<<1, 1, 0, s>>>(r, nullptr, Pc, Pw, nullptr, nullptr, nullptr, nullptr, Unew);
+  k_carry_fix<1, 1, 2><<<1, kCarryThreads, 0, s>>>(r, nullptr, Pc, Pw, nullptr, nullptr, nullptr, nullptr, Unew);
   return cudaGetLastError();
 }
 

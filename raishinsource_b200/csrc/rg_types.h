@@ -40,7 +40,9 @@ struct Scal {
 
 // Counters (device, atomically accumulated).
 enum Counter {
-  C_STEPS = 0, C_RECOV, C_NR2, C_FAIL, C_CARRY, C_CAP, C_FLOORCAP, C_CARRY_OVF, C_NCOUNTERS
+  C_STEPS = 0, C_RECOV, C_NR2, C_FAIL, C_CARRY, C_CAP, C_FLOORCAP, C_CARRY_OVF,
+  C_TMAWAIT,  // blocks whose TMA wait ran out (k_flux_tma); never expected
+  C_NCOUNTERS
 };
 
 // Everything a kernel needs, by value.  Arrays are structure-of-arrays with
@@ -107,6 +109,7 @@ struct DevRun {
   Scal* scal;
   unsigned long long* cnt;
   int* carry_list;       // interior cells queued for the W carry fix-up
+  int* carry_sorted;     // the same cells in loop order (carry_cap entries of scratch)
   int carry_cap;
   int* strag_list;       // interior cells whose Newton-Raphson passed kDeferIter iterations
   int strag_cap;
