@@ -63,10 +63,11 @@ BYTES_PER_UNIT = {"flux_r": 136, "flux_phi": 136, "flux_theta": 136, "update": 4
 # its units) on the 192x96x96 torus, whose state already exceeds the L2
 DRAM_BYTES_PER_UNIT = {"update": 469.0, "flux_r": 113.0, "flux_phi": 120.0, "flux_theta": 122.0}
 BYTES_PER_UNIT["flux"] = 136
-DRAM_BYTES_PER_UNIT["flux"] = (113.0 + 120.0 + 122.0) / 3
+# the TMA-staged face kernels (k_flux_tma) of the FP64 MP5 path, ncu on the 192x96x96 torus
+DRAM_BYTES_PER_UNIT["flux"] = (122.0 + 131.0 + 133.0) / 3
 # FP64 pipe utilisation of the face kernels from ncu (sm__inst_executed_pipe_fp64, percent of the peak
 # sustained rate while active), mean over the three directions on the 192x96x96 torus
-FP64_PIPE_FRAC = {"flux": 0.425, "update": 0.24}
+FP64_PIPE_FRAC = {"flux": 0.474, "update": 0.237}
 # algorithmic HBM bytes of one zone-update (FP64): only primitives persist between stages
 STEP_BYTES_PER_ZONE = 648
 # Executed FP64 operations per zone-update of one full RK3 step (MP5, FP64): ncu
@@ -310,7 +311,8 @@ def run_gpu(args) -> dict | None:
                     "unit": "GB/s", "frac": achieved / peak,
                     "traffic": None if traffic is None else traffic * u,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on the "
-                                      "192x96x96 torus, scaled by the units of one launch",
+                                      "192x96x96 torus, scaled by the units of one launch "
+                                      "(profiles/k_flux_tma_vs_k_flux_fm_torus_3d_192x96x96_mp5.md)",
                     "bytes_per_unit": BYTES_PER_UNIT[top], "units_per_launch": u, "ms_per_launch": per_launch_ms,
                     "share_of_step": round(kinds[top]["ms"] / total, 4),
                     "fp64_pipe_frac": FP64_PIPE_FRAC.get(top),
