@@ -513,9 +513,16 @@ def section_mixed(ctx, args) -> dict:
         ms = e0.elapsed_time(e1)
         st = r.stats()
         states[prec] = (r.prims(), r.horizon_flux(), st, r.radial_flux(shell))
+        # per-kind device time of 3 more steps (CUDA events around every launch)
+        ctx.profile(True)
+        r.step(3)
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        kinds_ms = {k: round(v["ms"] / 3, 4) for k, v in prof.items() if v["ms"] > 0}
         out[prec] = {"value": zones * (args.mixed_steps - 3) / (ms * 1e-3), "unit": "zone-updates/s",
                      "ms_per_step": ms / (args.mixed_steps - 3), "time": st["time"],
-                     "recov_nr2": st["recov_nr2"], "recov_fail": st["recov_fail"]}
+                     "recov_nr2": st["recov_nr2"], "recov_fail": st["recov_fail"],
+                     "kernel_ms_per_step": kinds_ms}
         r.release()
     (a, (ma, ea), _, (sma, sea)), (b, (mb, eb), _, (smb, seb)) = states["mixed"], states["fp64"]
     l1, linf = _rel_errs(a, b, config.ghost_widths(p["irec"], p.get("ict", 1))[1])

@@ -61,6 +61,7 @@ struct Run {
   // TMA tensor maps of the primitive buffers b.P[buffer] for the staged face
   // kernel, per direction (flux_tma_box); tma is set when all nine exist
   CUtensorMap tmap[3][3];
+  CUtensorMap tmap32[3];   // the FP32 copy P32 of a mixed run, per direction
   bool tma = false;
 };
 
@@ -146,9 +147,9 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Tensor maps of the three primitive buffers as 4D FP64 arrays (i, j, k, v)
-// with the boxes of the staged face kernel; a run they do not fit keeps the
-// generic face kernel.
+// Tensor maps of the three primitive buffers (and of P32 for a mixed run) as
+// 4D arrays (i, j, k, v) with the boxes of the staged face kernel; a run they
+// do not fit keeps the generic face kernel.
 void make_tmaps(Run* R) {
   R->tma = false;
   const DevRun& d = R->d;
@@ -156,18 +157,21 @@ void make_tmaps(Run* R) {
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return;
   const cuuint64_t dims[4] = {(cuuint64_t)d.imax, (cuuint64_t)d.jmax, (cuuint64_t)d.kmax, 9};
-  const cuuint64_t strides[3] = {(cuuint64_t)d.imax * 8, (cuuint64_t)d.imax * d.jmax * 8, (cuuint64_t)d.N * 8};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  for (int b = 0; b < 3; ++b)
-    for (int dir = 1; dir <= 3; ++dir) {
-      unsigned box[4];
-      flux_tma_box(dir, box);
-      const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
-      if (enc(&R->tmap[b][dir - 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, R->b.P[b], dims, strides, bx, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return;
-    }
+  auto encode = [&](CUtensorMap* tm, void* base, int eb, int dir) {
+    const cuuint64_t strides[3] = {(cuuint64_t)d.imax * eb, (cuuint64_t)d.imax * d.jmax * eb, (cuuint64_t)d.N * eb};
+    unsigned box[4];
+    flux_tma_box(dir, eb, box);
+    const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+    return enc(tm, eb == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims,
+               strides, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  for (int dir = 1; dir <= 3; ++dir) {
+    for (int b = 0; b < 3; ++b)
+      if (!encode(&R->tmap[b][dir - 1], R->b.P[b], 8, dir)) return;
+    if (d.mixed && !encode(&R->tmap32[dir - 1], d.P32, 4, dir)) return;
+  }
   R->tma = true;
 }
 
@@ -517,7 +521,7 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
   const int bi = (Pc == R->b.P[0]) ? 0 : (Pc == R->b.P[1] ? 1 : 2);
   const bool tma = R->tma && ctx->tma && Pc == R->b.P[bi];
   auto faces = [&](int dir) {
-    return tma ? launch_flux_tma(d, dir, &R->tmap[bi][dir - 1], R->b.F[dir - 1], s)
+    return tma ? launch_flux_tma(d, dir, &R->tmap[bi][dir - 1], &R->tmap32[dir - 1], R->b.F[dir - 1], s)
                : launch_flux(d, dir, Pc, R->b.F[dir - 1], s);
   };
   RG_CUDA(issue(ctx, K_FLUX1, nf, [&] { return faces(1); }));

@@ -1085,24 +1085,30 @@ template <int D, int IREC, typename T, typename S>
 __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_flux(DevRun r, const S* __restrict__ P, S* __restrict__ F,
                                               float* __restrict__ Fcopy, int icopy, int ilo, int ihi) { flux_body<D, IREC, T, S>(r, P, F, Fcopy, icopy, ilo, ihi, blockIdx); }
 
-// The FP64 MP5 face kernel with its stencil staged in shared memory by one
-// TMA tile load per block (cp.async.bulk.tensor, this GPU's own buffer, no
-// multicast).  A block takes the same 32 x 2 faces as k_flux (32 along i, two
-// rows along j, one k); the tensor map views the primitives as the 4D array
-// (i, j, k, v) and the box covers the block's stencil for all nine variables:
-// 40 x 2 x 1 cells for r faces (i-2 .. i+3 of 32 faces), 34 x 7 x 1 for phi
-// faces (two rows, j-2 .. j+3 each), 34 x 2 x 6 for theta faces.  Cells past
-// the array read as zeros (the TMA's out-of-bounds fill); only lanes working
-// on a clamped face could reach them, and those store nothing.  The wait on
-// the transaction barrier is bounded: if the copy has not landed after
-// kTmaWaitCap polls the block counts C_TMAWAIT, waits once more (bounded) for
-// the copy and returns without computing; the host reports RG_ECUDA.
+// The MP5 face kernel with its stencil staged in shared memory by one TMA
+// tile load per block (cp.async.bulk.tensor, this GPU's own buffer, no
+// multicast), in FP64 (S = double) or for the FP32 half of the mixed path
+// (S = float, over P32).  A block takes the same 32 x 2 faces as k_flux (32
+// along i, two rows along j, one k); the tensor map views the primitives as
+// the 4D array (i, j, k, v) and the box covers the block's stencil for all
+// nine variables: 40 x 2 x 1 cells for r faces (i-2 .. i+3 of 32 faces), X x
+// 7 x 1 for phi faces (two rows, j-2 .. j+3 each), X x 2 x 6 for theta faces,
+// with X = 34 (FP64) or 36 (FP32).  The box starts on a 16-byte boundary
+// along i (the TMA's rule): its origin is rounded down to an even (FP64) or
+// a multiple-of-four (FP32) index and the view offsets the lanes by the
+// remainder.  Cells past the array read as zeros (the TMA's out-of-bounds
+// fill); only lanes working on a clamped face could reach them, and those
+// store nothing.  The wait on the transaction barrier is bounded: if the copy
+// has not landed after kTmaWaitCap polls the block counts C_TMAWAIT, waits
+// once more (bounded) for the copy and returns without computing; the host
+// reports RG_ECUDA.
 constexpr int kTmaWaitCap = 1 << 22;
-template <int D>
+template <int D, typename S>
 struct TmaBox {
-  static constexpr int X = (D == 1) ? 40 : 34, Y = (D == 2) ? 7 : 2, Z = (D == 3) ? 6 : 1;
-  static constexpr int PLANE = X * Y * Z;                      // cells per variable
-  static constexpr unsigned BYTES = (unsigned)PLANE * 9u * 8u;  // whole box
+  static constexpr int X = (D == 1) ? 40 : (sizeof(S) == 8 ? 34 : 36), Y = (D == 2) ? 7 : 2, Z = (D == 3) ? 6 : 1;
+  static constexpr int PLANE = X * Y * Z;                                   // cells per variable
+  static constexpr unsigned BYTES = (unsigned)PLANE * 9u * (unsigned)sizeof(S);  // whole box
+  static constexpr int ALIGN = 16 / (int)sizeof(S);                         // elements per 16 bytes
 };
 
 __device__ __forceinline__ bool tma_wait(unsigned bar) {
@@ -1116,21 +1122,24 @@ __device__ __forceinline__ bool tma_wait(unsigned bar) {
   return done != 0;
 }
 
-template <int D>
-__global__ void __launch_bounds__(128, RG_FLUX_MINB64)
-    k_flux_tma(const __grid_constant__ CUtensorMap tm, DevRun r, double* __restrict__ F, int ilo, int ihi) {
-  extern __shared__ __align__(128) double box[];
+template <int D, typename T, typename S>
+__global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
+    k_flux_tma(const __grid_constant__ CUtensorMap tm, DevRun r, S* __restrict__ F, float* __restrict__ Fcopy,
+               int icopy, int ilo, int ihi) {
+  extern __shared__ __align__(128) unsigned char box_raw[];
   __shared__ __align__(8) unsigned long long bar;
   if (!r.scal->active) return;
-  using B = TmaBox<D>;
+  using B = TmaBox<D, S>;
+  S* box = reinterpret_cast<S*>(box_raw);
   const int nm0 = r.nm0;
   const int fi0 = ilo + (int)blockIdx.x * 32, fj0 = nm0 + 2 * (int)blockIdx.y, fk0 = nm0 + (int)blockIdx.z;
-  // 0-based origin of the box: the first stencil cell along D, the block's first face elsewhere
-  const int x0 = (D == 1) ? fi0 - 3 : fi0 - 1;
+  // 0-based origin of the box: the first stencil cell along D, the block's
+  // first face elsewhere; along i rounded down to a 16-byte boundary
+  const int x0 = ((D == 1) ? fi0 - 3 : fi0 - 1) & ~(B::ALIGN - 1);
   const int y0 = (D == 2) ? fj0 - 3 : fj0 - 1;
   const int z0 = (D == 3) ? fk0 - 3 : fk0 - 1;
   const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
-  const unsigned box_a = (unsigned)__cvta_generic_to_shared(box);
+  const unsigned box_a = (unsigned)__cvta_generic_to_shared(box_raw);
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
@@ -1154,7 +1163,7 @@ __global__ void __launch_bounds__(128, RG_FLUX_MINB64)
   const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(fk0, r.kmax - nm0);
   const size_t vc = (size_t)((i - 1 - x0) + B::X * ((j - 1 - y0) + B::Y * (k - 1 - z0)));
   const long long vst = (D == 1) ? 1 : (D == 2 ? B::X : B::X * B::Y);
-  face_lane<D, 6, double, double, true>(r, nullptr, F, nullptr, 0, i, j, k, side, valid, box, B::PLANE, vc, vst);
+  face_lane<D, 6, T, S, true>(r, nullptr, F, Fcopy, icopy, i, j, k, side, valid, box, B::PLANE, vc, vst);
 }
 
 // ---------------------------------------------------------------- flux-CT
@@ -2045,26 +2054,47 @@ static int fp64_split(const DevRun& r, int lo, int hi) {
 }
 
 bool flux_tma_eligible(const DevRun& r) {
-  return !r.mixed && r.irec == 6 && r.nm0 == 3 && !r.jfix && !r.kfix && !r.kmet && (r.imax % 2) == 0 &&
+  return r.irec == 6 && r.nm0 == 3 && !r.jfix && !r.kfix && !r.kmet && (r.imax % 4) == 0 &&
          r.N == (size_t)r.imax * r.jmax * r.kmax;
 }
 
-cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap, double* F, cudaStream_t s) {
-  const int lo = r.nm0, hi = r.imax - r.nm0;
-  const int n = hi - lo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
+template <typename T, typename S>
+static void launch_flux_tma_t(const DevRun& r, int dir, const CUtensorMap& tm, S* F, float* Fcopy, int icopy,
+                              int ilo, int ihi, cudaStream_t s) {
+  if (ihi < ilo) return;
+  const int n = ihi - ilo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b(64, 2, 1);
   const dim3 g((unsigned)((n + 31) / 32), (unsigned)((m + 1) / 2), (unsigned)l);
-  const CUtensorMap& tm = *static_cast<const CUtensorMap*>(tmap);
-  if (dir == 1) k_flux_tma<1><<<g, b, TmaBox<1>::BYTES, s>>>(tm, r, F, lo, hi);
-  else if (dir == 2) k_flux_tma<2><<<g, b, TmaBox<2>::BYTES, s>>>(tm, r, F, lo, hi);
-  else k_flux_tma<3><<<g, b, TmaBox<3>::BYTES, s>>>(tm, r, F, lo, hi);
+  if (dir == 1) k_flux_tma<1, T, S><<<g, b, TmaBox<1, S>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+  else if (dir == 2) k_flux_tma<2, T, S><<<g, b, TmaBox<2, S>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+  else k_flux_tma<3, T, S><<<g, b, TmaBox<3, S>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+}
+
+cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const void* tmap32, double* F,
+                            cudaStream_t s) {
+  const int lo = r.nm0, hi = r.imax - r.nm0;
+  const CUtensorMap& t64 = *static_cast<const CUtensorMap*>(tmap64);
+  if (!r.mixed) {
+    launch_flux_tma_t<double, double>(r, dir, t64, F, nullptr, 0, lo, hi, s);
+  } else {
+    // as launch_flux: FP64 faces up to i_fp64 + 1, copied to FP32 up to i_fp64; FP32 faces beyond
+    const int split = fp64_split(r, lo, hi);
+    if (split >= lo)
+      launch_flux_tma_t<double, double>(r, dir, t64, F, r.F32[dir - 1], split, lo, split < hi ? split + 1 : hi, s);
+    launch_flux_tma_t<float, float>(r, dir, *static_cast<const CUtensorMap*>(tmap32), r.F32[dir - 1], nullptr, 0,
+                                    split + 1, hi, s);
+  }
   return cudaGetLastError();
 }
 
-void flux_tma_box(int dir, unsigned box[4]) {
-  box[0] = dir == 1 ? TmaBox<1>::X : (dir == 2 ? TmaBox<2>::X : TmaBox<3>::X);
-  box[1] = dir == 1 ? TmaBox<1>::Y : (dir == 2 ? TmaBox<2>::Y : TmaBox<3>::Y);
-  box[2] = dir == 1 ? TmaBox<1>::Z : (dir == 2 ? TmaBox<2>::Z : TmaBox<3>::Z);
+void flux_tma_box(int dir, int elem_bytes, unsigned box[4]) {
+  if (elem_bytes == 8) {
+    box[0] = dir == 1 ? TmaBox<1, double>::X : (dir == 2 ? TmaBox<2, double>::X : TmaBox<3, double>::X);
+  } else {
+    box[0] = dir == 1 ? TmaBox<1, float>::X : (dir == 2 ? TmaBox<2, float>::X : TmaBox<3, float>::X);
+  }
+  box[1] = dir == 2 ? 7 : 2;
+  box[2] = dir == 3 ? 6 : 1;
   box[3] = 9;
 }
 
