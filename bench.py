@@ -576,7 +576,7 @@ def section_tubes(ctx, args) -> dict:
            "timed_steps": "to t = tmax" if args.tube_steps <= 0 else args.tube_steps,
            "note": ("zone-updates/s counts interior cells of active tubes; latencies are the wall time at which a "
                     "tube passed tmax, null unless all tubes finished in the timed steps")}
-    finals = {}
+    finals, fails = {}, {}
     for prec in ("fp64", "mixed"):
         runs = []
         for t, n in enumerate(lengths):
@@ -617,12 +617,19 @@ def section_tubes(ctx, args) -> dict:
                      "recov_nr2": int(sum(x["recov_nr2"] for x in st)),
                      "unfinished_tubes": len(runs) - len(done_at)}
         finals[prec] = [r.stored_prims()[0, 0, 0, :] for r in runs]  # rho along the tube
+        fails[prec] = [x["recov_fail"] + x["recov_cap"] for x in st]
         for r in runs:
             r.release()
     fin = [np.isfinite(a).all() and np.isfinite(b).all() for a, b in zip(finals["mixed"], finals["fp64"])]
     num = sum(np.abs(a - b).sum() for a, b, f in zip(finals["mixed"], finals["fp64"], fin) if f)
     den = sum(np.abs(b).sum() for b, f in zip(finals["fp64"], fin) if f)
     out["l1_rel_rho_mixed_vs_fp64"] = float(num / den) if den > 0 else None
+    # tubes whose recovery never failed nor capped in either precision
+    ok = [f and a == 0 and b == 0 for f, a, b in zip(fin, fails["fp64"], fails["mixed"])]
+    num = sum(np.abs(a - b).sum() for a, b, f in zip(finals["mixed"], finals["fp64"], ok) if f)
+    den = sum(np.abs(b).sum() for b, f in zip(finals["fp64"], ok) if f)
+    out["l1_rel_rho_mixed_vs_fp64_no_failed_recovery"] = {"tubes": int(sum(ok)),
+                                                          "value": float(num / den) if den > 0 else None}
     out["nonfinite_tubes"] = int(len(fin) - sum(fin))
     return out
 

@@ -91,6 +91,19 @@ print(json.dumps(res))
 """
 
 
+HEADLINE = PRELUDE + r"""
+set_pow_mode("rg")
+p = dict(config.torus(nr=256, nth=128, nph=128), guard=1)
+o = Oracle(p); o.ic_torus(seed=2012); o.init_cons()
+with Context(0) as ctx:
+    r = ctx.admit(p); r.upload_prims(o.prims())
+    o.step(1); r.step(1)
+    a, b = r.prims(), o.prims(); r.release()
+res = {"headline": compare(a, b)}
+res["libs"] = libs()
+print(json.dumps(res))
+"""
+
 TUBES = PRELUDE + r"""
 res = {}
 set_pow_mode("rg")
@@ -164,3 +177,11 @@ def test_exact_build_failing_tubes_match_oracle():
         assert r["equal"] and r["same_nonfinite"], (case, r)
         assert not r["finite_orc"], (case, r)  # these tubes do go non-finite
         assert r["dev"] == r["orc"], (case, r)
+
+
+def test_exact_build_bit_exact_on_the_headline_grid():
+    """One step of the benchmark's 256x128x128 torus (3.57 M interior cells,
+    MP5, guard 1): the exact build equals the oracle in every bit of every
+    cell."""
+    res = run_child(HEADLINE)
+    assert res["headline"]["equal"], res

@@ -276,6 +276,17 @@ def test_step_3d_mp5(gpu_ctx):
     assert errs.max() < TOL, errs
 
 
+def test_step_benchmark_grids(gpu_ctx):
+    """One step on the benchmark's own grids, MP5 with the positivity
+    fallback: the 3D torus 256x128x128 (the headline, 3.57 M interior cells)
+    and the 2D torus 256x256 (phi slab), within 1e-12 of each field's
+    maximum."""
+    for p in (dict(config.torus(nr=256, nth=128, nph=128), guard=1), dict(config.torus(nr=256, nth=256), guard=1)):
+        errs, st = _step_err(gpu_ctx, p, 1, seed=2012)
+        assert errs.max() < TOL, (p["imax"], p["jmax"], p["kmax"], errs)
+        assert st["steps"] == 1
+
+
 def test_step_3d_weno5(gpu_ctx):
     p = dict(config.torus(nr=40, nth=24, nph=16, irec=config.IREC_WENO5), guard=1)
     errs, _ = _step_err(gpu_ctx, p, 2, seed=78)
