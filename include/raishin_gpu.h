@@ -201,13 +201,37 @@ int rg_batch_info(rg_ctx* ctx, const int* runs, int nruns, int* width, int* grid
 int rg_profile(rg_ctx* ctx, int enable);
 int rg_profile_read(rg_ctx* ctx, double* ms, long long* launches, int nkinds);
 
-/* Reference-interface entry points (host arrays in the reference layout);
- * each runs the named routine(s) on the GPU for per-routine parity. */
+/* Reference-interface entry points (arrays in the reference layout); each
+ * runs the named routine(s) on the GPU for per-routine parity and swap-in.
+ * Their arrays may be host memory or device memory (unified addressing: the
+ * library copies with cudaMemcpyDefault), so a driver that keeps its arrays
+ * on the device passes device pointers; scalar outputs (rg_cdtcfl's dtcfl)
+ * are host memory. */
 /* caluu1 (caluu.f90:2-126) */
 int rg_caluu1(rg_ctx* ctx, int run, const double* uri, double* uu);
 /* rec2 + calcha + hll + ct (rec.f90:2-142, calflx.f90:391-795, calcha.f90:2-126,
  * hll.f90:47-192, ct.f90:30-118): ww(3,nv,i,j,k) on the hll range */
 int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww);
+/* The four calls of rg_calflx one at a time, as the reference makes them
+ * (main.f90:807-831), for a driver that swaps in one routine at a time.
+ * Face arrays come in sixes in the order ?l, ?r for ? = i, j, k, each
+ * a(nv,i,j,k) holding at cell f the state of the face f+1/2 (rec.f90's
+ * uriil(f) from cell f and uriir(f) from cell f+1); speeds come in the order
+ * cmaxi, cmini, cmaxj, cminj, cmaxk, cmink, one value per cell.  Only the hll
+ * range nm0..n-nm0 is written; rg_rec2 leaves its other entries 0, rg_hll and
+ * rg_ct leave the other entries of ww as given.
+ *  rg_rec2: rec2 with caluu3 and calflx3 (rec.f90:2-142): face primitives,
+ *    and, unless NULL, face conserved variables and face fluxes;
+ *  rg_calcha: calcha (calcha.f90:2-126, with cmink from the R state's plus
+ *    speed, calcha.f90:107) from face primitives;
+ *  rg_hll: hll (hll.f90:47-192) from face conserved variables, face fluxes and
+ *    speeds, into ww(3,nv,i,j,k) in place;
+ *  rg_ct: ct (ct.f90:4-27, the run's ict; guard bit 2 first zeroes the
+ *    normal-field fluxes) on ww in place, with the primitives uri. */
+int rg_rec2(rg_ctx* ctx, int run, const double* uri, double* face_prims, double* face_cons, double* face_flux);
+int rg_calcha(rg_ctx* ctx, int run, const double* face_prims, double* cha);
+int rg_hll(rg_ctx* ctx, int run, const double* face_cons, const double* face_flux, const double* cha, double* ww);
+int rg_ct(rg_ctx* ctx, int run, const double* uri, double* ww);
 /* recov1a (recov.f90:578-1228) on the interior: uu in (conserved), uri in/out */
 int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri);
 /* cdtcfl4 (cdtcfl.f90:2-129): dtcfl before the cfl factor */

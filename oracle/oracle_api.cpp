@@ -147,6 +147,59 @@ void orc_rec2(void* h, const double* uri, double* faces) {
   for (int m = 0; m < 6; ++m) std::memcpy(faces + m * s->uri.size(), f[m]->data(), s->uri.size() * sizeof(double));
 }
 
+// rec2 with its face conserved variables and fluxes (rec.f90:2-142: the
+// reconstruction, then caluu3 and calflx3 per direction): six arrays each of
+// face primitives, face conserved variables and face fluxes, in the order
+// ?il, ?ir for ? = i, j, k (each 9 per cell, reference layout; entries the
+// reference does not set are 0).  cons or flux may be null.
+void orc_rec2_full(void* h, const double* uri, double* prims, double* cons, double* flux) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  std::vector<double>* f[3][6] = {{&s->uriil, &s->uriir, &s->urijl, &s->urijr, &s->urikl, &s->urikr},
+                                  {&s->uuil, &s->uuir, &s->uujl, &s->uujr, &s->uukl, &s->uukr},
+                                  {&s->wwil, &s->wwir, &s->wwjl, &s->wwjr, &s->wwkl, &s->wwkr}};
+  for (auto& row : f)
+    for (auto* v : row) std::fill(v->begin(), v->end(), 0.0);
+  orc::rec2(*s);
+  double* out[3] = {prims, cons, flux};
+  const size_t n = s->uri.size();
+  for (int a = 0; a < 3; ++a)
+    if (out[a])
+      for (int m = 0; m < 6; ++m) std::memcpy(out[a] + m * n, f[a][m]->data(), n * sizeof(double));
+}
+
+// calcha (calcha.f90:2-126) from given face primitives (six arrays as
+// orc_rec2_full): cmaxi, cmini, cmaxj, cminj, cmaxk, cmink (one per cell each)
+void orc_calcha(void* h, const double* prims, double* cha) {
+  State* s = static_cast<State*>(h);
+  std::vector<double>* f[6] = {&s->uriil, &s->uriir, &s->urijl, &s->urijr, &s->urikl, &s->urikr};
+  const size_t n = s->uri.size();
+  for (int m = 0; m < 6; ++m) std::memcpy(f[m]->data(), prims + m * n, n * sizeof(double));
+  std::vector<double>* c[6] = {&s->cmaxi, &s->cmini, &s->cmaxj, &s->cminj, &s->cmaxk, &s->cmink};
+  for (auto* v : c) std::fill(v->begin(), v->end(), 0.0);
+  orc::calcha(*s);
+  for (int m = 0; m < 6; ++m) std::memcpy(cha + m * s->ncell, c[m]->data(), s->ncell * sizeof(double));
+}
+
+// hll (hll.f90:47-192) from given face conserved variables, face fluxes and
+// characteristic speeds: ww(3,nv,i,j,k) in/out (entries outside the hll
+// range keep their values)
+void orc_hll(void* h, const double* cons, const double* flux, const double* cha, double* ww) {
+  State* s = static_cast<State*>(h);
+  const size_t n = s->uri.size();
+  std::vector<double>* u[6] = {&s->uuil, &s->uuir, &s->uujl, &s->uujr, &s->uukl, &s->uukr};
+  std::vector<double>* w[6] = {&s->wwil, &s->wwir, &s->wwjl, &s->wwjr, &s->wwkl, &s->wwkr};
+  std::vector<double>* c[6] = {&s->cmaxi, &s->cmini, &s->cmaxj, &s->cminj, &s->cmaxk, &s->cmink};
+  for (int m = 0; m < 6; ++m) {
+    std::memcpy(u[m]->data(), cons + m * n, n * sizeof(double));
+    std::memcpy(w[m]->data(), flux + m * n, n * sizeof(double));
+    std::memcpy(c[m]->data(), cha + m * s->ncell, s->ncell * sizeof(double));
+  }
+  std::memcpy(s->ww.data(), ww, s->ww.size() * sizeof(double));
+  orc::hlle(*s);
+  std::memcpy(ww, s->ww.data(), s->ww.size() * sizeof(double));
+}
+
 // recov1a over the interior: uu (in/out, uu(6) rewritten), uri (in: guess, out)
 void orc_recov(void* h, double* uu, double* uri) {
   State* s = static_cast<State*>(h);

@@ -79,6 +79,9 @@ def _lib():
         lib.orc_rkt.argtypes = [P, C.c_int, C.c_double, D, D, D, D, D]
         lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
         lib.orc_get_array.restype = C.c_longlong
+        lib.orc_rec2_full.argtypes = [P, D, D, D, D]
+        lib.orc_calcha.argtypes = [P, D, D]
+        lib.orc_hll.argtypes = [P, D, D, D, D]
         lib.orc_output1.argtypes = [P, C.c_char_p, C.c_int, C.c_int]
         lib.orc_output1.restype = C.c_int
         lib.orc_set_pow_mode.argtypes = [C.c_int]
@@ -221,6 +224,32 @@ class Oracle:
         uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
         out = np.zeros((6,) + self.shape, dtype=np.float64)
         self.lib.orc_rec2(self.h, _ptr(uri), _ptr(out))
+        return out
+
+    def rec2_full(self, uri):
+        """rec2 with caluu3/calflx3: (prims, cons, flux), each of shape (6,) +
+        prims shape in the order ?il, ?ir for ? = i, j, k."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = [np.zeros((6,) + self.shape, dtype=np.float64) for _ in range(3)]
+        self.lib.orc_rec2_full(self.h, _ptr(uri), _ptr(out[0]), _ptr(out[1]), _ptr(out[2]))
+        return tuple(out)
+
+    def calcha(self, faces):
+        """calcha from face primitives (6, kmax, jmax, imax, 9): cmax/cmin per
+        direction, shape (6, kmax, jmax, imax) (cmaxi, cmini, cmaxj, cminj, cmaxk, cmink)."""
+        faces = np.ascontiguousarray(faces, dtype=np.float64)
+        out = np.zeros((6,) + self.shape[:3], dtype=np.float64)
+        self.lib.orc_calcha(self.h, _ptr(faces), _ptr(out))
+        return out
+
+    def hll(self, cons, flux, cha, ww):
+        """hll from face conserved variables and fluxes (6, ...) and speeds (6, ...);
+        returns the updated copy of ww (kmax, jmax, imax, 9, 3)."""
+        cons = np.ascontiguousarray(cons, dtype=np.float64)
+        flux = np.ascontiguousarray(flux, dtype=np.float64)
+        cha = np.ascontiguousarray(cha, dtype=np.float64)
+        out = np.array(ww, dtype=np.float64, order="C").reshape(self.shape + (3,))
+        self.lib.orc_hll(self.h, _ptr(cons), _ptr(flux), _ptr(cha), _ptr(out))
         return out
 
     def derived(self, uri, jslice: int = 0) -> np.ndarray:

@@ -29,7 +29,7 @@ EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ct
            "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_torus_device", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
-           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_divb", "rg_run_horizon_flux", "rg_run_radial_flux", "rg_run_store", "rg_run_restore", "rg_run_output", "rg_pow_eval", "rg_calflx_static")
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_rec2", "rg_calcha", "rg_hll", "rg_ct", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_divb", "rg_run_horizon_flux", "rg_run_radial_flux", "rg_run_store", "rg_run_restore", "rg_run_output", "rg_pow_eval", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -119,6 +119,10 @@ def load(path: str = LIB_PATH):
     lib.rg_caluu1.argtypes = [P, I, D, D]
     lib.rg_calflx.argtypes = [P, I, D, D]
     lib.rg_recov.argtypes = [P, I, D, D]
+    lib.rg_rec2.argtypes = [P, I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rg_calcha.argtypes = [P, I, C.c_void_p, C.c_void_p]
+    lib.rg_hll.argtypes = [P, I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rg_ct.argtypes = [P, I, C.c_void_p, C.c_void_p]
     lib.rg_cdtcfl.argtypes = [P, I, D, D]
     lib.rg_bnd_floor.argtypes = [P, I, D, D]
     lib.rg_calsf.argtypes = [P, I, D, D]
@@ -379,6 +383,40 @@ class Run:
         uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
         out = np.zeros(self.shape + (3,), dtype=np.float64)
         _check(self.lib, self.lib.rg_calflx(self.ctx.h, self.id, _dptr(uri), _dptr(out)))
+        return out
+
+    def rec2(self, uri, cons: bool = True):
+        """rg_rec2: (face primitives, face conserved variables, face fluxes),
+        each of shape (6, kmax, jmax, imax, 9) in the order ?l, ?r for ? = i, j, k
+        (the latter two None unless cons)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = [np.zeros((6,) + self.shape, dtype=np.float64) for _ in range(3 if cons else 1)]
+        ptrs = [o.ctypes.data for o in out] + [None] * (3 - len(out))
+        _check(self.lib, self.lib.rg_rec2(self.ctx.h, self.id, uri.ctypes.data, *ptrs))
+        return tuple(out) + (None,) * (3 - len(out))
+
+    def calcha(self, faces) -> np.ndarray:
+        """rg_calcha: speeds (6, kmax, jmax, imax) from face primitives (6, ...)."""
+        faces = np.ascontiguousarray(faces, dtype=np.float64)
+        out = np.zeros((6,) + self.shape[:3], dtype=np.float64)
+        _check(self.lib, self.lib.rg_calcha(self.ctx.h, self.id, faces.ctypes.data, out.ctypes.data))
+        return out
+
+    def hll(self, cons, flux, cha, ww) -> np.ndarray:
+        """rg_hll: the updated copy of ww (kmax, jmax, imax, 9, 3)."""
+        cons = np.ascontiguousarray(cons, dtype=np.float64)
+        flux = np.ascontiguousarray(flux, dtype=np.float64)
+        cha = np.ascontiguousarray(cha, dtype=np.float64)
+        out = np.array(ww, dtype=np.float64, order="C").reshape(self.shape + (3,))
+        _check(self.lib, self.lib.rg_hll(self.ctx.h, self.id, cons.ctypes.data, flux.ctypes.data, cha.ctypes.data,
+                                         out.ctypes.data))
+        return out
+
+    def ct(self, uri, ww) -> np.ndarray:
+        """rg_ct: the updated copy of ww (kmax, jmax, imax, 9, 3)."""
+        uri = np.ascontiguousarray(uri, dtype=np.float64).reshape(self.shape)
+        out = np.array(ww, dtype=np.float64, order="C").reshape(self.shape + (3,))
+        _check(self.lib, self.lib.rg_ct(self.ctx.h, self.id, uri.ctypes.data, out.ctypes.data))
         return out
 
     def recov(self, uu, uri) -> np.ndarray:

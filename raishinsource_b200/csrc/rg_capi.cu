@@ -48,6 +48,7 @@ struct Run {
   bool fb_ready = false;
   double* aos = nullptr;   // 9*Nfull staging buffer in the reference layout (allocated on first use)
   double* unew = nullptr;  // 9*Nfull output of rg_rkt (allocated on first use)
+  double* wwaos = nullptr; // 27*Nfull staging of ww(3,nv,i,j,k) (allocated on first use)
   // scalar block and counters of the per-routine entry points, so that those
   // calls never touch the run's own time state, buffer rotation or statistics
   Scal* fscal = nullptr;
@@ -448,7 +449,8 @@ int ensure_aos(Run* R) {
 int to_soa(rg_ctx* ctx, Run* R, const double* host_aos, double* dev_soa, const DevRun& v, bool check) {
   int rc = ensure_aos(R);
   if (rc) return rc;
-  RG_CUDA(cudaMemcpyAsync(R->aos, host_aos, 9 * R->nfull * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  // cudaMemcpyDefault: the caller's array may be host memory or device memory (unified addressing)
+  RG_CUDA(cudaMemcpyAsync(R->aos, host_aos, 9 * R->nfull * sizeof(double), cudaMemcpyDefault, ctx->stream));
   const bool slab = v.jfix || v.kfix;
   if (check && slab) RG_CUDA(cudaMemsetAsync(R->bad, 0, sizeof(int), ctx->stream));
   RG_CUDA(launch_aos_to_soa(v, R->aos, dev_soa, (check && slab) ? R->bad : nullptr, ctx->stream));
@@ -468,7 +470,36 @@ int from_soa(rg_ctx* ctx, Run* R, const double* dev_soa, double* host_aos, const
   int rc = ensure_aos(R);
   if (rc) return rc;
   RG_CUDA(launch_soa_to_aos(v, dev_soa, R->aos, ctx->stream));
-  RG_CUDA(cudaMemcpyAsync(host_aos, R->aos, 9 * R->nfull * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(host_aos, R->aos, 9 * R->nfull * sizeof(double), cudaMemcpyDefault, ctx->stream));
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+// ww(3,nv,i,j,k) (host or device array) <-> the full-layout flux planes B->F.
+int ww_scratch(Run* R, double** out) {
+  if (!R->wwaos) {
+    void* p = nullptr;
+    const int rc = dalloc(R, &p, 27 * R->nfull * sizeof(double));
+    if (rc) return rc;
+    R->wwaos = static_cast<double*>(p);
+  }
+  *out = R->wwaos;
+  return RG_OK;
+}
+int ww_in(rg_ctx* ctx, Run* R, DevBufs* B, const double* ww) {
+  double* a = nullptr;
+  int rc = ww_scratch(R, &a);
+  if (rc) return rc;
+  RG_CUDA(cudaMemcpyAsync(a, ww, 27 * R->nfull * sizeof(double), cudaMemcpyDefault, ctx->stream));
+  RG_CUDA(launch_ww_layout(a, B->F[0], B->F[1], B->F[2], R->nfull, true, ctx->stream));
+  return RG_OK;
+}
+int ww_out(rg_ctx* ctx, Run* R, DevBufs* B, double* ww) {
+  double* a = nullptr;
+  int rc = ww_scratch(R, &a);
+  if (rc) return rc;
+  RG_CUDA(launch_ww_layout(a, B->F[0], B->F[1], B->F[2], R->nfull, false, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(ww, a, 27 * R->nfull * sizeof(double), cudaMemcpyDefault, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
   return RG_OK;
 }
@@ -1375,40 +1406,14 @@ int rg_calflx(rg_ctx* ctx, int run, const double* uri, double* ww) {
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   if (!uri || !ww) return fail(RG_EINVAL_CONFIG, "null array");
   DevRun d = full_view(R);
-  const size_t N = d.N;
   DevBufs* B = nullptr;
   int rc = full_bufs(R, ctx->stream, &B);
   if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
   d.ctd = B->ctd;
   for (int dir = 1; dir <= 3; ++dir) RG_CUDA(launch_flux(d, dir, B->stage, B->F[dir - 1], ctx->stream));
   RG_CUDA(launch_ct(d, B->stage, B->F[0], B->F[1], B->F[2], B->CT, ctx->stream));
-  std::vector<double> F(27 * N), CT(6 * N);
-  for (int dir = 0; dir < 3; ++dir)
-    RG_CUDA(cudaMemcpyAsync(F.data() + (size_t)dir * 9 * N, B->F[dir], 9 * N * sizeof(double),
-                            cudaMemcpyDeviceToHost, ctx->stream));
-  RG_CUDA(cudaMemcpyAsync(CT.data(), B->CT, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  RG_CUDA(cudaStreamSynchronize(ctx->stream));
-  const int nm1 = d.nm1;
-  for (int k = 1; k <= d.kmax; ++k)
-    for (int j = 1; j <= d.jmax; ++j)
-      for (int i = 1; i <= d.imax; ++i) {
-        const size_t c = d.cell(i, j, k);
-        const bool in_ct = i >= nm1 && i <= d.imax - nm1 && j >= nm1 && j <= d.jmax - nm1 && k >= nm1 && k <= d.kmax - nm1;
-        for (int v = 0; v < 9; ++v)
-          for (int dir = 0; dir < 3; ++dir) {
-            double w = F[(size_t)dir * 9 * N + (size_t)v * N + c];
-            if (in_ct) {
-              if (dir == 1 && v == 6) w = CT[0 * N + c];
-              if (dir == 2 && v == 6) w = CT[1 * N + c];
-              if (dir == 0 && v == 7) w = CT[2 * N + c];
-              if (dir == 2 && v == 7) w = CT[3 * N + c];
-              if (dir == 0 && v == 8) w = CT[4 * N + c];
-              if (dir == 1 && v == 8) w = CT[5 * N + c];
-            }
-            ww[dir + 3 * (v + 9 * c)] = w;
-          }
-      }
-  return RG_OK;
+  RG_CUDA(launch_ct_apply(d, B->CT, B->F[0], B->F[1], B->F[2], ctx->stream));
+  return ww_out(ctx, R, B, ww);
 }
 
 int rg_calsf(rg_ctx* ctx, int run, const double* uri, double* sf) {
@@ -1421,11 +1426,12 @@ int rg_calsf(rg_ctx* ctx, int run, const double* uri, double* sf) {
   int rc = full_bufs(R, ctx->stream, &B);
   if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
   RG_CUDA(launch_calsf(d, B->stage, B->CT, ctx->stream));
-  std::vector<double> S(4 * N);
-  RG_CUDA(cudaMemcpyAsync(S.data(), B->CT, 4 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  // sf(2:5,i,j,k): the four planes into the reference layout in the ww staging buffer
+  double* a = nullptr;
+  if ((rc = ww_scratch(R, &a))) return rc;
+  RG_CUDA(launch_aos_planes(a, B->CT, N, 4, false, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(sf, a, 4 * N * sizeof(double), cudaMemcpyDefault, ctx->stream));
   RG_CUDA(cudaStreamSynchronize(ctx->stream));
-  for (size_t c = 0; c < N; ++c)
-    for (int n = 0; n < 4; ++n) sf[4 * c + n] = S[(size_t)n * N + c];
   return RG_OK;
 }
 
@@ -1445,18 +1451,13 @@ int rg_rkt(rg_ctx* ctx, int run, int stage, double dt, const double* ww, const d
     if ((rc = dalloc(R, &p, 9 * N * sizeof(double)))) return rc;
     R->unew = static_cast<double*>(p);
   }
-  // ww(3,nv,i,j,k) and sf(2:5,i,j,k) to planes (host side: this entry point
-  // serves per-routine swap-in and parity, not the step)
-  std::vector<double> W(9 * N), S(4 * N);
-  for (int dir = 0; dir < 3; ++dir) {
-    for (size_t c = 0; c < N; ++c)
-      for (int v = 0; v < 9; ++v) W[(size_t)v * N + c] = ww[dir + 3 * (v + 9 * c)];
-    RG_CUDA(cudaMemcpyAsync(B->F[dir], W.data(), 9 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    RG_CUDA(cudaStreamSynchronize(ctx->stream));  // W is refilled for the next direction
-  }
-  for (size_t c = 0; c < N; ++c)
-    for (int n = 0; n < 4; ++n) S[(size_t)n * N + c] = sf[4 * c + n];
-  RG_CUDA(cudaMemcpyAsync(B->CT, S.data(), 4 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  // ww(3,nv,i,j,k) and sf(2:5,i,j,k) to planes on the device
+  if ((rc = ww_in(ctx, R, B, ww))) return rc;
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));  // the staging buffer is reused for sf
+  double* a = nullptr;
+  if ((rc = ww_scratch(R, &a))) return rc;
+  RG_CUDA(cudaMemcpyAsync(a, sf, 4 * N * sizeof(double), cudaMemcpyDefault, ctx->stream));
+  RG_CUDA(launch_aos_planes(a, B->CT, N, 4, true, ctx->stream));
   if ((rc = to_soa(ctx, R, ucur, B->stage, d, false))) return rc;
   if (stage > 1 && (rc = to_soa(ctx, R, uo, B->stage2, d, false))) return rc;
   if ((rc = to_soa(ctx, R, unew, R->unew, d, false))) return rc;
@@ -1739,6 +1740,117 @@ int rg_run_divb(rg_ctx* ctx, int run, double* divb_max, double* b_scale) {
   std::memcpy(divb_max, &h[0], sizeof(double));
   std::memcpy(b_scale, &h[1], sizeof(double));
   return RG_OK;
+}
+
+// ---- rec2, calcha, hll and ct one at a time (the reference's separate calls,
+// main.f90:807-831).  Arrays in the reference layout, host or device memory.
+namespace {
+// Device scratch of the per-routine calls below, freed on return.
+struct Scratch {
+  double* p = nullptr;
+  ~Scratch() { cudaFree(p); }
+  int alloc(size_t n) {
+    if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return fail(RG_ENOMEM_ADMIT, "per-routine scratch does not fit");
+    }
+    return RG_OK;
+  }
+};
+}  // namespace
+
+int rg_rec2(rg_ctx* ctx, int run, const double* uri, double* face_prims, double* face_cons, double* face_flux) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!uri || !face_prims) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  const size_t N = d.N, n9 = 9 * N;
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
+  Scratch S;  // 18 face arrays: prims, cons, flux x (il, ir, jl, jr, kl, kr)
+  if ((rc = S.alloc(18 * n9))) return rc;
+  RG_CUDA(cudaMemsetAsync(S.p, 0, 18 * n9 * sizeof(double), ctx->stream));
+  for (int dir = 1; dir <= 3; ++dir) {
+    double* const q[2] = {S.p + (2 * (dir - 1)) * n9, S.p + (2 * (dir - 1) + 1) * n9};
+    double* const u[2] = {q[0] + 6 * n9, q[1] + 6 * n9};
+    double* const w[2] = {q[0] + 12 * n9, q[1] + 12 * n9};
+    RG_CUDA(launch_rec2(d, dir, B->stage, B->F[dir - 1], q, u, w, ctx->stream));
+  }
+  double* outs[3] = {face_prims, face_cons, face_flux};
+  for (int a = 0; a < 3; ++a) {
+    if (!outs[a]) continue;
+    for (int m = 0; m < 6; ++m)
+      if ((rc = from_soa(ctx, R, S.p + (size_t)(6 * a + m) * n9, outs[a] + (size_t)m * n9, d))) return rc;
+  }
+  return RG_OK;
+}
+
+int rg_calcha(rg_ctx* ctx, int run, const double* face_prims, double* cha) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!face_prims || !cha) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  const size_t N = d.N, n9 = 9 * N;
+  Scratch S;  // 6 face arrays, then 6 speed arrays
+  int rc = S.alloc(6 * n9 + 6 * N);
+  if (rc) return rc;
+  for (int m = 0; m < 6; ++m)
+    if ((rc = to_soa(ctx, R, face_prims + (size_t)m * n9, S.p + (size_t)m * n9, d, false))) return rc;
+  double* C = S.p + 6 * n9;
+  RG_CUDA(cudaMemsetAsync(C, 0, 6 * N * sizeof(double), ctx->stream));
+  for (int dir = 1; dir <= 3; ++dir)
+    RG_CUDA(launch_calcha(d, dir, S.p + (2 * (dir - 1)) * n9, S.p + (2 * (dir - 1) + 1) * n9,
+                          C + (2 * (dir - 1)) * N, C + (2 * (dir - 1) + 1) * N, ctx->stream));
+  RG_CUDA(cudaMemcpyAsync(cha, C, 6 * N * sizeof(double), cudaMemcpyDefault, ctx->stream));
+  RG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+int rg_hll(rg_ctx* ctx, int run, const double* face_cons, const double* face_flux, const double* cha, double* ww) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!face_cons || !face_flux || !cha || !ww) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  const size_t N = d.N, n9 = 9 * N;
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc) return rc;
+  Scratch S;  // 6 conserved, 6 flux face arrays, 6 speed arrays
+  if ((rc = S.alloc(12 * n9 + 6 * N))) return rc;
+  for (int m = 0; m < 6; ++m) {
+    if ((rc = to_soa(ctx, R, face_cons + (size_t)m * n9, S.p + (size_t)m * n9, d, false))) return rc;
+    if ((rc = to_soa(ctx, R, face_flux + (size_t)m * n9, S.p + (size_t)(6 + m) * n9, d, false))) return rc;
+  }
+  double* C = S.p + 12 * n9;
+  RG_CUDA(cudaMemcpyAsync(C, cha, 6 * N * sizeof(double), cudaMemcpyDefault, ctx->stream));
+  if ((rc = ww_in(ctx, R, B, ww))) return rc;
+  for (int dir = 1; dir <= 3; ++dir) {
+    const size_t l = 2 * (dir - 1), rr = l + 1;
+    RG_CUDA(launch_hll(d, dir, S.p + l * n9, S.p + rr * n9, S.p + (6 + l) * n9, S.p + (6 + rr) * n9, C + l * N,
+                       C + rr * N, B->F[dir - 1], ctx->stream));
+  }
+  return ww_out(ctx, R, B, ww);
+}
+
+int rg_ct(rg_ctx* ctx, int run, const double* uri, double* ww) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!uri || !ww) return fail(RG_EINVAL_CONFIG, "null array");
+  DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
+  d.ctd = B->ctd;
+  if ((rc = ww_in(ctx, R, B, ww))) return rc;
+  if (d.guard & 2) {  // the zero normal-field fluxes come before the CT averages read the planes
+    DevRun z = d;
+    z.ict = 0;  // zeroing only
+    RG_CUDA(launch_ct_apply(z, B->CT, B->F[0], B->F[1], B->F[2], ctx->stream));
+  }
+  RG_CUDA(launch_ct(d, B->stage, B->F[0], B->F[1], B->F[2], B->CT, ctx->stream));
+  RG_CUDA(launch_ct_apply(d, B->CT, B->F[0], B->F[1], B->F[2], ctx->stream));
+  return ww_out(ctx, R, B, ww);
 }
 
 int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri) {

@@ -924,11 +924,21 @@ __device__ __forceinline__ const float* met_of<3, float>(const DevRun& r) { retu
 // of the primitives instead of P: variable v of the lane's cell at
 // Vp[v * Vn + Vc], neighbours along D Vst apart (the shared-memory box of
 // k_flux_tma).  Stores, metric and coordinates stay global.
-template <int D, int IREC, typename T, typename S, bool VIEW = false>
+//
+// OUT (the per-routine rg_rec2): the lane also stores its face state, face
+// conserved variables and face flux, all nine variables (the sixth included),
+// into fo->q/u/w[side] at the face's cell index (rec.f90's uri?l/uri?r,
+// uu?l/uu?r, ww?l/ww?r of face f+1/2 at index f).
+struct FaceOut {
+  double* q[2];
+  double* u[2];
+  double* w[2];
+};
+template <int D, int IREC, typename T, typename S, bool VIEW = false, bool OUT = false>
 __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__ P, S* __restrict__ F,
                                           float* __restrict__ Fcopy, int icopy, int i, int j, int k, int side,
                                           bool valid, const S* Vp = nullptr, size_t Vn = 0, size_t Vc = 0,
-                                          long long Vst = 0) {
+                                          long long Vst = 0, const FaceOut* fo = nullptr) {
   const unsigned mask = __activemask();
   const size_t N = r.N, c = r.cell(i, j, k);
   const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.sj : (long long)r.sk);
@@ -945,8 +955,8 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     for (int o = -2; o <= 2; ++o) dx[o + 4] = T(__ldg(dxs + f - 1 + o));
 #pragma unroll
     for (int o = -1; o <= 1; ++o) xx[o + 4] = T(__ldg(xs + f - 1 + o));
-    if (side == 0) ppm_cell<D>(Pv + cv, Nv, sv, dx, xx, T(r.gam), other, q);  // uriil(f)
-    else ppm_cell<D>(Pv + cv + sv, Nv, sv, dx, xx, T(r.gam), q, other);       // uriir(f)
+    if (side == 0) ppm_cell<D, T, S, OUT>(Pv + cv, Nv, sv, dx, xx, T(r.gam), other, q);  // uriil(f)
+    else ppm_cell<D, T, S, OUT>(Pv + cv + sv, Nv, sv, dx, xx, T(r.gam), q, other);       // uriir(f)
   } else if (IREC == 1 || IREC == 2 || IREC == 11 || IREC == 12 || IREC == 13) {
     // owner cell f of this lane's state and its coordinate's coefficients
     const int f = ((D == 1) ? i : (D == 2 ? j : k)) + side;
@@ -960,7 +970,7 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     const T hpi = cross ? T(__ldg(r.lim[0] + i - 1)) : T(0);
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
-      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
+      if (v == 5 && !OUT) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       const S* p = Pv + (size_t)v * Nv + cv + side * sv;
       const T u0 = T(p[0]);
       T tmp_b = T(0);
@@ -977,21 +987,21 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     for (int a = 0; a < 10; ++a) co[a] = T(__ldg(lc + a * n + f - 1));
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
-      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
+      if (v == 5 && !OUT) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       const S* p = Pv + (size_t)v * Nv + cv + side * sv;
       q[v] = ceno_state(T(p[-2 * sv]), T(p[-sv]), T(p[0]), T(p[sv]), T(p[2 * sv]), co, side, D == 3 && side == 0);
     }
   } else if (IREC == 3) {
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
-      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
+      if (v == 5 && !OUT) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       const S* p = Pv + (size_t)v * Nv + cv + side * sv;
       q[v] = muscl_state(T(p[-sv]), T(p[0]), T(p[sv]), side);
     }
   } else {
 #pragma unroll
     for (int v = 0; v < 9; ++v) {
-      if (v == 5) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
+      if (v == 5 && !OUT) { q[v] = T(0); continue; }  // var 6 faces are never read downstream
       // owner cell f + side; the right state reads its stencil mirrored
       const long long sd = side ? -sv : sv;
       const S* p = Pv + (size_t)v * Nv + cv + side * sv;
@@ -1029,6 +1039,16 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     p2c(s, gam, m.detg, u, sr);
     flux<D>(s, gam, m.detg, w, sr);
     wavespeed<D>(q, s, m, gam, vp, vm);
+  }
+  if constexpr (OUT) {
+    if (valid) {
+#pragma unroll
+      for (int v = 0; v < 9; ++v) {
+        fo->q[side][(size_t)v * N + c] = double(q[v]);
+        fo->u[side][(size_t)v * N + c] = double(u[v]);
+        fo->w[side][(size_t)v * N + c] = double(w[v]);
+      }
+    }
   }
   const T vpo = __shfl_xor_sync(mask, vp, 1), vmo = __shfl_xor_sync(mask, vm, 1);
   const T vpL = side ? vpo : vp, vpR = side ? vp : vpo;
@@ -1164,6 +1184,126 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
   const size_t vc = (size_t)((i - 1 - x0) + B::X * ((j - 1 - y0) + B::Y * (k - 1 - z0)));
   const long long vst = (D == 1) ? 1 : (D == 2 ? B::X : B::X * B::Y);
   face_lane<D, 6, T, S, true>(r, nullptr, F, Fcopy, icopy, i, j, k, side, valid, box, B::PLANE, vc, vst);
+}
+
+// ------------------------------------------- per-routine rec2 / calcha / hll
+// rec2 with caluu3 and calflx3 (rec.f90:2-142) for one direction: the face
+// lanes of k_flux with their states, conserved variables and fluxes stored
+// (FaceOut); the LLF fluxes go to F, which the caller discards.
+template <int D, int IREC>
+__global__ void __launch_bounds__(128, RG_FLUX_MINB64) k_rec2(DevRun r, const double* __restrict__ P,
+                                                             double* __restrict__ F, FaceOut fo) {
+  const int nm0 = r.nm0, ilo = nm0, ihi = r.imax - nm0;
+  const int side = threadIdx.x & 1;
+  const int i0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 1) + ilo;
+  const int j0 = jidx(r, nm0, blockIdx);
+  const int k0 = kidx(r, nm0, blockIdx);
+  const bool valid = i0 <= ihi && j0 <= r.jmax - nm0 && k0 <= r.kmax - nm0;
+  const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(k0, r.kmax - nm0);
+  face_lane<D, IREC, double, double, false, true>(r, P, F, nullptr, 0, i, j, k, side, valid, nullptr, 0, 0, 0, &fo);
+}
+
+// calcha (calcha.f90:2-126, with cmink built from the R state's plus speed,
+// calcha.f90:107) from given face primitives QL (uri?l) and QR (uri?r) of
+// direction D, over the hll range nm0..n-nm0.
+template <int D>
+__global__ void __launch_bounds__(128) k_calcha(DevRun r, const double* __restrict__ QL, const double* __restrict__ QR,
+                                                double* __restrict__ cmax, double* __restrict__ cmin) {
+  const int nm0 = r.nm0;
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) + nm0;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) + nm0;
+  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z) + nm0;
+  if (i > r.imax - nm0 || j > r.jmax - nm0 || k > r.kmax - nm0) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  Met m;
+  load_met(met_of<D, double>(r), r.nik, r.ik(i, k), m);
+  double qL[9], qR[9], vpL, vmL, vpR, vmR;
+  load9(QL, N, c, qL);
+  load9(QR, N, c, qR);
+  {
+    PS s;
+    pstate(qL, m, r.gam, s);
+    wavespeed<D>(qL, s, m, r.gam, vpL, vmL);
+  }
+  {
+    PS s;
+    pstate(qR, m, r.gam, s);
+    wavespeed<D>(qR, s, m, r.gam, vpR, vmR);
+  }
+  cmax[c] = fmax3(0.0, vpR, vpL);
+  cmin[c] = (D == 3) ? fmin3(0.0, vpR, vmL) : fmin3(0.0, vmR, vmL);
+}
+
+// hll (hll.f90:83-183) for direction D from given face conserved variables,
+// face fluxes and speeds: the fluxes F of the hll range, in place (a face with
+// NaN speeds keeps its value, as the reference's ww does).
+template <int D>
+__global__ void __launch_bounds__(128) k_hll(DevRun r, const double* __restrict__ UL, const double* __restrict__ UR,
+                                             const double* __restrict__ WL, const double* __restrict__ WR,
+                                             const double* __restrict__ CX, const double* __restrict__ CN,
+                                             double* __restrict__ F) {
+  const int nm0 = r.nm0;
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) + nm0;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) + nm0;
+  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z) + nm0;
+  if (i > r.imax - nm0 || j > r.jmax - nm0 || k > r.kmax - nm0) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  const double cmin = CN[c], cmax = CX[c];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    const size_t o = (size_t)v * N + c;
+    double f;
+    if (cmin > 0.0) f = WL[o];
+    else if (cmin <= 0.0 && cmax > 0.0) {
+      const double c1 = dmax2(fabs(cmax), fabs(cmin));
+      f = 0.5 * (WL[o] + WR[o] - c1 * (UR[o] - UL[o]));
+    } else if (cmax <= 0.0) f = WR[o];
+    else continue;
+    if (fabs(f) < 1.0e-40) f = 0.0;
+    F[o] = f;
+  }
+}
+
+// ww(3,nv,i,j,k) of the reference (direction fastest) <-> the three flux
+// planes F[d][v*N + c] of the full layout.
+__global__ void k_ww_layout(double* __restrict__ ww, double* __restrict__ F1, double* __restrict__ F2,
+                            double* __restrict__ F3, size_t N, int to_planes) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  double* F[3] = {F1, F2, F3};
+#pragma unroll
+  for (int v = 0; v < 9; ++v)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double& a = ww[d + 3 * (v + 9 * c)];
+      double& b = F[d][(size_t)v * N + c];
+      if (to_planes) b = a;
+      else a = b;
+    }
+}
+
+// ct's results into the flux planes: with guard bit 2 the normal-field
+// fluxes ww(1,7), ww(2,8), ww(3,9) are zero on the hll range (the oracle's ct
+// does that first); the six CT values replace the transverse induction fluxes
+// on the CT range nm1..n-nm1 (ct.f90:98-109).
+__global__ void k_ct_apply(DevRun r, const double* __restrict__ CT, double* __restrict__ F1, double* __restrict__ F2,
+                           double* __restrict__ F3) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) + 1;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) + 1;
+  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z) + 1;
+  if (i > r.imax || j > r.jmax || k > r.kmax) return;
+  const size_t N = r.N, c = r.cell(i, j, k);
+  const int nm0 = r.nm0, nm1 = r.nm1;
+  double* F[3] = {F1, F2, F3};
+  if ((r.guard & 2) && i >= nm0 && i <= r.imax - nm0 && j >= nm0 && j <= r.jmax - nm0 && k >= nm0 &&
+      k <= r.kmax - nm0)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[d][(size_t)(6 + d) * N + c] = 0.0;
+  if (r.ict == 0 || i < nm1 || i > r.imax - nm1 || j < nm1 || j > r.jmax - nm1 || k < nm1 || k > r.kmax - nm1) return;
+  // (direction, variable) of the six replaced fluxes: ww(2,7) ww(3,7) ww(1,8) ww(3,8) ww(1,9) ww(2,9)
+  const int dir[6] = {1, 2, 0, 2, 0, 1}, var[6] = {6, 6, 7, 7, 8, 8};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) F[dir[q]][(size_t)var[q] * N + c] = CT[(size_t)q * N + c];
 }
 
 // ---------------------------------------------------------------- flux-CT
@@ -2335,6 +2475,82 @@ cudaError_t launch_output1(const DevRun& r, const double* P, const double* cx, c
   k_output1<<<(unsigned)((nrec + 127) / 128), 128, 0, s>>>(r, P, cx, cy, cz, rec0, nrec, out);
   return cudaGetLastError();
 }
+template <int D>
+static void launch_rec2_d(const DevRun& r, const double* P, double* F, const FaceOut& fo, dim3 g, dim3 b,
+                          cudaStream_t s) {
+  switch (r.irec) {
+    case 1: k_rec2<D, 1><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 2: k_rec2<D, 2><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 3: k_rec2<D, 3><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 4: k_rec2<D, 4><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 5: k_rec2<D, 5><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 6: k_rec2<D, 6><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 7: k_rec2<D, 7><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 8: k_rec2<D, 8><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 9: k_rec2<D, 9><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 10: k_rec2<D, 10><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 11: k_rec2<D, 11><<<g, b, 0, s>>>(r, P, F, fo); break;
+    case 12: k_rec2<D, 12><<<g, b, 0, s>>>(r, P, F, fo); break;
+    default: k_rec2<D, 13><<<g, b, 0, s>>>(r, P, F, fo); break;
+  }
+}
+
+cudaError_t launch_rec2(const DevRun& r, int dir, const double* P, double* F, double* const q[2], double* const u[2],
+                        double* const w[2], cudaStream_t s) {
+  const int n = r.imax - 2 * r.nm0 + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
+  const dim3 b(64, 2, 1);
+  const dim3 g = grid3(2 * n, m, l, b);
+  const FaceOut fo{{q[0], q[1]}, {u[0], u[1]}, {w[0], w[1]}};
+  if (dir == 1) launch_rec2_d<1>(r, P, F, fo, g, b, s);
+  else if (dir == 2) launch_rec2_d<2>(r, P, F, fo, g, b, s);
+  else launch_rec2_d<3>(r, P, F, fo, g, b, s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_calcha(const DevRun& r, int dir, const double* QL, const double* QR, double* cmax, double* cmin,
+                          cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  const dim3 g = grid3(r.imax - 2 * r.nm0 + 1, r.jmax - 2 * r.nm0 + 1, r.kmax - 2 * r.nm0 + 1, b);
+  if (dir == 1) k_calcha<1><<<g, b, 0, s>>>(r, QL, QR, cmax, cmin);
+  else if (dir == 2) k_calcha<2><<<g, b, 0, s>>>(r, QL, QR, cmax, cmin);
+  else k_calcha<3><<<g, b, 0, s>>>(r, QL, QR, cmax, cmin);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hll(const DevRun& r, int dir, const double* UL, const double* UR, const double* WL,
+                       const double* WR, const double* CX, const double* CN, double* F, cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  const dim3 g = grid3(r.imax - 2 * r.nm0 + 1, r.jmax - 2 * r.nm0 + 1, r.kmax - 2 * r.nm0 + 1, b);
+  if (dir == 1) k_hll<1><<<g, b, 0, s>>>(r, UL, UR, WL, WR, CX, CN, F);
+  else if (dir == 2) k_hll<2><<<g, b, 0, s>>>(r, UL, UR, WL, WR, CX, CN, F);
+  else k_hll<3><<<g, b, 0, s>>>(r, UL, UR, WL, WR, CX, CN, F);
+  return cudaGetLastError();
+}
+
+__global__ void k_aos_planes(double* __restrict__ aos, double* __restrict__ planes, size_t N, int m, int to_planes) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  for (int a = 0; a < m; ++a) {
+    if (to_planes) planes[(size_t)a * N + c] = aos[(size_t)m * c + a];
+    else aos[(size_t)m * c + a] = planes[(size_t)a * N + c];
+  }
+}
+cudaError_t launch_aos_planes(double* aos, double* planes, size_t N, int m, bool to_planes, cudaStream_t s) {
+  k_aos_planes<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(aos, planes, N, m, to_planes ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_ww_layout(double* ww, double* F1, double* F2, double* F3, size_t N, bool to_planes,
+                             cudaStream_t s) {
+  k_ww_layout<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(ww, F1, F2, F3, N, to_planes ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ct_apply(const DevRun& r, const double* CT, double* F1, double* F2, double* F3, cudaStream_t s) {
+  const dim3 b(64, 2, 1);
+  k_ct_apply<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, CT, F1, F2, F3);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_divb(const DevRun& r, const double* P, unsigned long long* red, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(red, 0, 2 * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;

@@ -48,6 +48,22 @@ cudaError_t launch_stage_recov2(const DevRun& r, int stage, const double* Pc, do
                                 double* F3, const double* CT, double* Uc, double* SF, double* Unew, cudaStream_t s);
 cudaError_t launch_p2c(const DevRun& r, const double* P, double* U, cudaStream_t s);
 cudaError_t launch_calsf(const DevRun& r, const double* P, double* SF, cudaStream_t s);
+// per-routine rec2 / calcha / hll / ct on the full layout: q/u/w[0] (L) and
+// [1] (R) are the face primitives, conserved variables and fluxes of one
+// direction (9 planes of N each); F receives the LLF fluxes (rec2: scratch)
+cudaError_t launch_rec2(const DevRun& r, int dir, const double* P, double* F, double* const q[2], double* const u[2],
+                        double* const w[2], cudaStream_t s);
+cudaError_t launch_calcha(const DevRun& r, int dir, const double* QL, const double* QR, double* cmax, double* cmin,
+                          cudaStream_t s);
+cudaError_t launch_hll(const DevRun& r, int dir, const double* UL, const double* UR, const double* WL,
+                       const double* WR, const double* CX, const double* CN, double* F, cudaStream_t s);
+// m values per cell (value fastest) <-> m planes of N
+cudaError_t launch_aos_planes(double* aos, double* planes, size_t N, int m, bool to_planes, cudaStream_t s);
+// ww(3,nv,i,j,k) <-> flux planes F1..F3 (9 planes of N each)
+cudaError_t launch_ww_layout(double* ww, double* F1, double* F2, double* F3, size_t N, bool to_planes,
+                             cudaStream_t s);
+// guard bit 2's zero normal-field fluxes and the CT values into the flux planes
+cudaError_t launch_ct_apply(const DevRun& r, const double* CT, double* F1, double* F2, double* F3, cudaStream_t s);
 // corner-centred div(sqrt(-g) B) of P over the interior: red[0] = max |D|,
 // red[1] = max |sqrt(-g) B^d| / dx_d (bit patterns of doubles)
 cudaError_t launch_divb(const DevRun& r, const double* P, unsigned long long* red, cudaStream_t s);

@@ -303,7 +303,8 @@ __device__ __forceinline__ T ppm_face(T u0, T u1, T dma0, T dma1, T dxm, T dx0, 
 // Both face states of the cell at p (primitive v at p[v*N], storage type S),
 // stride st along direction D; dx[o+4], x[o+4] are the shifted spacing and
 // centre at offset o from the cell.  gam enters the contact test (rec.f90:1623).
-template <int D, typename T, typename S>
+// ALL: also the sixth variable (the per-routine rec2 outputs every face state).
+template <int D, typename T, typename S, bool ALL = false>
 __device__ void ppm_cell(const S* __restrict__ p, size_t N, long long st, const T dx[9], const T x[9], T gam,
                          T L[9], T R[9]) {
   auto U = [&](int v, int o) { return T(p[(size_t)v * N + o * st]); };
@@ -358,7 +359,7 @@ __device__ void ppm_cell(const S* __restrict__ p, size_t N, long long st, const 
   }
 #pragma unroll 1
   for (int v = 0; v < 9; ++v) {
-    if (v == 5) { L[v] = T(0); R[v] = T(0); continue; }  // var 6 faces are never read downstream
+    if (v == 5 && !ALL) { L[v] = T(0); R[v] = T(0); continue; }  // var 6 faces are never read downstream
     const T um2 = U(v, -2), um1 = U(v, -1), u0 = U(v, 0), up1 = U(v, 1), up2 = U(v, 2);
     const T dm = ppm_dma(um2, um1, u0, DX(-2), DX(-1), DX(0), D == 3);
     const T d0 = ppm_dma(um1, u0, up1, DX(-1), DX(0), DX(1), D == 3);

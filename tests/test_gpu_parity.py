@@ -609,3 +609,86 @@ def test_recov2(gpu_ctx, nph):
     with pytest.raises(RgError):
         gpu_ctx.step_batch([r])
     r.release()
+
+
+def _hll_region(o):
+    """Slices (k, j, i) of the hll range nm0..n-nm0 (1-based) in every direction."""
+    m = o.nm1 - o.params.get("ict", 1) - 1  # nm0 - 1
+    return (slice(m, -(m + 1)),) * 3
+
+
+def _rel(a, b, axis):
+    """max |a-b| relative to the largest |b| of the same variable over all six
+    face arrays (a component that vanishes in exact arithmetic on one face
+    carries the round-off residue of the others' size)."""
+    axis = (0,) + tuple(axis)
+    scale = np.maximum(np.abs(b).max(axis=axis), 1e-300)
+    return (np.abs(a - b).max(axis=axis) / scale).max()
+
+
+@pytest.mark.parametrize("irec,guard", [(config.IREC_MP5, 1), (config.IREC_MP5, 3), (config.IREC_PPM, 0),
+                                        (config.IREC_WENO5, 1), (config.IREC_MC, 1)])
+def test_rec2_calcha_hll_ct_one_at_a_time(gpu_ctx, irec, guard):
+    """rg_rec2, rg_calcha, rg_hll and rg_ct, each fed the oracle's inputs,
+    against the oracle's rec2 (with caluu3/calflx3), calcha, hll and ct on the
+    hll range; chained on the device they give rg_calflx's fluxes."""
+    p = dict(config.torus(nr=48, nth=40, nph=12, irec=irec), guard=guard)
+    o, r = _pair(gpu_ctx, p, seed=19)
+    u = o.prims()
+    reg = (slice(None),) + _hll_region(o)
+    fo = o.rec2_full(u)
+    fd = r.rec2(u)
+    for a, b in zip(fd, fo):  # face primitives, conserved variables, fluxes
+        assert _rel(a[reg], b[reg], (1, 2, 3)) < TOL
+    cho = o.calcha(fo[0])
+    chd = r.calcha(fo[0])
+    assert _rel(chd[reg], cho[reg], (1, 2, 3)) < TOL
+    ww0 = np.random.default_rng(3).standard_normal(u.shape + (3,))
+    wo = o.hll(fo[1], fo[2], cho, ww0)
+    wd = r.hll(fo[1], fo[2], cho, ww0)
+    assert flux_err(wd, wo).max() < TOL
+    co, cd = o.ct(u, wo), r.ct(u, wo)
+    assert flux_err(cd, co).max() < TOL
+    # the device chain equals the fused call
+    chain = r.ct(u, r.hll(fd[1], fd[2], r.calcha(fd[0]), ww0))
+    fused = r.calflx(u)
+    n = o.nm1 - 1
+    sl = (slice(n, -n),) * 3
+    assert flux_err(chain[sl], fused[sl]).max() < TOL
+    r.release()
+
+
+def test_per_routine_entry_points_take_device_arrays(gpu_ctx):
+    """The reference-interface entry points accept device pointers in place
+    of host arrays (cudaMemcpyDefault): a driver that keeps its arrays on the
+    GPU gets the same results without host copies."""
+    import torch
+
+    from raishinsource_b200.capi import _check
+    p = dict(config.torus(nr=40, nth=32, nph=12), guard=1)
+    o, r = _pair(gpu_ctx, p, seed=23)
+    u = o.prims()
+    lib, h, rid = r.lib, gpu_ctx.h, r.id
+    du = torch.from_numpy(u).cuda()
+
+    def dev(shape):
+        return torch.zeros(shape, dtype=torch.float64, device="cuda")
+
+    uu = dev(u.shape)
+    _check(lib, lib.rg_caluu1(h, rid, ctypes_ptr(du), ctypes_ptr(uu)))
+    assert np.array_equal(uu.cpu().numpy(), r.caluu1(u))
+    ww = dev(u.shape + (3,))
+    _check(lib, lib.rg_calflx(h, rid, ctypes_ptr(du), ctypes_ptr(ww)))
+    assert np.array_equal(ww.cpu().numpy(), r.calflx(u))
+    fp = dev((6,) + u.shape)
+    _check(lib, lib.rg_rec2(h, rid, du.data_ptr(), fp.data_ptr(), None, None))
+    assert np.array_equal(fp.cpu().numpy(), r.rec2(u, cons=False)[0])
+    sf = dev(u.shape[:3] + (4,))
+    _check(lib, lib.rg_calsf(h, rid, ctypes_ptr(du), ctypes_ptr(sf)))
+    assert np.array_equal(sf.cpu().numpy(), r.calsf(u))
+    r.release()
+
+
+def ctypes_ptr(t):
+    import ctypes
+    return ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))
