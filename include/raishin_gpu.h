@@ -238,6 +238,15 @@ int rg_recov(rg_ctx* ctx, int run, const double* uu, double* uri);
 int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl);
 /* bnd4 + infchk + atmosphere1a + pminmax2b (bnd.f90, correction.f90) on uri in/out */
 int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio);
+/* The same four one at a time (main.f90:860-878), uri in/out: bnd4
+ * (bnd.f90:4-1058, single-rank branches; urio the previous state), infchk
+ * (bnd.f90:1636-1824, for models 7-20), atmosphere1a (correction.f90:226-447,
+ * models 7-15) and pminmax2b (correction.f90:744-999), each with the model
+ * condition the reference's driver applies. */
+int rg_bnd4(rg_ctx* ctx, int run, double* uri, const double* urio);
+int rg_infchk(rg_ctx* ctx, int run, double* uri);
+int rg_atmosphere1a(rg_ctx* ctx, int run, double* uri);
+int rg_pminmax2b(rg_ctx* ctx, int run, double* uri);
 /* caltenr + calsf (calsf.f90:6-151) on every cell: sf(2:5,i,j,k), 4 doubles
  * per cell */
 int rg_calsf(rg_ctx* ctx, int run, const double* uri, double* sf);

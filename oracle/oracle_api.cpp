@@ -253,6 +253,19 @@ double orc_cdtcfl(void* h, const double* uri) {
 }
 
 // bnd4 + infchk + atmosphere1a + pminmax2b on uri (in/out) with urio
+// One of bnd4 (which 0), infchk (1), atmosphere1a (2), pminmax2b (3) alone on
+// uri in place, each with the reference's model condition (main.f90:860-878).
+void orc_bnd_part(void* h, int which, double* uri, const double* urio) {
+  State* s = static_cast<State*>(h);
+  std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));
+  if (urio) std::memcpy(s->urio.data(), urio, s->urio.size() * sizeof(double));
+  if (which == 0) orc::bnd4(*s);
+  else if (which == 1) { if (s->p.model >= 7 && s->p.model <= 20) orc::infchk(*s); }
+  else if (which == 2) { if (s->p.model >= 7 && s->p.model <= 15) orc::atmosphere1a(*s); }
+  else orc::pminmax2b(*s);
+  std::memcpy(uri, s->uri.data(), s->uri.size() * sizeof(double));
+}
+
 void orc_bnd_floor(void* h, double* uri, const double* urio) {
   State* s = static_cast<State*>(h);
   std::memcpy(s->uri.data(), uri, s->uri.size() * sizeof(double));

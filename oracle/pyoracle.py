@@ -80,6 +80,7 @@ def _lib():
         lib.orc_get_array.argtypes = [P, C.c_char_p, D, C.c_longlong]
         lib.orc_get_array.restype = C.c_longlong
         lib.orc_rec2_full.argtypes = [P, D, D, D, D]
+        lib.orc_bnd_part.argtypes = [P, C.c_int, D, D]
         lib.orc_calcha.argtypes = [P, D, D]
         lib.orc_hll.argtypes = [P, D, D, D, D]
         lib.orc_output1.argtypes = [P, C.c_char_p, C.c_int, C.c_int]
@@ -288,6 +289,17 @@ class Oracle:
         """Write the current primitives as output1's structr file (restar.f90:91-185)."""
         if self.lib.orc_output1(self.h, os.fsencode(path), myrank, npe) != 0:
             raise OSError("orc_output1 failed: " + path)
+
+    def bnd_part(self, which: str, uri, urio=None):
+        """bnd4, infchk, atmosphere1a or pminmax2b alone; returns the updated copy of uri."""
+        out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
+        po = None
+        if urio is not None:
+            urio = np.ascontiguousarray(urio, dtype=np.float64).reshape(self.shape)
+            po = _ptr(urio)
+        code = {"bnd4": 0, "infchk": 1, "atmosphere1a": 2, "pminmax2b": 3}[which]
+        self.lib.orc_bnd_part(self.h, code, _ptr(out), po)
+        return out
 
     def bnd_floor(self, uri, urio):
         uri = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)

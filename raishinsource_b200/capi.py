@@ -29,7 +29,7 @@ EXPORTS = ("rg_last_error", "rg_ctx_create", "rg_ctx_destroy", "rg_sync", "rg_ct
            "rg_ctx_set_stream", "rg_run_admit", "rg_run_release",
            "rg_prep_create", "rg_prep_ic_torus", "rg_run_admit_prep", "rg_prep_destroy",
            "rg_run_footprint", "rg_run_ic_torus", "rg_run_ic_torus_device", "rg_run_ic_tube", "rg_run_upload_prims", "rg_run_download_prims", "rg_run_layout", "rg_run_download_stored", "rg_step",
-           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_rec2", "rg_calcha", "rg_hll", "rg_ct", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_divb", "rg_run_horizon_flux", "rg_run_radial_flux", "rg_run_store", "rg_run_restore", "rg_run_output", "rg_pow_eval", "rg_calflx_static")
+           "rg_run_stats", "rg_step_batch", "rg_batch_info", "rg_profile", "rg_profile_read", "rg_caluu1", "rg_calflx", "rg_rec2", "rg_calcha", "rg_hll", "rg_ct", "rg_recov", "rg_cdtcfl", "rg_bnd_floor", "rg_bnd4", "rg_infchk", "rg_atmosphere1a", "rg_pminmax2b", "rg_calsf", "rg_rkt", "rg_run_derived", "rg_run_divb", "rg_run_horizon_flux", "rg_run_radial_flux", "rg_run_store", "rg_run_restore", "rg_run_output", "rg_pow_eval", "rg_calflx_static")
 
 
 class RgError(RuntimeError):
@@ -125,6 +125,9 @@ def load(path: str = LIB_PATH):
     lib.rg_ct.argtypes = [P, I, C.c_void_p, C.c_void_p]
     lib.rg_cdtcfl.argtypes = [P, I, D, D]
     lib.rg_bnd_floor.argtypes = [P, I, D, D]
+    lib.rg_bnd4.argtypes = [P, I, D, D]
+    for f in ("rg_infchk", "rg_atmosphere1a", "rg_pminmax2b"):
+        getattr(lib, f).argtypes = [P, I, D]
     lib.rg_calsf.argtypes = [P, I, D, D]
     lib.rg_rkt.argtypes = [P, I, I, C.c_double, D, D, D, D, D]
     lib.rg_run_derived.argtypes = [P, I, I, D]
@@ -505,6 +508,18 @@ class Run:
         m, b = C.c_double(0), C.c_double(0)
         _check(self.lib, self.lib.rg_run_divb(self.ctx.h, self.id, C.byref(m), C.byref(b)))
         return m.value, b.value
+
+    def bnd_part(self, which: str, uri, urio=None) -> np.ndarray:
+        """bnd4 (needs urio), infchk, atmosphere1a or pminmax2b alone; the updated copy of uri."""
+        out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)
+        if which == "bnd4":
+            urio = np.ascontiguousarray(urio, dtype=np.float64).reshape(self.shape)
+            _check(self.lib, self.lib.rg_bnd4(self.ctx.h, self.id, _dptr(out), _dptr(urio)))
+        else:
+            fn = {"infchk": self.lib.rg_infchk, "atmosphere1a": self.lib.rg_atmosphere1a,
+                  "pminmax2b": self.lib.rg_pminmax2b}[which]
+            _check(self.lib, fn(self.ctx.h, self.id, _dptr(out)))
+        return out
 
     def bnd_floor(self, uri, urio) -> np.ndarray:
         out = np.array(uri, dtype=np.float64, order="C").reshape(self.shape)

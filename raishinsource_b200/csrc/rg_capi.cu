@@ -1882,6 +1882,37 @@ int rg_cdtcfl(rg_ctx* ctx, int run, const double* uri, double* dtcfl) {
   return RG_OK;
 }
 
+int rg_bnd4(rg_ctx* ctx, int run, double* uri, const double* urio) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!uri || !urio) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false))) return rc;
+  if ((rc = to_soa(ctx, R, urio, B->stage2, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
+  RG_CUDA(launch_bc(d, B->stage, B->stage2, ctx->stream));
+  return from_soa(ctx, R, B->stage, uri, d);
+}
+
+namespace {
+int floor_part(rg_ctx* ctx, int run, int part, double* uri) {
+  Run* R = find(ctx, run);
+  if (!R) return fail(RG_ENOTFOUND, "unknown run");
+  if (!uri) return fail(RG_EINVAL_CONFIG, "null array");
+  const DevRun d = full_view(R);
+  DevBufs* B = nullptr;
+  int rc = full_bufs(R, ctx->stream, &B);
+  if (rc || (rc = to_soa(ctx, R, uri, B->stage, d, false)) || (rc = reset_fscal(ctx, R))) return rc;
+  RG_CUDA(launch_floor_part(d, part, B->stage, ctx->stream));
+  return from_soa(ctx, R, B->stage, uri, d);
+}
+}  // namespace
+
+int rg_infchk(rg_ctx* ctx, int run, double* uri) { return floor_part(ctx, run, 1, uri); }
+int rg_atmosphere1a(rg_ctx* ctx, int run, double* uri) { return floor_part(ctx, run, 2, uri); }
+int rg_pminmax2b(rg_ctx* ctx, int run, double* uri) { return floor_part(ctx, run, 4, uri); }
+
 int rg_bnd_floor(rg_ctx* ctx, int run, double* uri, const double* urio) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");

@@ -1581,6 +1581,9 @@ __global__ void k_bc_phys(DevRun r, double* __restrict__ P, const double* __rest
 // (correction.f90:226-447) and pminmax2b (correction.f90:744-999) over every
 // cell, in place.  pminmax2b stores rho alone when its rescale loop changed rho
 // (the "elseif" at correction.f90:887-893).
+// PARTS selects the routines (bit 0 infchk, 1 atmosphere1a, 2 pminmax2b) for
+// the per-routine entry points; the step runs all three.
+template <int PARTS = 7>
 __device__ __forceinline__ void floor_body(const DevRun& r, double* __restrict__ P, const uint3 bid) {
   if (!r.scal->active) return;
   const int i = bid.x * blockDim.x + threadIdx.x + 1;
@@ -1593,7 +1596,7 @@ __device__ __forceinline__ void floor_body(const DevRun& r, double* __restrict__
   Met m;
   load_met(r.mc, r.nik, r.ik(i, k), m);
   const double gam = r.gam;
-  if (r.model >= 7 && r.model <= 20 && i > r.imax - r.nm1) {
+  if ((PARTS & 1) && r.model >= 7 && r.model <= 20 && i > r.imax - r.nm1) {
     const double gflmax = 10.0;
     double gfl = calgfl(q[1], q[2], q[3], m);
     double vel[4] = {0.0, q[1] * (1. / gfl), q[2] * (1. / gfl), q[3] * (1. / gfl)};
@@ -1605,7 +1608,7 @@ __device__ __forceinline__ void floor_body(const DevRun& r, double* __restrict__
       q[1] = vel[1] * gfl; q[2] = vel[2] * gfl; q[3] = vel[3] * gfl;
     }
   }
-  if (r.model >= 7 && r.model <= 15) {
+  if ((PARTS & 2) && r.model >= 7 && r.model <= 15) {
     const double epsilon = 1.e-2, gflmax = 10.0;
     const double demin = __ldg(r.fl_de + i - 1);
     const double prmin = __ldg(r.fl_pr + i - 1);
@@ -1623,7 +1626,7 @@ __device__ __forceinline__ void floor_body(const DevRun& r, double* __restrict__
     }
     q[5] = 0.0;
   }
-  {  // pminmax2b
+  if (PARTS & 4) {  // pminmax2b
     const double gflmax = 20.0;
     double de = q[0], pr = q[4];
     double gfl = calgfl(q[1], q[2], q[3], m);
@@ -1676,6 +1679,10 @@ __device__ __forceinline__ void floor_body(const DevRun& r, double* __restrict__
     for (int v = 0; v < 9; ++v) r.P32[(size_t)v * N + c] = (float)q[v];
 }
 __global__ void __launch_bounds__(128) k_floor(DevRun r, double* __restrict__ P) { floor_body(r, P, blockIdx); }
+template <int PARTS>
+__global__ void __launch_bounds__(128) k_floor_part(DevRun r, double* __restrict__ P) {
+  floor_body<PARTS>(r, P, blockIdx);
+}
 
 // FP32 copy of a primitive array (mixed runs, after initial data or upload).
 __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
@@ -2548,6 +2555,15 @@ cudaError_t launch_ww_layout(double* ww, double* F1, double* F2, double* F3, siz
 cudaError_t launch_ct_apply(const DevRun& r, const double* CT, double* F1, double* F2, double* F3, cudaStream_t s) {
   const dim3 b(64, 2, 1);
   k_ct_apply<<<grid3(r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, CT, F1, F2, F3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_floor_part(const DevRun& r, int part, double* P, cudaStream_t s) {
+  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 g = sgrid(r, r.imax, r.jmax, r.kmax, b);
+  if (part == 1) k_floor_part<1><<<g, b, 0, s>>>(r, P);
+  else if (part == 2) k_floor_part<2><<<g, b, 0, s>>>(r, P);
+  else k_floor_part<4><<<g, b, 0, s>>>(r, P);
   return cudaGetLastError();
 }
 

@@ -40,6 +40,8 @@ cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const do
                           const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s);
 cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t s);
 cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s);
+// one floor routine alone: part 1 infchk, 2 atmosphere1a, 4 pminmax2b
+cudaError_t launch_floor_part(const DevRun& r, int part, double* P, cudaStream_t s);
 // per-routine entry points
 cudaError_t launch_recov_only(const DevRun& r, const double* U, const double* Pold, double* Pw, cudaStream_t s);
 // One RK stage of a recov2 run after its fluxes and CT: the CT values are

@@ -692,3 +692,22 @@ def test_per_routine_entry_points_take_device_arrays(gpu_ctx):
 def ctypes_ptr(t):
     import ctypes
     return ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))
+
+
+@pytest.mark.parametrize("which", ["bnd4", "infchk", "atmosphere1a", "pminmax2b"])
+def test_bnd4_and_floors_one_at_a_time(torus3d, which):
+    """bnd4, infchk, atmosphere1a and pminmax2b as separate calls (main.f90:860-878)
+    on a perturbed state that triggers the floors, against the oracle's routines."""
+    _, o, r = torus3d
+    u = o.prims()
+    rng = np.random.default_rng(11)
+    pert = u.copy()
+    pert[..., 0] *= np.exp(rng.uniform(-4.0, 0.5, pert.shape[:3]))  # densities below the floor, some
+    pert[..., 1:4] *= 1 + 3 * rng.standard_normal(pert.shape[:3] + (3,))
+    urio = u
+    got = r.bnd_part(which, pert, urio)
+    want = o.bnd_part(which, pert, urio if which == "bnd4" else None)
+    assert np.isfinite(got).all()
+    err = field_err(got, want)
+    assert err[[0, 1, 2, 3, 4, 6, 7, 8]].max() < TOL, err
+    assert not np.array_equal(want, pert) or which == "infchk"
