@@ -162,7 +162,7 @@ void make_tmaps(Run* R) {
   auto encode = [&](CUtensorMap* tm, void* base, int eb, int dir) {
     const cuuint64_t strides[3] = {(cuuint64_t)d.imax * eb, (cuuint64_t)d.imax * d.jmax * eb, (cuuint64_t)d.N * eb};
     unsigned box[4];
-    flux_tma_box(dir, eb, box);
+    flux_tma_box(dir, eb, d.irec, box);
     const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
     return enc(tm, eb == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims,
                strides, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

@@ -1105,7 +1105,7 @@ template <int D, int IREC, typename T, typename S>
 __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_flux(DevRun r, const S* __restrict__ P, S* __restrict__ F,
                                               float* __restrict__ Fcopy, int icopy, int ilo, int ihi) { flux_body<D, IREC, T, S>(r, P, F, Fcopy, icopy, ilo, ihi, blockIdx); }
 
-// The MP5 face kernel with its stencil staged in shared memory by one TMA
+// The face kernel (PPM, MP5, WENO5, WENO-Z, WENO-M) with its stencil staged in shared memory by one TMA
 // tile load per block (cp.async.bulk.tensor, this GPU's own buffer, no
 // multicast), in FP64 (S = double) or for the FP32 half of the mixed path
 // (S = float, over P32).  A block takes the same 32 x 2 faces as k_flux (32
@@ -1123,13 +1123,22 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_fl
 // once more (bounded) for the copy and returns without computing; the host
 // reports RG_ECUDA.
 constexpr int kTmaWaitCap = 1 << 22;
-template <int D, typename S>
+// LO: cells a face's state reads beyond its owner cell on either side (2
+// for the five-point schemes; 3 for PPM, whose flattening reads the pressure
+// three cells out), so the faces f of a block need cells f-LO .. f+1+LO.
+template <int D, typename S, int LO>
 struct TmaBox {
-  static constexpr int X = (D == 1) ? 40 : (sizeof(S) == 8 ? 34 : 36), Y = (D == 2) ? 7 : 2, Z = (D == 3) ? 6 : 1;
+  static constexpr int ALIGN = 16 / (int)sizeof(S);  // elements per 16 bytes
+  __host__ __device__ static constexpr int up(int n) { return (n + ALIGN - 1) / ALIGN * ALIGN; }
+  // along D: 32 faces + 2 LO + 1 cells, plus the alignment slack; across: 32 faces plus slack
+  static constexpr int X = (D == 1) ? up(33 + 2 * LO + ALIGN - 1) : up(32 + ALIGN - 1);
+  static constexpr int Y = (D == 2) ? 2 + 2 * LO + 1 : 2;
+  static constexpr int Z = (D == 3) ? 1 + 2 * LO + 1 : 1;
   static constexpr int PLANE = X * Y * Z;                                   // cells per variable
   static constexpr unsigned BYTES = (unsigned)PLANE * 9u * (unsigned)sizeof(S);  // whole box
-  static constexpr int ALIGN = 16 / (int)sizeof(S);                         // elements per 16 bytes
 };
+template <int IREC>
+__host__ __device__ constexpr int tma_lo() { return IREC == 5 ? 3 : 2; }
 
 __device__ __forceinline__ bool tma_wait(unsigned bar) {
   unsigned done = 0;
@@ -1142,22 +1151,23 @@ __device__ __forceinline__ bool tma_wait(unsigned bar) {
   return done != 0;
 }
 
-template <int D, typename T, typename S>
+template <int D, int IREC, typename T, typename S>
 __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
     k_flux_tma(const __grid_constant__ CUtensorMap tm, DevRun r, S* __restrict__ F, float* __restrict__ Fcopy,
                int icopy, int ilo, int ihi) {
   extern __shared__ __align__(128) unsigned char box_raw[];
   __shared__ __align__(8) unsigned long long bar;
   if (!r.scal->active) return;
-  using B = TmaBox<D, S>;
+  using B = TmaBox<D, S, tma_lo<IREC>()>;
   S* box = reinterpret_cast<S*>(box_raw);
   const int nm0 = r.nm0;
   const int fi0 = ilo + (int)blockIdx.x * 32, fj0 = nm0 + 2 * (int)blockIdx.y, fk0 = nm0 + (int)blockIdx.z;
   // 0-based origin of the box: the first stencil cell along D, the block's
   // first face elsewhere; along i rounded down to a 16-byte boundary
-  const int x0 = ((D == 1) ? fi0 - 3 : fi0 - 1) & ~(B::ALIGN - 1);
-  const int y0 = (D == 2) ? fj0 - 3 : fj0 - 1;
-  const int z0 = (D == 3) ? fk0 - 3 : fk0 - 1;
+  constexpr int LO = tma_lo<IREC>();
+  const int x0 = ((D == 1) ? fi0 - 1 - LO : fi0 - 1) & ~(B::ALIGN - 1);
+  const int y0 = (D == 2) ? fj0 - 1 - LO : fj0 - 1;
+  const int z0 = (D == 3) ? fk0 - 1 - LO : fk0 - 1;
   const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
   const unsigned box_a = (unsigned)__cvta_generic_to_shared(box_raw);
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
@@ -1183,7 +1193,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
   const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(fk0, r.kmax - nm0);
   const size_t vc = (size_t)((i - 1 - x0) + B::X * ((j - 1 - y0) + B::Y * (k - 1 - z0)));
   const long long vst = (D == 1) ? 1 : (D == 2 ? B::X : B::X * B::Y);
-  face_lane<D, 6, T, S, true>(r, nullptr, F, Fcopy, icopy, i, j, k, side, valid, box, B::PLANE, vc, vst);
+  face_lane<D, IREC, T, S, true>(r, nullptr, F, Fcopy, icopy, i, j, k, side, valid, box, B::PLANE, vc, vst);
 }
 
 // ------------------------------------------- per-routine rec2 / calcha / hll
@@ -2200,11 +2210,28 @@ static int fp64_split(const DevRun& r, int lo, int hi) {
   return r.i_fp64 < lo ? lo - 1 : (r.i_fp64 > hi ? hi : r.i_fp64);
 }
 
+// The staged kernel covers the reconstructions whose lanes read their
+// stencil alone, at most two cells either side of the owner cell (the box
+// holds i-2 .. i+3 of its faces): PPM, MP5, WENO5, WENO-Z and WENO-M, whose
+// ghost widths (nm0 = 3, 4) keep the box origin at or above index 0.  MP-WENO
+// also reads a cell eleven away, the second-order schemes are cheap to read.
 bool flux_tma_eligible(const DevRun& r) {
-  return r.irec == 6 && r.nm0 == 3 && !r.jfix && !r.kfix && !r.kmet && (r.imax % 4) == 0 &&
+  const bool scheme = r.irec == 5 || r.irec == 6 || r.irec == 7 || r.irec == 9 || r.irec == 10;
+  return scheme && r.nm0 >= 3 && !r.jfix && !r.kfix && !r.kmet && (r.imax % 4) == 0 &&
          r.N == (size_t)r.imax * r.jmax * r.kmax;
 }
 
+template <int IREC, typename T, typename S>
+static void launch_flux_tma_irec(const DevRun& r, int dir, const CUtensorMap& tm, S* F, float* Fcopy, int icopy,
+                                 int ilo, int ihi, dim3 g, dim3 b, cudaStream_t s) {
+  constexpr int LO = tma_lo<IREC>();
+  if (dir == 1)
+    k_flux_tma<1, IREC, T, S><<<g, b, TmaBox<1, S, LO>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+  else if (dir == 2)
+    k_flux_tma<2, IREC, T, S><<<g, b, TmaBox<2, S, LO>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+  else
+    k_flux_tma<3, IREC, T, S><<<g, b, TmaBox<3, S, LO>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+}
 template <typename T, typename S>
 static void launch_flux_tma_t(const DevRun& r, int dir, const CUtensorMap& tm, S* F, float* Fcopy, int icopy,
                               int ilo, int ihi, cudaStream_t s) {
@@ -2212,9 +2239,13 @@ static void launch_flux_tma_t(const DevRun& r, int dir, const CUtensorMap& tm, S
   const int n = ihi - ilo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b(64, 2, 1);
   const dim3 g((unsigned)((n + 31) / 32), (unsigned)((m + 1) / 2), (unsigned)l);
-  if (dir == 1) k_flux_tma<1, T, S><<<g, b, TmaBox<1, S>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
-  else if (dir == 2) k_flux_tma<2, T, S><<<g, b, TmaBox<2, S>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
-  else k_flux_tma<3, T, S><<<g, b, TmaBox<3, S>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+  switch (r.irec) {
+    case 5: launch_flux_tma_irec<5, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    case 7: launch_flux_tma_irec<7, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    case 9: launch_flux_tma_irec<9, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    case 10: launch_flux_tma_irec<10, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    default: launch_flux_tma_irec<6, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+  }
 }
 
 cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const void* tmap32, double* F,
@@ -2234,15 +2265,22 @@ cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const 
   return cudaGetLastError();
 }
 
-void flux_tma_box(int dir, int elem_bytes, unsigned box[4]) {
-  if (elem_bytes == 8) {
-    box[0] = dir == 1 ? TmaBox<1, double>::X : (dir == 2 ? TmaBox<2, double>::X : TmaBox<3, double>::X);
-  } else {
-    box[0] = dir == 1 ? TmaBox<1, float>::X : (dir == 2 ? TmaBox<2, float>::X : TmaBox<3, float>::X);
-  }
-  box[1] = dir == 2 ? 7 : 2;
-  box[2] = dir == 3 ? 6 : 1;
+template <typename S, int LO>
+static void tma_box_of(int dir, unsigned box[4]) {
+  box[0] = dir == 1 ? TmaBox<1, S, LO>::X : (dir == 2 ? TmaBox<2, S, LO>::X : TmaBox<3, S, LO>::X);
+  box[1] = dir == 1 ? TmaBox<1, S, LO>::Y : (dir == 2 ? TmaBox<2, S, LO>::Y : TmaBox<3, S, LO>::Y);
+  box[2] = dir == 1 ? TmaBox<1, S, LO>::Z : (dir == 2 ? TmaBox<2, S, LO>::Z : TmaBox<3, S, LO>::Z);
   box[3] = 9;
+}
+void flux_tma_box(int dir, int elem_bytes, int irec, unsigned box[4]) {
+  const bool ppm = (irec == 5);
+  if (elem_bytes == 8) {
+    if (ppm) tma_box_of<double, tma_lo<5>()>(dir, box);
+    else tma_box_of<double, tma_lo<6>()>(dir, box);
+  } else {
+    if (ppm) tma_box_of<float, tma_lo<5>()>(dir, box);
+    else tma_box_of<float, tma_lo<6>()>(dir, box);
+  }
 }
 
 cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s) {

@@ -25,12 +25,13 @@ cudaError_t launch_step_begin(const DevRun& r, cudaStream_t s);
 cudaError_t launch_dt(const DevRun& r, cudaStream_t s);
 cudaError_t launch_step_end(const DevRun& r, cudaStream_t s);
 cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cudaStream_t s);
-// MP5 faces of a run stored in full (no slab direction, imax a multiple of
-// 4) with the stencil staged in shared memory by TMA: tmap64 is the
+// Faces (PPM, MP5, WENO5, WENO-Z, WENO-M) of a run stored in full (no slab
+// direction, imax a multiple of 4) with the stencil staged in shared memory
+// by TMA: tmap64 is the
 // CUtensorMap of the FP64 primitive buffer, tmap32 that of P32 (mixed runs;
-// 4D: i, j, k, v; box flux_tma_box(dir, element bytes))
+// 4D: i, j, k, v; box flux_tma_box(dir, element bytes, irec))
 bool flux_tma_eligible(const DevRun& r);
-void flux_tma_box(int dir, int elem_bytes, unsigned box[4]);
+void flux_tma_box(int dir, int elem_bytes, int irec, unsigned box[4]);
 cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const void* tmap32, double* F,
                             cudaStream_t s);
 // P: the stage's primitives (upflct's upwinding reads their velocities)
