@@ -1512,7 +1512,8 @@ __device__ __forceinline__ size_t col_cell(const DevRun& r, int t1, int t2, int 
 // bnd.f90:45-70, 156-180, 266-292: single-rank periodic copy for columns whose
 // transverse indices are interior.
 template <int D>
-__device__ __forceinline__ void bc_periodic_body(const DevRun& r, double* __restrict__ P, const uint3 bid) {
+__device__ __forceinline__ void bc_periodic_body(const DevRun& r, double* __restrict__ P, const uint3 bid,
+                                                 int vlo = 0, int vhi = 9) {
   if (!r.scal->active) return;
   const int nm1 = r.nm1;
   const int n1 = (D == 1) ? r.jmax : r.imax;
@@ -1524,7 +1525,7 @@ __device__ __forceinline__ void bc_periodic_body(const DevRun& r, double* __rest
   const int ib0 = 1 + nm1, ib1 = len - nm1;
   const size_t N = r.N;
   for (int n = 1; n <= nm1; ++n)
-    for (int v = 0; v < 9; ++v) {
+    for (int v = vlo; v < vhi; ++v) {
       if (r.ibc[2 * (D - 1)][v] == 1 || r.ibc[2 * (D - 1) + 1][v] == 1) {
         double* p = P + (size_t)v * N;
         p[col_cell<D>(r, t1, t2, ib0 - n)] = p[col_cell<D>(r, t1, t2, ib1 + 1 - n)];
@@ -1532,12 +1533,18 @@ __device__ __forceinline__ void bc_periodic_body(const DevRun& r, double* __rest
       }
     }
 }
+// The standalone passes take one variable per grid z index (the variables of
+// a column are independent: each code reads only its own variable, and the
+// outflow check of code 18 an interior cell).
 template <int D>
-__global__ void k_bc_periodic(DevRun r, double* __restrict__ P) { bc_periodic_body<D>(r, P, blockIdx); }
+__global__ void k_bc_periodic(DevRun r, double* __restrict__ P) {
+  bc_periodic_body<D>(r, P, blockIdx, (int)blockIdx.z, (int)blockIdx.z + 1);
+}
 
 // bnd.f90:384-1058: physical boundary codes for every column of direction D.
 template <int D>
-__device__ __forceinline__ void bc_phys_body(const DevRun& r, double* __restrict__ P, const double* __restrict__ Po, const uint3 bid) {
+__device__ __forceinline__ void bc_phys_body(const DevRun& r, double* __restrict__ P, const double* __restrict__ Po,
+                                             const uint3 bid, int vlo = 0, int vhi = 9) {
   if (!r.scal->active) return;
   const int n1 = (D == 1) ? r.jmax : r.imax;
   const int n2 = (D == 3) ? r.jmax : r.kmax;
@@ -1547,7 +1554,7 @@ __device__ __forceinline__ void bc_phys_body(const DevRun& r, double* __restrict
   const int nm1 = r.nm1;
   const int L = (D == 1) ? r.imax : (D == 2 ? r.jmax : r.kmax);
   const size_t N = r.N;
-  for (int v = 0; v < 9; ++v) {
+  for (int v = vlo; v < vhi; ++v) {
     double* u = P + (size_t)v * N;
     const double* uo = Po + (size_t)v * N;
     auto at = [&](int n) { return col_cell<D>(r, t1, t2, n); };
@@ -1584,7 +1591,9 @@ __device__ __forceinline__ void bc_phys_body(const DevRun& r, double* __restrict
   }
 }
 template <int D>
-__global__ void k_bc_phys(DevRun r, double* __restrict__ P, const double* __restrict__ Po) { bc_phys_body<D>(r, P, Po, blockIdx); }
+__global__ void k_bc_phys(DevRun r, double* __restrict__ P, const double* __restrict__ Po) {
+  bc_phys_body<D>(r, P, Po, blockIdx, (int)blockIdx.z, (int)blockIdx.z + 1);
+}
 
 // ----------------------------------------------------------------- floors
 // infchk (bnd.f90:1636-1824, outer radial ghosts), atmosphere1a
@@ -2335,12 +2344,17 @@ cudaError_t launch_ct(const DevRun& r, const double* P, const double* F1, const 
   return cudaGetLastError();
 }
 
+// Block of the stage update: RG_UPDATE_BX cells along i times 128 / RG_UPDATE_BX
+// rows along j (the rows share the metric of their (i, k) points).
+#ifndef RG_UPDATE_BX
+#define RG_UPDATE_BX 64
+#endif
 template <bool MIX>
 static void launch_update_t(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                             const double* F1, const double* F2, const double* F3, const double* CT, int ilo,
                             int ihi, cudaStream_t s) {
   if (ihi < ilo) return;
-  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 b = sblock(r, dim3(RG_UPDATE_BX, 128 / RG_UPDATE_BX, 1));
   const dim3 g = sgrid(r, ihi - ilo + 1, r.jmax, r.kmax, b);
   if (stage == 1) k_update<1, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
   else if (stage == 2) k_update<2, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
@@ -2406,6 +2420,11 @@ static void bc_shape(int n1, int n2, bool fix1, bool fix2, dim3& g, dim3& b) {
   b = dim3(fix1 ? 1 : (fix2 ? 128 : 32), fix2 ? 1 : (fix1 ? 128 : 4), 1);
   g = grid3(fix1 ? 1 : n1, fix2 ? 1 : n2, 1, b);
 }
+// The standalone passes: one variable per grid z index.
+static void bc_shape9(int n1, int n2, bool fix1, bool fix2, dim3& g, dim3& b) {
+  bc_shape(n1, n2, fix1, fix2, g, b);
+  g.z = 9;
+}
 
 int n_bc_launches(const DevRun& r) {
   int n = 0;
@@ -2424,27 +2443,27 @@ cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t
   // periodic passes on interior columns (bndpefb4), then physical passes on all
   // columns (bndryfb4); a slab direction's own passes copy its plane onto itself
   if (any_code(r, 0, true)) {
-    bc_shape(r.jmax - 2 * nm1, r.kmax - 2 * nm1, jf, kf, g, b);
+    bc_shape9(r.jmax - 2 * nm1, r.kmax - 2 * nm1, jf, kf, g, b);
     k_bc_periodic<1><<<g, b, 0, s>>>(r, P);
   }
   if (!jf && any_code(r, 2, true)) {
-    bc_shape(r.imax - 2 * nm1, r.kmax - 2 * nm1, false, kf, g, b);
+    bc_shape9(r.imax - 2 * nm1, r.kmax - 2 * nm1, false, kf, g, b);
     k_bc_periodic<2><<<g, b, 0, s>>>(r, P);
   }
   if (!kf && any_code(r, 4, true)) {
-    bc_shape(r.imax - 2 * nm1, r.jmax - 2 * nm1, false, jf, g, b);
+    bc_shape9(r.imax - 2 * nm1, r.jmax - 2 * nm1, false, jf, g, b);
     k_bc_periodic<3><<<g, b, 0, s>>>(r, P);
   }
   if (any_code(r, 0, false)) {
-    bc_shape(r.jmax, r.kmax, jf, kf, g, b);
+    bc_shape9(r.jmax, r.kmax, jf, kf, g, b);
     k_bc_phys<1><<<g, b, 0, s>>>(r, P, Po);
   }
   if (!jf && any_code(r, 2, false)) {
-    bc_shape(r.imax, r.kmax, false, kf, g, b);
+    bc_shape9(r.imax, r.kmax, false, kf, g, b);
     k_bc_phys<2><<<g, b, 0, s>>>(r, P, Po);
   }
   if (!kf && any_code(r, 4, false)) {
-    bc_shape(r.imax, r.jmax, false, jf, g, b);
+    bc_shape9(r.imax, r.jmax, false, jf, g, b);
     k_bc_phys<3><<<g, b, 0, s>>>(r, P, Po);
   }
   return cudaGetLastError();
