@@ -64,6 +64,9 @@ struct Run {
   CUtensorMap tmap[3][3];
   CUtensorMap tmap32[3];   // the FP32 copy P32 of a mixed run, per direction
   bool tma = false;
+  // tensor maps of the staged update (F1, F2, F3, CT, U^n; update_tma_box)
+  CUtensorMap umap[5];
+  bool utma = false;
 };
 
 }  // namespace
@@ -108,6 +111,7 @@ struct rg_ctx {
   bool own_stream = true;              // false after rg_ctx_set_stream
   cudaEvent_t marks[RG_MAX_MARKS] = {};  // rg_ctx_mark / rg_ctx_wait_mark
   bool tma = true;                     // staged face kernel where a run allows it (RAISHIN_FLUX_TMA=0: off)
+  bool utma = true;                    // staged update kernel where a run allows it (RAISHIN_UPDATE_TMA=0: off)
 };
 
 namespace {
@@ -149,31 +153,49 @@ EncodeTiledFn encode_tiled() {
 }
 
 // Tensor maps of the three primitive buffers (and of P32 for a mixed run) as
-// 4D arrays (i, j, k, v) with the boxes of the staged face kernel; a run they
-// do not fit keeps the generic face kernel.
+// 4D arrays (i, j, k, v) with the boxes of the staged face kernel, and of the
+// update's flux, flux-CT and U^n arrays with the boxes of the staged update;
+// a run they do not fit keeps the generic kernels.
 void make_tmaps(Run* R) {
   R->tma = false;
+  R->utma = false;
   const DevRun& d = R->d;
-  if (!flux_tma_eligible(d)) return;
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return;
-  const cuuint64_t dims[4] = {(cuuint64_t)d.imax, (cuuint64_t)d.jmax, (cuuint64_t)d.kmax, 9};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  auto encode = [&](CUtensorMap* tm, void* base, int eb, int dir) {
+  auto encode = [&](CUtensorMap* tm, void* base, int eb, int nv, const unsigned box[4]) {
+    const cuuint64_t dims[4] = {(cuuint64_t)d.imax, (cuuint64_t)d.jmax, (cuuint64_t)d.kmax, (cuuint64_t)nv};
     const cuuint64_t strides[3] = {(cuuint64_t)d.imax * eb, (cuuint64_t)d.imax * d.jmax * eb, (cuuint64_t)d.N * eb};
-    unsigned box[4];
-    flux_tma_box(dir, eb, d.irec, box);
     const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
     return enc(tm, eb == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims,
                strides, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   };
-  for (int dir = 1; dir <= 3; ++dir) {
-    for (int b = 0; b < 3; ++b)
-      if (!encode(&R->tmap[b][dir - 1], R->b.P[b], 8, dir)) return;
-    if (d.mixed && !encode(&R->tmap32[dir - 1], d.P32, 4, dir)) return;
+  if (flux_tma_eligible(d)) {
+    bool ok = true;
+    for (int dir = 1; dir <= 3 && ok; ++dir) {
+      unsigned box[4];
+      flux_tma_box(dir, 8, d.irec, box);
+      for (int b = 0; b < 3 && ok; ++b) ok = encode(&R->tmap[b][dir - 1], R->b.P[b], 8, 9, box);
+      if (ok && d.mixed) {
+        flux_tma_box(dir, 4, d.irec, box);
+        ok = encode(&R->tmap32[dir - 1], d.P32, 4, 9, box);
+      }
+    }
+    R->tma = ok;
   }
-  R->tma = true;
+  if (update_tma_eligible(d) && prepare_update_tma() == cudaSuccess) {
+    void* bases[5] = {R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, d.Un};
+    bool ok = true;
+    for (int w = 0; w < 5 && ok; ++w) {
+      unsigned box[4];
+      update_tma_box(w, box);
+      ok = encode(&R->umap[w], bases[w], 8, (int)box[3], box);
+    }
+    R->utma = ok;
+  } else {
+    (void)cudaGetLastError();
+  }
 }
 
 // Ghost widths of the reconstruction (main.f90:179-190): nm0 = 2 for the
@@ -567,7 +589,8 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
     }));
   } else {
     RG_CUDA(issue(ctx, K_UPDATE, n_update_launches(d), [&] {
-      return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s);
+      return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s,
+                           (R->utma && ctx->utma) ? static_cast<const void*>(R->umap) : nullptr);
     }));
   }
   RG_CUDA(issue(ctx, K_BC, n_bc_launches(d), [&] { return launch_bc(d, Pw, Pn, s); }));
@@ -592,7 +615,7 @@ int read_stats(rg_ctx* ctx, Run* R, rg_step_stats* st) {
   st->carry_overflow = (long long)c[C_CARRY_OVF];
   st->time = sc.timeh;
   st->dt = sc.dt;
-  if (c[C_TMAWAIT]) return fail(RG_ECUDA, "a TMA wait of the staged face kernel ran out");
+  if (c[C_TMAWAIT]) return fail(RG_ECUDA, "a TMA wait of a staged face or update kernel ran out");
   if (c[C_CARRY_OVF]) return fail(RG_EOVERFLOW, "W-carry list overflowed");
   if (c[C_CAP] || c[C_FLOORCAP]) return fail(RG_ENR_CAP, "a capped rescale loop was hit");
   return RG_OK;
@@ -830,6 +853,7 @@ int rg_ctx_create(int device, rg_ctx** out) {
   rg_ctx* c = new rg_ctx();
   c->device = device;
   if (const char* t = std::getenv("RAISHIN_FLUX_TMA")) c->tma = std::strcmp(t, "0") != 0;
+  if (const char* t = std::getenv("RAISHIN_UPDATE_TMA")) c->utma = std::strcmp(t, "0") != 0;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;

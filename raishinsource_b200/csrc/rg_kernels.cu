@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <functional>
 #include <vector>
 
@@ -522,34 +523,39 @@ __device__ __forceinline__ double rk_add_source(double u, double sf, double dt) 
 // Conserved state after the RK combine and source (rkt.f90:2-320) of one
 // interior cell.  U = P2C(P) always holds in the reference (caluu1 runs after
 // every stage, main.f90:899), so the stage inputs uu/uo/uh/us are recomputed
-// from the stored primitives here.
+// from the stored primitives here.  Two halves: stage_pre (P2C of the stage
+// input, U^n stored in stage 1, the geometric source) and stage_combine (the
+// RK combine with the flux differences and the source), which reads the flux
+// differences through an accessor: FluxDiffGlobal from the flux arrays, or
+// the shared-memory rows of the TMA-staged update.
 template <int STAGE>
-__device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pn,
-                          const double* __restrict__ Pc, const double* __restrict__ F1, const double* __restrict__ F2,
-                          const double* __restrict__ F3, const double* __restrict__ CT, double dt, double u[9]) {
+__device__ __forceinline__ void stage_pre(const DevRun& r, int i, int j, int k, const Met& m,
+                                          const double* __restrict__ Pc, double ucur[9], double sf[4]) {
   const size_t N = r.N, c = r.cell(i, j, k), q = r.ik(i, k);
   const double gam = r.gam;
   double qc[9];
   load9(Pc, N, c, qc);
   PS s;
   pstate(qc, m, gam, s);
-  double ucur[9];
   p2c(s, gam, r.gkind, m.detg, ucur);
   // U^n = P2C(P^n) is this stage's ucur in stage 1; stages 2 and 3 read it back
   if (STAGE == 1)
 #pragma unroll
     for (int v = 0; v < 9; ++v) r.Un[(size_t)v * N + c] = ucur[v];
   // geometric source (calsf.f90:6-151): S_nu = sqrt(-g) T^m_n Gamma^n_{nu m}
-  double sf[4];
   geom_source(r, s, q, m.detg, sf);
-  double uo[9];
-  if (STAGE > 1) load9(r.Un, N, c, uo);
-  const double a1 = dt / __ldg(r.dx1b + i - 1), a2 = dt / __ldg(r.dx2b + j - 1), a3 = dt / __ldg(r.dx3b + k - 1);
-  const size_t ci = c - 1, cj = c - r.sj, ck = c - r.sk;
-#pragma unroll
-  for (int v = 0; v < 9; ++v) {
-    // flux-CT replaces ww(2,7) ww(3,7) ww(1,8) ww(3,8) ww(1,9) ww(2,9) (ct.f90:98-109)
-    double d1, d2, d3;
+}
+
+// Flux differences of variable v along the three directions at cell c from
+// the flux arrays; flux-CT replaces ww(2,7) ww(3,7) ww(1,8) ww(3,8) ww(1,9)
+// ww(2,9) (ct.f90:98-109).
+struct FluxDiffGlobal {
+  const double* __restrict__ F1;
+  const double* __restrict__ F2;
+  const double* __restrict__ F3;
+  const double* __restrict__ CT;
+  size_t N, c, ci, cj, ck;
+  __device__ __forceinline__ void operator()(int v, double& d1, double& d2, double& d3) const {
     if (v == 7) d1 = CT[2 * N + c] - CT[2 * N + ci];
     else if (v == 8) d1 = CT[4 * N + c] - CT[4 * N + ci];
     else d1 = F1[(size_t)v * N + c] - F1[(size_t)v * N + ci];
@@ -559,10 +565,35 @@ __device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, co
     if (v == 6) d3 = CT[1 * N + c] - CT[1 * N + ck];
     else if (v == 7) d3 = CT[3 * N + c] - CT[3 * N + ck];
     else d3 = F3[(size_t)v * N + c] - F3[(size_t)v * N + ck];
+  }
+};
+
+template <int STAGE, typename Diff>
+__device__ __forceinline__ void stage_combine(const DevRun& r, int i, int j, int k, const double ucur[9],
+                                              const double sf[4], const double uo[9], double dt, const Diff& diff,
+                                              double u[9]) {
+  const double a1 = dt / __ldg(r.dx1b + i - 1), a2 = dt / __ldg(r.dx2b + j - 1), a3 = dt / __ldg(r.dx3b + k - 1);
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    double d1, d2, d3;
+    diff(v, d1, d2, d3);
     u[v] = rk_combine<STAGE>(STAGE > 1 ? uo[v] : 0.0, ucur[v], a1, d1, a2, d2, a3, d3);
   }
 #pragma unroll
   for (int v = 1; v <= 4; ++v) u[v] = rk_add_source<STAGE>(u[v], sf[v - 1], dt);
+}
+
+template <int STAGE>
+__device__ void stage_rhs(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pn,
+                          const double* __restrict__ Pc, const double* __restrict__ F1, const double* __restrict__ F2,
+                          const double* __restrict__ F3, const double* __restrict__ CT, double dt, double u[9]) {
+  const size_t N = r.N, c = r.cell(i, j, k);
+  double ucur[9], sf[4];
+  stage_pre<STAGE>(r, i, j, k, m, Pc, ucur, sf);
+  double uo[9];
+  if (STAGE > 1) load9(r.Un, N, c, uo);
+  const FluxDiffGlobal diff{F1, F2, F3, CT, N, c, c - 1, c - r.sj, c - r.sk};
+  stage_combine<STAGE>(r, i, j, k, ucur, sf, uo, dt, diff, u);
 }
 
 // Compensated FP32 accumulation (Kahan/Knuth two-sum, FMA two-product):
@@ -710,6 +741,41 @@ __device__ __forceinline__ bool queue_straggler(const DevRun& r, int i, int j, i
 #ifndef RG_UPDATE_MINB
 #define RG_UPDATE_MINB 3
 #endif
+// Block of the stage update: RG_UPDATE_BX cells along i times 128 / RG_UPDATE_BX
+// rows along j (the rows share the metric of their (i, k) points; 32 x 4
+// measured 0.4% faster than 64 x 2 and 16 x 8 on the 256x128x128 torus).
+#ifndef RG_UPDATE_BX
+#define RG_UPDATE_BX 32
+#endif
+
+// recov1a of one interior cell from its stage conserved state u, with
+// straggler deferral (the cell is queued for k_straggler when its iteration
+// count passes kDeferIter and the list has room) and the loop-order W carry
+// for cells without a root; the primitives go to Pw.
+__device__ __forceinline__ void update_recov(const DevRun& r, int i, int j, int k, const Met& m,
+                                             const double* __restrict__ Pc, double* __restrict__ Pw,
+                                             const double u[9]) {
+  const size_t N = r.N, c = r.cell(i, j, k);
+  double qo[9], qn[9];
+  load9(Pc, N, c, qo);
+  RecovOut o{0.0, false, false, false};
+  const double dei = __ldg(r.fl_de + i - 1), pri = __ldg(r.fl_pr + i - 1);
+  bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, dei, pri, nullptr, o, r.strag_list ? kDeferIter : 0x7fffffff);
+  if (o.deferred) {
+    if (queue_straggler(r, i, j, k)) return;
+    o = RecovOut{0.0, false, false, false};
+    ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, dei, pri, nullptr, o);
+  }
+  if (!ok) {
+    queue_carry(r, i, j, k);
+  } else {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = qn[v];
+  }
+  count_event(r, C_NR2, ok && o.nr2);
+  count_event(r, C_FAIL, ok && o.fail);
+  count_event(r, C_CAP, ok && o.cap);
+}
 
 // One stage of every cell with radial index in [ilo, ihi]: interior cells get
 // the RK combine (FP64, or MIX = mixed precision for the cells beyond
@@ -736,25 +802,7 @@ __device__ __forceinline__ void update_body(const DevRun& r, const double* __res
   double u[9];
   if (MIX) stage_rhs_mixed<STAGE>(r, i, j, k, m, Pc, r.scal->dt, u);
   else stage_rhs<STAGE>(r, i, j, k, m, Pn, Pc, F1, F2, F3, CT, r.scal->dt, u);
-  double qo[9], qn[9];
-  load9(Pc, N, c, qo);
-  RecovOut o{0.0, false, false, false};
-  const double dei = __ldg(r.fl_de + i - 1), pri = __ldg(r.fl_pr + i - 1);
-  bool ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, dei, pri, nullptr, o, r.strag_list ? kDeferIter : 0x7fffffff);
-  if (o.deferred) {
-    if (queue_straggler(r, i, j, k)) return;
-    o = RecovOut{0.0, false, false, false};
-    ok = recov_cell(u, qo, qn, m, r.gam, r.gkind, r.iter, dei, pri, nullptr, o);
-  }
-  if (!ok) {
-    queue_carry(r, i, j, k);
-  } else {
-#pragma unroll
-    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = qn[v];
-  }
-  count_event(r, C_NR2, ok && o.nr2);
-  count_event(r, C_FAIL, ok && o.fail);
-  count_event(r, C_CAP, ok && o.cap);
+  update_recov(r, i, j, k, m, Pc, Pw, u);
 }
 
 // The straggler pass: slot t of the run's list, recomputed without deferral
@@ -1119,10 +1167,21 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8) k_fl
 // remainder.  Cells past the array read as zeros (the TMA's out-of-bounds
 // fill); only lanes working on a clamped face could reach them, and those
 // store nothing.  The wait on the transaction barrier is bounded: if the copy
-// has not landed after kTmaWaitCap polls the block counts C_TMAWAIT, waits
-// once more (bounded) for the copy and returns without computing; the host
-// reports RG_ECUDA.
+// has not landed after kTmaWaitCap polls or kTmaWaitNs of the global timer,
+// the block counts C_TMAWAIT, waits once more (bounded) for the copy and
+// returns without computing; the host reports RG_ECUDA.  A block still
+// waiting after 1024 polls also gives up once the run's count is set, so a
+// launch whose copies never land ends after about one timed-out wave.  (The
+// count is read only there: the normal path issues its copy at once.)
 constexpr int kTmaWaitCap = 1 << 22;
+constexpr unsigned long long kTmaWaitNs = 50000000ull;  // 50 ms
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // LO: cells a face's state reads beyond its owner cell on either side (2
 // for the five-point schemes; 3 for PPM, whose flattening reads the pressure
 // three cells out), so the faces f of a block need cells f-LO .. f+1+LO.
@@ -1140,14 +1199,23 @@ struct TmaBox {
 template <int IREC>
 __host__ __device__ constexpr int tma_lo() { return IREC == 5 ? 3 : 2; }
 
-__device__ __forceinline__ bool tma_wait(unsigned bar) {
+// abandon: the run's C_TMAWAIT counter (nullptr: wait the full bound)
+__device__ __forceinline__ bool tma_wait(unsigned bar, const unsigned long long* abandon) {
   unsigned done = 0;
-  for (int it = 0; it < kTmaWaitCap && !done; ++it)
+  unsigned long long t0 = 0;
+  for (int it = 0; it < kTmaWaitCap && !done; ++it) {
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
         : "r"(bar), "r"(0)
         : "memory");
+    if (!done && (it & 1023) == 1023) {  // the clock is read only by a block that has waited a while
+      if (abandon && *reinterpret_cast<volatile const unsigned long long*>(abandon) != 0ull) break;
+      const unsigned long long t = global_ns();
+      if (t0 == 0) t0 = t;
+      else if (t - t0 > kTmaWaitNs) break;
+    }
+  }
   return done != 0;
 }
 
@@ -1182,9 +1250,9 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
         : "memory");
   }
   __syncthreads();
-  if (!tma_wait(bar_a)) {
+  if (!tma_wait(bar_a, r.cnt + C_TMAWAIT)) {
     if (tid == 0) atomicAdd(r.cnt + C_TMAWAIT, 1ull);
-    tma_wait(bar_a);  // the copy in flight writes this block's shared memory: give it one more bounded wait
+    tma_wait(bar_a, nullptr);  // the copy in flight writes this block's shared memory: give it one more bounded wait
     return;
   }
   const int side = threadIdx.x & 1;
@@ -1194,6 +1262,136 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
   const size_t vc = (size_t)((i - 1 - x0) + B::X * ((j - 1 - y0) + B::Y * (k - 1 - z0)));
   const long long vst = (D == 1) ? 1 : (D == 2 ? B::X : B::X * B::Y);
   face_lane<D, IREC, T, S, true>(r, nullptr, F, Fcopy, icopy, i, j, k, side, valid, box, B::PLANE, vc, vst);
+}
+
+// ------------------------------------------------ TMA-staged stage update
+// k_update with the rows its RK combine reads staged in shared memory: a
+// block of BX cells along i, BY rows along j and one k issues, when it
+// starts, one 4D tile load (cp.async.bulk.tensor, this GPU's own buffers, no
+// multicast) per array -- the three face-flux arrays, the flux-CT components
+// and, in stages 2 and 3, U^n -- each box covering the block's cells and the
+// lower neighbours the flux differences need (i-1 for F1 and CT, j-1 for F2
+// and CT, k-1 for F3 and CT).  While the copies travel the threads load the
+// metric, compute P2C of the stage input and the geometric source
+// (stage_pre); they then wait on the transaction barrier (bounded, as in
+// k_flux_tma) and take the flux differences from shared memory.  The values
+// and the operations are those of k_update.  The box origins along i are
+// even (16-byte aligned in FP64): the F1 and CT boxes start two cells before
+// the block, the others at its first cell; cells before index 0 or past the
+// array read as zeros and are never used.
+template <int BX, int BY>
+struct UpdBox {
+  // (x, y, z) extents per array; variables are the 4th dimension
+  static constexpr int X1 = BX + 2, Y1 = BY, Z1 = 1;      // F1: i-2 .. i+BX-1
+  static constexpr int X2 = BX, Y2 = BY + 1, Z2 = 1;      // F2: rows j-1 .. j+BY-1
+  static constexpr int X3 = BX, Y3 = BY, Z3 = 2;          // F3: planes k-1, k
+  static constexpr int XC = BX + 2, YC = BY + 1, ZC = 2;  // CT: all three neighbours
+  static constexpr int XU = BX, YU = BY, ZU = 1;          // U^n
+  static constexpr unsigned up128(unsigned n) { return (n + 127u) / 128u * 128u; }
+  static constexpr unsigned B1 = X1 * Y1 * Z1 * 9 * 8, B2 = X2 * Y2 * Z2 * 9 * 8, B3 = X3 * Y3 * Z3 * 9 * 8;
+  static constexpr unsigned BC = XC * YC * ZC * 6 * 8, BU = XU * YU * ZU * 9 * 8;
+  static constexpr unsigned O1 = 0, O2 = up128(O1 + B1), O3 = up128(O2 + B2), OC = up128(O3 + B3),
+                            OU = up128(OC + BC), BYTES = up128(OU + BU);
+};
+using UpdB = UpdBox<RG_UPDATE_BX, 128 / RG_UPDATE_BX>;
+
+// The five tensor maps of a run's update (F1, F2, F3, CT, U^n).
+struct UpdMaps {
+  CUtensorMap m[5];
+};
+
+__device__ __forceinline__ void tma_load4(unsigned dst, const CUtensorMap* tm, int x, int y, int z, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(tm)), "r"(x), "r"(y), "r"(z), "r"(0), "r"(bar)
+      : "memory");
+}
+
+// Flux differences from the staged rows of one thread's cell (pointers at the
+// cell in each box; neighbours one element, one row or one plane back).
+struct FluxDiffStaged {
+  const double* f1;
+  const double* f2;
+  const double* f3;
+  const double* ct;
+  __device__ __forceinline__ void operator()(int v, double& d1, double& d2, double& d3) const {
+    using B = UpdB;
+    constexpr int P1 = B::X1 * B::Y1 * B::Z1, P2 = B::X2 * B::Y2 * B::Z2, P3 = B::X3 * B::Y3 * B::Z3;
+    constexpr int PC = B::XC * B::YC * B::ZC, SJC = B::XC, SKC = B::XC * B::YC, SK3 = B::X3 * B::Y3;
+    if (v == 7) d1 = ct[2 * PC] - ct[2 * PC - 1];
+    else if (v == 8) d1 = ct[4 * PC] - ct[4 * PC - 1];
+    else d1 = f1[v * P1] - f1[v * P1 - 1];
+    if (v == 6) d2 = ct[0 * PC] - ct[0 * PC - SJC];
+    else if (v == 8) d2 = ct[5 * PC] - ct[5 * PC - SJC];
+    else d2 = f2[v * P2] - f2[v * P2 - B::X2];
+    if (v == 6) d3 = ct[1 * PC] - ct[1 * PC - SKC];
+    else if (v == 7) d3 = ct[3 * PC] - ct[3 * PC - SKC];
+    else d3 = f3[v * P3] - f3[v * P3 - SK3];
+  }
+};
+
+template <int STAGE>
+__global__ void __launch_bounds__(128, RG_UPDATE_MINB)
+    k_update_tma(const __grid_constant__ UpdMaps tm, DevRun r, const double* __restrict__ Pc, double* __restrict__ Pw) {
+  using B = UpdB;
+  extern __shared__ __align__(128) unsigned char upd_raw[];
+  __shared__ __align__(8) unsigned long long bar;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + RG_UPDATE_BX * ty;
+  const int x0 = (int)blockIdx.x * RG_UPDATE_BX, y0 = (int)blockIdx.y * (128 / RG_UPDATE_BX), z0 = (int)blockIdx.z;
+  const int i = x0 + tx + 1, j = y0 + ty + 1, k = z0 + 1;
+  const bool inr = i <= r.imax && j <= r.jmax && k <= r.kmax;
+  const size_t N = r.N, c = inr ? r.cell(i, j, k) : 0;
+  if (!r.scal->active) {  // a finished run copies its state through (as k_update)
+    if (inr)
+#pragma unroll
+      for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = Pc[(size_t)v * N + c];
+    return;
+  }
+  const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
+  const unsigned base = (unsigned)__cvta_generic_to_shared(upd_raw);
+  if (tid == 0) {
+    const unsigned bytes = B::B1 + B::B2 + B::B3 + B::BC + (STAGE > 1 ? B::BU : 0u);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+    tma_load4(base + B::O1, &tm.m[0], x0 - 2, y0, z0, bar_a);
+    tma_load4(base + B::O2, &tm.m[1], x0, y0 - 1, z0, bar_a);
+    tma_load4(base + B::O3, &tm.m[2], x0, y0, z0 - 1, bar_a);
+    tma_load4(base + B::OC, &tm.m[3], x0 - 2, y0 - 1, z0 - 1, bar_a);
+    if (STAGE > 1) tma_load4(base + B::OU, &tm.m[4], x0, y0, z0, bar_a);
+  }
+  __syncthreads();
+  const bool interior = inr && is_interior(r, i, j, k);
+  if (inr && !interior)
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = Pc[(size_t)v * N + c];
+  Met m;
+  double ucur[9], sf[4];
+  if (interior) {
+    load_met(r.mc, r.nik, r.ik(i, k), m);
+    stage_pre<STAGE>(r, i, j, k, m, Pc, ucur, sf);
+  }
+  if (!tma_wait(bar_a, r.cnt + C_TMAWAIT)) {
+    if (tid == 0) atomicAdd(r.cnt + C_TMAWAIT, 1ull);
+    tma_wait(bar_a, nullptr);  // the copies in flight write this block's shared memory: one more bounded wait
+    return;
+  }
+  if (!interior) return;
+  const double* sm = reinterpret_cast<const double*>(upd_raw);
+  const FluxDiffStaged diff{sm + B::O1 / 8 + (tx + 2) + B::X1 * ty,
+                            sm + B::O2 / 8 + tx + B::X2 * (ty + 1),
+                            sm + B::O3 / 8 + tx + B::X3 * ty + B::X3 * B::Y3,
+                            sm + B::OC / 8 + (tx + 2) + B::XC * (ty + 1) + B::XC * B::YC};
+  double uo[9];
+  if (STAGE > 1) {
+    const double* un = sm + B::OU / 8 + tx + B::XU * ty;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) uo[v] = un[v * B::XU * B::YU];
+  }
+  double u[9];
+  stage_combine<STAGE>(r, i, j, k, ucur, sf, uo, r.scal->dt, diff, u);
+  update_recov(r, i, j, k, m, Pc, Pw, u);
 }
 
 // ------------------------------------------- per-routine rec2 / calcha / hll
@@ -2344,11 +2542,6 @@ cudaError_t launch_ct(const DevRun& r, const double* P, const double* F1, const 
   return cudaGetLastError();
 }
 
-// Block of the stage update: RG_UPDATE_BX cells along i times 128 / RG_UPDATE_BX
-// rows along j (the rows share the metric of their (i, k) points).
-#ifndef RG_UPDATE_BX
-#define RG_UPDATE_BX 64
-#endif
 template <bool MIX>
 static void launch_update_t(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                             const double* F1, const double* F2, const double* F3, const double* CT, int ilo,
@@ -2361,9 +2554,45 @@ static void launch_update_t(const DevRun& r, int stage, const double* Pn, const 
   else k_update<3, MIX><<<g, b, 0, s>>>(r, Pn, Pc, Pw, F1, F2, F3, CT, ilo, ihi);
 }
 
+bool update_tma_eligible(const DevRun& r) {
+  return !r.mixed && !r.jfix && !r.kfix && r.iwvec != 2 && (r.imax % 2) == 0 &&
+         r.N == (size_t)r.imax * r.jmax * r.kmax;
+}
+
+void update_tma_box(int which, unsigned box[4]) {
+  using B = UpdB;
+  const unsigned x[5] = {B::X1, B::X2, B::X3, B::XC, B::XU}, y[5] = {B::Y1, B::Y2, B::Y3, B::YC, B::YU};
+  const unsigned z[5] = {B::Z1, B::Z2, B::Z3, B::ZC, B::ZU};
+  box[0] = x[which];
+  box[1] = y[which];
+  box[2] = z[which];
+  box[3] = which == 3 ? 6 : 9;
+}
+
+cudaError_t prepare_update_tma() {
+  const void* fns[3] = {reinterpret_cast<const void*>(k_update_tma<1>), reinterpret_cast<const void*>(k_update_tma<2>),
+                        reinterpret_cast<const void*>(k_update_tma<3>)};
+  for (const void* f : fns) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UpdB::BYTES);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
-                          const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s) {
-  if (!r.mixed) {
+                          const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s,
+                          const void* umaps) {
+  if (umaps && update_tma_eligible(r)) {
+    UpdMaps maps;
+    memcpy(&maps, umaps, sizeof maps);
+    const dim3 b(RG_UPDATE_BX, 128 / RG_UPDATE_BX, 1);
+    const dim3 g = grid3(r.imax, r.jmax, r.kmax, b);
+    if (stage == 1) k_update_tma<1><<<g, b, UpdB::BYTES, s>>>(maps, r, Pc, Pw);
+    else if (stage == 2) k_update_tma<2><<<g, b, UpdB::BYTES, s>>>(maps, r, Pc, Pw);
+    else k_update_tma<3><<<g, b, UpdB::BYTES, s>>>(maps, r, Pc, Pw);
+  } else if (!r.mixed) {
     launch_update_t<false>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, 1, r.imax, s);
   } else {
     const int split = fp64_split(r, 1, r.imax);

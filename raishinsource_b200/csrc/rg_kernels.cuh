@@ -37,8 +37,17 @@ cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const 
 // P: the stage's primitives (upflct's upwinding reads their velocities)
 cudaError_t launch_ct(const DevRun& r, const double* P, const double* F1, const double* F2, const double* F3,
                       double* CT, cudaStream_t s);
+// umaps: the run's five update tensor maps (F1, F2, F3, CT, U^n; CUtensorMap[5])
+// for the TMA-staged update where update_tma_eligible, else nullptr
 cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
-                          const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s);
+                          const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s,
+                          const void* umaps = nullptr);
+// TMA-staged update: runs stored in full, FP64, recov1a, imax even
+bool update_tma_eligible(const DevRun& r);
+// box of update tensor map `which` (0 F1, 1 F2, 2 F3, 3 CT, 4 U^n) as (x, y, z, variables)
+void update_tma_box(int which, unsigned box[4]);
+// shared-memory attributes of the staged update kernels (on the current device)
+cudaError_t prepare_update_tma();
 cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t s);
 cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s);
 // one floor routine alone: part 1 infchk, 2 atmosphere1a, 4 pminmax2b
