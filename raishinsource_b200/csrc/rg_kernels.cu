@@ -1199,22 +1199,24 @@ struct TmaBox {
 template <int IREC>
 __host__ __device__ constexpr int tma_lo() { return IREC == 5 ? 3 : 2; }
 
-// abandon: the run's C_TMAWAIT counter (nullptr: wait the full bound)
+// abandon: the run's C_TMAWAIT counter (nullptr: wait the full bound).  The
+// polls run in rounds of 1024, so the clock and the counter are read only by a
+// block that has waited a whole round.
 __device__ __forceinline__ bool tma_wait(unsigned bar, const unsigned long long* abandon) {
   unsigned done = 0;
   unsigned long long t0 = 0;
-  for (int it = 0; it < kTmaWaitCap && !done; ++it) {
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(0)
-        : "memory");
-    if (!done && (it & 1023) == 1023) {  // the clock is read only by a block that has waited a while
-      if (abandon && *reinterpret_cast<volatile const unsigned long long*>(abandon) != 0ull) break;
-      const unsigned long long t = global_ns();
-      if (t0 == 0) t0 = t;
-      else if (t - t0 > kTmaWaitNs) break;
-    }
+  for (int round = 0; round < kTmaWaitCap / 1024; ++round) {
+    for (int it = 0; it < 1024 && !done; ++it)
+      asm volatile(
+          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+          : "=r"(done)
+          : "r"(bar), "r"(0)
+          : "memory");
+    if (done) break;
+    if (abandon && *reinterpret_cast<volatile const unsigned long long*>(abandon) != 0ull) break;
+    const unsigned long long t = global_ns();
+    if (t0 == 0) t0 = t;
+    else if (t - t0 > kTmaWaitNs) break;
   }
   return done != 0;
 }
