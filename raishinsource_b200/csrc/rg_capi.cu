@@ -63,6 +63,7 @@ struct Run {
   // kernel, per direction (flux_tma_box); tma is set when all nine exist
   CUtensorMap tmap[3][3];
   CUtensorMap tmap32[3];   // the FP32 copy P32 of a mixed run, per direction
+  CUtensorMap tmapm[3];    // the FP64 face metric per direction (mi, mc, mk; flux_tma_met_box)
   bool tma = false;
   // tensor maps of the staged update (F1, F2, F3, CT, U^n; update_tma_box)
   CUtensorMap umap[5];
@@ -181,6 +182,18 @@ void make_tmaps(Run* R) {
         flux_tma_box(dir, 4, d.irec, box);
         ok = encode(&R->tmap32[dir - 1], d.P32, 4, 9, box);
       }
+    }
+    // face metric (i, k, component): kMetComps components nik apart
+    const double* met[3] = {d.mi, d.mc, d.mk};
+    unsigned mb[3];
+    flux_tma_met_box(mb);
+    for (int dir = 1; dir <= 3 && ok; ++dir) {
+      const cuuint64_t dims[3] = {(cuuint64_t)d.imax, (cuuint64_t)d.kmax, (cuuint64_t)kMetComps};
+      const cuuint64_t strides[2] = {(cuuint64_t)d.imax * 8, (cuuint64_t)d.nik * 8};
+      const cuuint32_t bx[3] = {mb[0], mb[1], mb[2]};
+      ok = enc(&R->tmapm[dir - 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(met[dir - 1]), dims,
+               strides, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     }
     R->tma = ok;
   }
@@ -574,7 +587,8 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
   const int bi = (Pc == R->b.P[0]) ? 0 : (Pc == R->b.P[1] ? 1 : 2);
   const bool tma = R->tma && ctx->tma && Pc == R->b.P[bi];
   auto faces = [&](int dir) {
-    return tma ? launch_flux_tma(d, dir, &R->tmap[bi][dir - 1], &R->tmap32[dir - 1], R->b.F[dir - 1], s)
+    return tma ? launch_flux_tma(d, dir, &R->tmap[bi][dir - 1], &R->tmap32[dir - 1], &R->tmapm[dir - 1],
+                                 R->b.F[dir - 1], s)
                : launch_flux(d, dir, Pc, R->b.F[dir - 1], s);
   };
   RG_CUDA(issue(ctx, K_FLUX1, nf, [&] { return faces(1); }));

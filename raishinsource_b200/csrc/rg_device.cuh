@@ -89,21 +89,27 @@ using Met = MetT<double>;
 // order of the MetT fields (FP64, with FP32 copies for the mixed path's FP32
 // kernels).  Components a kernel does
 // not use are never loaded (dead loads are removed by the compiler).
-template <typename T, typename S>
+template <typename T, typename S, bool LDG = true>
 __device__ __forceinline__ void load_met(const S* __restrict__ base, size_t nik, size_t q, MetT<T>& m) {
+  // LDG: through the read-only cache (global memory); otherwise plain loads
+  // (a shared-memory copy of the cache, component stride nik)
   const S* b = base + q;
-  m.g00 = T(__ldg(b + 0 * nik)); m.g01 = T(__ldg(b + 1 * nik)); m.g02 = T(__ldg(b + 2 * nik));
-  m.g11 = T(__ldg(b + 3 * nik)); m.g12 = T(__ldg(b + 4 * nik)); m.g22 = T(__ldg(b + 5 * nik));
-  m.g33 = T(__ldg(b + 6 * nik));
-  m.c00 = T(__ldg(b + 7 * nik)); m.c01 = T(__ldg(b + 8 * nik)); m.c02 = T(__ldg(b + 9 * nik));
-  m.c10 = T(__ldg(b + 10 * nik)); m.c11 = T(__ldg(b + 11 * nik)); m.c12 = T(__ldg(b + 12 * nik));
-  m.c20 = T(__ldg(b + 13 * nik)); m.c21 = T(__ldg(b + 14 * nik)); m.c22 = T(__ldg(b + 15 * nik));
-  m.c33 = T(__ldg(b + 16 * nik));
-  m.detg = T(__ldg(b + 17 * nik));
-  m.al = T(__ldg(b + 18 * nik)); m.ial = T(__ldg(b + 19 * nik));
-  m.be1 = T(__ldg(b + 20 * nik)); m.be2 = T(__ldg(b + 21 * nik));
-  m.g3_11 = T(__ldg(b + 22 * nik)); m.g3_22 = T(__ldg(b + 23 * nik)); m.g3_33 = T(__ldg(b + 24 * nik));
-  m.idetg = T(__ldg(b + 25 * nik));
+  auto ld = [&](int c) -> T {
+    if constexpr (LDG) return T(__ldg(b + c * nik));
+    else return T(b[c * nik]);
+  };
+  m.g00 = ld(0); m.g01 = ld(1); m.g02 = ld(2);
+  m.g11 = ld(3); m.g12 = ld(4); m.g22 = ld(5);
+  m.g33 = ld(6);
+  m.c00 = ld(7); m.c01 = ld(8); m.c02 = ld(9);
+  m.c10 = ld(10); m.c11 = ld(11); m.c12 = ld(12);
+  m.c20 = ld(13); m.c21 = ld(14); m.c22 = ld(15);
+  m.c33 = ld(16);
+  m.detg = ld(17);
+  m.al = ld(18); m.ial = ld(19);
+  m.be1 = ld(20); m.be2 = ld(21);
+  m.g3_11 = ld(22); m.g3_22 = ld(23); m.g3_33 = ld(24);
+  m.idetg = ld(25);
 }
 
 // The derived fields of one point from its base fields: calucon's

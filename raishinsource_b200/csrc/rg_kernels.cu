@@ -986,7 +986,8 @@ template <int D, int IREC, typename T, typename S, bool VIEW = false, bool OUT =
 __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__ P, S* __restrict__ F,
                                           float* __restrict__ Fcopy, int icopy, int i, int j, int k, int side,
                                           bool valid, const S* Vp = nullptr, size_t Vn = 0, size_t Vc = 0,
-                                          long long Vst = 0, const FaceOut* fo = nullptr) {
+                                          long long Vst = 0, const FaceOut* fo = nullptr,
+                                          const S* Mv = nullptr, int Mst = 0) {
   const unsigned mask = __activemask();
   const size_t N = r.N, c = r.cell(i, j, k);
   const long long st = (D == 1) ? 1 : (D == 2 ? (long long)r.sj : (long long)r.sk);
@@ -1077,7 +1078,8 @@ __device__ __forceinline__ void face_lane(const DevRun& r, const S* __restrict__
     for (int v = 0; v < 9; ++v) q[v] = T(Pv[(size_t)v * Nv + cv + side * sv]);
   }
   MetT<T> m;
-  load_met(met_of<D, S>(r), r.nik, r.ik(i, k), m);
+  if (VIEW && Mv) load_met<T, S, false>(Mv, (size_t)Mst, 0, m);  // the face metric staged with the stencil
+  else load_met(met_of<D, S>(r), r.nik, r.ik(i, k), m);
   const T gam = T(r.gam);
   T u[9], w[9], vp, vm;
   {
@@ -1195,6 +1197,18 @@ struct TmaBox {
   static constexpr int Z = (D == 3) ? 1 + 2 * LO + 1 : 1;
   static constexpr int PLANE = X * Y * Z;                                   // cells per variable
   static constexpr unsigned BYTES = (unsigned)PLANE * 9u * (unsigned)sizeof(S);  // whole box
+  // FP64 runs also stage the face metric of the block's faces (MetT's
+  // components at each face's (i, k) point): MX points along i from the
+  // block's first face rounded down to 16 bytes, one k, kMetComps components,
+  // placed after the stencil box at MOFF -- where five blocks per SM still fit
+  // (at most 45 KB each; PPM's theta box leaves no room and reads the metric
+  // through L1)
+  static constexpr int MX = up(32 + ALIGN - 1);
+  static constexpr unsigned MOFF = (BYTES + 127u) / 128u * 128u;
+  static constexpr unsigned MSIZE = (unsigned)MX * (unsigned)kMetComps * (unsigned)sizeof(S);
+  static constexpr bool MET = sizeof(S) == 8 && MOFF + MSIZE <= 45u * 1024u;
+  static constexpr unsigned MBYTES = MET ? MSIZE : 0u;
+  static constexpr unsigned SMEM = MET ? MOFF + MBYTES : BYTES;
 };
 template <int IREC>
 __host__ __device__ constexpr int tma_lo() { return IREC == 5 ? 3 : 2; }
@@ -1223,8 +1237,8 @@ __device__ __forceinline__ bool tma_wait(unsigned bar, const unsigned long long*
 
 template <int D, int IREC, typename T, typename S>
 __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
-    k_flux_tma(const __grid_constant__ CUtensorMap tm, DevRun r, S* __restrict__ F, float* __restrict__ Fcopy,
-               int icopy, int ilo, int ihi) {
+    k_flux_tma(const __grid_constant__ CUtensorMap tm, const __grid_constant__ CUtensorMap tmm, DevRun r,
+               S* __restrict__ F, float* __restrict__ Fcopy, int icopy, int ilo, int ihi) {
   extern __shared__ __align__(128) unsigned char box_raw[];
   __shared__ __align__(8) unsigned long long bar;
   if (!r.scal->active) return;
@@ -1238,18 +1252,26 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
   const int x0 = ((D == 1) ? fi0 - 1 - LO : fi0 - 1) & ~(B::ALIGN - 1);
   const int y0 = (D == 2) ? fj0 - 1 - LO : fj0 - 1;
   const int z0 = (D == 3) ? fk0 - 1 - LO : fk0 - 1;
+  const int mx0 = (fi0 - 1) & ~(B::ALIGN - 1);  // first metric point (0-based i) of the metric box
   const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
   const unsigned box_a = (unsigned)__cvta_generic_to_shared(box_raw);
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(B::BYTES) : "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(B::BYTES + B::MBYTES)
+                 : "memory");
     asm volatile(
         "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
         "%5}], [%6];" ::"r"(box_a),
         "l"(reinterpret_cast<unsigned long long>(&tm)), "r"(x0), "r"(y0), "r"(z0), "r"(0), "r"(bar_a)
         : "memory");
+    if (B::MET)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+          "%4}], [%5];" ::"r"(box_a + B::MOFF),
+          "l"(reinterpret_cast<unsigned long long>(&tmm)), "r"(mx0), "r"(fk0 - 1), "r"(0), "r"(bar_a)
+          : "memory");
   }
   __syncthreads();
   if (!tma_wait(bar_a, r.cnt + C_TMAWAIT)) {
@@ -1263,7 +1285,9 @@ __global__ void __launch_bounds__(128, sizeof(T) == 8 ? RG_FLUX_MINB64 : 8)
   const int i = min(i0, ihi), j = min(j0, r.jmax - nm0), k = min(fk0, r.kmax - nm0);
   const size_t vc = (size_t)((i - 1 - x0) + B::X * ((j - 1 - y0) + B::Y * (k - 1 - z0)));
   const long long vst = (D == 1) ? 1 : (D == 2 ? B::X : B::X * B::Y);
-  face_lane<D, IREC, T, S, true>(r, nullptr, F, Fcopy, icopy, i, j, k, side, valid, box, B::PLANE, vc, vst);
+  const S* met = B::MET ? reinterpret_cast<const S*>(box_raw + B::MOFF) + (i - 1 - mx0) : nullptr;
+  face_lane<D, IREC, T, S, true>(r, nullptr, F, Fcopy, icopy, i, j, k, side, valid, box, B::PLANE, vc, vst, nullptr,
+                                 met, B::MX);
 }
 
 // ------------------------------------------------ TMA-staged stage update
@@ -2431,47 +2455,56 @@ bool flux_tma_eligible(const DevRun& r) {
 }
 
 template <int IREC, typename T, typename S>
-static void launch_flux_tma_irec(const DevRun& r, int dir, const CUtensorMap& tm, S* F, float* Fcopy, int icopy,
-                                 int ilo, int ihi, dim3 g, dim3 b, cudaStream_t s) {
+static void launch_flux_tma_irec(const DevRun& r, int dir, const CUtensorMap& tm, const CUtensorMap& tmm, S* F,
+                                 float* Fcopy, int icopy, int ilo, int ihi, dim3 g, dim3 b, cudaStream_t s) {
   constexpr int LO = tma_lo<IREC>();
   if (dir == 1)
-    k_flux_tma<1, IREC, T, S><<<g, b, TmaBox<1, S, LO>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+    k_flux_tma<1, IREC, T, S><<<g, b, TmaBox<1, S, LO>::SMEM, s>>>(tm, tmm, r, F, Fcopy, icopy, ilo, ihi);
   else if (dir == 2)
-    k_flux_tma<2, IREC, T, S><<<g, b, TmaBox<2, S, LO>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+    k_flux_tma<2, IREC, T, S><<<g, b, TmaBox<2, S, LO>::SMEM, s>>>(tm, tmm, r, F, Fcopy, icopy, ilo, ihi);
   else
-    k_flux_tma<3, IREC, T, S><<<g, b, TmaBox<3, S, LO>::BYTES, s>>>(tm, r, F, Fcopy, icopy, ilo, ihi);
+    k_flux_tma<3, IREC, T, S><<<g, b, TmaBox<3, S, LO>::SMEM, s>>>(tm, tmm, r, F, Fcopy, icopy, ilo, ihi);
 }
 template <typename T, typename S>
-static void launch_flux_tma_t(const DevRun& r, int dir, const CUtensorMap& tm, S* F, float* Fcopy, int icopy,
-                              int ilo, int ihi, cudaStream_t s) {
+static void launch_flux_tma_t(const DevRun& r, int dir, const CUtensorMap& tm, const CUtensorMap& tmm, S* F,
+                              float* Fcopy, int icopy, int ilo, int ihi, cudaStream_t s) {
   if (ihi < ilo) return;
   const int n = ihi - ilo + 1, m = r.jmax - 2 * r.nm0 + 1, l = r.kmax - 2 * r.nm0 + 1;
   const dim3 b(64, 2, 1);
   const dim3 g((unsigned)((n + 31) / 32), (unsigned)((m + 1) / 2), (unsigned)l);
   switch (r.irec) {
-    case 5: launch_flux_tma_irec<5, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
-    case 7: launch_flux_tma_irec<7, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
-    case 9: launch_flux_tma_irec<9, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
-    case 10: launch_flux_tma_irec<10, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
-    default: launch_flux_tma_irec<6, T, S>(r, dir, tm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    case 5: launch_flux_tma_irec<5, T, S>(r, dir, tm, tmm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    case 7: launch_flux_tma_irec<7, T, S>(r, dir, tm, tmm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    case 9: launch_flux_tma_irec<9, T, S>(r, dir, tm, tmm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    case 10: launch_flux_tma_irec<10, T, S>(r, dir, tm, tmm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
+    default: launch_flux_tma_irec<6, T, S>(r, dir, tm, tmm, F, Fcopy, icopy, ilo, ihi, g, b, s); break;
   }
 }
 
-cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const void* tmap32, double* F,
-                            cudaStream_t s) {
+cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const void* tmap32, const void* tmapm,
+                            double* F, cudaStream_t s) {
   const int lo = r.nm0, hi = r.imax - r.nm0;
   const CUtensorMap& t64 = *static_cast<const CUtensorMap*>(tmap64);
+  const CUtensorMap& tm = *static_cast<const CUtensorMap*>(tmapm);
   if (!r.mixed) {
-    launch_flux_tma_t<double, double>(r, dir, t64, F, nullptr, 0, lo, hi, s);
+    launch_flux_tma_t<double, double>(r, dir, t64, tm, F, nullptr, 0, lo, hi, s);
   } else {
     // as launch_flux: FP64 faces up to i_fp64 + 1, copied to FP32 up to i_fp64; FP32 faces beyond
     const int split = fp64_split(r, lo, hi);
     if (split >= lo)
-      launch_flux_tma_t<double, double>(r, dir, t64, F, r.F32[dir - 1], split, lo, split < hi ? split + 1 : hi, s);
-    launch_flux_tma_t<float, float>(r, dir, *static_cast<const CUtensorMap*>(tmap32), r.F32[dir - 1], nullptr, 0,
-                                    split + 1, hi, s);
+      launch_flux_tma_t<double, double>(r, dir, t64, tm, F, r.F32[dir - 1], split, lo, split < hi ? split + 1 : hi,
+                                        s);
+    launch_flux_tma_t<float, float>(r, dir, *static_cast<const CUtensorMap*>(tmap32), tm, r.F32[dir - 1], nullptr,
+                                    0, split + 1, hi, s);
   }
   return cudaGetLastError();
+}
+
+// Box of the face-metric tensor map (i, k, component) of the staged FP64 face kernel.
+void flux_tma_met_box(unsigned box[3]) {
+  box[0] = TmaBox<1, double, 2>::MX;
+  box[1] = 1;
+  box[2] = kMetComps;
 }
 
 template <typename S, int LO>

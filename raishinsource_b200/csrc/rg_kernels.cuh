@@ -32,8 +32,11 @@ cudaError_t launch_flux(const DevRun& r, int dir, const double* P, double* F, cu
 // 4D: i, j, k, v; box flux_tma_box(dir, element bytes, irec))
 bool flux_tma_eligible(const DevRun& r);
 void flux_tma_box(int dir, int elem_bytes, int irec, unsigned box[4]);
-cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const void* tmap32, double* F,
-                            cudaStream_t s);
+// tmapm: the FP64 face-metric map of direction dir (3D: i, k, component; box
+// flux_tma_met_box), staged with the stencil
+cudaError_t launch_flux_tma(const DevRun& r, int dir, const void* tmap64, const void* tmap32, const void* tmapm,
+                            double* F, cudaStream_t s);
+void flux_tma_met_box(unsigned box[3]);
 // P: the stage's primitives (upflct's upwinding reads their velocities)
 cudaError_t launch_ct(const DevRun& r, const double* P, const double* F1, const double* F2, const double* F3,
                       double* CT, cudaStream_t s);
