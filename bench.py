@@ -61,13 +61,16 @@ BYTES_PER_UNIT = {"flux_r": 136, "flux_phi": 136, "flux_theta": 136, "update": 4
                   "floors": 120, "cfl": 72}
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one launch divided by
 # its units) on the 192x96x96 torus, whose state already exceeds the L2
-DRAM_BYTES_PER_UNIT = {"update": 469.0, "flux_r": 113.0, "flux_phi": 120.0, "flux_theta": 122.0}
+# (update: the TMA-staged k_update_tma, stages 2 and 3, whose boxes re-read their j-1 / k-1 halos)
+DRAM_BYTES_PER_UNIT = {"update": 472.0, "flux_r": 113.0, "flux_phi": 120.0, "flux_theta": 122.0}
 BYTES_PER_UNIT["flux"] = 136
-# the TMA-staged face kernels (k_flux_tma) of the FP64 MP5 path, ncu on the 192x96x96 torus
-DRAM_BYTES_PER_UNIT["flux"] = (122.0 + 131.0 + 133.0) / 3
+# the TMA-staged face kernels (k_flux_tma, stencil and face metric staged) of the FP64 MP5 path, ncu on the
+# 192x96x96 torus
+DRAM_BYTES_PER_UNIT["flux"] = (124.0 + 132.0 + 135.0) / 3
 # FP64 pipe utilisation of the face kernels from ncu (sm__inst_executed_pipe_fp64, percent of the peak
-# sustained rate while active), mean over the three directions on the 192x96x96 torus
-FP64_PIPE_FRAC = {"flux": 0.474, "update": 0.237}
+# sustained rate while active), mean over the three directions (update: over the three stages) on the
+# 192x96x96 torus
+FP64_PIPE_FRAC = {"flux": 0.481, "update": 0.271}
 # algorithmic HBM bytes of one zone-update (FP64): only primitives persist between stages
 STEP_BYTES_PER_ZONE = 648
 # Executed FP64 operations per zone-update of one full RK3 step (MP5, FP64): ncu

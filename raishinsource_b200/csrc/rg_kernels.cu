@@ -2400,8 +2400,13 @@ cudaError_t launch_step_end(const DevRun& r, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Block of the CFL and floor passes: RG_CELL_BX cells along i times
+// 128 / RG_CELL_BX rows along j (rows share their (i, k) metric points).
+#ifndef RG_CELL_BX
+#define RG_CELL_BX 32
+#endif
 cudaError_t launch_cfl(const DevRun& r, const double* P, cudaStream_t s) {
-  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 b = sblock(r, dim3(RG_CELL_BX, 128 / RG_CELL_BX, 1));
   k_cfl<<<sgrid(r, r.imax - 2, r.jmax - 2, r.kmax - 2, b), b, 0, s>>>(r, P);
   return cudaGetLastError();
 }
@@ -2734,7 +2739,7 @@ cudaError_t launch_bc(const DevRun& r, double* P, const double* Po, cudaStream_t
 }
 
 cudaError_t launch_floor(const DevRun& r, double* P, cudaStream_t s) {
-  const dim3 b = sblock(r, dim3(64, 2, 1));
+  const dim3 b = sblock(r, dim3(RG_CELL_BX, 128 / RG_CELL_BX, 1));
   k_floor<<<sgrid(r, r.imax, r.jmax, r.kmax, b), b, 0, s>>>(r, P);
   return cudaGetLastError();
 }
