@@ -63,12 +63,13 @@ typedef struct rg_run_params {
   int ict;       /* constrained transport as pram.f90's ict (pram.f90:148-151, ct.f90:4-27):
                     0 none, 1 flux-CT (Toth 2000; the reference's setting), 2 modified flux-CT
                     (Gardiner & Stone 2005, mflct), 3 upwind flux-CT (upflct; FP64 precision
-                    only, stepped by rg_step alone: rg_step_batch and rg_calflx_static refuse it).
+                    only; in rg_step_batch such a run takes its own launches; rg_calflx_static
+                    refuses it).
                     Ghost width nm1 = nm0 + ict (main.f90:192-199). */
   int iwvec;     /* primitive recovery as pram.f90's iwvec (pram.f90:160-161, recov.f90:2-47):
                     1 (or 0) recov1a, the reference's setting; 2 recov2 (Mignone & McKinney,
-                    one-variable W; FP64 precision only, stepped by rg_step alone:
-                    rg_step_batch refuses it). */
+                    one-variable W; FP64 precision only; in rg_step_batch such a run takes
+                    its own launches). */
 } rg_run_params;
 
 /* rg_run_params.flags.  A direction of extent 2*nm1+1 (one interior cell)
@@ -167,16 +168,19 @@ int rg_run_download_stored(rg_ctx* ctx, int run, double* soa);
 /* Advance nsteps full RK3 steps of main.f90:586-1147 on the device (CFL
  * reduction, three stages, ghost fill, floors).  Stops early once the loop-top
  * time exceeds tmax.  Asynchronous on the context stream unless stats != NULL.
- * A run with a slab direction steps as a batch of one (rg_step_batch). */
+ * A run with a slab direction steps as a batch of one (rg_step_batch), unless
+ * it uses upwind flux-CT or recov2, which have no batched kernels. */
 int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats);
 int rg_run_stats(rg_ctx* ctx, int run, rg_step_stats* stats);
 
-/* Advance nruns runs together by nsteps full RK3 steps.  Runs that share
- * reconstruction, precision and slab class (see RG_FLAG_FULL) form one batch,
- * whose step is one launch per kernel kind over a per-run tile table
- * (persistent grid), captured once in a CUDA graph and replayed each step.
- * Meant for many small runs (2D slabs, 1D tubes); a large 3D run alone is
- * faster through rg_step.  The launch shape (block width, cells per tile
+/* Advance nruns runs together by nsteps full RK3 steps.  Runs with a slab
+ * direction that share reconstruction, precision and slab class (see
+ * RG_FLAG_FULL) form one batch, whose step is one launch per kernel kind over
+ * a per-run tile table (persistent grid), captured once in a CUDA graph and
+ * replayed each step: many small runs (2D slabs, 1D tubes).  Runs without a
+ * slab direction (3D runs, which fill the GPU alone) and runs with upwind
+ * flux-CT or recov2 take each step with their own launches, after the
+ * batches of that step, exactly as rg_step steps them.  The launch shape (block width, cells per tile
  * along i, persistent grid size) is tuned per batch class and context: a new
  * class starts with a default shape and, at the first segment boundary after
  * 32 steps of its batch, times every candidate shape on trial steps from a

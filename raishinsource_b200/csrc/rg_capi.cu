@@ -1278,28 +1278,41 @@ int rg_run_download_stored(rg_ctx* ctx, int run, double* soa) {
   return RG_OK;
 }
 
+// One full step of a run with its own launches (CFL, three stages, scalars).
+static int step_alone(rg_ctx* ctx, Run* R) {
+  cudaStream_t s = ctx->stream;
+  double* Pn = R->b.P[R->cur];
+  double* P1 = R->b.P[(R->cur + 1) % 3];
+  double* P2 = R->b.P[(R->cur + 2) % 3];
+  RG_CUDA(issue(ctx, K_SCALAR, 1, [&] { return launch_step_begin(R->d, s); }));
+  RG_CUDA(issue(ctx, K_CFL, 1, [&] { return launch_cfl(R->d, Pn, s); }));
+  RG_CUDA(issue(ctx, K_SCALAR, 1, [&] { return launch_dt(R->d, s); }));
+  int rc;
+  if ((rc = run_stage(ctx, R, 1, Pn, Pn, P1))) return rc;
+  if ((rc = run_stage(ctx, R, 2, Pn, P1, P2))) return rc;
+  if ((rc = run_stage(ctx, R, 3, Pn, P2, P1))) return rc;
+  RG_CUDA(issue(ctx, K_SCALAR, 1, [&] { return launch_step_end(R->d, s); }));
+  R->cur = (R->cur + 1) % 3;
+  return RG_OK;
+}
+
+// Runs that a batch steps with their own launches: no slab direction (they
+// fill the GPU alone, and the single-run kernels stage their stencils and
+// rows by TMA), or a scheme without batched kernels (upwind flux-CT, recov2).
+static bool steps_alone(const Run* R) {
+  return !(R->d.jfix || R->d.kfix) || R->d.ict == 3 || R->d.iwvec == 2;
+}
+
 int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats) {
   Run* R = find(ctx, run);
   if (!R) return fail(RG_ENOTFOUND, "unknown run");
   // A run with a slab direction steps as a batch of one: it then runs the same
   // compiled kernels alone as in any batch, so its results do not depend on
   // the company it keeps, and its step is replayed from a CUDA graph.
-  // (upwind flux-CT and recov2 have no batched kernels: such a run keeps the launches below)
-  if ((R->d.jfix || R->d.kfix) && R->d.ict != 3 && R->d.iwvec != 2) return rg_step_batch(ctx, &run, 1, nsteps, stats);
-  cudaStream_t s = ctx->stream;
+  if (!steps_alone(R)) return rg_step_batch(ctx, &run, 1, nsteps, stats);
   for (int n = 0; n < nsteps; ++n) {
-    double* Pn = R->b.P[R->cur];
-    double* P1 = R->b.P[(R->cur + 1) % 3];
-    double* P2 = R->b.P[(R->cur + 2) % 3];
-    RG_CUDA(issue(ctx, K_SCALAR, 1, [&] { return launch_step_begin(R->d, s); }));
-    RG_CUDA(issue(ctx, K_CFL, 1, [&] { return launch_cfl(R->d, Pn, s); }));
-    RG_CUDA(issue(ctx, K_SCALAR, 1, [&] { return launch_dt(R->d, s); }));
-    int rc;
-    if ((rc = run_stage(ctx, R, 1, Pn, Pn, P1))) return rc;
-    if ((rc = run_stage(ctx, R, 2, Pn, P1, P2))) return rc;
-    if ((rc = run_stage(ctx, R, 3, Pn, P2, P1))) return rc;
-    RG_CUDA(issue(ctx, K_SCALAR, 1, [&] { return launch_step_end(R->d, s); }));
-    R->cur = (R->cur + 1) % 3;
+    const int rc = step_alone(ctx, R);
+    if (rc) return rc;
   }
   if (ctx->prof) {
     int rc = drain_events(ctx);
@@ -1312,12 +1325,18 @@ int rg_step(rg_ctx* ctx, int run, int nsteps, rg_step_stats* stats) {
 int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_stats* stats) {
   if (!ctx || !runs || nruns <= 0) return fail(RG_EINVAL_CONFIG, "empty batch");
   std::map<long long, std::vector<int>> groups;
+  std::vector<Run*> alone;  // stepped with their own launches, after the batch classes of each step
+  {
+    std::vector<int> all(runs, runs + nruns);
+    std::sort(all.begin(), all.end());
+    if (std::adjacent_find(all.begin(), all.end()) != all.end())
+      return fail(RG_EINVAL_CONFIG, "a run appears twice in the batch");
+  }
   for (int a = 0; a < nruns; ++a) {
     Run* R = find(ctx, runs[a]);
     if (!R) return fail(RG_ENOTFOUND, "unknown run in batch");
-    if (R->d.ict == 3) return fail(RG_EINVAL_CONFIG, "upwind flux-CT (ict 3) runs step alone (rg_step)");
-    if (R->d.iwvec == 2) return fail(RG_EINVAL_CONFIG, "recov2 (iwvec 2) runs step alone (rg_step)");
-    groups[batch_class(R)].push_back(runs[a]);
+    if (steps_alone(R)) alone.push_back(R);
+    else groups[batch_class(R)].push_back(runs[a]);
   }
   std::vector<BatchEntry*> es;
   for (auto& kv : groups) {
@@ -1348,7 +1367,7 @@ int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_s
       }
       if (E->tune_pending) seg = std::min<long long>(seg, kTuneAfter - E->steps_run);
     }
-    for (int n = 0; n < seg; ++n)
+    for (int n = 0; n < seg; ++n) {
       for (BatchEntry* E : es) {
         const int nl = batch_launch_count(E->plan);
         if (!ctx->prof) {
@@ -1360,9 +1379,14 @@ int rg_step_batch(rg_ctx* ctx, const int* runs, int nruns, int nsteps, rg_step_s
         }
         E->steps_run += 1;
       }
+      for (Run* R : alone) {  // advances its own buffer rotation
+        const int rc = step_alone(ctx, R);
+        if (rc) return rc;
+      }
+    }
     for (int a = 0; a < nruns; ++a) {
       Run* R = find(ctx, runs[a]);
-      R->cur = (R->cur + seg) % 3;
+      if (!steps_alone(R)) R->cur = (R->cur + seg) % 3;
     }
     done += seg;
   }

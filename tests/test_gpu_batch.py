@@ -63,7 +63,7 @@ def test_tube_runs_to_tmax(gpu_ctx):
     assert 0 < st["steps"] < 100000
 
 
-def _alone_vs_batch(gpu_ctx, params, ics, steps):
+def _alone_vs_batch(gpu_ctx, params, ics, steps, info=True):
     alone, batch = [], []
     for p, ic in zip(params, ics):
         a = gpu_ctx.admit(p)
@@ -76,8 +76,9 @@ def _alone_vs_batch(gpu_ctx, params, ics, steps):
         a.step(steps)
     st = gpu_ctx.step_batch(batch, steps, stats=True)
     # one batch per class (precision etc.); report the tuned shape of the first run's class
-    same = [b for b, p in zip(batch, params) if p.get("precision", "fp64") == params[0].get("precision", "fp64")]
-    info = gpu_ctx.batch_info(same)
+    if info:
+        same = [b for b, p in zip(batch, params) if p.get("precision", "fp64") == params[0].get("precision", "fp64")]
+        info = gpu_ctx.batch_info(same)
     out = []
     for a, b, s in zip(alone, batch, st):
         sa = a.stats()
@@ -117,6 +118,30 @@ def test_batch_tori_fp64_and_mixed_equal_alone(gpu_ctx):
         assert np.isfinite(b).all()
         assert np.array_equal(a, b)
         assert sa["time"] == sb["time"]
+
+
+def test_batch_with_3d_and_unbatched_schemes_equals_alone(gpu_ctx):
+    """Runs without a slab direction (3D tori, which fill the GPU alone) and
+    runs whose schemes have no batched kernels (upwind flux-CT, recov2) join a
+    batch and take each step with their own launches, after the tubes' batched
+    step: every run, the tubes included, equals itself stepped alone (rg_step)
+    bit for bit."""
+    params = [
+        dict(config.torus(nr=40, nth=24, nph=16), guard=1),                 # 3D, MP5, staged kernels
+        dict(config.torus(nr=36, nth=20, nph=18, irec=5), guard=1),         # 3D PPM
+        dict(config.torus(nr=48, nth=40, ict=3), guard=1),                  # 2D slab, upwind flux-CT
+        dict(config.torus(nr=40, nth=28, nph=12), guard=1, iwvec=2),        # 3D recov2
+        config.tube(n=300, tmax=0.4),
+        config.tube(n=517, tmax=0.4),
+    ]
+    ics = [lambda r: r.ic_torus(seed=31), lambda r: r.ic_torus(seed=32), lambda r: r.ic_torus(seed=33),
+           lambda r: r.ic_torus(seed=34), lambda r: r.ic_tube(seed=2012, tube=1),
+           lambda r: r.ic_tube(seed=2012, tube=2)]
+    out, _ = _alone_vs_batch(gpu_ctx, params, ics, 6, info=False)
+    for n, (a, b, sa, sb) in enumerate(out):
+        assert np.isfinite(b).all(), n
+        assert np.array_equal(a, b), n
+        assert sa["time"] == sb["time"] and sa["steps"] == sb["steps"] == 6, n
 
 
 def test_batch_membership_change_and_release(gpu_ctx):
