@@ -6,9 +6,9 @@ power of the step with the library's own rg_pow (include/rg_pow.h).  The
 oracle is compiled with -ffp-contract=off (gfortran -O2 on x86-64 emits no
 FMA) and, in its "rg" power mode, calls the same rg_pow.  The two then carry
 out the same IEEE operations in the same order, so their states agree in
-every bit after one step and after a thousand: the north star's long-horizon
-bound (1e-10 L1 in rho, u and B after 1000 steps) holds with zero difference
-for this build, MP5 included.  With the C library's pow in the oracle (the
+every bit after one step and after a thousand: the long-horizon parity bound
+(1e-10 L1 in rho, u and B after 1000 steps) holds with zero difference for
+this build, for MP5, PPM and WENO5.  With the C library's pow in the oracle (the
 reference's own powers) one step still agrees to a few units of 1e-16.
 
 The library is process-global, so the checks run in child processes, which
