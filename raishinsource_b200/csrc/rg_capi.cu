@@ -65,9 +65,12 @@ struct Run {
   CUtensorMap tmap32[3];   // the FP32 copy P32 of a mixed run, per direction
   CUtensorMap tmapm[3];    // the FP64 face metric per direction (mi, mc, mk; flux_tma_met_box)
   bool tma = false;
-  // tensor maps of the staged update (F1, F2, F3, CT, U^n; update_tma_box)
+  // tensor maps of the staged update (F1, F2, F3, CT, U^n; update_tma_box) and
+  // of a mixed run's FP32 region (F32[0..2], CT32, U^n; update_tma_mix_box)
   CUtensorMap umap[5];
+  CUtensorMap umap32[5];
   bool utma = false;
+  bool utma32 = false;
 };
 
 }  // namespace
@@ -160,6 +163,7 @@ EncodeTiledFn encode_tiled() {
 void make_tmaps(Run* R) {
   R->tma = false;
   R->utma = false;
+  R->utma32 = false;
   const DevRun& d = R->d;
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return;
@@ -208,6 +212,16 @@ void make_tmaps(Run* R) {
     R->utma = ok;
   } else {
     (void)cudaGetLastError();
+  }
+  if (update_tma_mix_eligible(d)) {
+    void* bases[5] = {d.F32[0], d.F32[1], d.F32[2], d.CT32, d.Un};
+    bool ok = true;
+    for (int w = 0; w < 5 && ok; ++w) {
+      unsigned box[4];
+      update_tma_mix_box(w, box);
+      ok = encode(&R->umap32[w], bases[w], w == 4 ? 8 : 4, (int)box[3], box);
+    }
+    R->utma32 = ok;
   }
 }
 
@@ -604,7 +618,8 @@ int run_stage(rg_ctx* ctx, Run* R, int stage, const double* Pn, const double* Pc
   } else {
     RG_CUDA(issue(ctx, K_UPDATE, n_update_launches(d), [&] {
       return launch_update(d, stage, Pn, Pc, Pw, R->b.F[0], R->b.F[1], R->b.F[2], R->b.CT, s,
-                           (R->utma && ctx->utma) ? static_cast<const void*>(R->umap) : nullptr);
+                           (R->utma && ctx->utma) ? static_cast<const void*>(R->umap) : nullptr,
+                           (R->utma32 && ctx->utma) ? static_cast<const void*>(R->umap32) : nullptr);
     }));
   }
   RG_CUDA(issue(ctx, K_BC, n_bc_launches(d), [&] { return launch_bc(d, Pw, Pn, s); }));

@@ -629,61 +629,53 @@ __device__ __forceinline__ void split(double x, float& hi, float& lo) {
 // P2C(P).  Those inputs, the stored-state stand-ins of the reference's uu/uo
 // arrays, stay FP64, as does the primitive recovery that follows.
 template <int STAGE>
-__device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pc,
-                                double dt, double u[9]) {
+__device__ __forceinline__ void stage_pre_mixed(const DevRun& r, int i, int j, int k, const Met& m,
+                                                const double* __restrict__ Pc, double ucur[9], float sf[4]) {
   const size_t N = r.N, c = r.cell(i, j, k), q = r.ik(i, k);
   const double gam = r.gam;
   double qc[9];
   load9(Pc, N, c, qc);
   PS s;
   pstate(qc, m, gam, s);
-  double ucur[9];
   p2c(s, gam, r.gkind, m.detg, ucur);
   if (STAGE == 1)
 #pragma unroll
     for (int v = 0; v < 9; ++v) r.Un[(size_t)v * N + c] = ucur[v];
-  float sf[4];
-  {
-    const size_t nik = r.nik;
-    const float a = (float)(s.roh + s.bbsq), b = (float)(s.pr + 0.5 * s.bbsq);
-    float uc[4], ul[4], bc[4], bl[4];
+  const size_t nik = r.nik;
+  const float a = (float)(s.roh + s.bbsq), b = (float)(s.pr + 0.5 * s.bbsq);
+  float uc[4], ul[4], bc[4], bl[4];
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      uc[n] = (float)s.ucon[n]; ul[n] = (float)s.ucov[n]; bc[n] = (float)s.bbcon[n]; bl[n] = (float)s.bbcov[n];
-    }
-    float ta = 0.f, tb = 0.f, tc = 0.f, td = 0.f;
-#pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      float g[4][4];
-      load_christ_row(r.chr32, nik, q, n, g);
-#pragma unroll
-      for (int mm = 0; mm < 4; ++mm) {
-        const float t = a * uc[mm] * ul[n] + (mm == n ? b : 0.f) - bc[mm] * bl[n];
-        ta = ta + t * g[1][mm];
-        tb = tb + t * g[2][mm];
-        tc = tc + t * g[3][mm];
-        td = td + t * g[0][mm];
-      }
-    }
-    const float dg = (float)m.detg;
-    sf[0] = dg * ta; sf[1] = dg * tb; sf[2] = dg * tc; sf[3] = dg * td;
+  for (int n = 0; n < 4; ++n) {
+    uc[n] = (float)s.ucon[n]; ul[n] = (float)s.ucov[n]; bc[n] = (float)s.bbcon[n]; bl[n] = (float)s.bbcov[n];
   }
-  const float a1 = (float)(dt / __ldg(r.dx1b + i - 1)), a2 = (float)(dt / __ldg(r.dx2b + j - 1)),
-              a3 = (float)(dt / __ldg(r.dx3b + k - 1));
-  const float fdt = (float)dt;
-  // stage weights: U = wo*uo + wc*ucur + wf*(flux divergence + dt*S)
-  const float wo = (STAGE == 1) ? 0.f : (STAGE == 2 ? 0.75f : 1.0f / 3.0f);
-  const float wc = (STAGE == 1) ? 1.f : (STAGE == 2 ? 0.25f : 2.0f / 3.0f);
-  const float wf = wc;
-  const size_t ci = c - 1, cj = c - r.sj, ck = c - r.sk;
-  const float* F1 = r.F32[0];
-  const float* F2 = r.F32[1];
-  const float* F3 = r.F32[2];
-  const float* CT = r.CT32;
-  auto fd = [&](const float* A, size_t x, size_t xm) { return A[x] - A[xm]; };
+  float ta = 0.f, tb = 0.f, tc = 0.f, td = 0.f;
 #pragma unroll
-  for (int v = 0; v < 9; ++v) {
-    float d1, d2, d3;
+  for (int n = 0; n < 4; ++n) {
+    float g[4][4];
+    load_christ_row(r.chr32, nik, q, n, g);
+#pragma unroll
+    for (int mm = 0; mm < 4; ++mm) {
+      const float t = a * uc[mm] * ul[n] + (mm == n ? b : 0.f) - bc[mm] * bl[n];
+      ta = ta + t * g[1][mm];
+      tb = tb + t * g[2][mm];
+      tc = tc + t * g[3][mm];
+      td = td + t * g[0][mm];
+    }
+  }
+  const float dg = (float)m.detg;
+  sf[0] = dg * ta; sf[1] = dg * tb; sf[2] = dg * tc; sf[3] = dg * td;
+}
+
+// FP32 flux differences of variable v from the FP32 face fluxes and flux-CT
+// values (global arrays).
+struct FluxDiffGlobal32 {
+  const float* __restrict__ F1;
+  const float* __restrict__ F2;
+  const float* __restrict__ F3;
+  const float* __restrict__ CT;
+  size_t N, c, ci, cj, ck;
+  __device__ __forceinline__ void operator()(int v, float& d1, float& d2, float& d3) const {
+    auto fd = [&](const float* A, size_t x, size_t xm) { return A[x] - A[xm]; };
     if (v == 7) d1 = fd(CT + 2 * N, c, ci);
     else if (v == 8) d1 = fd(CT + 4 * N, c, ci);
     else d1 = fd(F1 + (size_t)v * N, c, ci);
@@ -693,10 +685,29 @@ __device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met&
     if (v == 6) d3 = fd(CT + 1 * N, c, ck);
     else if (v == 7) d3 = fd(CT + 3 * N, c, ck);
     else d3 = fd(F3 + (size_t)v * N, c, ck);
+  }
+};
+
+// The compensated FP32 combine of the mixed path (uo = U^n in stages 2, 3).
+template <int STAGE, typename Diff>
+__device__ __forceinline__ void stage_combine_mixed(const DevRun& r, int i, int j, int k, const double ucur[9],
+                                                    const float sf[4], const double uo[9], double dt,
+                                                    const Diff& diff, double u[9]) {
+  const float a1 = (float)(dt / __ldg(r.dx1b + i - 1)), a2 = (float)(dt / __ldg(r.dx2b + j - 1)),
+              a3 = (float)(dt / __ldg(r.dx3b + k - 1));
+  const float fdt = (float)dt;
+  // stage weights: U = wo*uo + wc*ucur + wf*(flux divergence + dt*S)
+  const float wo = (STAGE == 1) ? 0.f : (STAGE == 2 ? 0.75f : 1.0f / 3.0f);
+  const float wc = (STAGE == 1) ? 1.f : (STAGE == 2 ? 0.25f : 2.0f / 3.0f);
+  const float wf = wc;
+#pragma unroll
+  for (int v = 0; v < 9; ++v) {
+    float d1, d2, d3;
+    diff(v, d1, d2, d3);
     Acc32 acc;
     float hi, lo;
     if (STAGE > 1) {
-      split(r.Un[(size_t)v * N + c], hi, lo);
+      split(uo[v], hi, lo);
       acc.add_scaled(wo, hi, lo);
     }
     split(ucur[v], hi, lo);
@@ -706,6 +717,19 @@ __device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met&
     acc.add(wf * inc);
     u[v] = acc.value();
   }
+}
+
+template <int STAGE>
+__device__ void stage_rhs_mixed(const DevRun& r, int i, int j, int k, const Met& m, const double* __restrict__ Pc,
+                                double dt, double u[9]) {
+  const size_t N = r.N, c = r.cell(i, j, k);
+  double ucur[9];
+  float sf[4];
+  stage_pre_mixed<STAGE>(r, i, j, k, m, Pc, ucur, sf);
+  double uo[9];
+  if (STAGE > 1) load9(r.Un, N, c, uo);
+  const FluxDiffGlobal32 diff{r.F32[0], r.F32[1], r.F32[2], r.CT32, N, c, c - 1, c - r.sj, c - r.sk};
+  stage_combine_mixed<STAGE>(r, i, j, k, ucur, sf, uo, dt, diff, u);
 }
 
 __device__ __forceinline__ bool is_interior(const DevRun& r, int i, int j, int k) {
@@ -936,7 +960,9 @@ template <int MODE, int STAGE, int IWVEC = 1>
 __global__ void __launch_bounds__(kCarryThreads) k_carry_fix(DevRun r, const double* __restrict__ Pn, const double* __restrict__ Pc,
                             double* __restrict__ Pw, const double* __restrict__ F1, const double* __restrict__ F2,
                             const double* __restrict__ F3, const double* __restrict__ CT, const double* __restrict__ U) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) carry_fix_body<MODE, STAGE, IWVEC>(r, Pn, Pc, Pw, F1, F2, F3, CT, U);
+  // one block: every thread takes part (the body ranks the queued cells and
+  // runs the chains with the whole block, with block barriers)
+  carry_fix_body<MODE, STAGE, IWVEC>(r, Pn, Pc, Pw, F1, F2, F3, CT, U);
 }
 
 // ------------------------------------------------------------- face fluxes
@@ -1417,6 +1443,114 @@ __global__ void __launch_bounds__(128, RG_UPDATE_MINB)
   }
   double u[9];
   stage_combine<STAGE>(r, i, j, k, ucur, sf, uo, r.scal->dt, diff, u);
+  update_recov(r, i, j, k, m, Pc, Pw, u);
+}
+
+// The same staging for the FP32 region of a mixed run (cells i >= ilo, the
+// first cell beyond r = 2 r_H): FP32 face fluxes and flux-CT values, FP64 U^n.
+// The region starts at any i, so each box starts at the 16-byte boundary at
+// or below its first cell (a multiple of 4 cells in FP32, of 2 in FP64) and
+// a thread's cell sits `off` cells into it.
+constexpr unsigned round_up128(unsigned n) { return (n + 127u) / 128u * 128u; }
+struct UpdBoxMix {
+  static constexpr int BX = RG_UPDATE_BX, BY = 128 / RG_UPDATE_BX;
+  static constexpr int X1 = BX + 4, Y1 = BY, Z1 = 1;      // F1 (FP32): from i0-1 rounded down to 4
+  static constexpr int X2 = BX + 4, Y2 = BY + 1, Z2 = 1;  // F2 (FP32): from i0 rounded down
+  static constexpr int X3 = BX + 4, Y3 = BY, Z3 = 2;      // F3 (FP32)
+  static constexpr int XC = BX + 4, YC = BY + 1, ZC = 2;  // CT (FP32): from i0-1 rounded down
+  static constexpr int XU = BX + 2, YU = BY, ZU = 1;      // U^n (FP64): from i0 rounded down to 2
+  static constexpr unsigned B1 = X1 * Y1 * Z1 * 9 * 4, B2 = X2 * Y2 * Z2 * 9 * 4, B3 = X3 * Y3 * Z3 * 9 * 4;
+  static constexpr unsigned BC = XC * YC * ZC * 6 * 4, BU = XU * YU * ZU * 9 * 8;
+  static constexpr unsigned O1 = 0, O2 = round_up128(O1 + B1), O3 = round_up128(O2 + B2),
+                            OC = round_up128(O3 + B3), OU = round_up128(OC + BC), BYTES = round_up128(OU + BU);
+};
+
+struct FluxDiffStaged32 {
+  const float* f1;
+  const float* f2;
+  const float* f3;
+  const float* ct;
+  __device__ __forceinline__ void operator()(int v, float& d1, float& d2, float& d3) const {
+    using B = UpdBoxMix;
+    constexpr int P1 = B::X1 * B::Y1 * B::Z1, P2 = B::X2 * B::Y2 * B::Z2, P3 = B::X3 * B::Y3 * B::Z3;
+    constexpr int PC = B::XC * B::YC * B::ZC, SJC = B::XC, SKC = B::XC * B::YC, SK3 = B::X3 * B::Y3;
+    if (v == 7) d1 = ct[2 * PC] - ct[2 * PC - 1];
+    else if (v == 8) d1 = ct[4 * PC] - ct[4 * PC - 1];
+    else d1 = f1[v * P1] - f1[v * P1 - 1];
+    if (v == 6) d2 = ct[0 * PC] - ct[0 * PC - SJC];
+    else if (v == 8) d2 = ct[5 * PC] - ct[5 * PC - SJC];
+    else d2 = f2[v * P2] - f2[v * P2 - B::X2];
+    if (v == 6) d3 = ct[1 * PC] - ct[1 * PC - SKC];
+    else if (v == 7) d3 = ct[3 * PC] - ct[3 * PC - SKC];
+    else d3 = f3[v * P3] - f3[v * P3 - SK3];
+  }
+};
+
+template <int STAGE>
+__global__ void __launch_bounds__(128, RG_UPDATE_MINB)
+    k_update_tma_mix(const __grid_constant__ UpdMaps tm, DevRun r, const double* __restrict__ Pc,
+                     double* __restrict__ Pw, int ilo) {
+  using B = UpdBoxMix;
+  extern __shared__ __align__(128) unsigned char upd_raw[];
+  __shared__ __align__(8) unsigned long long bar;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + B::BX * ty;
+  const int i0 = ilo + (int)blockIdx.x * B::BX, y0 = (int)blockIdx.y * B::BY, z0 = (int)blockIdx.z;
+  const int i = i0 + tx, j = y0 + ty + 1, k = z0 + 1;
+  const bool inr = i <= r.imax && j <= r.jmax && k <= r.kmax;
+  const size_t N = r.N, c = inr ? r.cell(i, j, k) : 0;
+  if (!r.scal->active) {  // a finished run copies its state through (as k_update)
+    if (inr)
+#pragma unroll
+      for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = Pc[(size_t)v * N + c];
+    return;
+  }
+  // 0-based box origins along i: F1 and CT start at or below cell i0-1, the others at or below i0
+  const int xa = (i0 - 2) & ~3, xb = (i0 - 1) & ~3, xu = (i0 - 1) & ~1;
+  const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
+  const unsigned base = (unsigned)__cvta_generic_to_shared(upd_raw);
+  if (tid == 0) {
+    const unsigned bytes = B::B1 + B::B2 + B::B3 + B::BC + (STAGE > 1 ? B::BU : 0u);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+    tma_load4(base + B::O1, &tm.m[0], xa, y0, z0, bar_a);
+    tma_load4(base + B::O2, &tm.m[1], xb, y0 - 1, z0, bar_a);
+    tma_load4(base + B::O3, &tm.m[2], xb, y0, z0 - 1, bar_a);
+    tma_load4(base + B::OC, &tm.m[3], xa, y0 - 1, z0 - 1, bar_a);
+    if (STAGE > 1) tma_load4(base + B::OU, &tm.m[4], xu, y0, z0, bar_a);
+  }
+  __syncthreads();
+  const bool interior = inr && is_interior(r, i, j, k);
+  if (inr && !interior)
+#pragma unroll
+    for (int v = 0; v < 9; ++v) Pw[(size_t)v * N + c] = Pc[(size_t)v * N + c];
+  Met m;
+  double ucur[9];
+  float sf[4];
+  if (interior) {
+    load_met(r.mc, r.nik, r.ik(i, k), m);
+    stage_pre_mixed<STAGE>(r, i, j, k, m, Pc, ucur, sf);
+  }
+  if (!tma_wait(bar_a, r.cnt + C_TMAWAIT)) {
+    if (tid == 0) atomicAdd(r.cnt + C_TMAWAIT, 1ull);
+    tma_wait(bar_a, nullptr);  // the copies in flight write this block's shared memory: one more bounded wait
+    return;
+  }
+  if (!interior) return;
+  const float* sm = reinterpret_cast<const float*>(upd_raw);
+  const int oa = (i - 1) - xa, ob = (i - 1) - xb;  // the cell's index along i in each box
+  const FluxDiffStaged32 diff{sm + B::O1 / 4 + oa + B::X1 * ty,
+                              sm + B::O2 / 4 + ob + B::X2 * (ty + 1),
+                              sm + B::O3 / 4 + ob + B::X3 * ty + B::X3 * B::Y3,
+                              sm + B::OC / 4 + oa + B::XC * (ty + 1) + B::XC * B::YC};
+  double uo[9];
+  if (STAGE > 1) {
+    const double* un = reinterpret_cast<const double*>(upd_raw + B::OU) + ((i - 1) - xu) + B::XU * ty;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) uo[v] = un[v * B::XU * B::YU];
+  }
+  double u[9];
+  stage_combine_mixed<STAGE>(r, i, j, k, ucur, sf, uo, r.scal->dt, diff, u);
   update_recov(r, i, j, k, m, Pc, Pw, u);
 }
 
@@ -2621,9 +2755,33 @@ cudaError_t prepare_update_tma() {
   return cudaSuccess;
 }
 
+bool update_tma_mix_eligible(const DevRun& r) {
+  return r.mixed && !r.jfix && !r.kfix && r.iwvec != 2 && (r.imax % 4) == 0 &&
+         r.N == (size_t)r.imax * r.jmax * r.kmax;
+}
+
+void update_tma_mix_box(int which, unsigned box[4]) {
+  using B = UpdBoxMix;
+  const unsigned x[5] = {B::X1, B::X2, B::X3, B::XC, B::XU}, y[5] = {B::Y1, B::Y2, B::Y3, B::YC, B::YU};
+  const unsigned z[5] = {B::Z1, B::Z2, B::Z3, B::ZC, B::ZU};
+  box[0] = x[which];
+  box[1] = y[which];
+  box[2] = z[which];
+  box[3] = which == 3 ? 6 : 9;
+}
+
+template <int STAGE>
+static void launch_update_tma_mix(const DevRun& r, const UpdMaps& maps, const double* Pc, double* Pw, int ilo,
+                                  cudaStream_t s) {
+  if (ilo > r.imax) return;
+  const dim3 b(RG_UPDATE_BX, 128 / RG_UPDATE_BX, 1);
+  const dim3 g = grid3(r.imax - ilo + 1, r.jmax, r.kmax, b);
+  k_update_tma_mix<STAGE><<<g, b, UpdBoxMix::BYTES, s>>>(maps, r, Pc, Pw, ilo);
+}
+
 cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                           const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s,
-                          const void* umaps) {
+                          const void* umaps, const void* umaps_mix) {
   if (umaps && update_tma_eligible(r)) {
     UpdMaps maps;
     memcpy(&maps, umaps, sizeof maps);
@@ -2637,7 +2795,15 @@ cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const do
   } else {
     const int split = fp64_split(r, 1, r.imax);
     launch_update_t<false>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, 1, split, s);
-    launch_update_t<true>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, split + 1, r.imax, s);
+    if (umaps_mix && update_tma_mix_eligible(r)) {
+      UpdMaps maps;
+      memcpy(&maps, umaps_mix, sizeof maps);
+      if (stage == 1) launch_update_tma_mix<1>(r, maps, Pc, Pw, split + 1, s);
+      else if (stage == 2) launch_update_tma_mix<2>(r, maps, Pc, Pw, split + 1, s);
+      else launch_update_tma_mix<3>(r, maps, Pc, Pw, split + 1, s);
+    } else {
+      launch_update_t<true>(r, stage, Pn, Pc, Pw, F1, F2, F3, CT, split + 1, r.imax, s);
+    }
   }
   if (r.strag_list) {
     const unsigned gs = (unsigned)((r.strag_cap + 127) / 128);

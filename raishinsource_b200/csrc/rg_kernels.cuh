@@ -41,10 +41,15 @@ void flux_tma_met_box(unsigned box[3]);
 cudaError_t launch_ct(const DevRun& r, const double* P, const double* F1, const double* F2, const double* F3,
                       double* CT, cudaStream_t s);
 // umaps: the run's five update tensor maps (F1, F2, F3, CT, U^n; CUtensorMap[5])
-// for the TMA-staged update where update_tma_eligible, else nullptr
+// for the TMA-staged update where update_tma_eligible, else nullptr;
+// umaps_mix: those of a mixed run's FP32 region (F32[0..2], CT32, U^n) where
+// update_tma_mix_eligible, else nullptr
 cudaError_t launch_update(const DevRun& r, int stage, const double* Pn, const double* Pc, double* Pw,
                           const double* F1, const double* F2, const double* F3, const double* CT, cudaStream_t s,
-                          const void* umaps = nullptr);
+                          const void* umaps = nullptr, const void* umaps_mix = nullptr);
+// TMA-staged FP32 region of a mixed run's update: stored in full, recov1a, imax a multiple of 4
+bool update_tma_mix_eligible(const DevRun& r);
+void update_tma_mix_box(int which, unsigned box[4]);
 // TMA-staged update: runs stored in full, FP64, recov1a, imax even
 bool update_tma_eligible(const DevRun& r);
 // box of update tensor map `which` (0 F1, 1 F2, 2 F3, 3 CT, 4 U^n) as (x, y, z, variables)

@@ -1,9 +1,10 @@
 """GPU: the TMA-staged stage update (k_update_tma) against the generic one
 (k_update).
 
-For runs stored in full in FP64 the stage update stages the rows its RK
-combine reads -- the three face-flux arrays, the flux-CT components and U^n
-(rkt.f90:2-180 with ct.f90:98-109) -- in shared memory by TMA tile loads.  It
+For runs stored in full the stage update stages the rows its RK combine
+reads -- the three face-flux arrays, the flux-CT components and U^n
+(rkt.f90:2-180 with ct.f90:98-109; in the FP32 region of a mixed run the
+FP32 fluxes) -- in shared memory by TMA tile loads.  It
 reads the same values and performs the same operations as the generic
 kernel.  In the uncontracted build (libraishin_gpu_exact.so) a context with
 it (the default) and one without it (RAISHIN_UPDATE_TMA=0, read when the
@@ -29,6 +30,10 @@ CASES = {
     "mp5_40x26x16": dict(nr=40, nth=16, nph=26, irec=6),
     "ppm_48x24x20": dict(nr=48, nth=20, nph=24, irec=5),
     "mc_ict2_36x20x18": dict(nr=36, nth=18, nph=20, irec=1, ict=2),
+    # imax = 2 (mod 4): the update is staged, the faces are not (their TMA wants imax a multiple of 4)
+    "mp5_42x20x16": dict(nr=42, nth=16, nph=20, irec=6),
+    # a mixed run: FP64 update inside 2 r_H, the staged FP32-region kernel (FP32 fluxes, FP64 U^n) beyond
+    "mixed_mp5_40x24x16": dict(nr=40, nth=16, nph=24, irec=6, precision="mixed"),
 }
 
 CHILD = r"""
