@@ -98,6 +98,11 @@ typedef struct rg_ctx rg_ctx;
 
 /* Library / context ------------------------------------------------------ */
 const char* rg_last_error(void);
+/* A context on one device with its own stream.  The environment variables
+ * RAISHIN_FLUX_TMA=0 and RAISHIN_UPDATE_TMA=0, read here, make the context's
+ * runs use the face and stage-update kernels that read global memory
+ * directly instead of the TMA-staged ones (for comparisons; the results are
+ * the same operations on the same values). */
 int rg_ctx_create(int device, rg_ctx** out);
 int rg_ctx_destroy(rg_ctx* ctx);
 int rg_sync(rg_ctx* ctx);
