@@ -153,6 +153,25 @@ print(json.dumps(res))
 """
 
 
+RECOV_CHAINS = PRELUDE + r"""
+set_pow_mode("rg")
+p = dict(config.torus(nr=40, nth=24, nph=16), guard=1)
+o = Oracle(p); o.ic_torus(seed=3); o.init_cons()
+u = o.prims()
+uu = o.caluu1(u)
+pert = uu.copy()
+for sl in ((8, 6, slice(12, 18)), (9, 10, slice(20, 24))):  # (k, j, i range) of each run of cells
+    pert[sl + (4,)] = pert[sl + (0,)] - 0.5 * (pert[sl + (4,)] - pert[sl + (0,)])
+before = o.stats()["recov_carry"]
+_, want = o.recov(pert, u)
+carried = o.stats()["recov_carry"] - before
+with Context(0) as ctx:
+    r = ctx.admit(p); got = r.recov(pert, u); r.release()
+res = {"recov": compare(got, want), "carried": carried, "libs": libs()}
+print(json.dumps(res))
+"""
+
+
 def run_child(script, *args, timeout=1200):
     env = dict(os.environ, RAISHIN_GPU_LIB="exact")
     out = subprocess.run([sys.executable, "-c", script, ROOT, *map(str, args)], env=env, cwd=ROOT,
@@ -217,6 +236,19 @@ def test_exact_build_3d_loop_order_carry_matches_oracle():
         assert r["equal"], (case, r)
         assert r["dev"] == r["orc"], (case, r)
     assert res["steps_1"]["orc"][2] > 0  # cells were carried
+
+
+def test_exact_build_recov_carry_chains_match_oracle():
+    """rg_recov on conserved variables with two separate runs of cells whose W
+    quadratic has no non-negative root (their energy u(5) - u(1) flipped to
+    -0.5 times its value in two rows of a 3D torus): each run is one chain of
+    the loop-order W carry (recov.f90:810-815), resolved by the carry pass with
+    the whole block, and every cell equals the oracle's bit for bit.  (In the
+    FMA build a cell of such a state whose root sits at zero can take the other
+    branch, so this check belongs to the uncontracted build.)"""
+    res = run_child(RECOV_CHAINS)
+    assert res["carried"] == 10, res  # both runs of cells were carried
+    assert res["recov"]["equal"], res
 
 
 def test_exact_build_failing_tubes_match_oracle():
